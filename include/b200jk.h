@@ -1,0 +1,112 @@
+/*
+ * b200jk.h — C ABI of the B200 direct-SCF Coulomb/exchange (J/K) engine.
+ *
+ * Every entry point returns an int status (B200JK_OK = 0); on failure
+ * b200jk_last_error() gives a message for the calling thread.  No torch or
+ * CUDA types appear in the signatures: densities and outputs are plain
+ * double arrays, either host memory or device memory of the plan's GPU
+ * (flag dev_ptrs), and a stream is passed as void* (NULL = the plan's own).
+ *
+ * The entry points replace PySCF 2.12.1's direct-SCF path:
+ *
+ *   b200jk_plan_create     SCF.init_direct_scf / _vhf._VHFOpt(mol, 'int2e',
+ *                          'CVHFnrs8_prescreen', 'CVHFnr_int2e_q_cond',
+ *                          'CVHFnr_dm_cond', direct_scf_tol)
+ *                          (pyscf/scf/hf.py:2045-2054, pyscf/scf/_vhf.py:151-206);
+ *                          the Schwarz conditioner is CVHFnr_int2e_q_cond
+ *                          (pyscf/lib/vhf/optimizer.c:408-454)
+ *   b200jk_get_q_cond      _VHFOpt.q_cond (pyscf/scf/_vhf.py:240-249)
+ *   b200jk_get_jk          _vhf.direct(dms, atm, bas, env, vhfopt, hermi, cart,
+ *                          with_j, with_k) (pyscf/scf/_vhf.py:405-464), i.e.
+ *                          CVHFnr_direct_drv + CVHFdot_nrs8 + int2e_sph +
+ *                          CVHFnrs8_ji_s2kl / CVHFnrs8_li_s2kj (hermi=1) or
+ *                          CVHFnrs8_li_s1kj (hermi=0), followed by
+ *                          lib.hermi_triu (pyscf/lib/vhf/nr_direct.c:355-476,
+ *                          pyscf/lib/vhf/nr_direct_dot.c:1293-1647)
+ *   b200jk_plan_destroy    CVHFdel_optimizer (pyscf/lib/vhf/optimizer.c:48-62)
+ *
+ * Input arrays use PySCF's own layout: atm int32 [natm][6], bas int32
+ * [nbas][8], env float64 (pyscf/gto/mole.py:58-88, 965-1031).  Densities
+ * and outputs are C-ordered (n_dm, nao, nao) float64 in PySCF's AO order
+ * (spherical unless cart=1).
+ */
+#ifndef B200JK_H
+#define B200JK_H
+
+#include <stdint.h>
+#include <stddef.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define B200JK_OK            0
+#define B200JK_EINVAL        1   /* bad argument */
+#define B200JK_EUNSUPPORTED  2   /* input outside what the engine implements */
+#define B200JK_ECUDA         3   /* CUDA runtime error */
+#define B200JK_ENOMEM        4   /* device allocation failed */
+#define B200JK_ENOTBUILT     5   /* library built without device code */
+
+#define B200JK_PREC_FP64     0   /* all quartets in float64 */
+
+typedef struct b200jk_plan b200jk_plan;
+
+typedef struct {
+    int64_t quartets;            /* shell quartets evaluated by the last build */
+    int64_t prim_quartets;       /* primitive quartets evaluated by the last build */
+    int64_t shell_pairs;         /* significant shell pairs in the plan */
+    int64_t prim_pairs;          /* primitive pairs in the plan */
+    double  flops;               /* modelled FP64 flops of the last build */
+    double  last_build_ms;       /* device time of the last J/K build */
+    int32_t nao, nao_cart, nbas, nseg;
+} b200jk_stats_t;
+
+/* Library version, (major << 16) | minor. */
+int b200jk_version(void);
+
+/* Message of the last failure on this thread ("" if none). */
+const char *b200jk_last_error(void);
+
+/* Number of CUDA devices visible to the library (0 when none). */
+int b200jk_device_count(int *count);
+
+/* Build a plan for one molecule/basis: shell pairs, primitive pairs and the
+ * Schwarz conditioner q_cond on GPU `device`.  direct_scf_tol <= 0 disables
+ * screening (the reference's vhfopt=None). */
+int b200jk_plan_create(const int32_t *atm, int natm, const int32_t *bas, int nbas,
+                       const double *env, int env_len, int cart, double direct_scf_tol,
+                       int device, b200jk_plan **out);
+
+int b200jk_plan_destroy(b200jk_plan *plan);
+
+/* nao in the output basis, nbas. */
+int b200jk_plan_dims(const b200jk_plan *plan, int *nao, int *nbas);
+
+/* Copy q_cond (nbas x nbas, C order) to host memory. */
+int b200jk_get_q_cond(const b200jk_plan *plan, double *q_cond);
+
+/* J/K for n_dm densities.  dms, vj, vk are (n_dm, nao, nao) C-ordered;
+ * vj / vk may be NULL when with_j / with_k is 0.  Outputs are overwritten.
+ * hermi: 1 symmetric densities, 0 general, 2 antisymmetric (as PySCF).
+ * dev_ptrs: 0 host arrays, 1 device arrays on the plan's GPU.
+ * stream: a cudaStream_t or NULL. */
+int b200jk_get_jk(b200jk_plan *plan, const double *dms, int n_dm, int hermi,
+                  int with_j, int with_k, double *vj, double *vk,
+                  int dev_ptrs, int precision_mode, void *stream);
+
+/* Counters of the last build. */
+int b200jk_stats(const b200jk_plan *plan, b200jk_stats_t *stats);
+
+/* Host replay of the device integral code for one shell quartet (no GPU is
+ * used): the Cartesian block (ab|cd) of shells shls[0..3] of the given
+ * basis, primitives contracted with env's coefficients, without angular
+ * normalisation; out is C-ordered [a][b][c][d] (cart components in PySCF
+ * order).  For validating the kernels' arithmetic against a CPU reference. */
+int b200jk_hostcheck_cart_quartet(const int32_t *atm, int natm, const int32_t *bas, int nbas,
+                                  const double *env, const int32_t *shls, double *out);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif

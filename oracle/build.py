@@ -255,6 +255,10 @@ def reference_env():
     env = dict(os.environ)
     env['PYSCF_EXT_PATH'] = os.path.join(OUT_REF, 'pyext')
     env['PYSCF_CONFIG_FILE'] = os.path.join(OUT_REF, 'pyscf_conf.py')
+    # the reference drivers call dgemm_ inside OpenMP regions; PySCF itself
+    # pins a pthreads OpenBLAS to one thread for that reason
+    # (pyscf/lib/misc.py:69-80)
+    env['OPENBLAS_NUM_THREADS'] = '1'
     pp = [REF_ROOT, os.path.join(OUT_REF, 'pystub')]
     if env.get('PYTHONPATH'):
         pp.append(env['PYTHONPATH'])

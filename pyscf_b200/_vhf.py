@@ -1,0 +1,141 @@
+"""Drop-in for the direct-SCF entry points of ``pyscf.scf._vhf``.
+
+Same names, arguments and return conventions as PySCF 2.12.1:
+
+* ``direct(dms, atm, bas, env, vhfopt=None, hermi=0, cart=False, with_j=True,
+  with_k=True, out=None, optimize_sr=False) -> (vj, vk)``
+  (pyscf/scf/_vhf.py:405-464): J = 'ji->s2kl', K = 'li->s2kj' (hermi=1) or
+  'li->s1kj' (otherwise), then hermi_triu.  Here the whole build runs in
+  libb200jk on the GPU.
+* ``VHFOpt`` mirrors ``_VHFOpt(mol, 'int2e', 'CVHFnrs8_prescreen',
+  'CVHFnr_int2e_q_cond', 'CVHFnr_dm_cond', direct_scf_tol)`` as created by
+  ``SCF.init_direct_scf`` (pyscf/scf/hf.py:2045-2054): it owns the device plan
+  (shell pairs, primitive pairs, q_cond).
+
+Errors follow the reference: shape mismatches raise RuntimeError
+(pyscf/scf/_vhf.py:594-597); inputs the engine does not implement raise
+NotImplementedError; CUDA failures raise lib.B200JKError.
+"""
+import hashlib
+
+import numpy
+
+from . import lib
+
+_plan_cache = {}
+_PLAN_CACHE_MAX = 8
+
+
+def _key(atm, bas, env, cart, tol, device):
+    h = hashlib.sha1()
+    for a in (atm, bas, env):
+        h.update(numpy.ascontiguousarray(a).tobytes())
+    return (h.hexdigest(), bool(cart), float(tol), int(device))
+
+
+def cached_plan(atm, bas, env, cart=False, direct_scf_tol=0.0, device=0):
+    """A Plan for these arrays, reused across calls with the same molecule."""
+    k = _key(atm, bas, env, cart, direct_scf_tol, device)
+    p = _plan_cache.get(k)
+    if p is None:
+        if len(_plan_cache) >= _PLAN_CACHE_MAX:
+            _plan_cache.pop(next(iter(_plan_cache))).close()
+        p = lib.Plan(atm, bas, env, cart=cart, direct_scf_tol=direct_scf_tol, device=device)
+        _plan_cache[k] = p
+    return p
+
+
+def _check_env(env):
+    env = numpy.asarray(env)
+    if env.size > 8 and env[8] != 0:
+        raise NotImplementedError('range-separated Coulomb (omega != 0) is not implemented in pyscf_b200')
+
+
+class VHFOpt:
+    """Direct-SCF optimizer: holds the device plan for one molecule.
+
+    ``mol`` is a PySCF Mole or any object with ``_atm``, ``_bas``, ``_env``
+    and ``cart``."""
+
+    def __init__(self, mol, intor='int2e', prescreen='CVHFnrs8_prescreen',
+                 qcondname='CVHFnr_int2e_q_cond', dmcondname='CVHFnr_dm_cond',
+                 direct_scf_tol=1e-13, device=0):
+        if intor not in ('int2e', 'int2e_sph', 'int2e_cart'):
+            raise NotImplementedError('VHFOpt supports the int2e Coulomb kernel only, not %s' % intor)
+        if prescreen not in ('CVHFnrs8_prescreen', 'CVHFnoscreen', None):
+            raise NotImplementedError('prescreen %s is not implemented' % prescreen)
+        _check_env(mol._env)
+        self.mol = mol
+        self._intor = intor
+        self._prescreen = prescreen
+        self._qcondname = qcondname
+        self._dmcondname = dmcondname
+        tol = direct_scf_tol if prescreen == 'CVHFnrs8_prescreen' else 0.0
+        self.plan = lib.Plan(mol._atm, mol._bas, mol._env, cart=getattr(mol, 'cart', False),
+                             direct_scf_tol=tol, device=device)
+        self._direct_scf_tol = direct_scf_tol
+
+    @property
+    def direct_scf_tol(self):
+        return self._direct_scf_tol
+
+    @property
+    def q_cond(self):
+        return self.plan.q_cond
+
+    def matches(self, atm, bas, env, cart):
+        return (self.plan.atm.shape == numpy.shape(atm) and self.plan.bas.shape == numpy.shape(bas)
+                and numpy.array_equal(self.plan.atm, atm) and numpy.array_equal(self.plan.bas, bas)
+                and self.plan.env.shape == numpy.shape(env) and numpy.array_equal(self.plan.env, env)
+                and self.plan.cart == bool(cart))
+
+
+def _resolve_plan(vhfopt, atm, bas, env, cart):
+    if isinstance(vhfopt, VHFOpt) and vhfopt.matches(atm, bas, env, cart):
+        return vhfopt.plan
+    if vhfopt is None:
+        # the reference runs CVHFnr_direct_drv without any screening here
+        return cached_plan(atm, bas, env, cart, 0.0)
+    tol = getattr(vhfopt, 'direct_scf_tol', 1e-13)
+    return cached_plan(atm, bas, env, cart, tol)
+
+
+def direct(dms, atm, bas, env, vhfopt=None, hermi=0, cart=False,
+           with_j=True, with_k=True, out=None, optimize_sr=False):
+    """J and K of one or several densities (pyscf/scf/_vhf.py:405-464)."""
+    _check_env(env)
+    try:
+        import torch
+        is_torch = isinstance(dms, torch.Tensor)
+    except ImportError:
+        is_torch = False
+    if not with_j and not with_k:
+        return None, None
+    if is_torch and dms.is_cuda:
+        plan = _resolve_plan(vhfopt, atm, bas, env, cart)
+        return plan.get_jk_device(dms.to(torch.float64), hermi=hermi, with_j=with_j, with_k=with_k)
+    dms = numpy.asarray(dms, order='C', dtype=numpy.double)
+    dms_shape = dms.shape
+    nao = dms_shape[-1]
+    dms = dms.reshape(-1, nao, nao)
+    plan = _resolve_plan(vhfopt, atm, bas, env, cart)
+    if plan.nao != nao:
+        raise RuntimeError('dm shape %s is inconsistent with nao=%d of the basis' % (dms_shape, plan.nao))
+    n_dm = dms.shape[0]
+    out_j = out_k = None
+    if out is not None:
+        out = numpy.asarray(out)
+        n_jk = int(bool(with_j)) + int(bool(with_k))
+        if out.shape != (n_jk * n_dm, nao, nao) or out.dtype != numpy.double or not out.flags.c_contiguous:
+            raise RuntimeError('out must be a C-contiguous float64 array of shape %s'
+                               % ((n_jk * n_dm, nao, nao),))
+        if with_j:
+            out_j = out[:n_dm]
+        if with_k:
+            out_k = out[n_dm:] if with_j else out[:n_dm]
+    vj, vk = plan.get_jk(dms, hermi=hermi, with_j=with_j, with_k=with_k, out_j=out_j, out_k=out_k)
+    if with_j:
+        vj = vj.reshape(dms_shape)
+    if with_k:
+        vk = vk.reshape(dms_shape)
+    return vj, vk

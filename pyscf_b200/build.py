@@ -1,0 +1,108 @@
+"""Build the CUDA engine in-tree: pyscf_b200/libb200jk.so for sm_100a.
+
+    python -m pyscf_b200.build          (or python pyscf_b200/build.py)
+
+The library is a plain shared object with a C ABI (include/b200jk.h); the
+Python package loads it with ctypes.  It is built next to the sources so it
+travels with the repository snapshot.  The per-class kernels are split into
+one translation unit per quartet class (jk_classes.cu compiled 55 times) and
+compiled in parallel.
+"""
+import os
+import subprocess
+import sys
+import shutil
+from concurrent.futures import ThreadPoolExecutor
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+ROOT = os.path.dirname(HERE)
+CSRC = os.path.join(HERE, 'csrc')
+OBJ = os.path.join(HERE, '_build')
+LIB = os.path.join(HERE, 'libb200jk.so')
+HEADERS = ['rys_math.cuh', 'jk_kernels.cuh', 'jk_launch.h', 'rys_table.inc']
+ARCH = ['-gencode', 'arch=compute_100a,code=sm_100a']
+PAIR_CLASSES = [(la, lb) for la in range(4) for lb in range(la + 1)]
+QUARTET_CLASSES = [(la, lb, lc, ld) for x, (la, lb) in enumerate(PAIR_CLASSES)
+                   for y, (lc, ld) in enumerate(PAIR_CLASSES) if y <= x]
+
+
+def nvcc_path():
+    for p in (os.environ.get('NVCC'), shutil.which('nvcc'), '/usr/local/cuda/bin/nvcc'):
+        if p and os.path.exists(p):
+            return p
+    raise RuntimeError('nvcc not found')
+
+
+def _deps():
+    files = [os.path.join(CSRC, f) for f in
+             ['b200jk.cu', 'jk_classes.cu', 'jk_qcond.cu', 'hostcheck.cpp'] + HEADERS]
+    files.append(os.path.join(ROOT, 'include', 'b200jk.h'))
+    files.append(os.path.abspath(__file__))
+    return files
+
+
+def up_to_date(target=LIB):
+    if not os.path.exists(target):
+        return False
+    t = os.path.getmtime(target)
+    return all(os.path.getmtime(f) <= t for f in _deps())
+
+
+def _units():
+    nvcc = nvcc_path()
+    common = [nvcc, *ARCH, '-O3', '-lineinfo', '-std=c++17', '-Xcompiler', '-fPIC',
+              '-I', os.path.join(ROOT, 'include'), '-I', CSRC, '-c']
+    units = []
+    units.append((common + [os.path.join(CSRC, 'b200jk.cu'), '-o', os.path.join(OBJ, 'b200jk.o')],
+                  os.path.join(OBJ, 'b200jk.o')))
+    units.append((common + [os.path.join(CSRC, 'jk_qcond.cu'), '-o', os.path.join(OBJ, 'jk_qcond.o')],
+                  os.path.join(OBJ, 'jk_qcond.o')))
+    for la, lb, lc, ld in QUARTET_CLASSES:
+        tag = '%d%d%d%d' % (la, lb, lc, ld)
+        o = os.path.join(OBJ, 'jk_%s.o' % tag)
+        units.append((common + ['-DB2_BRA_LA=%d' % la, '-DB2_BRA_LB=%d' % lb, '-DB2_KET_LC=%d' % lc,
+                                '-DB2_KET_LD=%d' % ld, '-DB2_FN_NAME=launch_jk_%s' % tag,
+                                os.path.join(CSRC, 'jk_classes.cu'), '-o', o], o))
+    o = os.path.join(OBJ, 'hostcheck.o')
+    units.append((['g++', '-O2', '-std=c++17', '-fPIC', '-I', os.path.join(ROOT, 'include'), '-I', CSRC,
+                   '-c', os.path.join(CSRC, 'hostcheck.cpp'), '-o', o], o))
+    return units
+
+
+def build(force=False, verbose=False, extra=(), jobs=None):
+    if not force and up_to_date():
+        return LIB
+    os.makedirs(OBJ, exist_ok=True)
+    units = _units()
+    if extra:
+        units = [(cmd[:-3] + list(extra) + cmd[-3:] if cmd[0] != 'g++' else cmd, o) for cmd, o in units]
+
+    def run(u):
+        cmd, o = u
+        r = subprocess.run(cmd, capture_output=True, text=True)
+        return cmd, r
+
+    with ThreadPoolExecutor(jobs or min(12, os.cpu_count() or 4)) as ex:
+        results = list(ex.map(run, units))
+    msgs = []
+    for cmd, r in results:
+        if r.returncode != 0:
+            raise RuntimeError('compile failed: %s\n%s%s' % (' '.join(cmd), r.stdout, r.stderr))
+        if verbose and (r.stdout or r.stderr):
+            msgs.append(r.stdout + r.stderr)
+    link = [nvcc_path(), *ARCH, '--shared', '-Xcompiler', '-fPIC', '-o', LIB + '.tmp'] + [o for _, o in units]
+    r = subprocess.run(link, capture_output=True, text=True)
+    if r.returncode != 0:
+        raise RuntimeError('link failed:\n' + r.stdout + r.stderr)
+    os.replace(LIB + '.tmp', LIB)
+    if verbose:
+        print('\n'.join(msgs))
+    return LIB
+
+
+if __name__ == '__main__':
+    extra = []
+    if '--ptxas-v' in sys.argv:
+        extra += ['-Xptxas', '-v']
+    build(force='--force' in sys.argv or bool(extra), verbose=True, extra=extra)
+    print('built', LIB)

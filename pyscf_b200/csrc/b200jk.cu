@@ -1,0 +1,761 @@
+// b200jk.cu — host planner, kernel dispatch and C ABI of the B200 J/K engine.
+//
+// The ABI (include/b200jk.h) is the drop-in for PySCF's direct-SCF path
+// (pyscf/scf/_vhf.py:405-464 -> pyscf/lib/vhf/nr_direct.c:355-476).  The
+// planner turns PySCF's _atm/_bas/_env (pyscf/gto/mole.py:58-88, 965-1031)
+// into device tables:
+//   segments      one per (shell, contraction column); a generally contracted
+//                 shell (nctr > 1) becomes nctr segments sharing its exponents;
+//   shell pairs   unordered segment pairs, oriented la >= lb, grouped into 10
+//                 angular classes, sorted by the parent-shell Schwarz bound;
+//   prim pairs    (P, p, K_ab c_a c_b, a) per surviving primitive pair
+//                 (exp(-ab/(a+b) |AB|^2) >= e^-60, the libcint default cutoff);
+//   q_cond        CVHFnr_int2e_q_cond on parent shells, computed on the GPU.
+#include <cuda_runtime.h>
+#include <cub/device/device_scan.cuh>
+#include <stdint.h>
+#include <string.h>
+#include <stdio.h>
+#include <math.h>
+#include <string>
+#include <vector>
+#include <algorithm>
+#include <numeric>
+#include <mutex>
+
+#define RYS_TABLE_QUALIFIER static const
+#include "rys_math.cuh"
+#include "jk_launch.h"
+#include "../../include/b200jk.h"
+
+using namespace b200jk;
+
+// ---------------------------------------------------------------------------
+// errors
+
+static thread_local std::string g_last_error;
+
+static int fail(int code, const std::string &msg)
+{
+        g_last_error = msg;
+        return code;
+}
+
+#define CUDA_TRY(expr)                                                                 \
+        do {                                                                           \
+                cudaError_t _e = (expr);                                               \
+                if (_e != cudaSuccess)                                                 \
+                        return fail(B200JK_ECUDA, std::string(#expr) + ": " +          \
+                                                      cudaGetErrorString(_e));         \
+        } while (0)
+
+// slot layout of PySCF's _atm/_bas/_env (pyscf/gto/mole.py:58-88)
+enum { CHARGE_OF = 0, PTR_COORD = 1, ATM_SLOTS = 6 };
+enum { ATOM_OF = 0, ANG_OF = 1, NPRIM_OF = 2, NCTR_OF = 3, PTR_EXP = 5, PTR_COEFF = 6, BAS_SLOTS = 8 };
+enum { PTR_RANGE_OMEGA = 8 };
+
+static const int LMAX = 3;
+static const int NPAIRCLASS = (LMAX + 1) * (LMAX + 2) / 2;
+static inline int pair_class(int la, int lb) { return la * (la + 1) / 2 + lb; }
+
+__device__ double d_rys_table[RYS_TABLE_SIZE];
+
+// ---------------------------------------------------------------------------
+// real solid harmonics r^l Y_lm (unit-normalised Y_lm), rows m = -l..l
+// (p ordered x, y, z), columns Cartesian components in PySCF order.
+// Helgaker, Jorgensen & Olsen, Molecular Electronic-Structure Theory,
+// eqs. 6.4.47-6.4.50, times sqrt((2l+1)/(4 pi)).
+
+static double factd(int n) { double r = 1; for (int i = 2; i <= n; i++) r *= i; return r; }
+static double binomd(int n, int k) { return (k < 0 || k > n) ? 0.0 : factd(n) / (factd(k) * factd(n - k)); }
+
+static void solid_harmonics(int l, double *rows /* [2l+1][ncart(l)] */)
+{
+        const int nc = ncart(l);
+        for (int i = 0; i < (2 * l + 1) * nc; i++) rows[i] = 0;
+        const double scale = sqrt((2 * l + 1) / (4 * M_PI));
+        for (int m = -l; m <= l; m++) {
+                const int am = abs(m);
+                const int wm = m < 0 ? 1 : 0;   // 2*v_m
+                const double nlm = 1.0 / (pow(2.0, am) * factd(l)) *
+                                   sqrt(2 * factd(l + am) * factd(l - am) / (m == 0 ? 2.0 : 1.0));
+                const int row = (l == 1) ? (m == 1 ? 0 : (m == -1 ? 1 : 2)) : m + l;
+                for (int t = 0; t <= (l - am) / 2; t++)
+                        for (int u = 0; u <= t; u++) {
+                                const int wmax = 2 * ((am - wm) / 2) + wm;
+                                for (int w = wm; w <= wmax; w += 2) {
+                                        const int sgn = ((t + (w - wm) / 2) % 2) ? -1 : 1;
+                                        const double cf = sgn * pow(0.25, t) * binomd(l, t) * binomd(l - t, am + t) *
+                                                          binomd(t, u) * binomd(am, w);
+                                        const int px = 2 * t + am - 2 * u - w, py = 2 * u + w, pz = l - 2 * t - am;
+                                        if (px < 0 || py < 0 || pz < 0) continue;
+                                        int idx = -1;
+                                        for (int k = 0; k < nc; k++)
+                                                if (cart_lx(l, k) == px && cart_ly(l, k) == py) idx = k;
+                                        rows[row * nc + idx] += scale * nlm * cf;
+                                }
+                        }
+        }
+}
+
+// c2s[l][row][cart] with 10x10 slots per l: output-basis rows of the Cartesian map
+static std::vector<double> build_c2s(int cart)
+{
+        std::vector<double> t((LMAX + 1) * 100, 0.0);
+        for (int l = 0; l <= LMAX; l++) {
+                const int nc = ncart(l);
+                if (cart || l < 2) {
+                        const double f = l == 0 ? 0.282094791773878143 : (l == 1 ? 0.488602511902919921 : 1.0);
+                        for (int k = 0; k < nc; k++) t[l * 100 + k * 10 + k] = f;
+                } else {
+                        std::vector<double> rows((2 * l + 1) * nc);
+                        solid_harmonics(l, rows.data());
+                        for (int m = 0; m < 2 * l + 1; m++)
+                                for (int k = 0; k < nc; k++) t[l * 100 + m * 10 + k] = rows[m * nc + k];
+                }
+        }
+        return t;
+}
+
+// ---------------------------------------------------------------------------
+// plan
+
+struct Seg {
+        int parent, l, nprim, ctr;
+        const double *exp;
+        std::vector<double> coef;
+        double R[3];
+        int out_off, cart_off;
+};
+
+template <typename T>
+struct DevArr {
+        T *p = nullptr;
+        size_t n = 0;
+        void release() { if (p) cudaFree(p); p = nullptr; n = 0; }
+};
+
+template <typename T>
+static int dev_upload(DevArr<T> &d, const std::vector<T> &h)
+{
+        d.release();
+        d.n = h.size();
+        if (d.n == 0) return B200JK_OK;
+        if (cudaMalloc(&d.p, sizeof(T) * d.n) != cudaSuccess) {
+                d.p = nullptr;
+                return fail(B200JK_ENOMEM, "cudaMalloc failed for a plan table");
+        }
+        CUDA_TRY(cudaMemcpy(d.p, h.data(), sizeof(T) * d.n, cudaMemcpyHostToDevice));
+        return B200JK_OK;
+}
+
+template <typename T>
+static int dev_alloc(DevArr<T> &d, size_t n)
+{
+        if (d.n >= n && d.p) return B200JK_OK;
+        d.release();
+        if (n == 0) return B200JK_OK;
+        if (cudaMalloc(&d.p, sizeof(T) * n) != cudaSuccess) {
+                d.p = nullptr;
+                return fail(B200JK_ENOMEM, "cudaMalloc failed for a workspace buffer");
+        }
+        d.n = n;
+        return B200JK_OK;
+}
+
+struct PairClassDev {
+        int la = 0, lb = 0, n = 0;
+        DevArr<int4> sh;
+        DevArr<int2> pr;
+        DevArr<double> q;
+        DevArr<double4> A, AB;
+        PairView view() const
+        {
+                PairView v;
+                v.sh = sh.p; v.pr = pr.p; v.q = q.p; v.A = A.p; v.AB = AB.p; v.n = n;
+                return v;
+        }
+        void release() { sh.release(); pr.release(); q.release(); A.release(); AB.release(); n = 0; }
+};
+
+struct b200jk_plan {
+        int device = 0, cart = 0, natm = 0, nbas = 0, nao = 0, naoc = 0, nseg = 0;
+        double tol = 0;
+        std::vector<int> ao_loc;
+        std::vector<double> h_qcond;
+        PairClassDev pc[NPAIRCLASS];
+        DevArr<double4> PP;
+        DevArr<double2> PK;
+        DevArr<double> c2s, qcond, dm_cond;
+        DevArr<int> goff_all;
+        std::vector<size_t> goff_at;   // per quartet class
+        DevArr<int4> seg_info;
+        DevArr<int> out_seg, out_comp, cart_seg, cart_comp, ao_loc_d;
+        // workspace
+        int ws_ndm = 0;
+        DevArr<double> D, Dc, Ds, Jacc, Kacc, outJ, outK;
+        DevArr<unsigned long long> dmax, stats;
+        DevArr<int> nkl;
+        DevArr<long long> nchunk, chunk_off;
+        DevArr<unsigned char> cub_tmp;
+        cudaStream_t stream = nullptr;
+        cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+        int nsm = 148;
+        int64_t shell_pairs = 0, prim_pairs = 0;
+        b200jk_stats_t st;
+        ~b200jk_plan()
+        {
+                for (auto &c : pc) c.release();
+                PP.release(); PK.release(); c2s.release(); qcond.release(); dm_cond.release();
+                goff_all.release(); seg_info.release(); out_seg.release(); out_comp.release();
+                cart_seg.release(); cart_comp.release(); ao_loc_d.release();
+                D.release(); Dc.release(); Ds.release(); Jacc.release(); Kacc.release(); outJ.release(); outK.release();
+                dmax.release(); stats.release(); nkl.release(); nchunk.release(); chunk_off.release(); cub_tmp.release();
+                if (ev0) cudaEventDestroy(ev0);
+                if (ev1) cudaEventDestroy(ev1);
+                if (stream) cudaStreamDestroy(stream);
+        }
+};
+
+// ---------------------------------------------------------------------------
+// quartet classes: bra class X >= ket class Y
+
+struct QClass { int X, Y; };
+static std::vector<QClass> quartet_classes()
+{
+        std::vector<QClass> v;
+        for (int X = 0; X < NPAIRCLASS; X++)
+                for (int Y = 0; Y <= X; Y++) v.push_back({X, Y});
+        return v;
+}
+static void class_l(int X, int &la, int &lb)
+{
+        for (int a = 0; a <= LMAX; a++)
+                for (int b = 0; b <= a; b++)
+                        if (pair_class(a, b) == X) { la = a; lb = b; return; }
+}
+
+typedef int (*jk_launcher_t)(const JKArgs &, cudaStream_t, int, std::string &);
+
+static int dispatch_jk(b200jk_plan *P, int la, int lb, int lc, int ld, const JKArgs &a, cudaStream_t s)
+{
+        struct Entry { int la, lb, lc, ld; jk_launcher_t fn; };
+        static const Entry table[] = {
+                {0, 0, 0, 0, launch_jk_0000},
+                {1, 0, 0, 0, launch_jk_1000},
+                {1, 0, 1, 0, launch_jk_1010},
+                {1, 1, 0, 0, launch_jk_1100},
+                {1, 1, 1, 0, launch_jk_1110},
+                {1, 1, 1, 1, launch_jk_1111},
+                {2, 0, 0, 0, launch_jk_2000},
+                {2, 0, 1, 0, launch_jk_2010},
+                {2, 0, 1, 1, launch_jk_2011},
+                {2, 0, 2, 0, launch_jk_2020},
+                {2, 1, 0, 0, launch_jk_2100},
+                {2, 1, 1, 0, launch_jk_2110},
+                {2, 1, 1, 1, launch_jk_2111},
+                {2, 1, 2, 0, launch_jk_2120},
+                {2, 1, 2, 1, launch_jk_2121},
+                {2, 2, 0, 0, launch_jk_2200},
+                {2, 2, 1, 0, launch_jk_2210},
+                {2, 2, 1, 1, launch_jk_2211},
+                {2, 2, 2, 0, launch_jk_2220},
+                {2, 2, 2, 1, launch_jk_2221},
+                {2, 2, 2, 2, launch_jk_2222},
+                {3, 0, 0, 0, launch_jk_3000},
+                {3, 0, 1, 0, launch_jk_3010},
+                {3, 0, 1, 1, launch_jk_3011},
+                {3, 0, 2, 0, launch_jk_3020},
+                {3, 0, 2, 1, launch_jk_3021},
+                {3, 0, 2, 2, launch_jk_3022},
+                {3, 0, 3, 0, launch_jk_3030},
+                {3, 1, 0, 0, launch_jk_3100},
+                {3, 1, 1, 0, launch_jk_3110},
+                {3, 1, 1, 1, launch_jk_3111},
+                {3, 1, 2, 0, launch_jk_3120},
+                {3, 1, 2, 1, launch_jk_3121},
+                {3, 1, 2, 2, launch_jk_3122},
+                {3, 1, 3, 0, launch_jk_3130},
+                {3, 1, 3, 1, launch_jk_3131},
+                {3, 2, 0, 0, launch_jk_3200},
+                {3, 2, 1, 0, launch_jk_3210},
+                {3, 2, 1, 1, launch_jk_3211},
+                {3, 2, 2, 0, launch_jk_3220},
+                {3, 2, 2, 1, launch_jk_3221},
+                {3, 2, 2, 2, launch_jk_3222},
+                {3, 2, 3, 0, launch_jk_3230},
+                {3, 2, 3, 1, launch_jk_3231},
+                {3, 2, 3, 2, launch_jk_3232},
+                {3, 3, 0, 0, launch_jk_3300},
+                {3, 3, 1, 0, launch_jk_3310},
+                {3, 3, 1, 1, launch_jk_3311},
+                {3, 3, 2, 0, launch_jk_3320},
+                {3, 3, 2, 1, launch_jk_3321},
+                {3, 3, 2, 2, launch_jk_3322},
+                {3, 3, 3, 0, launch_jk_3330},
+                {3, 3, 3, 1, launch_jk_3331},
+                {3, 3, 3, 2, launch_jk_3332},
+                {3, 3, 3, 3, launch_jk_3333},
+        };
+        for (const Entry &e : table) {
+                if (e.la == la && e.lb == lb && e.lc == lc && e.ld == ld) {
+                        std::string err;
+                        if (e.fn(a, s, P->nsm, err)) return fail(B200JK_ECUDA, err);
+                        return B200JK_OK;
+                }
+        }
+        return fail(B200JK_EUNSUPPORTED, "quartet class outside l <= 3");
+}
+
+// packed 2D-integral offsets for every Cartesian component of a class
+static void class_goff(int la, int lb, int lc, int ld, std::vector<int> &out)
+{
+        const int na = ncart(la), nb = ncart(lb), nc = ncart(lc), nd = ncart(ld);
+        auto hidx = [&](int a, int b, int c, int d) { return ((a * (lb + 1) + b) * (lc + 1) + c) * (ld + 1) + d; };
+        for (int a = 0; a < na; a++)
+                for (int b = 0; b < nb; b++)
+                        for (int c = 0; c < nc; c++)
+                                for (int d = 0; d < nd; d++) {
+                                        const int ox = hidx(cart_lx(la, a), cart_lx(lb, b), cart_lx(lc, c), cart_lx(ld, d));
+                                        const int oy = hidx(cart_ly(la, a), cart_ly(lb, b), cart_ly(lc, c), cart_ly(ld, d));
+                                        const int oz = hidx(cart_lz(la, a), cart_lz(lb, b), cart_lz(lc, c), cart_lz(ld, d));
+                                        out.push_back(ox | (oy << 10) | (oz << 20));
+                                }
+}
+
+static std::once_flag g_table_once[64];
+static int g_table_status[64];
+
+static int ensure_tables(int device)
+{
+        if (device < 0 || device >= 64) return fail(B200JK_EINVAL, "device index out of range");
+        std::call_once(g_table_once[device], [device]() {
+                g_table_status[device] = (cudaMemcpyToSymbol(d_rys_table, rys_table_data,
+                                                             sizeof(double) * RYS_TABLE_SIZE) == cudaSuccess)
+                                                 ? 0 : 1;
+        });
+        if (g_table_status[device]) return fail(B200JK_ECUDA, "could not upload the Rys tables");
+        return B200JK_OK;
+}
+
+static const double *table_ptr()
+{
+        void *p = nullptr;
+        cudaGetSymbolAddress(&p, d_rys_table);
+        return (const double *)p;
+}
+
+// ---------------------------------------------------------------------------
+// C ABI
+
+extern "C" {
+
+int b200jk_version(void) { return (0 << 16) | 1; }
+
+const char *b200jk_last_error(void) { return g_last_error.c_str(); }
+
+int b200jk_device_count(int *count)
+{
+        if (!count) return fail(B200JK_EINVAL, "count is NULL");
+        int n = 0;
+        cudaError_t e = cudaGetDeviceCount(&n);
+        if (e != cudaSuccess) n = 0;
+        *count = n;
+        return B200JK_OK;
+}
+
+int b200jk_plan_dims(const b200jk_plan *plan, int *nao, int *nbas)
+{
+        if (!plan) return fail(B200JK_EINVAL, "plan is NULL");
+        if (nao) *nao = plan->nao;
+        if (nbas) *nbas = plan->nbas;
+        return B200JK_OK;
+}
+
+int b200jk_plan_destroy(b200jk_plan *plan)
+{
+        if (!plan) return B200JK_OK;
+        cudaSetDevice(plan->device);
+        delete plan;
+        return B200JK_OK;
+}
+
+static int build_segments(b200jk_plan *P, const int32_t *atm, int natm, const int32_t *bas, int nbas,
+                          const double *env, int env_len, std::vector<Seg> &segs)
+{
+        P->ao_loc.assign(nbas + 1, 0);
+        int cart_off = 0;
+        for (int I = 0; I < nbas; I++) {
+                const int32_t *b = bas + (size_t)I * BAS_SLOTS;
+                const int ia = b[ATOM_OF], l = b[ANG_OF], np = b[NPRIM_OF], nc = b[NCTR_OF];
+                if (ia < 0 || ia >= natm) return fail(B200JK_EINVAL, "bas: atom index out of range");
+                if (l < 0) return fail(B200JK_EINVAL, "bas: negative angular momentum");
+                if (l > LMAX) return fail(B200JK_EUNSUPPORTED, "angular momentum above f (l > 3) is not implemented");
+                if (np <= 0 || nc <= 0) return fail(B200JK_EINVAL, "bas: empty shell");
+                if (b[PTR_EXP] < 0 || b[PTR_EXP] + np > env_len || b[PTR_COEFF] < 0 || b[PTR_COEFF] + np * nc > env_len)
+                        return fail(B200JK_EINVAL, "bas: exponent/coefficient pointer outside env");
+                const int pc = atm[(size_t)ia * ATM_SLOTS + PTR_COORD];
+                if (pc < 0 || pc + 3 > env_len) return fail(B200JK_EINVAL, "atm: coordinate pointer outside env");
+                const int nf = P->cart ? ncart(l) : 2 * l + 1;
+                P->ao_loc[I + 1] = P->ao_loc[I] + nf * nc;
+                for (int c = 0; c < nc; c++) {
+                        Seg s;
+                        s.parent = I; s.l = l; s.nprim = np; s.ctr = c;
+                        s.exp = env + b[PTR_EXP];
+                        s.coef.assign(env + b[PTR_COEFF] + c * np, env + b[PTR_COEFF] + (c + 1) * np);
+                        for (int x = 0; x < 3; x++) s.R[x] = env[pc + x];
+                        s.out_off = P->ao_loc[I] + c * nf;
+                        s.cart_off = cart_off;
+                        cart_off += ncart(l);
+                        segs.push_back(std::move(s));
+                }
+        }
+        P->nao = P->ao_loc[nbas];
+        P->naoc = cart_off;
+        P->nseg = (int)segs.size();
+        return B200JK_OK;
+}
+
+struct HostPair {
+        int i, j;              // segments, l_i >= l_j
+        int prim0, nprim;
+        double q;
+};
+
+int b200jk_plan_create(const int32_t *atm, int natm, const int32_t *bas, int nbas,
+                       const double *env, int env_len, int cart, double direct_scf_tol,
+                       int device, b200jk_plan **out)
+{
+        if (!out) return fail(B200JK_EINVAL, "out is NULL");
+        *out = nullptr;
+        if (!atm || !bas || !env || natm <= 0 || nbas <= 0 || env_len <= PTR_RANGE_OMEGA)
+                return fail(B200JK_EINVAL, "empty or NULL molecule arrays");
+        if (env[PTR_RANGE_OMEGA] != 0.0)
+                return fail(B200JK_EUNSUPPORTED, "range-separated Coulomb (env[PTR_RANGE_OMEGA] != 0) is not implemented");
+        int ndev = 0;
+        if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0)
+                return fail(B200JK_ECUDA, "no CUDA device is available");
+        if (device < 0 || device >= ndev) return fail(B200JK_EINVAL, "device index out of range");
+        CUDA_TRY(cudaSetDevice(device));
+        int rc = ensure_tables(device);
+        if (rc) return rc;
+
+        b200jk_plan *P = new b200jk_plan();
+        P->device = device;
+        P->cart = cart ? 1 : 0;
+        P->natm = natm;
+        P->nbas = nbas;
+        P->tol = direct_scf_tol > 0 ? direct_scf_tol : 0.0;
+        auto bail = [&](int code) { delete P; return code; };
+        cudaDeviceProp prop;
+        if (cudaGetDeviceProperties(&prop, device) != cudaSuccess) return bail(fail(B200JK_ECUDA, "cudaGetDeviceProperties failed"));
+        P->nsm = prop.multiProcessorCount;
+        if (cudaStreamCreateWithFlags(&P->stream, cudaStreamNonBlocking) != cudaSuccess ||
+            cudaEventCreate(&P->ev0) != cudaSuccess || cudaEventCreate(&P->ev1) != cudaSuccess)
+                return bail(fail(B200JK_ECUDA, "stream/event creation failed"));
+
+        std::vector<Seg> segs;
+        rc = build_segments(P, atm, natm, bas, nbas, env, env_len, segs);
+        if (rc) return bail(rc);
+
+        // segment info and basis maps
+        std::vector<int4> seg_info(segs.size());
+        std::vector<int> out_seg(P->nao), out_comp(P->nao), cart_seg(P->naoc), cart_comp(P->naoc);
+        for (size_t s = 0; s < segs.size(); s++) {
+                const Seg &g = segs[s];
+                seg_info[s] = make_int4(g.l, g.out_off, g.cart_off, g.parent);
+                const int nf = P->cart ? ncart(g.l) : 2 * g.l + 1;
+                for (int k = 0; k < nf; k++) { out_seg[g.out_off + k] = (int)s; out_comp[g.out_off + k] = k; }
+                for (int k = 0; k < ncart(g.l); k++) { cart_seg[g.cart_off + k] = (int)s; cart_comp[g.cart_off + k] = k; }
+        }
+        if ((rc = dev_upload(P->seg_info, seg_info)) || (rc = dev_upload(P->out_seg, out_seg)) ||
+            (rc = dev_upload(P->out_comp, out_comp)) || (rc = dev_upload(P->cart_seg, cart_seg)) ||
+            (rc = dev_upload(P->cart_comp, cart_comp)) || (rc = dev_upload(P->ao_loc_d, P->ao_loc)) ||
+            (rc = dev_upload(P->c2s, build_c2s(P->cart))))
+                return bail(rc);
+
+        // shell pairs and primitive pairs
+        std::vector<HostPair> pairs[NPAIRCLASS];
+        std::vector<double4> hPP;
+        std::vector<double2> hPK;
+        const double expcut = 60.0;
+        for (int si = 0; si < (int)segs.size(); si++) {
+                for (int sj = 0; sj <= si; sj++) {
+                        int i = si, j = sj;
+                        if (segs[j].l > segs[i].l) std::swap(i, j);
+                        const Seg &A = segs[i], &B = segs[j];
+                        double AB[3], rr = 0;
+                        for (int x = 0; x < 3; x++) { AB[x] = A.R[x] - B.R[x]; rr += AB[x] * AB[x]; }
+                        HostPair hp;
+                        hp.i = i; hp.j = j; hp.prim0 = (int)hPP.size(); hp.nprim = 0; hp.q = 0;
+                        for (int pa = 0; pa < A.nprim; pa++) {
+                                for (int pb = 0; pb < B.nprim; pb++) {
+                                        const double a = A.exp[pa], b = B.exp[pb], p = a + b;
+                                        const double mu = a * b / p;
+                                        if (mu * rr > expcut) continue;
+                                        const double cc = A.coef[pa] * B.coef[pb];
+                                        if (cc == 0.0) continue;
+                                        double4 P4;
+                                        P4.x = (a * A.R[0] + b * B.R[0]) / p;
+                                        P4.y = (a * A.R[1] + b * B.R[1]) / p;
+                                        P4.z = (a * A.R[2] + b * B.R[2]) / p;
+                                        P4.w = p;
+                                        hPP.push_back(P4);
+                                        hPK.push_back(make_double2(cc * exp(-mu * rr), a));
+                                        hp.nprim++;
+                                }
+                        }
+                        if (hp.nprim == 0) continue;
+                        pairs[pair_class(A.l, B.l)].push_back(hp);
+                }
+        }
+        P->prim_pairs = (int64_t)hPP.size();
+        if ((rc = dev_upload(P->PP, hPP)) || (rc = dev_upload(P->PK, hPK))) return bail(rc);
+
+        // Cartesian offset tables of all quartet classes (also used by q_cond)
+        {
+                std::vector<int> all;
+                auto qcs = quartet_classes();
+                P->goff_at.assign(qcs.size(), 0);
+                for (size_t t = 0; t < qcs.size(); t++) {
+                        int la, lb, lc, ld;
+                        class_l(qcs[t].X, la, lb);
+                        class_l(qcs[t].Y, lc, ld);
+                        P->goff_at[t] = all.size();
+                        class_goff(la, lb, lc, ld, all);
+                }
+                if ((rc = dev_upload(P->goff_all, all))) return bail(rc);
+        }
+
+        // upload unsorted pairs, compute q_cond on the GPU
+        auto upload_class = [&](int X, const std::vector<HostPair> &hv) -> int {
+                PairClassDev &c = P->pc[X];
+                class_l(X, c.la, c.lb);
+                c.n = (int)hv.size();
+                std::vector<int4> sh(hv.size());
+                std::vector<int2> pr(hv.size());
+                std::vector<double> q(hv.size());
+                std::vector<double4> Av(hv.size()), ABv(hv.size());
+                for (size_t t = 0; t < hv.size(); t++) {
+                        const Seg &A = segs[hv[t].i], &B = segs[hv[t].j];
+                        sh[t] = make_int4(A.cart_off, B.cart_off, A.parent, B.parent);
+                        pr[t] = make_int2(hv[t].prim0, hv[t].nprim);
+                        q[t] = hv[t].q;
+                        Av[t] = make_double4(A.R[0], A.R[1], A.R[2], hv[t].i == hv[t].j ? 1.0 : 0.0);
+                        ABv[t] = make_double4(A.R[0] - B.R[0], A.R[1] - B.R[1], A.R[2] - B.R[2], 0.0);
+                }
+                int r;
+                if ((r = dev_upload(c.sh, sh)) || (r = dev_upload(c.pr, pr)) || (r = dev_upload(c.q, q)) ||
+                    (r = dev_upload(c.A, Av)) || (r = dev_upload(c.AB, ABv)))
+                        return r;
+                return B200JK_OK;
+        };
+        for (int X = 0; X < NPAIRCLASS; X++)
+                if ((rc = upload_class(X, pairs[X]))) return bail(rc);
+
+        std::vector<double> h_q((size_t)nbas * nbas, 1e-100);
+        if ((rc = dev_upload(P->qcond, h_q))) return bail(rc);
+        {
+                auto qcs = quartet_classes();
+                for (int X = 0; X < NPAIRCLASS; X++) {
+                        QArgs qa;
+                        qa.pairs = P->pc[X].view();
+                        qa.PP = P->PP.p; qa.PK = P->PK.p;
+                        qa.table = table_ptr();
+                        size_t gi = 0;
+                        for (size_t t = 0; t < qcs.size(); t++) if (qcs[t].X == X && qcs[t].Y == X) gi = t;
+                        qa.goff = P->goff_all.p + P->goff_at[gi];
+                        qa.c2s = P->c2s.p;
+                        qa.qcond = (unsigned long long *)P->qcond.p;
+                        qa.nbas = nbas;
+                        qa.cart = P->cart;
+                        {
+                                std::string err;
+                                if (launch_qcond(P->pc[X].la, P->pc[X].lb, qa, P->stream, err)) return bail(fail(B200JK_ECUDA, err));
+                        }
+                }
+                if (cudaStreamSynchronize(P->stream) != cudaSuccess)
+                        return bail(fail(B200JK_ECUDA, std::string("q_cond kernels: ") + cudaGetErrorString(cudaGetLastError())));
+                if (cudaMemcpy(h_q.data(), P->qcond.p, sizeof(double) * h_q.size(), cudaMemcpyDeviceToHost) != cudaSuccess)
+                        return bail(fail(B200JK_ECUDA, "q_cond download failed"));
+        }
+        P->h_qcond = h_q;
+
+        // keep pairs that can pass q_ij q_kl > tol for some kl; sort by q
+        double qmax = 0;
+        for (double v : h_q) qmax = std::max(qmax, v);
+        P->shell_pairs = 0;
+        for (int X = 0; X < NPAIRCLASS; X++) {
+                std::vector<HostPair> &hv = pairs[X];
+                for (auto &p : hv) p.q = h_q[(size_t)segs[p.i].parent * nbas + segs[p.j].parent];
+                if (P->tol > 0) {
+                        hv.erase(std::remove_if(hv.begin(), hv.end(),
+                                                [&](const HostPair &p) { return !(p.q * qmax > P->tol); }),
+                                 hv.end());
+                }
+                std::stable_sort(hv.begin(), hv.end(), [](const HostPair &a, const HostPair &b) { return a.q > b.q; });
+                P->shell_pairs += (int64_t)hv.size();
+                if ((rc = upload_class(X, hv))) return bail(rc);
+        }
+        memset(&P->st, 0, sizeof(P->st));
+        P->st.nao = P->nao; P->st.nao_cart = P->naoc; P->st.nbas = nbas; P->st.nseg = P->nseg;
+        P->st.shell_pairs = P->shell_pairs; P->st.prim_pairs = P->prim_pairs;
+        *out = P;
+        return B200JK_OK;
+}
+
+int b200jk_get_q_cond(const b200jk_plan *plan, double *q_cond)
+{
+        if (!plan || !q_cond) return fail(B200JK_EINVAL, "NULL argument");
+        memcpy(q_cond, plan->h_qcond.data(), sizeof(double) * plan->h_qcond.size());
+        return B200JK_OK;
+}
+
+static int ensure_workspace(b200jk_plan *P, int n_dm)
+{
+        const size_t nn = (size_t)P->nao * P->nao, nc = (size_t)P->naoc * P->naoc;
+        int rc;
+        if ((rc = dev_alloc(P->D, nn * n_dm)) || (rc = dev_alloc(P->Dc, nc * n_dm * 2)) ||
+            (rc = dev_alloc(P->Ds, nc * n_dm)) || (rc = dev_alloc(P->Jacc, nc * n_dm)) ||
+            (rc = dev_alloc(P->Kacc, nc * n_dm * 2)) || (rc = dev_alloc(P->outJ, nn * n_dm)) ||
+            (rc = dev_alloc(P->outK, nn * n_dm)) || (rc = dev_alloc(P->dm_cond, (size_t)P->nbas * P->nbas)) ||
+            (rc = dev_alloc(P->dmax, 1)) || (rc = dev_alloc(P->stats, 2)))
+                return rc;
+        int maxn = 1;
+        for (auto &c : P->pc) maxn = std::max(maxn, c.n);
+        if ((rc = dev_alloc(P->nkl, maxn)) || (rc = dev_alloc(P->nchunk, maxn + 1)) ||
+            (rc = dev_alloc(P->chunk_off, maxn + 1)))
+                return rc;
+        size_t tmp = 0;
+        cub::DeviceScan::ExclusiveSum(nullptr, tmp, P->nchunk.p, P->chunk_off.p, maxn + 1);
+        if ((rc = dev_alloc(P->cub_tmp, tmp + 16))) return rc;
+        P->ws_ndm = std::max(P->ws_ndm, n_dm);
+        return B200JK_OK;
+}
+
+static inline unsigned grid_for(long long n, int block) { return (unsigned)((n + block - 1) / block); }
+
+int b200jk_get_jk(b200jk_plan *P, const double *dms, int n_dm, int hermi, int with_j, int with_k,
+                  double *vj, double *vk, int dev_ptrs, int precision_mode, void *stream)
+{
+        if (!P) return fail(B200JK_EINVAL, "plan is NULL");
+        if (!dms || n_dm <= 0) return fail(B200JK_EINVAL, "no density matrices");
+        if (hermi < 0 || hermi > 2) return fail(B200JK_EINVAL, "hermi must be 0, 1 or 2");
+        if (with_j && !vj) return fail(B200JK_EINVAL, "vj is NULL while with_j is set");
+        if (with_k && !vk) return fail(B200JK_EINVAL, "vk is NULL while with_k is set");
+        if (precision_mode != B200JK_PREC_FP64) return fail(B200JK_EUNSUPPORTED, "only precision_mode 0 (FP64) is implemented");
+        CUDA_TRY(cudaSetDevice(P->device));
+        int rc = ensure_workspace(P, n_dm);
+        if (rc) return rc;
+        cudaStream_t s = stream ? (cudaStream_t)stream : P->stream;
+        const size_t nn = (size_t)P->nao * P->nao, nc = (size_t)P->naoc * P->naoc;
+        const int nk = hermi == 1 ? 1 : 2;
+        CUDA_TRY(cudaEventRecord(P->ev0, s));
+        const double *dD = dms;
+        if (!dev_ptrs) {
+                CUDA_TRY(cudaMemcpyAsync(P->D.p, dms, sizeof(double) * nn * n_dm, cudaMemcpyHostToDevice, s));
+                dD = P->D.p;
+        }
+        // screening data
+        CUDA_TRY(cudaMemsetAsync(P->dmax.p, 0, sizeof(unsigned long long), s));
+        CUDA_TRY(cudaMemsetAsync(P->stats.p, 0, 2 * sizeof(unsigned long long), s));
+        {
+                const long long npair = (long long)P->nbas * (P->nbas + 1) / 2;
+                dm_cond_kernel<<<grid_for(npair, 256), 256, 0, s>>>(dD, n_dm, P->nao, P->ao_loc_d.p, P->nbas,
+                                                                  P->dm_cond.p, P->dmax.p);
+                CUDA_TRY(cudaGetLastError());
+        }
+        // densities in the Cartesian basis
+        for (int d = 0; d < n_dm; d++) {
+                double *Dc = P->Dc.p + (size_t)d * nk * nc;
+                out_to_cart_kernel<<<grid_for((long long)nc, 256), 256, 0, s>>>(
+                        dD + (size_t)d * nn, P->nao, P->naoc, P->cart_seg.p, P->cart_comp.p, P->seg_info.p,
+                        P->c2s.p, P->cart, Dc, nk == 2 ? Dc + nc : nullptr, nullptr);
+                CUDA_TRY(cudaGetLastError());
+                sym_sum_kernel<<<grid_for((long long)nc, 256), 256, 0, s>>>(Dc, P->naoc, P->Ds.p + (size_t)d * nc);
+                CUDA_TRY(cudaGetLastError());
+        }
+        if (with_j) CUDA_TRY(cudaMemsetAsync(P->Jacc.p, 0, sizeof(double) * nc * n_dm, s));
+        if (with_k) CUDA_TRY(cudaMemsetAsync(P->Kacc.p, 0, sizeof(double) * nc * n_dm * nk, s));
+
+        const double *tbl = table_ptr();
+        auto qcs = quartet_classes();
+        {
+                for (size_t t = 0; t < qcs.size(); t++) {
+                        const PairClassDev &bra = P->pc[qcs[t].X], &ket = P->pc[qcs[t].Y];
+                        if (bra.n == 0 || ket.n == 0) continue;
+                        int la = bra.la, lb = bra.lb, lc = ket.la, ld = ket.lb;
+                        const int same = qcs[t].X == qcs[t].Y;
+                        // chunk size of the family the dispatcher will pick
+                        const int chunk = family_chunk(la, lb, lc, ld);
+                        count_kernel<<<grid_for(bra.n, 256), 256, 0, s>>>(bra.view(), ket.view(), same,
+                                                                         P->tol > 0 ? P->tol : 0.0,
+                                                                         (const double *)P->dmax.p, chunk,
+                                                                         P->nkl.p, P->nchunk.p);
+                        CUDA_TRY(cudaGetLastError());
+                        CUDA_TRY(cudaMemsetAsync(P->nchunk.p + bra.n, 0, sizeof(long long), s));
+                        size_t tmp = P->cub_tmp.n;
+                        CUDA_TRY(cub::DeviceScan::ExclusiveSum(P->cub_tmp.p, tmp, P->nchunk.p, P->chunk_off.p, bra.n + 1, s));
+                        JKArgs a;
+                        a.bra = bra.view();
+                        a.ket = ket.view();
+                        a.PP = P->PP.p; a.PK = P->PK.p;
+                        a.chunk_off = P->chunk_off.p;
+                        a.nkl = P->nkl.p;
+                        a.dm_cond = P->dm_cond.p;
+                        a.table = tbl;
+                        a.goff = P->goff_all.p + P->goff_at[t];
+                        a.Jacc = P->Jacc.p; a.Kacc = P->Kacc.p;
+                        a.Ds = P->Ds.p; a.Dk = P->Dc.p;
+                        a.stats = P->stats.p;
+                        a.tol = P->tol > 0 ? P->tol : -1.0;
+                        a.nbas = P->nbas; a.naoc = P->naoc; a.n_dm = n_dm; a.nk = nk;
+                        a.with_j = with_j; a.with_k = with_k; a.same = same;
+                        if ((rc = dispatch_jk(P, la, lb, lc, ld, a, s))) return rc;
+                }
+        }
+        // back to the output basis
+        for (int d = 0; d < n_dm; d++) {
+                if (with_j) {
+                        const double *J = P->Jacc.p + (size_t)d * nc;
+                        double *o = dev_ptrs ? vj + (size_t)d * nn : P->outJ.p + (size_t)d * nn;
+                        cart_to_out_kernel<<<grid_for((long long)nn, 256), 256, 0, s>>>(
+                                J, J, P->nao, P->naoc, P->out_seg.p, P->out_comp.p, P->seg_info.p, P->c2s.p,
+                                P->cart, 1, o);
+                        CUDA_TRY(cudaGetLastError());
+                }
+                if (with_k) {
+                        const double *K1 = P->Kacc.p + (size_t)d * nk * nc;
+                        const double *K2 = nk == 2 ? K1 + nc : K1;
+                        double *o = dev_ptrs ? vk + (size_t)d * nn : P->outK.p + (size_t)d * nn;
+                        cart_to_out_kernel<<<grid_for((long long)nn, 256), 256, 0, s>>>(
+                                K1, K2, P->nao, P->naoc, P->out_seg.p, P->out_comp.p, P->seg_info.p, P->c2s.p,
+                                P->cart, hermi, o);
+                        CUDA_TRY(cudaGetLastError());
+                }
+        }
+        CUDA_TRY(cudaEventRecord(P->ev1, s));
+        if (!dev_ptrs) {
+                if (with_j) CUDA_TRY(cudaMemcpyAsync(vj, P->outJ.p, sizeof(double) * nn * n_dm, cudaMemcpyDeviceToHost, s));
+                if (with_k) CUDA_TRY(cudaMemcpyAsync(vk, P->outK.p, sizeof(double) * nn * n_dm, cudaMemcpyDeviceToHost, s));
+        }
+        unsigned long long hs[2] = {0, 0};
+        CUDA_TRY(cudaMemcpyAsync(hs, P->stats.p, sizeof(hs), cudaMemcpyDeviceToHost, s));
+        CUDA_TRY(cudaStreamSynchronize(s));
+        float ms = 0;
+        CUDA_TRY(cudaEventElapsedTime(&ms, P->ev0, P->ev1));
+        P->st.quartets = (int64_t)hs[0];
+        P->st.prim_quartets = (int64_t)hs[1];
+        P->st.last_build_ms = ms;
+        return B200JK_OK;
+}
+
+int b200jk_stats(const b200jk_plan *plan, b200jk_stats_t *stats)
+{
+        if (!plan || !stats) return fail(B200JK_EINVAL, "NULL argument");
+        *stats = plan->st;
+        return B200JK_OK;
+}
+
+} // extern "C"
+

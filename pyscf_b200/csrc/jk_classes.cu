@@ -1,0 +1,77 @@
+// jk_classes.cu — the kernel of one quartet class (la lb | lc ld), compiled
+// once per class with -DB2_BRA_LA -DB2_BRA_LB -DB2_KET_LC -DB2_KET_LD so the
+// 55 classes of l <= 3 build in parallel.
+#include <mutex>
+#include "jk_launch.h"
+
+#ifndef B2_KET_LD
+#error "compile with -DB2_BRA_LA -DB2_BRA_LB -DB2_KET_LC -DB2_KET_LD"
+#endif
+
+namespace b200jk {
+
+namespace {
+
+struct LaunchCfg {
+        int grid = 0, block = 128;
+        size_t smem = 0;
+        bool ready = false;
+        cudaError_t status = cudaSuccess;
+};
+
+template <int LA, int LB, int LC, int LD>
+int launch_one(const JKArgs &a, cudaStream_t s, int nsm, std::string &err)
+{
+        using K = Class4<LA, LB, LC, LD>;
+        constexpr bool thread = (K::NG + 3 * K::SA) <= 80;
+        static LaunchCfg cfg;
+        static std::mutex mu;
+        {
+                std::lock_guard<std::mutex> lk(mu);
+                if (!cfg.ready) {
+                        int nb = 0;
+                        if constexpr (thread) {
+                                cfg.block = 128;
+                                cfg.smem = 0;
+                                cfg.status = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, jk_thread_kernel<LA, LB, LC, LD>, 128, 0);
+                        } else {
+                                const size_t per_warp = sizeof(double) * WarpSmem<LA, LB, LC, LD>::SIZE;
+                                const int wpb = (int)std::min<size_t>(4, std::max<size_t>(1, (200 * 1024) / per_warp));
+                                cfg.block = 32 * wpb;
+                                cfg.smem = per_warp * wpb;
+                                cfg.status = cudaFuncSetAttribute(jk_warp_kernel<LA, LB, LC, LD>,
+                                                                  cudaFuncAttributeMaxDynamicSharedMemorySize, (int)cfg.smem);
+                                if (cfg.status == cudaSuccess)
+                                        cfg.status = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, jk_warp_kernel<LA, LB, LC, LD>,
+                                                                                                   cfg.block, cfg.smem);
+                        }
+                        cfg.grid = (nb > 0 ? nb : 1) * nsm;
+                        cfg.ready = true;
+                }
+        }
+        if (cfg.status != cudaSuccess) {
+                err = std::string("kernel configuration: ") + cudaGetErrorString(cfg.status);
+                return 1;
+        }
+        if constexpr (thread) {
+                jk_thread_kernel<LA, LB, LC, LD><<<cfg.grid, cfg.block, 0, s>>>(a);
+        } else {
+                jk_warp_kernel<LA, LB, LC, LD><<<cfg.grid, cfg.block, cfg.smem, s>>>(a, 8);
+        }
+        cudaError_t e = cudaGetLastError();
+        if (e != cudaSuccess) {
+                err = std::string("kernel launch: ") + cudaGetErrorString(e);
+                return 1;
+        }
+        return 0;
+}
+
+} // namespace
+
+// B2_FN_NAME is launch_jk_<la><lb><lc><ld>, declared in jk_launch.h
+int B2_FN_NAME(const JKArgs &a, cudaStream_t s, int nsm, std::string &err)
+{
+        return launch_one<B2_BRA_LA, B2_BRA_LB, B2_KET_LC, B2_KET_LD>(a, s, nsm, err);
+}
+
+} // namespace b200jk

@@ -1,0 +1,714 @@
+// jk_kernels.cuh — sm_100a kernels of the direct-SCF J/K build.
+//
+// Work decomposition.  Shell pairs (i,j) are grouped into angular classes
+// (la >= lb) and, inside a class, sorted by descending Schwarz bound q_ij.
+// A quartet class (X|Y) pairs bra class X with ket class Y (X >= Y).  For a
+// bra pair ij the ket pairs that can survive the screen
+//     q_ij q_kl max(4 D_ji, 4 D_lk, D_jk, D_jl, D_ik, D_il) > tol
+// (CVHFnrs8_prescreen, pyscf/lib/vhf/optimizer.c:90-117) form a prefix of the
+// sorted ket list, so the work of a class is  sum_ij nkl(ij)  quartets; it is
+// cut into chunks (32 quartets for the thread-per-quartet family, 8 for the
+// warp-per-quartet family) and a grid-stride loop of warps walks the chunks
+// (warp -> chunk -> bra pair by binary search of the chunk prefix sum).  The
+// exact per-quartet test is then applied with the parent-shell density bound.
+//
+// Arithmetic.  Integrals are Cartesian; the density enters in the Cartesian
+// AO basis D_c = C^T D C and the results leave as C J_c C^T (C the block
+// diagonal real-solid-harmonic map), so no per-quartet transform is done.
+// Each unique quartet scatters to its symmetry images with weight 1/deg:
+//     Jacc[c,d] += v Ds[a,b],  Jacc[a,b] += v Ds[c,d]      (Ds = D + D^T)
+//     Kacc[a,d] += v X[b,c],  Kacc[a,c] += v X[b,d],
+//     Kacc[b,d] += v X[a,c],  Kacc[b,c] += v X[a,d]
+// and  J = Jacc + Jacc^T,  K = Kacc[D] + Kacc[D^T]^T  (Kacc[D] + Kacc[D]^T for
+// symmetric D).  These are the images PySCF's 'ji->s2kl' and 'li->s2kj' /
+// 'li->s1kj' scripts accumulate (pyscf/lib/vhf/nr_direct_dot.c:1293-1647).
+#pragma once
+#include "rys_math.cuh"
+
+namespace b200jk {
+
+struct PairView {
+        const int4 *sh;      // (cart AO of i, cart AO of j, parent shell i, parent shell j)
+        const int2 *pr;      // (first primitive pair, number of primitive pairs)
+        const double *q;     // parent-shell Schwarz bound (descending)
+        const double4 *A;    // (A, 1 if i == j else 0)
+        const double4 *AB;   // (A - B, 0)
+        int n;
+};
+
+struct JKArgs {
+        PairView bra, ket;
+        const double4 *PP;           // primitive pair (P, p)
+        const double2 *PK;           // primitive pair (K_ab c_i c_j, a_i)
+        const long long *chunk_off;  // bra.n + 1 entries
+        const int *nkl;              // per bra pair
+        const double *dm_cond;       // nbas x nbas (parent shells)
+        const double *table;         // Rys tables
+        const int *goff;             // packed (ox, oy, oz) per Cartesian component (warp family)
+        double *Jacc, *Kacc;
+        const double *Ds, *Dk;
+        unsigned long long *stats;   // [0] quartets, [1] primitive quartets
+        double tol;
+        int nbas, naoc, n_dm, nk;
+        int with_j, with_k, same;
+};
+
+__device__ __forceinline__ double warp_sum(double v)
+{
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+        return v;
+}
+
+__device__ __forceinline__ int find_bra(const long long *off, int n, long long chunk)
+{
+        int lo = 0, hi = n;  // off[lo] <= chunk < off[hi]
+        while (hi - lo > 1) {
+                int mid = (lo + hi) >> 1;
+                if (__ldg(off + mid) <= chunk) lo = mid;
+                else hi = mid;
+        }
+        return lo;
+}
+
+__device__ __forceinline__ bool quartet_passes(const JKArgs &a, int4 sb, double qij, int4 sk, double qkl)
+{
+        const double qq = qij * qkl;
+        if (!(qq > a.tol)) return false;
+        const size_t n = (size_t)a.nbas;
+        const double *dc = a.dm_cond;
+        const int pi = sb.z, pj = sb.w, pk = sk.z, pl = sk.w;
+        double d = 4.0 * fmax(__ldg(dc + pj * n + pi), __ldg(dc + pl * n + pk));
+        d = fmax(d, fmax(__ldg(dc + pj * n + pk), __ldg(dc + pj * n + pl)));
+        d = fmax(d, fmax(__ldg(dc + pi * n + pk), __ldg(dc + pi * n + pl)));
+        return d * qq > a.tol;
+}
+
+// 2 pi^{5/2}
+#define B2_TWO_PI_2P5 34.98683665524972497
+
+// ---------------------------------------------------------------------------
+// Count kernel: ket prefix length per bra pair, and chunks of `chunk` quartets.
+static __global__ void count_kernel(PairView bra, PairView ket, int same, double tol, const double *dmax4,
+                             int chunk, int *nkl, long long *nchunk)
+{
+        const int ij = blockIdx.x * blockDim.x + threadIdx.x;
+        if (ij >= bra.n) return;
+        const double qij = bra.q[ij];
+        const double dm = *dmax4;
+        int cnt = 0;
+        if (dm > 0 && qij > 0) {
+                const double thr = tol / (qij * dm);
+                // ket.q is descending: count entries with q > thr
+                int lo = 0, hi = ket.n;
+                while (lo < hi) {
+                        int mid = (lo + hi) >> 1;
+                        if (ket.q[mid] > thr) lo = mid + 1;
+                        else hi = mid;
+                }
+                cnt = lo;
+                if (same) cnt = min(cnt, ij + 1);
+        }
+        nkl[ij] = cnt;
+        nchunk[ij] = (cnt + chunk - 1) / chunk;
+}
+
+// ---------------------------------------------------------------------------
+// Thread-per-quartet family: the whole Cartesian block lives in registers.
+template <int LA, int LB, int LC, int LD>
+__global__ void __launch_bounds__(128) jk_thread_kernel(JKArgs a)
+{
+        using K = Class4<LA, LB, LC, LD>;
+        const int lane = threadIdx.x & 31;
+        const long long total = a.chunk_off[a.bra.n];
+        const long long nwarps = ((long long)gridDim.x * blockDim.x) >> 5;
+        const size_t n = (size_t)a.naoc, nn = n * n;
+        unsigned long long nq = 0, npq = 0;
+        for (long long chunk = ((long long)blockIdx.x * blockDim.x + threadIdx.x) >> 5; chunk < total;
+             chunk += nwarps) {
+                const int ij = find_bra(a.chunk_off, a.bra.n, chunk);
+                const int kl = (int)(chunk - a.chunk_off[ij]) * 32 + lane;
+                const int4 sb = a.bra.sh[ij];
+                const int2 pb = a.bra.pr[ij];
+                const double qij = a.bra.q[ij];
+                const double4 Ab = a.bra.A[ij];
+                const double4 ABb = a.bra.AB[ij];
+                bool active = kl < a.nkl[ij];
+                int4 sk = make_int4(0, 0, 0, 0);
+                double G[K::NG];
+#pragma unroll
+                for (int t = 0; t < K::NG; t++) G[t] = 0.0;
+                if (active) {
+                        sk = a.ket.sh[kl];
+                        active = quartet_passes(a, sb, qij, sk, a.ket.q[kl]);
+                }
+                if (active) {
+                        const int2 pk = a.ket.pr[kl];
+                        const double4 Ak = a.ket.A[kl];
+                        const double4 CDk = a.ket.AB[kl];
+                        double fac = 1.0;
+                        if (Ab.w != 0.0) fac *= 0.5;
+                        if (Ak.w != 0.0) fac *= 0.5;
+                        if (a.same && ij == kl) fac *= 0.5;
+                        const double A[3] = {Ab.x, Ab.y, Ab.z}, AB[3] = {ABb.x, ABb.y, ABb.z};
+                        const double C[3] = {Ak.x, Ak.y, Ak.z}, CD[3] = {CDk.x, CDk.y, CDk.z};
+                        nq++;
+                        for (int ip = 0; ip < pb.y; ip++) {
+                                const double4 P = a.PP[pb.x + ip];
+                                const double Kab = a.PK[pb.x + ip].x * fac;
+                                const double Pv[3] = {P.x, P.y, P.z};
+                                for (int kp = 0; kp < pk.y; kp++) {
+                                        const double4 Q = a.PP[pk.x + kp];
+                                        const double Kcd = a.PK[pk.x + kp].x;
+                                        const double Qv[3] = {Q.x, Q.y, Q.z};
+                                        const double pref = B2_TWO_PI_2P5 / (P.w * Q.w * sqrt(P.w + Q.w)) * Kab * Kcd;
+                                        add_prim_quartet<LA, LB, LC, LD>(G, a.table, P.w, Pv, Q.w, Qv, A, C, AB, CD, pref);
+                                }
+                        }
+                        npq += (unsigned long long)pb.y * pk.y;
+                }
+                const int ia = sb.x, ib = sb.y, ic = sk.x, id = sk.y;
+                for (int s = 0; s < a.n_dm; s++) {
+                        if (a.with_j) {
+                                const double *Ds = a.Ds + s * nn;
+                                double *J = a.Jacc + s * nn;
+                                if (active) {
+                                        double dab[K::NAB];
+#pragma unroll
+                                        for (int x = 0; x < K::NA; x++)
+#pragma unroll
+                                                for (int y = 0; y < K::NB; y++) dab[x * K::NB + y] = __ldg(Ds + (ia + x) * n + ib + y);
+#pragma unroll
+                                        for (int x = 0; x < K::NC; x++)
+#pragma unroll
+                                        for (int y = 0; y < K::ND; y++) {
+                                                double v = 0.0;
+#pragma unroll
+                                                for (int t = 0; t < K::NAB; t++) v += G[t * K::NCD + x * K::ND + y] * dab[t];
+                                                atomicAdd(J + (ic + x) * n + id + y, v);
+                                        }
+                                }
+                                double dcd[K::NCD];
+#pragma unroll
+                                for (int x = 0; x < K::NC; x++)
+#pragma unroll
+                                        for (int y = 0; y < K::ND; y++)
+                                                dcd[x * K::ND + y] = active ? __ldg(Ds + (ic + x) * n + id + y) : 0.0;
+#pragma unroll
+                                for (int t = 0; t < K::NAB; t++) {
+                                        double v = 0.0;
+#pragma unroll
+                                        for (int u = 0; u < K::NCD; u++) v += G[t * K::NCD + u] * dcd[u];
+                                        v = warp_sum(v);
+                                        if (lane == 0 && v != 0.0) atomicAdd(J + (ia + t / K::NB) * n + ib + t % K::NB, v);
+                                }
+                        }
+                        if (a.with_k && active) {
+                                for (int t = 0; t < a.nk; t++) {
+                                        const double *X = a.Dk + (s * a.nk + t) * nn;
+                                        double *Kt = a.Kacc + (s * a.nk + t) * nn;
+                                        // K[a,d] += G X[b,c]
+                                        {
+                                                double x_[K::NB * K::NC];
+#pragma unroll
+                                                for (int b = 0; b < K::NB; b++)
+#pragma unroll
+                                                        for (int c = 0; c < K::NC; c++) x_[b * K::NC + c] = __ldg(X + (ib + b) * n + ic + c);
+#pragma unroll
+                                                for (int x = 0; x < K::NA; x++)
+#pragma unroll
+                                                for (int d = 0; d < K::ND; d++) {
+                                                        double v = 0.0;
+#pragma unroll
+                                                        for (int b = 0; b < K::NB; b++)
+#pragma unroll
+                                                                for (int c = 0; c < K::NC; c++)
+                                                                        v += G[((x * K::NB + b) * K::NC + c) * K::ND + d] * x_[b * K::NC + c];
+                                                        atomicAdd(Kt + (ia + x) * n + id + d, v);
+                                                }
+                                        }
+                                        // K[a,c] += G X[b,d]
+                                        {
+                                                double x_[K::NB * K::ND];
+#pragma unroll
+                                                for (int b = 0; b < K::NB; b++)
+#pragma unroll
+                                                        for (int d = 0; d < K::ND; d++) x_[b * K::ND + d] = __ldg(X + (ib + b) * n + id + d);
+#pragma unroll
+                                                for (int x = 0; x < K::NA; x++)
+#pragma unroll
+                                                for (int c = 0; c < K::NC; c++) {
+                                                        double v = 0.0;
+#pragma unroll
+                                                        for (int b = 0; b < K::NB; b++)
+#pragma unroll
+                                                                for (int d = 0; d < K::ND; d++)
+                                                                        v += G[((x * K::NB + b) * K::NC + c) * K::ND + d] * x_[b * K::ND + d];
+                                                        atomicAdd(Kt + (ia + x) * n + ic + c, v);
+                                                }
+                                        }
+                                        // K[b,d] += G X[a,c]
+                                        {
+                                                double x_[K::NA * K::NC];
+#pragma unroll
+                                                for (int x = 0; x < K::NA; x++)
+#pragma unroll
+                                                        for (int c = 0; c < K::NC; c++) x_[x * K::NC + c] = __ldg(X + (ia + x) * n + ic + c);
+#pragma unroll
+                                                for (int b = 0; b < K::NB; b++)
+#pragma unroll
+                                                for (int d = 0; d < K::ND; d++) {
+                                                        double v = 0.0;
+#pragma unroll
+                                                        for (int x = 0; x < K::NA; x++)
+#pragma unroll
+                                                                for (int c = 0; c < K::NC; c++)
+                                                                        v += G[((x * K::NB + b) * K::NC + c) * K::ND + d] * x_[x * K::NC + c];
+                                                        atomicAdd(Kt + (ib + b) * n + id + d, v);
+                                                }
+                                        }
+                                        // K[b,c] += G X[a,d]
+                                        {
+                                                double x_[K::NA * K::ND];
+#pragma unroll
+                                                for (int x = 0; x < K::NA; x++)
+#pragma unroll
+                                                        for (int d = 0; d < K::ND; d++) x_[x * K::ND + d] = __ldg(X + (ia + x) * n + id + d);
+#pragma unroll
+                                                for (int b = 0; b < K::NB; b++)
+#pragma unroll
+                                                for (int c = 0; c < K::NC; c++) {
+                                                        double v = 0.0;
+#pragma unroll
+                                                        for (int x = 0; x < K::NA; x++)
+#pragma unroll
+                                                                for (int d = 0; d < K::ND; d++)
+                                                                        v += G[((x * K::NB + b) * K::NC + c) * K::ND + d] * x_[x * K::ND + d];
+                                                        atomicAdd(Kt + (ib + b) * n + ic + c, v);
+                                                }
+                                        }
+                                }
+                        }
+                }
+        }
+        if (a.stats) {
+                for (int o = 16; o > 0; o >>= 1) {
+                        nq += __shfl_xor_sync(0xffffffffu, nq, o);
+                        npq += __shfl_xor_sync(0xffffffffu, npq, o);
+                }
+                if (lane == 0 && nq) {
+                        atomicAdd(a.stats + 0, nq);
+                        atomicAdd(a.stats + 1, npq);
+                }
+        }
+}
+
+// ---------------------------------------------------------------------------
+// Warp-per-quartet family: 2D integrals and the Cartesian block in shared
+// memory, components spread over the lanes.
+template <int LA, int LB, int LC, int LD>
+struct WarpSmem {
+        using K = Class4<LA, LB, LC, LD>;
+        static constexpr int G = 0;
+        static constexpr int H = G + K::NG;                      // [3][NR][SA]
+        static constexpr int DSAB = H + 3 * K::NR * K::SA;
+        static constexpr int DSCD = DSAB + K::NAB;
+        static constexpr int XBC = DSCD + K::NCD;
+        static constexpr int XBD = XBC + K::NB * K::NC;
+        static constexpr int XAC = XBD + K::NB * K::ND;
+        static constexpr int XAD = XAC + K::NA * K::NC;
+        static constexpr int SIZE = ((XAD + K::NA * K::ND) + 1) & ~1;   // doubles per warp
+};
+
+template <int LA, int LB, int LC, int LD>
+__device__ __forceinline__ void warp_slice_to_smem(double *h, double g00, const RysCoef &rc, int dir,
+                                                   double ab, double cd)
+{
+        using K = Class4<LA, LB, LC, LD>;
+        double g[K::NE * K::NF];
+        const double c00 = dir == 0 ? rc.c00[0] : (dir == 1 ? rc.c00[1] : rc.c00[2]);
+        const double c00p = dir == 0 ? rc.c00p[0] : (dir == 1 ? rc.c00p[1] : rc.c00p[2]);
+        vrr2d<K::NE, K::NF>(g, g00, c00, c00p, rc.b10, rc.b01, rc.b00);
+        // ket transfer first: u[e][c][d]
+        constexpr int NCD1 = (LC + 1) * (LD + 1);
+        double u[K::NE * NCD1];
+        double cdp[LD + 1];
+        cdp[0] = 1.0;
+#pragma unroll
+        for (int k = 1; k <= LD; k++) cdp[k] = cdp[k - 1] * cd;
+#pragma unroll
+        for (int e = 0; e < K::NE; e++)
+#pragma unroll
+        for (int c = 0; c <= LC; c++)
+#pragma unroll
+        for (int d = 0; d <= LD; d++) {
+                double v = 0.0;
+#pragma unroll
+                for (int k = 0; k <= d; k++) v += (double)binom(d, k) * cdp[d - k] * g[e * K::NF + c + k];
+                u[e * NCD1 + c * (LD + 1) + d] = v;
+        }
+        double abp[LB + 1];
+        abp[0] = 1.0;
+#pragma unroll
+        for (int k = 1; k <= LB; k++) abp[k] = abp[k - 1] * ab;
+#pragma unroll
+        for (int x = 0; x <= LA; x++)
+#pragma unroll
+        for (int b = 0; b <= LB; b++)
+#pragma unroll
+        for (int t = 0; t < NCD1; t++) {
+                double v = 0.0;
+#pragma unroll
+                for (int k = 0; k <= b; k++) v += (double)binom(b, k) * abp[b - k] * u[(x + k) * NCD1 + t];
+                h[(x * (LB + 1) + b) * NCD1 + t] = v;
+        }
+}
+
+template <int LA, int LB, int LC, int LD>
+__device__ __forceinline__ void warp_eval_block(double *sm, const JKArgs &a, int2 pb, int2 pk,
+                                                const double A[3], const double AB[3],
+                                                const double C[3], const double CD[3], double fac)
+{
+        using K = Class4<LA, LB, LC, LD>;
+        using S = WarpSmem<LA, LB, LC, LD>;
+        const int lane = threadIdx.x & 31;
+        double *G = sm + S::G;
+        double *H = sm + S::H;
+        for (int t = lane; t < K::NG; t += 32) G[t] = 0.0;
+        for (int ip = 0; ip < pb.y; ip++) {
+                const double4 P = a.PP[pb.x + ip];
+                const double Kab = a.PK[pb.x + ip].x * fac;
+                for (int kp = 0; kp < pk.y; kp++) {
+                        const double4 Q = a.PP[pk.x + kp];
+                        const double Kcd = a.PK[pk.x + kp].x;
+                        __syncwarp();
+                        if (lane < 3 * K::NR) {
+                                const int r = lane / 3, dir = lane - 3 * r;
+                                const double PA[3] = {P.x - A[0], P.y - A[1], P.z - A[2]};
+                                const double QC[3] = {Q.x - C[0], Q.y - C[1], Q.z - C[2]};
+                                const double PQ[3] = {P.x - Q.x, P.y - Q.y, P.z - Q.z};
+                                const double p = P.w, q = Q.w;
+                                const double T = p * q / (p + q) * (PQ[0] * PQ[0] + PQ[1] * PQ[1] + PQ[2] * PQ[2]);
+                                double u[K::NR], w[K::NR];
+                                rys_roots<K::NR>(T, a.table, u, w);
+                                double ur = u[0], wr = w[0];
+#pragma unroll
+                                for (int i = 1; i < K::NR; i++)
+                                        if (r == i) { ur = u[i]; wr = w[i]; }
+                                RysCoef rc;
+                                rys_coef(rc, ur, p, q, PA, QC, PQ);
+                                const double pref = B2_TWO_PI_2P5 / (p * q * sqrt(p + q)) * Kab * Kcd;
+                                const double g00 = dir == 2 ? pref * wr : 1.0;
+                                const double abx = dir == 0 ? AB[0] : (dir == 1 ? AB[1] : AB[2]);
+                                const double cdx = dir == 0 ? CD[0] : (dir == 1 ? CD[1] : CD[2]);
+                                warp_slice_to_smem<LA, LB, LC, LD>(H + (dir * K::NR + r) * K::SA, g00, rc, dir, abx, cdx);
+                        }
+                        __syncwarp();
+                        for (int t = lane; t < K::NG; t += 32) {
+                                const int o = __ldg(a.goff + t);
+                                const int ox = o & 1023, oy = (o >> 10) & 1023, oz = o >> 20;
+                                double v = 0.0;
+#pragma unroll
+                                for (int r = 0; r < K::NR; r++)
+                                        v += H[r * K::SA + ox] * H[(K::NR + r) * K::SA + oy] * H[(2 * K::NR + r) * K::SA + oz];
+                                G[t] += v;
+                        }
+                }
+        }
+        __syncwarp();
+}
+
+template <int LA, int LB, int LC, int LD>
+__global__ void __launch_bounds__(128) jk_warp_kernel(JKArgs a, int chunk_q)
+{
+        using K = Class4<LA, LB, LC, LD>;
+        using S = WarpSmem<LA, LB, LC, LD>;
+        extern __shared__ double smem_dyn[];
+        const int lane = threadIdx.x & 31;
+        const int wib = threadIdx.x >> 5;
+        double *sm = smem_dyn + (size_t)wib * S::SIZE;
+        const long long total = a.chunk_off[a.bra.n];
+        const long long nwarps = ((long long)gridDim.x * blockDim.x) >> 5;
+        const size_t n = (size_t)a.naoc, nn = n * n;
+        unsigned long long nq = 0, npq = 0;
+        for (long long chunk = ((long long)blockIdx.x * blockDim.x + threadIdx.x) >> 5; chunk < total;
+             chunk += nwarps) {
+                const int ij = find_bra(a.chunk_off, a.bra.n, chunk);
+                const int kl0 = (int)(chunk - a.chunk_off[ij]) * chunk_q;
+                const int kl1 = min(kl0 + chunk_q, a.nkl[ij]);
+                const int4 sb = a.bra.sh[ij];
+                const int2 pb = a.bra.pr[ij];
+                const double qij = a.bra.q[ij];
+                const double4 Ab = a.bra.A[ij];
+                const double4 ABb = a.bra.AB[ij];
+                const double A[3] = {Ab.x, Ab.y, Ab.z}, AB[3] = {ABb.x, ABb.y, ABb.z};
+                const int ia = sb.x, ib = sb.y;
+                for (int kl = kl0; kl < kl1; kl++) {
+                        const int4 sk = a.ket.sh[kl];
+                        if (!quartet_passes(a, sb, qij, sk, a.ket.q[kl])) continue;
+                        const int2 pk = a.ket.pr[kl];
+                        const double4 Ak = a.ket.A[kl];
+                        const double4 CDk = a.ket.AB[kl];
+                        double fac = 1.0;
+                        if (Ab.w != 0.0) fac *= 0.5;
+                        if (Ak.w != 0.0) fac *= 0.5;
+                        if (a.same && ij == kl) fac *= 0.5;
+                        const double C[3] = {Ak.x, Ak.y, Ak.z}, CD[3] = {CDk.x, CDk.y, CDk.z};
+                        warp_eval_block<LA, LB, LC, LD>(sm, a, pb, pk, A, AB, C, CD, fac);
+                        nq++;
+                        npq += (unsigned long long)pb.y * pk.y;
+                        const double *G = sm + S::G;
+                        const int ic = sk.x, id = sk.y;
+                        for (int s = 0; s < a.n_dm; s++) {
+                                if (a.with_j) {
+                                        const double *Ds = a.Ds + s * nn;
+                                        double *J = a.Jacc + s * nn;
+                                        double *dsab = sm + S::DSAB, *dscd = sm + S::DSCD;
+                                        for (int t = lane; t < K::NAB; t += 32) dsab[t] = __ldg(Ds + (ia + t / K::NB) * n + ib + t % K::NB);
+                                        for (int t = lane; t < K::NCD; t += 32) dscd[t] = __ldg(Ds + (ic + t / K::ND) * n + id + t % K::ND);
+                                        __syncwarp();
+                                        for (int t = lane; t < K::NCD; t += 32) {
+                                                double v = 0.0;
+                                                for (int u = 0; u < K::NAB; u++) v += G[u * K::NCD + t] * dsab[u];
+                                                atomicAdd(J + (ic + t / K::ND) * n + id + t % K::ND, v);
+                                        }
+                                        for (int t = lane; t < K::NAB; t += 32) {
+                                                double v = 0.0;
+                                                for (int u = 0; u < K::NCD; u++) v += G[t * K::NCD + u] * dscd[u];
+                                                atomicAdd(J + (ia + t / K::NB) * n + ib + t % K::NB, v);
+                                        }
+                                        __syncwarp();
+                                }
+                                if (a.with_k) {
+                                        for (int tk = 0; tk < a.nk; tk++) {
+                                                const double *X = a.Dk + (s * a.nk + tk) * nn;
+                                                double *Kt = a.Kacc + (s * a.nk + tk) * nn;
+                                                double *xbc = sm + S::XBC, *xbd = sm + S::XBD;
+                                                double *xac = sm + S::XAC, *xad = sm + S::XAD;
+                                                for (int t = lane; t < K::NB * K::NC; t += 32) xbc[t] = __ldg(X + (ib + t / K::NC) * n + ic + t % K::NC);
+                                                for (int t = lane; t < K::NB * K::ND; t += 32) xbd[t] = __ldg(X + (ib + t / K::ND) * n + id + t % K::ND);
+                                                for (int t = lane; t < K::NA * K::NC; t += 32) xac[t] = __ldg(X + (ia + t / K::NC) * n + ic + t % K::NC);
+                                                for (int t = lane; t < K::NA * K::ND; t += 32) xad[t] = __ldg(X + (ia + t / K::ND) * n + id + t % K::ND);
+                                                __syncwarp();
+                                                // K[a,d] += G X[b,c]
+                                                for (int t = lane; t < K::NA * K::ND; t += 32) {
+                                                        const int x = t / K::ND, d = t % K::ND;
+                                                        double v = 0.0;
+                                                        for (int b = 0; b < K::NB; b++)
+                                                                for (int c = 0; c < K::NC; c++)
+                                                                        v += G[((x * K::NB + b) * K::NC + c) * K::ND + d] * xbc[b * K::NC + c];
+                                                        atomicAdd(Kt + (ia + x) * n + id + d, v);
+                                                }
+                                                // K[a,c] += G X[b,d]
+                                                for (int t = lane; t < K::NA * K::NC; t += 32) {
+                                                        const int x = t / K::NC, c = t % K::NC;
+                                                        double v = 0.0;
+                                                        for (int b = 0; b < K::NB; b++)
+                                                                for (int d = 0; d < K::ND; d++)
+                                                                        v += G[((x * K::NB + b) * K::NC + c) * K::ND + d] * xbd[b * K::ND + d];
+                                                        atomicAdd(Kt + (ia + x) * n + ic + c, v);
+                                                }
+                                                // K[b,d] += G X[a,c]
+                                                for (int t = lane; t < K::NB * K::ND; t += 32) {
+                                                        const int b = t / K::ND, d = t % K::ND;
+                                                        double v = 0.0;
+                                                        for (int x = 0; x < K::NA; x++)
+                                                                for (int c = 0; c < K::NC; c++)
+                                                                        v += G[((x * K::NB + b) * K::NC + c) * K::ND + d] * xac[x * K::NC + c];
+                                                        atomicAdd(Kt + (ib + b) * n + id + d, v);
+                                                }
+                                                // K[b,c] += G X[a,d]
+                                                for (int t = lane; t < K::NB * K::NC; t += 32) {
+                                                        const int b = t / K::NC, c = t % K::NC;
+                                                        double v = 0.0;
+                                                        for (int x = 0; x < K::NA; x++)
+                                                                for (int d = 0; d < K::ND; d++)
+                                                                        v += G[((x * K::NB + b) * K::NC + c) * K::ND + d] * xad[x * K::ND + d];
+                                                        atomicAdd(Kt + (ib + b) * n + ic + c, v);
+                                                }
+                                                __syncwarp();
+                                        }
+                                }
+                        }
+                }
+        }
+        if (a.stats && lane == 0 && nq) {
+                atomicAdd(a.stats + 0, nq);
+                atomicAdd(a.stats + 1, npq);
+        }
+}
+
+// ---------------------------------------------------------------------------
+// Schwarz conditioner: one warp per shell pair evaluates (ij|ij), transforms
+// the diagonal to the output basis and folds sqrt(max |(ab|ab)|) into the
+// parent-shell entry (CVHFnr_int2e_q_cond, pyscf/lib/vhf/optimizer.c:408-454).
+struct QArgs {
+        PairView pairs;
+        const double4 *PP;
+        const double2 *PK;
+        const double *table;
+        const int *goff;
+        const double *c2s;           // [l][10][10] transform rows for the output basis
+        unsigned long long *qcond;   // parent nbas x nbas, as bit patterns of positive doubles
+        int nbas, cart;
+};
+
+template <int LA, int LB>
+__global__ void __launch_bounds__(32) qcond_kernel(QArgs q)
+{
+        using K = Class4<LA, LB, LA, LB>;
+        using S = WarpSmem<LA, LB, LA, LB>;
+        extern __shared__ double smem_dyn[];
+        double *sm = smem_dyn;
+        const int lane = threadIdx.x & 31;
+        const int ij = blockIdx.x;
+        if (ij >= q.pairs.n) return;
+        JKArgs a;
+        a.PP = q.PP;
+        a.PK = q.PK;
+        a.table = q.table;
+        a.goff = q.goff;
+        const int4 sh = q.pairs.sh[ij];
+        const int2 pr = q.pairs.pr[ij];
+        const double4 Av = q.pairs.A[ij];
+        const double4 ABv = q.pairs.AB[ij];
+        const double A[3] = {Av.x, Av.y, Av.z}, AB[3] = {ABv.x, ABv.y, ABv.z};
+        warp_eval_block<LA, LB, LA, LB>(sm, a, pr, pr, A, AB, A, AB, 1.0);
+        const double *G = sm + S::G;
+        const int nsa = q.cart ? K::NA : 2 * LA + 1, nsb = q.cart ? K::NB : 2 * LB + 1;
+        const double *ca = q.c2s + LA * 100, *cb = q.c2s + LB * 100;
+        double m = 0.0;
+        for (int t = lane; t < nsa * nsb; t += 32) {
+                const int mi = t / nsb, ni = t % nsb;
+                double v = 0.0;
+                for (int x = 0; x < K::NA; x++) {
+                        const double c1 = ca[mi * 10 + x];
+                        if (c1 == 0.0) continue;
+                        for (int y = 0; y < K::NB; y++) {
+                                const double c2 = cb[ni * 10 + y];
+                                if (c2 == 0.0) continue;
+                                for (int x2 = 0; x2 < K::NA; x2++) {
+                                        const double c3 = ca[mi * 10 + x2];
+                                        if (c3 == 0.0) continue;
+                                        for (int y2 = 0; y2 < K::NB; y2++) {
+                                                const double c4 = cb[ni * 10 + y2];
+                                                if (c4 == 0.0) continue;
+                                                v += c1 * c2 * c3 * c4 * G[((x * K::NB + y) * K::NA + x2) * K::NB + y2];
+                                        }
+                                }
+                        }
+                }
+                m = fmax(m, fabs(v));
+        }
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) m = fmax(m, __shfl_xor_sync(0xffffffffu, m, o));
+        if (lane == 0) {
+                const double qv = sqrt(fmax(m, 1e-100));
+                const unsigned long long bits = (unsigned long long)__double_as_longlong(qv);
+                atomicMax(q.qcond + (size_t)sh.z * q.nbas + sh.w, bits);
+                atomicMax(q.qcond + (size_t)sh.w * q.nbas + sh.z, bits);
+        }
+}
+
+// ---------------------------------------------------------------------------
+// Density conditioner on parent shells (CVHFnr_dm_cond, optimizer.c:494-518)
+// and its global maximum.
+static __global__ void dm_cond_kernel(const double *dms, int n_dm, int nao, const int *ao_loc, int nbas,
+                               double *dm_cond, unsigned long long *dmax_bits)
+{
+        const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+        const long long npair = (long long)nbas * (nbas + 1) / 2;
+        if (t >= npair) return;
+        const int I = (int)((sqrt(8.0 * (double)t + 1.0) - 1.0) * 0.5);
+        int Ii = I;
+        // guard rounding of the triangular inverse
+        while ((long long)Ii * (Ii + 1) / 2 > t) Ii--;
+        while ((long long)(Ii + 1) * (Ii + 2) / 2 <= t) Ii++;
+        const int J = (int)(t - (long long)Ii * (Ii + 1) / 2);
+        const size_t n = nao;
+        double m = 0.0;
+        for (int s = 0; s < n_dm; s++) {
+                const double *D = dms + (size_t)s * n * n;
+                for (int a = ao_loc[Ii]; a < ao_loc[Ii + 1]; a++)
+                        for (int b = ao_loc[J]; b < ao_loc[J + 1]; b++)
+                                m = fmax(m, fabs(D[a * n + b]) + fabs(D[b * n + a]));
+        }
+        m *= 0.5;
+        dm_cond[(size_t)Ii * nbas + J] = m;
+        dm_cond[(size_t)J * nbas + Ii] = m;
+        atomicMax(dmax_bits, (unsigned long long)__double_as_longlong(4.0 * m));
+}
+
+// ---------------------------------------------------------------------------
+// Basis maps.  For output-basis AO mu: segment, component; for Cartesian AO:
+// segment, component.  seg_info[s] = (l, out offset, cart offset, 0).
+static __global__ void out_to_cart_kernel(const double *D, int nao, int naoc, const int *cart_seg,
+                                   const int *cart_comp, const int4 *seg_info, const double *c2s,
+                                   int cart, double *Dc, double *DcT, double *Ds)
+{
+        const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+        if (t >= (long long)naoc * naoc) return;
+        const int c = (int)(t / naoc), d = (int)(t % naoc);
+        const int sc = cart_seg[c], sd = cart_seg[d];
+        const int4 ic = seg_info[sc], id = seg_info[sd];
+        const int xc = cart_comp[c], xd = cart_comp[d];
+        const int nsc = cart ? (ic.x + 1) * (ic.x + 2) / 2 : 2 * ic.x + 1;
+        const int nsd = cart ? (id.x + 1) * (id.x + 2) / 2 : 2 * id.x + 1;
+        const double *cc = c2s + ic.x * 100, *cd = c2s + id.x * 100;
+        double v = 0.0;
+        for (int m = 0; m < nsc; m++) {
+                const double f1 = cc[m * 10 + xc];
+                if (f1 == 0.0) continue;
+                const double *row = D + (size_t)(ic.y + m) * nao + id.y;
+                double s = 0.0;
+                for (int k = 0; k < nsd; k++) s += row[k] * cd[k * 10 + xd];
+                v += f1 * s;
+        }
+        Dc[t] = v;
+        if (DcT) DcT[(size_t)d * naoc + c] = v;
+        (void)Ds;
+}
+
+static __global__ void sym_sum_kernel(const double *X, int n, double *Y)
+{
+        const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+        if (t >= (long long)n * n) return;
+        const int i = (int)(t / n), j = (int)(t % n);
+        Y[t] = X[t] + X[(size_t)j * n + i];
+}
+
+// out[mu,nu] = sum_ab C[mu,a] (A1[a,b] + A2[b,a]) C[nu,b];  hermi == 2 makes
+// the upper triangle the negative of the lower one (lib.hermi_triu).
+static __global__ void cart_to_out_kernel(const double *A1, const double *A2, int nao, int naoc,
+                                   const int *out_seg, const int *out_comp, const int4 *seg_info,
+                                   const double *c2s, int cart, int hermi, double *out)
+{
+        const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+        if (t >= (long long)nao * nao) return;
+        int mu = (int)(t / nao), nu = (int)(t % nao);
+        double sign = 1.0;
+        if (hermi == 2 && mu < nu) { const int tmp = mu; mu = nu; nu = tmp; sign = -1.0; }
+        const int sm = out_seg[mu], sn = out_seg[nu];
+        const int4 im = seg_info[sm], in_ = seg_info[sn];
+        const int km = out_comp[mu], kn = out_comp[nu];
+        const int ncm = (im.x + 1) * (im.x + 2) / 2, ncn = (in_.x + 1) * (in_.x + 2) / 2;
+        const double *cm = c2s + im.x * 100 + km * 10, *cn = c2s + in_.x * 100 + kn * 10;
+        double v = 0.0;
+        for (int x = 0; x < ncm; x++) {
+                const double f1 = cm[x];
+                if (f1 == 0.0) continue;
+                const size_t a = im.z + x;
+                double s = 0.0;
+                for (int y = 0; y < ncn; y++) {
+                        const double f2 = cn[y];
+                        if (f2 == 0.0) continue;
+                        const size_t b = in_.z + y;
+                        s += f2 * (A1[a * naoc + b] + A2[b * naoc + a]);
+                }
+                v += f1 * s;
+        }
+        out[t] = sign * v;
+        (void)cart;
+}
+
+} // namespace b200jk

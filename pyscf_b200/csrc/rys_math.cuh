@@ -1,0 +1,290 @@
+// rys_math.cuh — electron-repulsion integrals by Rys quadrature.
+//
+// Everything here is __host__ __device__ so that the exact code the CUDA
+// kernels run can also be replayed on the host (b200jk_hostcheck_* in
+// b200jk.cu) and compared with the CPU oracle without a GPU.
+//
+// Conventions (shared with PySCF/libcint, pyscf/gto/mole.py:157-187 and
+// pyscf/symm/sph.py:83-103):
+//   Cartesian components of degree l are ordered lx descending, then ly
+//   descending (xx, xy, xz, yy, yz, zz for l = 2).
+//   A primitive Cartesian Gaussian is (x-Ax)^ax (y-Ay)^ay (z-Az)^az e^{-a r_A^2}
+//   with no angular normalisation; the contraction coefficients (already
+//   radially normalised by PySCF) and the real-solid-harmonic transform are
+//   applied outside these routines.
+//
+// Method (Rys, Dupuis & King, J. Comput. Chem. 4, 154 (1983)):
+//   (ab|cd) = 2 pi^{5/2} / (p q sqrt(p+q)) K_ab K_cd
+//             * sum_r w_r I_x(r) I_y(r) I_z(r)
+//   with roots u_r = t_r^2 and weights w_r of the Rys rule of order
+//   n = floor(L/2) + 1, L = la+lb+lc+ld.  Per root and Cartesian direction the
+//   2D integrals obey, with rho = pq/(p+q),
+//     I(e+1,f) = C00 I(e,f) + e B10 I(e-1,f) + f B00 I(e,f-1)
+//     I(e,f+1) = C00' I(e,f) + f B01 I(e,f-1) + e B00 I(e-1,f)
+//     C00 = PA - (q/(p+q)) u PQ,  C00' = QC + (p/(p+q)) u PQ,
+//     B00 = u / (2(p+q)),  B10 = (1 - q u/(p+q)) / (2p),  B01 = (1 - p u/(p+q)) / (2q),
+//   and the transfer to the second centre of each pair is the binomial
+//   expansion (x-B)^b = sum_k C(b,k) (x-A)^k (A-B)^{b-k}.
+#pragma once
+#include <math.h>
+
+#ifdef __CUDACC__
+#define B2_HD __host__ __device__ __forceinline__
+#define B2_HDC __host__ __device__ constexpr
+#else
+#define B2_HD inline
+#define B2_HDC constexpr
+#endif
+
+#if defined(__CUDA_ARCH__)
+#define B2_LDG(p) __ldg(p)
+#else
+#define B2_LDG(p) (*(p))
+#endif
+
+#include "rys_table.inc"
+
+namespace b200jk {
+
+B2_HDC int ncart(int l) { return (l + 1) * (l + 2) / 2; }
+B2_HDC int nsph(int l) { return 2 * l + 1; }
+
+// Cartesian component n of degree l
+B2_HDC int cart_lx(int l, int n)
+{
+        int lx = l;
+        while (n > l - lx) { n -= l - lx + 1; lx--; }
+        return lx;
+}
+B2_HDC int cart_ly(int l, int n)
+{
+        int lx = l;
+        while (n > l - lx) { n -= l - lx + 1; lx--; }
+        return l - lx - n;
+}
+B2_HDC int cart_lz(int l, int n) { return l - cart_lx(l, n) - cart_ly(l, n); }
+
+B2_HDC int binom(int n, int k)
+{
+        int r = 1;
+        for (int i = 1; i <= k; i++) r = r * (n - k + i) / i;
+        return r;
+}
+
+B2_HDC int rys_nroots(int L) { return L / 2 + 1; }
+
+B2_HDC int rys_t_asym(int n)
+{
+        constexpr int t[] = {RYS_T_ASYM_LIST};
+        return t[n];
+}
+B2_HDC int rys_table_offset(int n)
+{
+        constexpr int t[] = {RYS_TABLE_OFFSET_LIST};
+        return t[n];
+}
+B2_HDC double rys_herm_x2(int k)
+{
+        constexpr double t[] = {RYS_HERMITE_X2_LIST};
+        return t[k];
+}
+B2_HDC double rys_herm_w(int k)
+{
+        constexpr double t[] = {RYS_HERMITE_W_LIST};
+        return t[k];
+}
+
+// Roots u[i] and weights w[i] of the order-NR Rys rule at argument T.
+// NaN or huge T take the asymptotic branch, so the table is never indexed
+// out of range.
+template <int NR>
+B2_HD void rys_roots(double T, const double *__restrict__ table, double *u, double *w)
+{
+        if (!(T < (double)rys_t_asym(NR))) {
+                const double it = 1.0 / T;
+                const double st = sqrt(it);
+#pragma unroll
+                for (int i = 0; i < NR; i++) {
+                        u[i] = rys_herm_x2(NR * (NR - 1) / 2 + i) * it;
+                        w[i] = rys_herm_w(NR * (NR - 1) / 2 + i) * st;
+                }
+                return;
+        }
+        const int p = (int)T;
+        const double x = 2.0 * (T - (double)p) - 1.0;
+        const double *c = table + rys_table_offset(NR) + p * (2 * NR * (RYS_DEG + 1));
+#pragma unroll
+        for (int f = 0; f < 2 * NR; f++) {
+                const double *cf = c + f * (RYS_DEG + 1);
+                double r = B2_LDG(cf + RYS_DEG);
+#pragma unroll
+                for (int k = RYS_DEG - 1; k >= 0; k--) r = fma(r, x, B2_LDG(cf + k));
+                if (f < NR) u[f] = r;
+                else w[f - NR] = r;
+        }
+}
+
+// 2D vertical recurrence: g[e*NF + f], e < NE, f < NF.
+template <int NE, int NF>
+B2_HD void vrr2d(double *g, double g00, double c00, double c00p, double b10, double b01, double b00)
+{
+        g[0] = g00;
+        if (NE > 1) g[NF] = c00 * g00;
+#pragma unroll
+        for (int e = 1; e < NE - 1; e++) g[(e + 1) * NF] = c00 * g[e * NF] + (double)e * b10 * g[(e - 1) * NF];
+        if (NF > 1) {
+#pragma unroll
+                for (int e = 0; e < NE; e++) {
+                        double v = c00p * g[e * NF];
+                        if (e > 0) v += (double)e * b00 * g[(e - 1) * NF];
+                        g[e * NF + 1] = v;
+                }
+#pragma unroll
+                for (int f = 1; f < NF - 1; f++) {
+#pragma unroll
+                        for (int e = 0; e < NE; e++) {
+                                double v = c00p * g[e * NF + f] + (double)f * b01 * g[e * NF + f - 1];
+                                if (e > 0) v += (double)e * b00 * g[(e - 1) * NF + f];
+                                g[e * NF + f + 1] = v;
+                        }
+                }
+        }
+}
+
+// 2D horizontal transfer: from g[e][f] (e <= LA+LB, f <= LC+LD) to
+// h[((a*(LB+1) + b)*(LC+1) + c)*(LD+1) + d].
+template <int LA, int LB, int LC, int LD>
+B2_HD void hrr2d(const double *g, double *h, double ab, double cd)
+{
+        constexpr int NF = LC + LD + 1;
+        double abp[LB + 1], cdp[LD + 1];
+        abp[0] = 1.0;
+#pragma unroll
+        for (int k = 1; k <= LB; k++) abp[k] = abp[k - 1] * ab;
+        cdp[0] = 1.0;
+#pragma unroll
+        for (int k = 1; k <= LD; k++) cdp[k] = cdp[k - 1] * cd;
+        // t[(a*(LB+1)+b)*NF + f]
+        double t[(LA + 1) * (LB + 1) * NF];
+#pragma unroll
+        for (int a = 0; a <= LA; a++) {
+#pragma unroll
+                for (int b = 0; b <= LB; b++) {
+#pragma unroll
+                        for (int f = 0; f < NF; f++) {
+                                double v = 0.0;
+#pragma unroll
+                                for (int k = 0; k <= b; k++)
+                                        v += (double)binom(b, k) * abp[b - k] * g[(a + k) * NF + f];
+                                t[(a * (LB + 1) + b) * NF + f] = v;
+                        }
+                }
+        }
+#pragma unroll
+        for (int ab_ = 0; ab_ < (LA + 1) * (LB + 1); ab_++) {
+#pragma unroll
+                for (int c = 0; c <= LC; c++) {
+#pragma unroll
+                        for (int d = 0; d <= LD; d++) {
+                                double v = 0.0;
+#pragma unroll
+                                for (int k = 0; k <= d; k++)
+                                        v += (double)binom(d, k) * cdp[d - k] * t[ab_ * NF + c + k];
+                                h[(ab_ * (LC + 1) + c) * (LD + 1) + d] = v;
+                        }
+                }
+        }
+}
+
+template <int LA, int LB, int LC, int LD>
+struct Class4 {
+        static constexpr int NR = rys_nroots(LA + LB + LC + LD);
+        static constexpr int NA = ncart(LA), NB = ncart(LB), NC = ncart(LC), ND = ncart(LD);
+        static constexpr int NAB = NA * NB, NCD = NC * ND, NG = NAB * NCD;
+        static constexpr int NE = LA + LB + 1, NF = LC + LD + 1;
+        static constexpr int SA = (LA + 1) * (LB + 1) * (LC + 1) * (LD + 1);
+        B2_HD static constexpr int hidx(int a, int b, int c, int d)
+        {
+                return ((a * (LB + 1) + b) * (LC + 1) + c) * (LD + 1) + d;
+        }
+};
+
+// Root-dependent recurrence coefficients of one primitive quartet.
+struct RysCoef {
+        double c00[3], c00p[3], b10, b01, b00;
+};
+
+B2_HD void rys_coef(RysCoef &rc, double u, double p, double q, const double PA[3],
+                    const double QC[3], const double PQ[3])
+{
+        const double ipq = 1.0 / (p + q);
+        const double qf = q * ipq * u, pf = p * ipq * u;
+        rc.b00 = 0.5 * u * ipq;
+        rc.b10 = 0.5 / p * (1.0 - qf);
+        rc.b01 = 0.5 / q * (1.0 - pf);
+#pragma unroll
+        for (int x = 0; x < 3; x++) {
+                rc.c00[x] = PA[x] - qf * PQ[x];
+                rc.c00p[x] = QC[x] + pf * PQ[x];
+        }
+}
+
+// Add one primitive quartet to the Cartesian block G[((a*NB+b)*NC+c)*ND+d].
+// pref = 2 pi^{5/2}/(pq sqrt(p+q)) K_ab K_cd (coefficients included).
+template <int LA, int LB, int LC, int LD>
+B2_HD void add_prim_quartet(double *G, const double *table, double p, const double P[3],
+                            double q, const double Q[3], const double A[3], const double C[3],
+                            const double AB[3], const double CD[3], double pref)
+{
+        using K = Class4<LA, LB, LC, LD>;
+        double PA[3], QC[3], PQ[3];
+#pragma unroll
+        for (int x = 0; x < 3; x++) {
+                PA[x] = P[x] - A[x];
+                QC[x] = Q[x] - C[x];
+                PQ[x] = P[x] - Q[x];
+        }
+        const double rho = p * q / (p + q);
+        const double T = rho * (PQ[0] * PQ[0] + PQ[1] * PQ[1] + PQ[2] * PQ[2]);
+        double u[K::NR], w[K::NR];
+        rys_roots<K::NR>(T, table, u, w);
+#pragma unroll
+        for (int r = 0; r < K::NR; r++) {
+                RysCoef rc;
+                rys_coef(rc, u[r], p, q, PA, QC, PQ);
+                double g[K::NE * K::NF];
+                double hx[K::SA], hy[K::SA], hz[K::SA];
+                vrr2d<K::NE, K::NF>(g, 1.0, rc.c00[0], rc.c00p[0], rc.b10, rc.b01, rc.b00);
+                hrr2d<LA, LB, LC, LD>(g, hx, AB[0], CD[0]);
+                vrr2d<K::NE, K::NF>(g, 1.0, rc.c00[1], rc.c00p[1], rc.b10, rc.b01, rc.b00);
+                hrr2d<LA, LB, LC, LD>(g, hy, AB[1], CD[1]);
+                vrr2d<K::NE, K::NF>(g, pref * w[r], rc.c00[2], rc.c00p[2], rc.b10, rc.b01, rc.b00);
+                hrr2d<LA, LB, LC, LD>(g, hz, AB[2], CD[2]);
+#pragma unroll
+                for (int ia = 0; ia < K::NA; ia++)
+#pragma unroll
+                for (int ib = 0; ib < K::NB; ib++)
+#pragma unroll
+                for (int ic = 0; ic < K::NC; ic++)
+#pragma unroll
+                for (int id = 0; id < K::ND; id++) {
+                        const int ox = K::hidx(cart_lx(LA, ia), cart_lx(LB, ib), cart_lx(LC, ic), cart_lx(LD, id));
+                        const int oy = K::hidx(cart_ly(LA, ia), cart_ly(LB, ib), cart_ly(LC, ic), cart_ly(LD, id));
+                        const int oz = K::hidx(cart_lz(LA, ia), cart_lz(LB, ib), cart_lz(LC, ic), cart_lz(LD, id));
+                        G[((ia * K::NB + ib) * K::NC + ic) * K::ND + id] += hx[ox] * hy[oy] * hz[oz];
+                }
+        }
+}
+
+// One (root, direction) slice of the 2D integrals after the transfer,
+// written to h (used by the warp-cooperative kernels).
+template <int LA, int LB, int LC, int LD>
+B2_HD void rys_2d_slice(double *h, double g00, const RysCoef &rc, int dir, double ab, double cd)
+{
+        using K = Class4<LA, LB, LC, LD>;
+        double g[K::NE * K::NF];
+        vrr2d<K::NE, K::NF>(g, g00, rc.c00[dir], rc.c00p[dir], rc.b10, rc.b01, rc.b00);
+        hrr2d<LA, LB, LC, LD>(g, h, ab, cd);
+}
+
+} // namespace b200jk

@@ -1,0 +1,190 @@
+"""ctypes binding of libb200jk.so (C ABI declared in include/b200jk.h).
+
+The library is built in-tree by ``pyscf_b200.build``.  Loading fails loudly:
+there is no CPU fallback for the J/K engine.
+"""
+import ctypes
+import os
+import threading
+
+import numpy
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, 'libb200jk.so')
+
+B200JK_OK = 0
+B200JK_EINVAL = 1
+B200JK_EUNSUPPORTED = 2
+B200JK_ECUDA = 3
+B200JK_ENOMEM = 4
+PREC_FP64 = 0
+
+# every entry point of include/b200jk.h
+EXPORTS = (
+    'b200jk_version', 'b200jk_last_error', 'b200jk_device_count', 'b200jk_plan_create',
+    'b200jk_plan_destroy', 'b200jk_plan_dims', 'b200jk_get_q_cond', 'b200jk_get_jk',
+    'b200jk_stats', 'b200jk_hostcheck_cart_quartet',
+)
+
+
+class B200JKError(RuntimeError):
+    def __init__(self, code, msg):
+        RuntimeError.__init__(self, 'b200jk error %d: %s' % (code, msg))
+        self.code = code
+
+
+class Stats(ctypes.Structure):
+    _fields_ = [('quartets', ctypes.c_int64), ('prim_quartets', ctypes.c_int64),
+                ('shell_pairs', ctypes.c_int64), ('prim_pairs', ctypes.c_int64),
+                ('flops', ctypes.c_double), ('last_build_ms', ctypes.c_double),
+                ('nao', ctypes.c_int32), ('nao_cart', ctypes.c_int32),
+                ('nbas', ctypes.c_int32), ('nseg', ctypes.c_int32)]
+
+
+_lib = None
+_lock = threading.Lock()
+
+
+def load(path=LIB_PATH):
+    """Load (once) and return the library handle with typed entry points."""
+    global _lib
+    with _lock:
+        if _lib is not None:
+            return _lib
+        if not os.path.exists(path):
+            raise B200JKError(5, 'libb200jk.so is not built (run python -m pyscf_b200.build): %s' % path)
+        lib = ctypes.CDLL(path)
+        vp, ip, dp = ctypes.c_void_p, ctypes.c_int, ctypes.c_double
+        lib.b200jk_version.restype = ip
+        lib.b200jk_last_error.restype = ctypes.c_char_p
+        lib.b200jk_device_count.argtypes = [ctypes.POINTER(ip)]
+        lib.b200jk_plan_create.argtypes = [vp, ip, vp, ip, vp, ip, ip, dp, ip, ctypes.POINTER(vp)]
+        lib.b200jk_plan_destroy.argtypes = [vp]
+        lib.b200jk_plan_dims.argtypes = [vp, ctypes.POINTER(ip), ctypes.POINTER(ip)]
+        lib.b200jk_get_q_cond.argtypes = [vp, vp]
+        lib.b200jk_get_jk.argtypes = [vp, vp, ip, ip, ip, ip, vp, vp, ip, ip, vp]
+        lib.b200jk_stats.argtypes = [vp, ctypes.POINTER(Stats)]
+        lib.b200jk_hostcheck_cart_quartet.argtypes = [vp, ip, vp, ip, vp, vp, vp]
+        _lib = lib
+        return lib
+
+
+def check(code):
+    if code != B200JK_OK:
+        msg = load().b200jk_last_error()
+        raise B200JKError(code, msg.decode() if msg else '')
+
+
+def device_count():
+    n = ctypes.c_int(0)
+    check(load().b200jk_device_count(ctypes.byref(n)))
+    return n.value
+
+
+def _ptr(a):
+    return a.ctypes.data_as(ctypes.c_void_p)
+
+
+class Plan:
+    """One molecule/basis on one GPU: shell pairs, primitive pairs and q_cond.
+
+    Mirrors what PySCF keeps in a _VHFOpt (pyscf/scf/_vhf.py:151-264)."""
+
+    def __init__(self, atm, bas, env, cart=False, direct_scf_tol=1e-13, device=0):
+        lib = load()
+        self.atm = numpy.asarray(atm, dtype=numpy.int32, order='C')
+        self.bas = numpy.asarray(bas, dtype=numpy.int32, order='C')
+        self.env = numpy.asarray(env, dtype=numpy.double, order='C')
+        self.cart = bool(cart)
+        self.direct_scf_tol = float(direct_scf_tol)
+        self.device = int(device)
+        h = ctypes.c_void_p()
+        check(lib.b200jk_plan_create(_ptr(self.atm), self.atm.shape[0], _ptr(self.bas), self.bas.shape[0],
+                                     _ptr(self.env), self.env.size, int(self.cart), self.direct_scf_tol,
+                                     self.device, ctypes.byref(h)))
+        self._h = h
+        nao, nbas = ctypes.c_int(), ctypes.c_int()
+        check(lib.b200jk_plan_dims(h, ctypes.byref(nao), ctypes.byref(nbas)))
+        self.nao, self.nbas = nao.value, nbas.value
+
+    def close(self):
+        if getattr(self, '_h', None):
+            load().b200jk_plan_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    @property
+    def q_cond(self):
+        q = numpy.empty((self.nbas, self.nbas))
+        check(load().b200jk_get_q_cond(self._h, _ptr(q)))
+        return q
+
+    def stats(self):
+        s = Stats()
+        check(load().b200jk_stats(self._h, ctypes.byref(s)))
+        return {k: getattr(s, k) for k, _ in Stats._fields_}
+
+    def get_jk(self, dms, hermi=1, with_j=True, with_k=True, out_j=None, out_k=None,
+               precision=PREC_FP64, stream=None):
+        """J/K of host densities (n_dm, nao, nao) -> host arrays."""
+        dms = numpy.asarray(dms, dtype=numpy.double, order='C')
+        shape = dms.shape
+        nao = shape[-1]
+        if nao != self.nao or shape[-2] != nao:
+            raise ValueError('density shape %s does not match nao=%d' % (shape, self.nao))
+        dms = dms.reshape(-1, nao, nao)
+        n_dm = dms.shape[0]
+        vj = vk = None
+        if with_j:
+            vj = out_j if out_j is not None else numpy.empty((n_dm, nao, nao))
+        if with_k:
+            vk = out_k if out_k is not None else numpy.empty((n_dm, nao, nao))
+        check(load().b200jk_get_jk(self._h, _ptr(dms), n_dm, int(hermi), int(bool(with_j)), int(bool(with_k)),
+                                   _ptr(vj) if with_j else None, _ptr(vk) if with_k else None,
+                                   0, int(precision), stream))
+        if with_j:
+            vj = vj.reshape(shape)
+        if with_k:
+            vk = vk.reshape(shape)
+        return vj, vk
+
+    def get_jk_device(self, dms, hermi=1, with_j=True, with_k=True, precision=PREC_FP64):
+        """J/K of CUDA torch tensors on the plan's device -> CUDA tensors."""
+        import torch
+        if not (isinstance(dms, torch.Tensor) and dms.is_cuda and dms.dtype == torch.float64):
+            raise TypeError('dms must be a float64 CUDA tensor')
+        if dms.device.index != self.device:
+            raise ValueError('dms is on cuda:%s, plan is on cuda:%d' % (dms.device.index, self.device))
+        shape = dms.shape
+        nao = shape[-1]
+        d = dms.reshape(-1, nao, nao).contiguous()
+        n_dm = d.shape[0]
+        vj = torch.empty_like(d) if with_j else None
+        vk = torch.empty_like(d) if with_k else None
+        stream = torch.cuda.current_stream(d.device).cuda_stream
+        check(load().b200jk_get_jk(self._h, ctypes.c_void_p(d.data_ptr()), n_dm, int(hermi),
+                                   int(bool(with_j)), int(bool(with_k)),
+                                   ctypes.c_void_p(vj.data_ptr()) if with_j else None,
+                                   ctypes.c_void_p(vk.data_ptr()) if with_k else None,
+                                   1, int(precision), ctypes.c_void_p(stream)))
+        return (vj.reshape(shape) if with_j else None), (vk.reshape(shape) if with_k else None)
+
+
+def hostcheck_cart_quartet(atm, bas, env, shls):
+    """Host replay of the kernels' integral arithmetic for one quartet of
+    segmented shells; returns the Cartesian block [a][b][c][d]."""
+    lib = load()
+    atm = numpy.asarray(atm, dtype=numpy.int32, order='C')
+    bas = numpy.asarray(bas, dtype=numpy.int32, order='C')
+    env = numpy.asarray(env, dtype=numpy.double, order='C')
+    shls = numpy.asarray(shls, dtype=numpy.int32)
+    nc = [(int(bas[s, 1]) + 1) * (int(bas[s, 1]) + 2) // 2 for s in shls]
+    out = numpy.zeros(nc)
+    check(lib.b200jk_hostcheck_cart_quartet(_ptr(atm), atm.shape[0], _ptr(bas), bas.shape[0],
+                                            _ptr(env), _ptr(shls), _ptr(out)))
+    return out

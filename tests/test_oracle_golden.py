@@ -1,0 +1,76 @@
+"""Pin the CPU oracle against the reference's own golden values.
+
+The oracle is this project's restatement of libcint's integrals and of
+CVHFnr_direct_drv (oracle/).  The fixtures hold J/K produced by the
+reference's own C drivers (pyscf/lib/vhf/nr_direct.c and friends, compiled
+from the reference sources) running on the oracle integral library, and the
+reference tests' published fingerprints are checked here too."""
+import numpy
+import pytest
+
+from conftest import load_fixture, lib_fp
+import oracle
+
+
+def test_h2o_vdz_identity_density_fingerprints():
+    # pyscf/scf/test/test_rhf.py:909-916: dm = I, fp(vj), fp(vk)
+    f = load_fixture('h2o_vdz')
+    nao = int(f['nao'])
+    vj, vk, _ = oracle.get_jk(numpy.eye(nao), f['atm'], f['bas'], f['env'], hermi=1)
+    assert abs(lib_fp(vj) - 1.6593323222866125) < 1e-9
+    assert abs(lib_fp(vk) - -1.4662135224053987) < 1e-9
+
+
+def test_h2o_vdz_random_density_norm_and_k():
+    # pyscf/scf/test/test_rhf.py:890-901 (|vj| = 77.035779188661465) and
+    # :918-928 (fp(vk, hermi=0) = -12.365527167710301), numpy.random.seed(1)
+    f = load_fixture('h2o_vdz')
+    nao = int(f['nao'])
+    numpy.random.seed(1)
+    dm = numpy.random.random((nao, nao))
+    vj, _, _ = oracle.get_jk(dm, f['atm'], f['bas'], f['env'], hermi=1)
+    assert abs(numpy.linalg.norm(vj) - 77.035779188661465) < 1e-9
+    _, vk, _ = oracle.get_jk(dm, f['atm'], f['bas'], f['env'], hermi=0)
+    assert abs(lib_fp(vk) - -12.365527167710301) < 1e-11
+
+
+def test_h2o_631g_direct_fingerprints():
+    # pyscf/scf/test/test_vhf.py:158-174: dm = r + r^T, numpy.random.seed(1),
+    # K by 'jk->s1il' (=(ij|kl) D_jk) and J by 'ji->s1kl', unscreened
+    f = load_fixture('h2o_631g')
+    nao = int(f['nao'])
+    numpy.random.seed(1)
+    dm = numpy.random.random((nao, nao))
+    dm = dm + dm.T
+    vj, vk, _ = oracle.get_jk(dm, f['atm'], f['bas'], f['env'], hermi=1, screen=False)
+    assert abs(lib_fp(vk) - 5.0067176755619975) < 1e-11
+    assert abs(lib_fp(vj) - 48.61070262547175) < 1e-11
+
+
+@pytest.mark.parametrize('name', ['h2o_631g', 'h2o_vdz', 'h2o2_vtz'])
+def test_restated_driver_matches_reference_drivers(name):
+    f = load_fixture(name)
+    vj, vk, nq = oracle.get_jk(f['dm_rand'], f['atm'], f['bas'], f['env'], hermi=1)
+    assert nq > 0
+    assert abs(vj - f['vj_rand']).max() < 1e-11
+    assert abs(vk - f['vk_rand']).max() < 1e-11
+    vj, vk, _ = oracle.get_jk(f['dm_ns'], f['atm'], f['bas'], f['env'], hermi=0)
+    assert abs(vj - f['vj_ns']).max() < 1e-11
+    assert abs(vk - f['vk_ns']).max() < 1e-11
+    vj, vk, _ = oracle.get_jk(f['dm_rand'], f['atm'], f['bas'], f['env'], hermi=1, screen=False)
+    assert abs(vj - f['vj_rand_noscreen']).max() < 1e-11
+    assert abs(vk - f['vk_rand_noscreen']).max() < 1e-11
+
+
+@pytest.mark.parametrize('name', ['h2o_631g', 'h2o_vdz', 'h2o2_vtz'])
+def test_q_cond_matches_reference(name):
+    f = load_fixture(name)
+    q = oracle.q_cond(f['atm'], f['bas'], f['env'])
+    assert abs(q - f['q_cond']).max() < 1e-13
+
+
+def test_reference_energies_in_fixture():
+    # pyscf/scf/test/test_h2o_vdz.py:45 and :98 (9 decimals)
+    f = load_fixture('h2o_vdz')
+    assert abs(float(f['e_rhf']) - -76.026765673120565) < 1e-9
+    assert abs(float(f['e_rhf']) - -76.026765673119627) < 1e-9
