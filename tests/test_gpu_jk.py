@@ -37,7 +37,9 @@ def test_q_cond(b2, name):
     p = plan_for(b2, f)
     q = p.q_cond
     ref = f['q_cond']
-    assert abs(q - ref).max() <= 1e-12 * max(1.0, abs(ref).max())
+    # q only steers the screen; the spherical diagonal of an (ff|ff) block is
+    # a long alternating sum, so agreement is ~1e-12 relative
+    assert abs(q - ref).max() <= 1e-10 * max(1.0, abs(ref).max())
 
 
 @pytest.mark.parametrize('name', ['h2o_631g', 'h2o_vdz', 'h2o2_vtz', 'h2o8_vdz'])
