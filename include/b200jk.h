@@ -59,7 +59,17 @@ typedef struct {
     double  flops;               /* modelled FP64 flops of the last build */
     double  last_build_ms;       /* device time of the last J/K build */
     int32_t nao, nao_cart, nbas, nseg;
+    int64_t kernel_launches;     /* kernels this library launched in the last build */
 } b200jk_stats_t;
+
+typedef struct {
+    int32_t la, lb, lc, ld;      /* quartet class (la lb | lc ld) */
+    int64_t quartets;            /* shell quartets evaluated in the last build */
+    int64_t prim_quartets;       /* primitive quartets evaluated in the last build */
+    double  ms;                  /* kernel time of the class (profiling on), else 0 */
+    int32_t family;              /* 0 thread-per-quartet, 1 warp-per-quartet */
+    int32_t pad;
+} b200jk_class_stat_t;
 
 /* Library version, (major << 16) | minor. */
 int b200jk_version(void);
@@ -96,6 +106,17 @@ int b200jk_get_jk(b200jk_plan *plan, const double *dms, int n_dm, int hermi,
 
 /* Counters of the last build. */
 int b200jk_stats(const b200jk_plan *plan, b200jk_stats_t *stats);
+
+/* Per-quartet-class counters of the last build; *n receives the number of
+ * classes (at most max are written).  With profiling on (b200jk_set_profiling)
+ * each class kernel is bracketed by CUDA events and ms is filled in. */
+int b200jk_class_stats(const b200jk_plan *plan, b200jk_class_stat_t *out, int max, int *n);
+int b200jk_set_profiling(b200jk_plan *plan, int on);
+
+/* Measured FP64 FMA throughput of device `device` (TFLOP/s), from a
+ * register-resident FMA loop over all SMs: the denominator of the FP64
+ * roofline fraction. */
+int b200jk_measure_fp64_peak(int device, double *tflops);
 
 /* Host replay of the device integral code for one shell quartet (no GPU is
  * used): the Cartesian block (ab|cd) of shells shls[0..3] of the given

@@ -177,7 +177,9 @@ def build_ref(force=False):
         out = os.path.join(OUT_LIBDIR, 'lib%s.so' % grp)
         cmd = ['gcc', '-shared', '-fopenmp', '-o', out] + objs[grp]
         cmd += ['-L', OUT_LIBDIR] + ['-l' + d for d in DEPS[grp]]
-        cmd += [blas, '-lm', '-Wl,-rpath,$ORIGIN', '-Wl,-rpath,' + blasdir]
+        # DT_RPATH (not RUNPATH) so that the BLAS's own dependency
+        # (libgfortran next to it) resolves through this search path too
+        cmd += [blas, '-lm', '-Wl,--disable-new-dtags', '-Wl,-rpath,$ORIGIN', '-Wl,-rpath,' + blasdir]
         _run(cmd)
     # Libraries of subsystems outside the J/K path (post-HF, DFT, PBC, ...)
     # are loaded at import time by modules that `pyscf.grad` pulls in.  Empty

@@ -203,6 +203,9 @@ struct b200jk_plan {
         int nsm = 148;
         int64_t shell_pairs = 0, prim_pairs = 0;
         b200jk_stats_t st;
+        int profiling = 0;
+        std::vector<b200jk_class_stat_t> cls;
+        std::vector<cudaEvent_t> cls_ev;
         ~b200jk_plan()
         {
                 for (auto &c : pc) c.release();
@@ -211,6 +214,7 @@ struct b200jk_plan {
                 cart_seg.release(); cart_comp.release(); ao_loc_d.release();
                 D.release(); Dc.release(); Ds.release(); Jacc.release(); Kacc.release(); outJ.release(); outK.release();
                 dmax.release(); stats.release(); nkl.release(); nchunk.release(); chunk_off.release(); cub_tmp.release();
+                for (auto e : cls_ev) cudaEventDestroy(e);
                 if (ev0) cudaEventDestroy(ev0);
                 if (ev1) cudaEventDestroy(ev1);
                 if (stream) cudaStreamDestroy(stream);
@@ -336,6 +340,20 @@ static int ensure_tables(int device)
         });
         if (g_table_status[device]) return fail(B200JK_ECUDA, "could not upload the Rys tables");
         return B200JK_OK;
+}
+
+// eight independent FMA chains per thread; the result is stored so the
+// chains cannot be removed
+__global__ void fp64_fma_kernel(double *sink, int iters, double m)
+{
+        double a0 = threadIdx.x * 1e-9, a1 = a0 + 1e-9, a2 = a0 + 2e-9, a3 = a0 + 3e-9;
+        double a4 = a0 + 4e-9, a5 = a0 + 5e-9, a6 = a0 + 6e-9, a7 = a0 + 7e-9;
+        const double c = 1e-12;
+        for (int i = 0; i < iters; i++) {
+                a0 = fma(a0, m, c); a1 = fma(a1, m, c); a2 = fma(a2, m, c); a3 = fma(a3, m, c);
+                a4 = fma(a4, m, c); a5 = fma(a5, m, c); a6 = fma(a6, m, c); a7 = fma(a7, m, c);
+        }
+        sink[(size_t)blockIdx.x * blockDim.x + threadIdx.x] = a0 + a1 + a2 + a3 + a4 + a5 + a6 + a7;
 }
 
 static const double *table_ptr()
@@ -619,7 +637,7 @@ static int ensure_workspace(b200jk_plan *P, int n_dm)
             (rc = dev_alloc(P->Ds, nc * n_dm)) || (rc = dev_alloc(P->Jacc, nc * n_dm)) ||
             (rc = dev_alloc(P->Kacc, nc * n_dm * 2)) || (rc = dev_alloc(P->outJ, nn * n_dm)) ||
             (rc = dev_alloc(P->outK, nn * n_dm)) || (rc = dev_alloc(P->dm_cond, (size_t)P->nbas * P->nbas)) ||
-            (rc = dev_alloc(P->dmax, 1)) || (rc = dev_alloc(P->stats, 2)))
+            (rc = dev_alloc(P->dmax, 1)) || (rc = dev_alloc(P->stats, 2 * 64)))
                 return rc;
         int maxn = 1;
         for (auto &c : P->pc) maxn = std::max(maxn, c.n);
@@ -658,7 +676,7 @@ int b200jk_get_jk(b200jk_plan *P, const double *dms, int n_dm, int hermi, int wi
         }
         // screening data
         CUDA_TRY(cudaMemsetAsync(P->dmax.p, 0, sizeof(unsigned long long), s));
-        CUDA_TRY(cudaMemsetAsync(P->stats.p, 0, 2 * sizeof(unsigned long long), s));
+        CUDA_TRY(cudaMemsetAsync(P->stats.p, 0, 2 * 64 * sizeof(unsigned long long), s));
         {
                 const long long npair = (long long)P->nbas * (P->nbas + 1) / 2;
                 dm_cond_kernel<<<grid_for(npair, 256), 256, 0, s>>>(dD, n_dm, P->nao, P->ao_loc_d.p, P->nbas,
@@ -680,6 +698,22 @@ int b200jk_get_jk(b200jk_plan *P, const double *dms, int n_dm, int hermi, int wi
 
         const double *tbl = table_ptr();
         auto qcs = quartet_classes();
+        int64_t launches = 1 + 2 * n_dm;   // dm_cond, to-Cartesian + symmetrise per density
+        if (P->cls.size() != qcs.size()) {
+                P->cls.assign(qcs.size(), b200jk_class_stat_t());
+                for (size_t t = 0; t < qcs.size(); t++) {
+                        int la, lb, lc, ld;
+                        class_l(qcs[t].X, la, lb);
+                        class_l(qcs[t].Y, lc, ld);
+                        P->cls[t].la = la; P->cls[t].lb = lb; P->cls[t].lc = lc; P->cls[t].ld = ld;
+                        P->cls[t].family = family_is_thread(la, lb, lc, ld) ? 0 : 1;
+                }
+        }
+        if (P->profiling && P->cls_ev.empty()) {
+                P->cls_ev.resize(2 * qcs.size());
+                for (auto &e : P->cls_ev) CUDA_TRY(cudaEventCreate(&e));
+        }
+        std::vector<char> ran(qcs.size(), 0);
         {
                 for (size_t t = 0; t < qcs.size(); t++) {
                         const PairClassDev &bra = P->pc[qcs[t].X], &ket = P->pc[qcs[t].Y];
@@ -707,11 +741,15 @@ int b200jk_get_jk(b200jk_plan *P, const double *dms, int n_dm, int hermi, int wi
                         a.goff = P->goff_all.p + P->goff_at[t];
                         a.Jacc = P->Jacc.p; a.Kacc = P->Kacc.p;
                         a.Ds = P->Ds.p; a.Dk = P->Dc.p;
-                        a.stats = P->stats.p;
+                        a.stats = P->stats.p + 2 * t;
                         a.tol = P->tol > 0 ? P->tol : -1.0;
                         a.nbas = P->nbas; a.naoc = P->naoc; a.n_dm = n_dm; a.nk = nk;
                         a.with_j = with_j; a.with_k = with_k; a.same = same;
+                        if (P->profiling) CUDA_TRY(cudaEventRecord(P->cls_ev[2 * t], s));
                         if ((rc = dispatch_jk(P, la, lb, lc, ld, a, s))) return rc;
+                        if (P->profiling) CUDA_TRY(cudaEventRecord(P->cls_ev[2 * t + 1], s));
+                        ran[t] = 1;
+                        launches += 2;   // count + class kernel (the scan is a CUB library kernel)
                 }
         }
         // back to the output basis
@@ -734,19 +772,77 @@ int b200jk_get_jk(b200jk_plan *P, const double *dms, int n_dm, int hermi, int wi
                         CUDA_TRY(cudaGetLastError());
                 }
         }
+        launches += (with_j ? n_dm : 0) + (with_k ? n_dm : 0);
         CUDA_TRY(cudaEventRecord(P->ev1, s));
         if (!dev_ptrs) {
                 if (with_j) CUDA_TRY(cudaMemcpyAsync(vj, P->outJ.p, sizeof(double) * nn * n_dm, cudaMemcpyDeviceToHost, s));
                 if (with_k) CUDA_TRY(cudaMemcpyAsync(vk, P->outK.p, sizeof(double) * nn * n_dm, cudaMemcpyDeviceToHost, s));
         }
-        unsigned long long hs[2] = {0, 0};
+        unsigned long long hs[2 * 64];
         CUDA_TRY(cudaMemcpyAsync(hs, P->stats.p, sizeof(hs), cudaMemcpyDeviceToHost, s));
         CUDA_TRY(cudaStreamSynchronize(s));
         float ms = 0;
         CUDA_TRY(cudaEventElapsedTime(&ms, P->ev0, P->ev1));
-        P->st.quartets = (int64_t)hs[0];
-        P->st.prim_quartets = (int64_t)hs[1];
+        P->st.quartets = 0;
+        P->st.prim_quartets = 0;
+        for (size_t t = 0; t < qcs.size(); t++) {
+                P->cls[t].quartets = (int64_t)hs[2 * t];
+                P->cls[t].prim_quartets = (int64_t)hs[2 * t + 1];
+                P->st.quartets += (int64_t)hs[2 * t];
+                P->st.prim_quartets += (int64_t)hs[2 * t + 1];
+                P->cls[t].ms = 0;
+                if (P->profiling && ran[t]) {
+                        float cm = 0;
+                        CUDA_TRY(cudaEventElapsedTime(&cm, P->cls_ev[2 * t], P->cls_ev[2 * t + 1]));
+                        P->cls[t].ms = cm;
+                }
+        }
         P->st.last_build_ms = ms;
+        P->st.kernel_launches = launches;
+        return B200JK_OK;
+}
+
+int b200jk_set_profiling(b200jk_plan *plan, int on)
+{
+        if (!plan) return fail(B200JK_EINVAL, "plan is NULL");
+        plan->profiling = on ? 1 : 0;
+        return B200JK_OK;
+}
+
+int b200jk_class_stats(const b200jk_plan *plan, b200jk_class_stat_t *out, int max, int *n)
+{
+        if (!plan || !n) return fail(B200JK_EINVAL, "NULL argument");
+        *n = (int)plan->cls.size();
+        for (int t = 0; t < *n && t < max && out; t++) out[t] = plan->cls[t];
+        return B200JK_OK;
+}
+
+int b200jk_measure_fp64_peak(int device, double *tflops)
+{
+        if (!tflops) return fail(B200JK_EINVAL, "tflops is NULL");
+        CUDA_TRY(cudaSetDevice(device));
+        cudaDeviceProp prop;
+        CUDA_TRY(cudaGetDeviceProperties(&prop, device));
+        const int block = 256, iters = 4096;
+        const int grid = prop.multiProcessorCount * 8;
+        DevArr<double> sink;
+        int rc = dev_alloc(sink, (size_t)grid * block);
+        if (rc) return rc;
+        cudaEvent_t e0, e1;
+        CUDA_TRY(cudaEventCreate(&e0));
+        CUDA_TRY(cudaEventCreate(&e1));
+        fp64_fma_kernel<<<grid, block>>>(sink.p, iters, 1.0000001);   // warm-up
+        CUDA_TRY(cudaEventRecord(e0));
+        for (int r = 0; r < 5; r++) fp64_fma_kernel<<<grid, block>>>(sink.p, iters, 1.0000001);
+        CUDA_TRY(cudaEventRecord(e1));
+        CUDA_TRY(cudaEventSynchronize(e1));
+        float ms = 0;
+        CUDA_TRY(cudaEventElapsedTime(&ms, e0, e1));
+        cudaEventDestroy(e0);
+        cudaEventDestroy(e1);
+        sink.release();
+        const double flops = 5.0 * grid * block * (double)iters * 8 * 2;
+        *tflops = flops / (ms * 1e-3) / 1e12;
         return B200JK_OK;
 }
 

@@ -23,7 +23,8 @@ PREC_FP64 = 0
 EXPORTS = (
     'b200jk_version', 'b200jk_last_error', 'b200jk_device_count', 'b200jk_plan_create',
     'b200jk_plan_destroy', 'b200jk_plan_dims', 'b200jk_get_q_cond', 'b200jk_get_jk',
-    'b200jk_stats', 'b200jk_hostcheck_cart_quartet',
+    'b200jk_stats', 'b200jk_hostcheck_cart_quartet', 'b200jk_class_stats', 'b200jk_set_profiling',
+    'b200jk_measure_fp64_peak',
 )
 
 
@@ -38,7 +39,14 @@ class Stats(ctypes.Structure):
                 ('shell_pairs', ctypes.c_int64), ('prim_pairs', ctypes.c_int64),
                 ('flops', ctypes.c_double), ('last_build_ms', ctypes.c_double),
                 ('nao', ctypes.c_int32), ('nao_cart', ctypes.c_int32),
-                ('nbas', ctypes.c_int32), ('nseg', ctypes.c_int32)]
+                ('nbas', ctypes.c_int32), ('nseg', ctypes.c_int32),
+                ('kernel_launches', ctypes.c_int64)]
+
+
+class ClassStat(ctypes.Structure):
+    _fields_ = [('la', ctypes.c_int32), ('lb', ctypes.c_int32), ('lc', ctypes.c_int32), ('ld', ctypes.c_int32),
+                ('quartets', ctypes.c_int64), ('prim_quartets', ctypes.c_int64), ('ms', ctypes.c_double),
+                ('family', ctypes.c_int32), ('pad', ctypes.c_int32)]
 
 
 _lib = None
@@ -65,6 +73,9 @@ def load(path=LIB_PATH):
         lib.b200jk_get_jk.argtypes = [vp, vp, ip, ip, ip, ip, vp, vp, ip, ip, vp]
         lib.b200jk_stats.argtypes = [vp, ctypes.POINTER(Stats)]
         lib.b200jk_hostcheck_cart_quartet.argtypes = [vp, ip, vp, ip, vp, vp, vp]
+        lib.b200jk_class_stats.argtypes = [vp, ctypes.POINTER(ClassStat), ip, ctypes.POINTER(ip)]
+        lib.b200jk_set_profiling.argtypes = [vp, ip]
+        lib.b200jk_measure_fp64_peak.argtypes = [ip, ctypes.POINTER(dp)]
         _lib = lib
         return lib
 
@@ -129,6 +140,15 @@ class Plan:
         check(load().b200jk_stats(self._h, ctypes.byref(s)))
         return {k: getattr(s, k) for k, _ in Stats._fields_}
 
+    def class_stats(self):
+        n = ctypes.c_int(0)
+        buf = (ClassStat * 64)()
+        check(load().b200jk_class_stats(self._h, buf, 64, ctypes.byref(n)))
+        return [{k: getattr(buf[i], k) for k, _ in ClassStat._fields_} for i in range(n.value)]
+
+    def set_profiling(self, on=True):
+        check(load().b200jk_set_profiling(self._h, int(bool(on))))
+
     def get_jk(self, dms, hermi=1, with_j=True, with_k=True, out_j=None, out_k=None,
                precision=PREC_FP64, stream=None):
         """J/K of host densities (n_dm, nao, nao) -> host arrays."""
@@ -173,6 +193,13 @@ class Plan:
                                    ctypes.c_void_p(vk.data_ptr()) if with_k else None,
                                    1, int(precision), ctypes.c_void_p(stream)))
         return (vj.reshape(shape) if with_j else None), (vk.reshape(shape) if with_k else None)
+
+
+def measure_fp64_peak(device=0):
+    """FP64 FMA throughput of the device in TFLOP/s (register-resident loop)."""
+    t = ctypes.c_double(0)
+    check(load().b200jk_measure_fp64_peak(int(device), ctypes.byref(t)))
+    return t.value
 
 
 def hostcheck_cart_quartet(atm, bas, env, shls):

@@ -95,4 +95,9 @@ def workloads():
         'c20h42_vdz': (alkane(20), 'cc-pvdz'),
         'h2o16_vdz': (water_cluster((2, 2, 4), 0.2, 505), 'cc-pvdz'),
         'h2o64_vtz': (water_cluster((4, 4, 4), 0.3, 303), 'cc-pvtz'),
+        # the first 4 / 8 / 16 waters of the (H2O)64 geometry: bounded samples of
+        # that workload for the CPU baseline and for scaling estimates
+        'h2o64_vtz_sub4': (water_cluster((4, 4, 4), 0.3, 303)[:12], 'cc-pvtz'),
+        'h2o64_vtz_sub8': (water_cluster((4, 4, 4), 0.3, 303)[:24], 'cc-pvtz'),
+        'h2o64_vtz_sub16': (water_cluster((4, 4, 4), 0.3, 303)[:48], 'cc-pvtz'),
     }
