@@ -165,6 +165,7 @@ static int dev_alloc(DevArr<T> &d, size_t n)
 
 struct PairClassDev {
         int la = 0, lb = 0, n = 0;
+        int boff[B2_NBUCKET + 1] = {0, 0, 0, 0, 0};
         DevArr<int4> sh;
         DevArr<int2> pr;
         DevArr<double> q;
@@ -173,6 +174,7 @@ struct PairClassDev {
         {
                 PairView v;
                 v.sh = sh.p; v.pr = pr.p; v.q = q.p; v.A = A.p; v.AB = AB.p; v.n = n;
+                for (int b = 0; b <= B2_NBUCKET; b++) v.boff[b] = boff[b];
                 return v;
         }
         void release() { sh.release(); pr.release(); q.release(); A.release(); AB.release(); n = 0; }
@@ -550,6 +552,9 @@ int b200jk_plan_create(const int32_t *atm, int natm, const int32_t *bas, int nba
                 PairClassDev &c = P->pc[X];
                 class_l(X, c.la, c.lb);
                 c.n = (int)hv.size();
+                for (int b = 0; b <= B2_NBUCKET; b++) c.boff[b] = 0;
+                for (const HostPair &p : hv) c.boff[prim_bucket(p.nprim) + 1]++;
+                for (int b = 0; b < B2_NBUCKET; b++) c.boff[b + 1] += c.boff[b];
                 std::vector<int4> sh(hv.size());
                 std::vector<int2> pr(hv.size());
                 std::vector<double> q(hv.size());
@@ -611,7 +616,12 @@ int b200jk_plan_create(const int32_t *atm, int natm, const int32_t *bas, int nba
                                                 [&](const HostPair &p) { return !(p.q * qmax > P->tol); }),
                                  hv.end());
                 }
-                std::stable_sort(hv.begin(), hv.end(), [](const HostPair &a, const HostPair &b) { return a.q > b.q; });
+                // bucket-major, descending q inside a bucket
+                std::stable_sort(hv.begin(), hv.end(), [](const HostPair &a, const HostPair &b) {
+                        const int ba = prim_bucket(a.nprim), bb = prim_bucket(b.nprim);
+                        if (ba != bb) return ba < bb;
+                        return a.q > b.q;
+                });
                 P->shell_pairs += (int64_t)hv.size();
                 if ((rc = upload_class(X, hv))) return bail(rc);
         }
@@ -640,7 +650,7 @@ static int ensure_workspace(b200jk_plan *P, int n_dm)
             (rc = dev_alloc(P->dmax, 1)) || (rc = dev_alloc(P->stats, 2 * 64)))
                 return rc;
         int maxn = 1;
-        for (auto &c : P->pc) maxn = std::max(maxn, c.n);
+        for (auto &c : P->pc) maxn = std::max(maxn, c.n * B2_NBUCKET);
         if ((rc = dev_alloc(P->nkl, maxn)) || (rc = dev_alloc(P->nchunk, maxn + 1)) ||
             (rc = dev_alloc(P->chunk_off, maxn + 1)))
                 return rc;
@@ -722,14 +732,15 @@ int b200jk_get_jk(b200jk_plan *P, const double *dms, int n_dm, int hermi, int wi
                         const int same = qcs[t].X == qcs[t].Y;
                         // chunk size of the family the dispatcher will pick
                         const int chunk = family_chunk(la, lb, lc, ld);
-                        count_kernel<<<grid_for(bra.n, 256), 256, 0, s>>>(bra.view(), ket.view(), same,
-                                                                         P->tol > 0 ? P->tol : 0.0,
-                                                                         (const double *)P->dmax.p, chunk,
-                                                                         P->nkl.p, P->nchunk.p);
+                        const int nseg = bra.n * B2_NBUCKET;
+                        count_kernel<<<grid_for(nseg, 256), 256, 0, s>>>(bra.view(), ket.view(), same,
+                                                                        P->tol > 0 ? P->tol : 0.0,
+                                                                        (const double *)P->dmax.p, chunk,
+                                                                        P->nkl.p, P->nchunk.p);
                         CUDA_TRY(cudaGetLastError());
-                        CUDA_TRY(cudaMemsetAsync(P->nchunk.p + bra.n, 0, sizeof(long long), s));
+                        CUDA_TRY(cudaMemsetAsync(P->nchunk.p + nseg, 0, sizeof(long long), s));
                         size_t tmp = P->cub_tmp.n;
-                        CUDA_TRY(cub::DeviceScan::ExclusiveSum(P->cub_tmp.p, tmp, P->nchunk.p, P->chunk_off.p, bra.n + 1, s));
+                        CUDA_TRY(cub::DeviceScan::ExclusiveSum(P->cub_tmp.p, tmp, P->nchunk.p, P->chunk_off.p, nseg + 1, s));
                         JKArgs a;
                         a.bra = bra.view();
                         a.ket = ket.view();

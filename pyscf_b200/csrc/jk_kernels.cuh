@@ -27,21 +27,32 @@
 
 namespace b200jk {
 
+// Pairs of one angular class are stored bucket by bucket (buckets of equal
+// primitive-pair count, so the lanes of a warp run loops of equal length),
+// each bucket sorted by descending q.  Pair order inside a class is
+// (bucket, rank); it defines the canonical ij >= kl of same-class quartets.
+#define B2_NBUCKET 4
+__host__ __device__ inline int prim_bucket(int nprim_pairs)
+{
+        return nprim_pairs <= 1 ? 0 : (nprim_pairs <= 4 ? 1 : (nprim_pairs <= 16 ? 2 : 3));
+}
+
 struct PairView {
         const int4 *sh;      // (cart AO of i, cart AO of j, parent shell i, parent shell j)
         const int2 *pr;      // (first primitive pair, number of primitive pairs)
-        const double *q;     // parent-shell Schwarz bound (descending)
+        const double *q;     // parent-shell Schwarz bound (descending inside a bucket)
         const double4 *A;    // (A, 1 if i == j else 0)
         const double4 *AB;   // (A - B, 0)
         int n;
+        int boff[B2_NBUCKET + 1];   // bucket b holds pairs [boff[b], boff[b+1])
 };
 
 struct JKArgs {
         PairView bra, ket;
         const double4 *PP;           // primitive pair (P, p)
         const double2 *PK;           // primitive pair (K_ab c_i c_j, a_i)
-        const long long *chunk_off;  // bra.n + 1 entries
-        const int *nkl;              // per bra pair
+        const long long *chunk_off;  // bra.n * B2_NBUCKET + 1 entries
+        const int *nkl;              // per (bra pair, ket bucket)
         const double *dm_cond;       // nbas x nbas (parent shells)
         const double *table;         // Rys tables
         const int *goff;             // packed (ox, oy, oz) per Cartesian component (warp family)
@@ -88,29 +99,37 @@ __device__ __forceinline__ bool quartet_passes(const JKArgs &a, int4 sb, double 
 #define B2_TWO_PI_2P5 34.98683665524972497
 
 // ---------------------------------------------------------------------------
-// Count kernel: ket prefix length per bra pair, and chunks of `chunk` quartets.
+// Count kernel: for bra pair ij and ket bucket b, the length of the prefix of
+// the bucket that can pass the screen, and its chunks of `chunk` quartets.
+// Same-class quartets keep kl <= ij in the (bucket, rank) order.
 static __global__ void count_kernel(PairView bra, PairView ket, int same, double tol, const double *dmax4,
-                             int chunk, int *nkl, long long *nchunk)
+                                    int chunk, int *nkl, long long *nchunk)
 {
-        const int ij = blockIdx.x * blockDim.x + threadIdx.x;
-        if (ij >= bra.n) return;
+        const int t = blockIdx.x * blockDim.x + threadIdx.x;
+        if (t >= bra.n * B2_NBUCKET) return;
+        const int ij = t / B2_NBUCKET, b = t % B2_NBUCKET;
         const double qij = bra.q[ij];
         const double dm = *dmax4;
         int cnt = 0;
-        if (dm > 0 && qij > 0) {
+        const int lo0 = ket.boff[b], hi0 = ket.boff[b + 1];
+        if (dm > 0 && qij > 0 && hi0 > lo0) {
                 const double thr = tol / (qij * dm);
-                // ket.q is descending: count entries with q > thr
-                int lo = 0, hi = ket.n;
+                int lo = lo0, hi = hi0;
                 while (lo < hi) {
                         int mid = (lo + hi) >> 1;
                         if (ket.q[mid] > thr) lo = mid + 1;
                         else hi = mid;
                 }
-                cnt = lo;
-                if (same) cnt = min(cnt, ij + 1);
+                cnt = lo - lo0;
+                if (same) {
+                        int bi = 0;
+                        while (bi < B2_NBUCKET - 1 && ij >= bra.boff[bi + 1]) bi++;
+                        if (b > bi) cnt = 0;
+                        else if (b == bi) cnt = min(cnt, ij - lo0 + 1);
+                }
         }
-        nkl[ij] = cnt;
-        nchunk[ij] = (cnt + chunk - 1) / chunk;
+        nkl[t] = cnt;
+        nchunk[t] = (cnt + chunk - 1) / chunk;
 }
 
 // ---------------------------------------------------------------------------
@@ -120,20 +139,23 @@ __global__ void __launch_bounds__(128) jk_thread_kernel(JKArgs a)
 {
         using K = Class4<LA, LB, LC, LD>;
         const int lane = threadIdx.x & 31;
-        const long long total = a.chunk_off[a.bra.n];
+        const int nseg = a.bra.n * B2_NBUCKET;
+        const long long total = a.chunk_off[nseg];
         const long long nwarps = ((long long)gridDim.x * blockDim.x) >> 5;
         const size_t n = (size_t)a.naoc, nn = n * n;
         unsigned long long nq = 0, npq = 0;
         for (long long chunk = ((long long)blockIdx.x * blockDim.x + threadIdx.x) >> 5; chunk < total;
              chunk += nwarps) {
-                const int ij = find_bra(a.chunk_off, a.bra.n, chunk);
-                const int kl = (int)(chunk - a.chunk_off[ij]) * 32 + lane;
+                const int sgi = find_bra(a.chunk_off, nseg, chunk);
+                const int ij = sgi / B2_NBUCKET;
+                const int pos = (int)(chunk - a.chunk_off[sgi]) * 32 + lane;
+                const int kl = a.ket.boff[sgi % B2_NBUCKET] + pos;
                 const int4 sb = a.bra.sh[ij];
                 const int2 pb = a.bra.pr[ij];
                 const double qij = a.bra.q[ij];
                 const double4 Ab = a.bra.A[ij];
                 const double4 ABb = a.bra.AB[ij];
-                bool active = kl < a.nkl[ij];
+                bool active = pos < a.nkl[sgi];
                 int4 sk = make_int4(0, 0, 0, 0);
                 double G[K::NG];
 #pragma unroll
@@ -427,15 +449,18 @@ __global__ void __launch_bounds__(128) jk_warp_kernel(JKArgs a, int chunk_q)
         const int lane = threadIdx.x & 31;
         const int wib = threadIdx.x >> 5;
         double *sm = smem_dyn + (size_t)wib * S::SIZE;
-        const long long total = a.chunk_off[a.bra.n];
+        const int nseg = a.bra.n * B2_NBUCKET;
+        const long long total = a.chunk_off[nseg];
         const long long nwarps = ((long long)gridDim.x * blockDim.x) >> 5;
         const size_t n = (size_t)a.naoc, nn = n * n;
         unsigned long long nq = 0, npq = 0;
         for (long long chunk = ((long long)blockIdx.x * blockDim.x + threadIdx.x) >> 5; chunk < total;
              chunk += nwarps) {
-                const int ij = find_bra(a.chunk_off, a.bra.n, chunk);
-                const int kl0 = (int)(chunk - a.chunk_off[ij]) * chunk_q;
-                const int kl1 = min(kl0 + chunk_q, a.nkl[ij]);
+                const int sgi = find_bra(a.chunk_off, nseg, chunk);
+                const int ij = sgi / B2_NBUCKET;
+                const int kb = a.ket.boff[sgi % B2_NBUCKET];
+                const int kl0 = kb + (int)(chunk - a.chunk_off[sgi]) * chunk_q;
+                const int kl1 = kb + min((int)(chunk - a.chunk_off[sgi]) * chunk_q + chunk_q, a.nkl[sgi]);
                 const int4 sb = a.bra.sh[ij];
                 const int2 pb = a.bra.pr[ij];
                 const double qij = a.bra.q[ij];

@@ -27,6 +27,7 @@
 //   expansion (x-B)^b = sum_k C(b,k) (x-A)^k (A-B)^{b-k}.
 #pragma once
 #include <math.h>
+#include <utility>
 
 #ifdef __CUDACC__
 #define B2_HD __host__ __device__ __forceinline__
@@ -229,6 +230,27 @@ B2_HD void rys_coef(RysCoef &rc, double u, double p, double q, const double PA[3
         }
 }
 
+// G[T] += I_x I_y I_z for Cartesian component T; the offsets into the 2D
+// integrals are constant expressions, so the whole assembly unrolls into
+// register operations.
+template <int LA, int LB, int LC, int LD, int T>
+B2_HD void assemble_one(double *G, const double *hx, const double *hy, const double *hz)
+{
+        using K = Class4<LA, LB, LC, LD>;
+        constexpr int id = T % K::ND, ic = (T / K::ND) % K::NC, ib = (T / K::NCD) % K::NB, ia = T / (K::NCD * K::NB);
+        constexpr int ox = K::hidx(cart_lx(LA, ia), cart_lx(LB, ib), cart_lx(LC, ic), cart_lx(LD, id));
+        constexpr int oy = K::hidx(cart_ly(LA, ia), cart_ly(LB, ib), cart_ly(LC, ic), cart_ly(LD, id));
+        constexpr int oz = K::hidx(cart_lz(LA, ia), cart_lz(LB, ib), cart_lz(LC, ic), cart_lz(LD, id));
+        G[T] += hx[ox] * hy[oy] * hz[oz];
+}
+
+template <int LA, int LB, int LC, int LD, int... Ts>
+B2_HD void assemble_all(double *G, const double *hx, const double *hy, const double *hz,
+                        std::integer_sequence<int, Ts...>)
+{
+        (assemble_one<LA, LB, LC, LD, Ts>(G, hx, hy, hz), ...);
+}
+
 // Add one primitive quartet to the Cartesian block G[((a*NB+b)*NC+c)*ND+d].
 // pref = 2 pi^{5/2}/(pq sqrt(p+q)) K_ab K_cd (coefficients included).
 template <int LA, int LB, int LC, int LD>
@@ -260,18 +282,22 @@ B2_HD void add_prim_quartet(double *G, const double *table, double p, const doub
                 hrr2d<LA, LB, LC, LD>(g, hy, AB[1], CD[1]);
                 vrr2d<K::NE, K::NF>(g, pref * w[r], rc.c00[2], rc.c00p[2], rc.b10, rc.b01, rc.b00);
                 hrr2d<LA, LB, LC, LD>(g, hz, AB[2], CD[2]);
-#pragma unroll
-                for (int ia = 0; ia < K::NA; ia++)
-#pragma unroll
-                for (int ib = 0; ib < K::NB; ib++)
-#pragma unroll
-                for (int ic = 0; ic < K::NC; ic++)
-#pragma unroll
-                for (int id = 0; id < K::ND; id++) {
-                        const int ox = K::hidx(cart_lx(LA, ia), cart_lx(LB, ib), cart_lx(LC, ic), cart_lx(LD, id));
-                        const int oy = K::hidx(cart_ly(LA, ia), cart_ly(LB, ib), cart_ly(LC, ic), cart_ly(LD, id));
-                        const int oz = K::hidx(cart_lz(LA, ia), cart_lz(LB, ib), cart_lz(LC, ic), cart_lz(LD, id));
-                        G[((ia * K::NB + ib) * K::NC + ic) * K::ND + id] += hx[ox] * hy[oy] * hz[oz];
+#if defined(__CUDA_ARCH__)
+                if constexpr (K::NG <= 128) {
+                        assemble_all<LA, LB, LC, LD>(G, hx, hy, hz, std::make_integer_sequence<int, K::NG>{});
+                } else
+#endif
+                {
+                        // same operations in the same order as assemble_all
+                        for (int ia = 0; ia < K::NA; ia++)
+                        for (int ib = 0; ib < K::NB; ib++)
+                        for (int ic = 0; ic < K::NC; ic++)
+                        for (int id = 0; id < K::ND; id++) {
+                                const int ox = K::hidx(cart_lx(LA, ia), cart_lx(LB, ib), cart_lx(LC, ic), cart_lx(LD, id));
+                                const int oy = K::hidx(cart_ly(LA, ia), cart_ly(LB, ib), cart_ly(LC, ic), cart_ly(LD, id));
+                                const int oz = K::hidx(cart_lz(LA, ia), cart_lz(LB, ib), cart_lz(LC, ic), cart_lz(LD, id));
+                                G[((ia * K::NB + ib) * K::NC + ic) * K::ND + id] += hx[ox] * hy[oy] * hz[oz];
+                        }
                 }
         }
 }
