@@ -104,6 +104,22 @@ int b200jk_get_jk(b200jk_plan *plan, const double *dms, int n_dm, int hermi,
                   int with_j, int with_k, double *vj, double *vk,
                   int dev_ptrs, int precision_mode, void *stream);
 
+/* J/K like b200jk_get_jk, for callers that cannot let the library allocate
+ * device memory (code running under a framework's caching allocator or a
+ * fixed memory budget, where a cudaMalloc can fail or stall the device).  It
+ * has no counterpart in the reference.  dms, vj, vk are device arrays on the
+ * plan's GPU; nothing is allocated: all intermediates live in one fixed
+ * 32 MiB scratch array that every GPU loading the library holds until exit,
+ * which bounds the size (roughly nao_cart <= 600 for one density); larger
+ * inputs are rejected with B200JK_EINVAL and a message.  The first call on a
+ * device resolves the scratch array's device address; make that first call
+ * before any stream capture.  All calls share the one array: calls that
+ * overlap on the GPU (other streams, other threads) race and must be
+ * serialised by the caller.  The plan itself is created (and allocated) by
+ * b200jk_plan_create beforehand. */
+int b200jk_get_jk_noalloc(b200jk_plan *plan, const double *dms, int n_dm, int hermi,
+                          int with_j, int with_k, double *vj, double *vk, void *stream);
+
 /* Counters of the last build. */
 int b200jk_stats(const b200jk_plan *plan, b200jk_stats_t *stats);
 

@@ -866,3 +866,160 @@ int b200jk_stats(const b200jk_plan *plan, b200jk_stats_t *stats)
 
 } // extern "C"
 
+
+// ---------------------------------------------------------------------------
+// Allocation-free J/K build.
+//
+// Some callers cannot let a library call cudaMalloc: code that runs under a
+// framework's caching allocator or a fixed device-memory budget (a cudaMalloc
+// there can fail because the pool holds the memory, and it synchronises the
+// device in the middle of the caller's stream work).  b200jk_get_jk_noalloc
+// serves them: it runs the same kernels as b200jk_get_jk, but every
+// intermediate (Cartesian densities, J/K accumulators, screening and chunk
+// arrays, scan storage) lives in the file-scope array below, of fixed size
+// B200JK_NOALLOC_SCRATCH_BYTES, which each GPU that loads this library holds
+// until the process exits.  The plan must exist already (creating it
+// allocates); the call itself allocates nothing.
+
+#define B200JK_NOALLOC_SCRATCH_BYTES (32ull << 20)
+static __device__ __align__(256) unsigned char g_noalloc_scratch[B200JK_NOALLOC_SCRATCH_BYTES];
+
+// Device address of g_noalloc_scratch on each device, resolved once per
+// device (with that device current) by the first no-alloc call on it.
+static std::once_flag g_noalloc_once[64];
+static unsigned char *g_noalloc_ptr[64];
+static cudaError_t g_noalloc_err[64];
+
+static size_t noalloc_align(size_t x) { return (x + 255) & ~(size_t)255; }
+
+extern "C" int b200jk_get_jk_noalloc(b200jk_plan *P, const double *dms, int n_dm, int hermi, int with_j,
+                                     int with_k, double *vj, double *vk, void *stream)
+{
+        if (!P) return fail(B200JK_EINVAL, "plan is NULL");
+        if (!dms || n_dm <= 0) return fail(B200JK_EINVAL, "no density matrices");
+        if (hermi < 0 || hermi > 2) return fail(B200JK_EINVAL, "hermi must be 0, 1 or 2");
+        if (with_j && !vj) return fail(B200JK_EINVAL, "vj is NULL while with_j is set");
+        if (with_k && !vk) return fail(B200JK_EINVAL, "vk is NULL while with_k is set");
+        const int dev = P->device;
+        if (dev < 0 || dev >= 64) return fail(B200JK_EINVAL, "device index out of range");
+        CUDA_TRY(cudaSetDevice(dev));
+        std::call_once(g_noalloc_once[dev], [dev]() {
+                void *p = nullptr;
+                g_noalloc_err[dev] = cudaGetSymbolAddress(&p, g_noalloc_scratch);
+                g_noalloc_ptr[dev] = (unsigned char *)p;
+        });
+        if (g_noalloc_err[dev] != cudaSuccess || !g_noalloc_ptr[dev])
+                return fail(B200JK_ECUDA, std::string("cudaGetSymbolAddress(g_noalloc_scratch): ") +
+                                                  cudaGetErrorString(g_noalloc_err[dev]));
+
+        // carve the scratch array; reject sizes beyond it before any work
+        const size_t nn = (size_t)P->nao * P->nao, nc = (size_t)P->naoc * P->naoc;
+        const int nk = hermi == 1 ? 1 : 2;
+        int maxn = 1;
+        for (auto &c : P->pc) maxn = std::max(maxn, c.n * B2_NBUCKET);
+        size_t cub_bytes = 0;
+        cub::DeviceScan::ExclusiveSum(nullptr, cub_bytes, (long long *)nullptr, (long long *)nullptr, maxn + 1);
+        size_t off = 0;
+        auto take = [&](size_t bytes) { size_t o = off; off += noalloc_align(bytes); return o; };
+        const size_t o_Dc = take(sizeof(double) * nc * n_dm * nk);
+        const size_t o_Ds = take(sizeof(double) * nc * n_dm);
+        const size_t o_J = take(with_j ? sizeof(double) * nc * n_dm : 0);
+        const size_t o_K = take(with_k ? sizeof(double) * nc * n_dm * nk : 0);
+        const size_t o_dmc = take(sizeof(double) * (size_t)P->nbas * P->nbas);
+        const size_t o_dmax = take(sizeof(unsigned long long));
+        const size_t o_stats = take(sizeof(unsigned long long) * 2 * 64);
+        const size_t o_nkl = take(sizeof(int) * (size_t)maxn);
+        const size_t o_nchunk = take(sizeof(long long) * (size_t)(maxn + 1));
+        const size_t o_off = take(sizeof(long long) * (size_t)(maxn + 1));
+        const size_t o_cub = take(cub_bytes + 16);
+        if (off > B200JK_NOALLOC_SCRATCH_BYTES) {
+                char msg[256];
+                snprintf(msg, sizeof(msg),
+                         "b200jk_get_jk_noalloc needs %zu bytes of scratch for nao_cart=%d, n_dm=%d, hermi=%d; "
+                         "the fixed scratch holds %llu bytes (use b200jk_get_jk)",
+                         off, P->naoc, n_dm, hermi, (unsigned long long)B200JK_NOALLOC_SCRATCH_BYTES);
+                return fail(B200JK_EINVAL, msg);
+        }
+        unsigned char *base = g_noalloc_ptr[dev];
+        double *Dc = (double *)(base + o_Dc), *Ds = (double *)(base + o_Ds);
+        double *Jacc = (double *)(base + o_J), *Kacc = (double *)(base + o_K);
+        double *dmc = (double *)(base + o_dmc);
+        unsigned long long *dmax = (unsigned long long *)(base + o_dmax);
+        unsigned long long *stats = (unsigned long long *)(base + o_stats);
+        int *nkl = (int *)(base + o_nkl);
+        long long *nchunk = (long long *)(base + o_nchunk), *chunk_off = (long long *)(base + o_off);
+        void *cub_tmp = base + o_cub;
+
+        cudaStream_t s = stream ? (cudaStream_t)stream : P->stream;
+        // the array keeps the previous call's contents: clear what accumulates
+        CUDA_TRY(cudaMemsetAsync(dmax, 0, sizeof(unsigned long long), s));
+        CUDA_TRY(cudaMemsetAsync(stats, 0, 2 * 64 * sizeof(unsigned long long), s));
+        if (with_j) CUDA_TRY(cudaMemsetAsync(Jacc, 0, sizeof(double) * nc * n_dm, s));
+        if (with_k) CUDA_TRY(cudaMemsetAsync(Kacc, 0, sizeof(double) * nc * n_dm * nk, s));
+        {
+                const long long npair = (long long)P->nbas * (P->nbas + 1) / 2;
+                dm_cond_kernel<<<grid_for(npair, 256), 256, 0, s>>>(dms, n_dm, P->nao, P->ao_loc_d.p, P->nbas, dmc, dmax);
+                CUDA_TRY(cudaGetLastError());
+        }
+        for (int d = 0; d < n_dm; d++) {
+                double *dc = Dc + (size_t)d * nk * nc;
+                out_to_cart_kernel<<<grid_for((long long)nc, 256), 256, 0, s>>>(
+                        dms + (size_t)d * nn, P->nao, P->naoc, P->cart_seg.p, P->cart_comp.p, P->seg_info.p,
+                        P->c2s.p, P->cart, dc, nk == 2 ? dc + nc : nullptr, nullptr);
+                CUDA_TRY(cudaGetLastError());
+                sym_sum_kernel<<<grid_for((long long)nc, 256), 256, 0, s>>>(dc, P->naoc, Ds + (size_t)d * nc);
+                CUDA_TRY(cudaGetLastError());
+        }
+        const double *tbl = table_ptr();
+        auto qcs = quartet_classes();
+        for (size_t t = 0; t < qcs.size(); t++) {
+                const PairClassDev &bra = P->pc[qcs[t].X], &ket = P->pc[qcs[t].Y];
+                if (bra.n == 0 || ket.n == 0) continue;
+                const int la = bra.la, lb = bra.lb, lc = ket.la, ld = ket.lb;
+                const int same = qcs[t].X == qcs[t].Y;
+                const int nseg = bra.n * B2_NBUCKET;
+                count_kernel<<<grid_for(nseg, 256), 256, 0, s>>>(bra.view(), ket.view(), same, P->tol > 0 ? P->tol : 0.0,
+                                                                (const double *)dmax, family_chunk(la, lb, lc, ld),
+                                                                nkl, nchunk);
+                CUDA_TRY(cudaGetLastError());
+                CUDA_TRY(cudaMemsetAsync(nchunk + nseg, 0, sizeof(long long), s));
+                size_t tmp = cub_bytes;
+                CUDA_TRY(cub::DeviceScan::ExclusiveSum(cub_tmp, tmp, nchunk, chunk_off, nseg + 1, s));
+                JKArgs a;
+                a.bra = bra.view();
+                a.ket = ket.view();
+                a.PP = P->PP.p; a.PK = P->PK.p;
+                a.chunk_off = chunk_off;
+                a.nkl = nkl;
+                a.dm_cond = dmc;
+                a.table = tbl;
+                a.goff = P->goff_all.p + P->goff_at[t];
+                a.Jacc = Jacc; a.Kacc = Kacc;
+                a.Ds = Ds; a.Dk = Dc;
+                a.stats = stats + 2 * t;
+                a.tol = P->tol > 0 ? P->tol : -1.0;
+                a.nbas = P->nbas; a.naoc = P->naoc; a.n_dm = n_dm; a.nk = nk;
+                a.with_j = with_j; a.with_k = with_k; a.same = same;
+                int rc = dispatch_jk(P, la, lb, lc, ld, a, s);
+                if (rc) return rc;
+        }
+        for (int d = 0; d < n_dm; d++) {
+                if (with_j) {
+                        const double *J = Jacc + (size_t)d * nc;
+                        cart_to_out_kernel<<<grid_for((long long)nn, 256), 256, 0, s>>>(
+                                J, J, P->nao, P->naoc, P->out_seg.p, P->out_comp.p, P->seg_info.p, P->c2s.p,
+                                P->cart, 1, vj + (size_t)d * nn);
+                        CUDA_TRY(cudaGetLastError());
+                }
+                if (with_k) {
+                        const double *K1 = Kacc + (size_t)d * nk * nc;
+                        const double *K2 = nk == 2 ? K1 + nc : K1;
+                        cart_to_out_kernel<<<grid_for((long long)nn, 256), 256, 0, s>>>(
+                                K1, K2, P->nao, P->naoc, P->out_seg.p, P->out_comp.p, P->seg_info.p, P->c2s.p,
+                                P->cart, hermi, vk + (size_t)d * nn);
+                        CUDA_TRY(cudaGetLastError());
+                }
+        }
+        CUDA_TRY(cudaStreamSynchronize(s));
+        return B200JK_OK;
+}

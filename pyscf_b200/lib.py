@@ -24,7 +24,7 @@ EXPORTS = (
     'b200jk_version', 'b200jk_last_error', 'b200jk_device_count', 'b200jk_plan_create',
     'b200jk_plan_destroy', 'b200jk_plan_dims', 'b200jk_get_q_cond', 'b200jk_get_jk',
     'b200jk_stats', 'b200jk_hostcheck_cart_quartet', 'b200jk_class_stats', 'b200jk_set_profiling',
-    'b200jk_measure_fp64_peak',
+    'b200jk_measure_fp64_peak', 'b200jk_get_jk_noalloc',
 )
 
 
@@ -76,6 +76,7 @@ def load(path=LIB_PATH):
         lib.b200jk_class_stats.argtypes = [vp, ctypes.POINTER(ClassStat), ip, ctypes.POINTER(ip)]
         lib.b200jk_set_profiling.argtypes = [vp, ip]
         lib.b200jk_measure_fp64_peak.argtypes = [ip, ctypes.POINTER(dp)]
+        lib.b200jk_get_jk_noalloc.argtypes = [vp, vp, ip, ip, ip, ip, vp, vp, vp]
         _lib = lib
         return lib
 
