@@ -271,6 +271,13 @@ def run_gpu(args):
                     's_per_build': t_e2e, 'h2d_bytes_per_step': int(nao * nao * 8),
                     'd2h_bytes_per_step': int(2 * nao * nao * 8),
                     'timing': 'wall clock around pyscf_b200._vhf.direct with pinned host arrays'},
+            'classes': [{'class': '(%d%d|%d%d)' % (c['la'], c['lb'], c['lc'], c['ld']),
+                         'family': 'thread' if c['family'] == 0 else 'group',
+                         'ms_per_build': c['ms'] / args.steps,
+                         'share': c['ms'] * 1e-3 / t_total,
+                         'quartets_per_build': c['quartets'] / args.steps,
+                         'tflops': flops.class_flops(c) / (c['ms'] * 1e-3) / 1e12 if c['ms'] > 0 else None}
+                        for c in sorted(cls, key=lambda c: -c['ms'])[:12]],
             'gpu_launches': int(launches),
             'clocks': clocks,
         }

@@ -35,7 +35,8 @@ int launch_one(const JKArgs &a, cudaStream_t s, int nsm, std::string &err)
                                 cfg.smem = 0;
                                 cfg.status = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, jk_thread_kernel<LA, LB, LC, LD>, 128, 0);
                         } else {
-                                const size_t per_warp = sizeof(double) * WarpSmem<LA, LB, LC, LD>::SIZE;
+                                const size_t per_warp = sizeof(double) * WarpSmem<LA, LB, LC, LD>::SIZE *
+                                                        (32 / group_size<LA, LB, LC, LD>());
                                 const int wpb = (int)std::min<size_t>(4, std::max<size_t>(1, (200 * 1024) / per_warp));
                                 cfg.block = 32 * wpb;
                                 cfg.smem = per_warp * wpb;
@@ -56,7 +57,8 @@ int launch_one(const JKArgs &a, cudaStream_t s, int nsm, std::string &err)
         if constexpr (thread) {
                 jk_thread_kernel<LA, LB, LC, LD><<<cfg.grid, cfg.block, 0, s>>>(a);
         } else {
-                jk_warp_kernel<LA, LB, LC, LD><<<cfg.grid, cfg.block, cfg.smem, s>>>(a, 8);
+                jk_warp_kernel<LA, LB, LC, LD><<<cfg.grid, cfg.block, cfg.smem, s>>>(
+                        a, 8 * (32 / group_size<LA, LB, LC, LD>()));
         }
         cudaError_t e = cudaGetLastError();
         if (e != cudaSuccess) {

@@ -386,47 +386,58 @@ __device__ __forceinline__ void warp_slice_to_smem(double *h, double g00, const 
         }
 }
 
-template <int LA, int LB, int LC, int LD>
-__device__ __forceinline__ void warp_eval_block(double *sm, const JKArgs &a, int2 pb, int2 pk,
-                                                const double A[3], const double AB[3],
-                                                const double C[3], const double CD[3], double fac)
+// Lanes of one group (GS consecutive lanes of a warp) evaluate one quartet:
+// the (root, direction) slices of the 2D integrals are spread over the group,
+// then the Cartesian block is accumulated with components spread over it.
+// `gl` is the lane index inside the group, `gmask` the group's lane mask.
+template <int LA, int LB, int LC, int LD, int GS>
+__device__ __forceinline__ void group_eval_block(double *sm, const JKArgs &a, int2 pb, int2 pk,
+                                                 const double A[3], const double AB[3],
+                                                 const double C[3], const double CD[3], double fac,
+                                                 int gl, unsigned gmask)
 {
         using K = Class4<LA, LB, LC, LD>;
         using S = WarpSmem<LA, LB, LC, LD>;
-        const int lane = threadIdx.x & 31;
         double *G = sm + S::G;
         double *H = sm + S::H;
-        for (int t = lane; t < K::NG; t += 32) G[t] = 0.0;
+        for (int t = gl; t < K::NG; t += GS) G[t] = 0.0;
         for (int ip = 0; ip < pb.y; ip++) {
                 const double4 P = a.PP[pb.x + ip];
                 const double Kab = a.PK[pb.x + ip].x * fac;
                 for (int kp = 0; kp < pk.y; kp++) {
                         const double4 Q = a.PP[pk.x + kp];
                         const double Kcd = a.PK[pk.x + kp].x;
-                        __syncwarp();
-                        if (lane < 3 * K::NR) {
-                                const int r = lane / 3, dir = lane - 3 * r;
+                        __syncwarp(gmask);
+                        // one task per root (all three directions) when the slices
+                        // are small, else one per (root, direction)
+                        constexpr bool PER_ROOT = K::SA <= 16;
+                        constexpr int NTASK = PER_ROOT ? K::NR : 3 * K::NR;
+                        for (int task = gl; task < NTASK; task += GS) {
+                                const int r = PER_ROOT ? task : task / 3;
                                 const double PA[3] = {P.x - A[0], P.y - A[1], P.z - A[2]};
                                 const double QC[3] = {Q.x - C[0], Q.y - C[1], Q.z - C[2]};
                                 const double PQ[3] = {P.x - Q.x, P.y - Q.y, P.z - Q.z};
                                 const double p = P.w, q = Q.w;
                                 const double T = p * q / (p + q) * (PQ[0] * PQ[0] + PQ[1] * PQ[1] + PQ[2] * PQ[2]);
-                                double u[K::NR], w[K::NR];
-                                rys_roots<K::NR>(T, a.table, u, w);
-                                double ur = u[0], wr = w[0];
-#pragma unroll
-                                for (int i = 1; i < K::NR; i++)
-                                        if (r == i) { ur = u[i]; wr = w[i]; }
+                                double ur, wr;
+                                rys_root_one<K::NR>(T, a.table, r, ur, wr);
                                 RysCoef rc;
                                 rys_coef(rc, ur, p, q, PA, QC, PQ);
                                 const double pref = B2_TWO_PI_2P5 / (p * q * sqrt(p + q)) * Kab * Kcd;
-                                const double g00 = dir == 2 ? pref * wr : 1.0;
-                                const double abx = dir == 0 ? AB[0] : (dir == 1 ? AB[1] : AB[2]);
-                                const double cdx = dir == 0 ? CD[0] : (dir == 1 ? CD[1] : CD[2]);
-                                warp_slice_to_smem<LA, LB, LC, LD>(H + (dir * K::NR + r) * K::SA, g00, rc, dir, abx, cdx);
+                                if constexpr (PER_ROOT) {
+                                        warp_slice_to_smem<LA, LB, LC, LD>(H + (0 * K::NR + r) * K::SA, 1.0, rc, 0, AB[0], CD[0]);
+                                        warp_slice_to_smem<LA, LB, LC, LD>(H + (1 * K::NR + r) * K::SA, 1.0, rc, 1, AB[1], CD[1]);
+                                        warp_slice_to_smem<LA, LB, LC, LD>(H + (2 * K::NR + r) * K::SA, pref * wr, rc, 2, AB[2], CD[2]);
+                                } else {
+                                        const int dir = task - 3 * r;
+                                        const double g00 = dir == 2 ? pref * wr : 1.0;
+                                        const double abx = dir == 0 ? AB[0] : (dir == 1 ? AB[1] : AB[2]);
+                                        const double cdx = dir == 0 ? CD[0] : (dir == 1 ? CD[1] : CD[2]);
+                                        warp_slice_to_smem<LA, LB, LC, LD>(H + (dir * K::NR + r) * K::SA, g00, rc, dir, abx, cdx);
+                                }
                         }
-                        __syncwarp();
-                        for (int t = lane; t < K::NG; t += 32) {
+                        __syncwarp(gmask);
+                        for (int t = gl; t < K::NG; t += GS) {
                                 const int o = __ldg(a.goff + t);
                                 const int ox = o & 1023, oy = (o >> 10) & 1023, oz = o >> 20;
                                 double v = 0.0;
@@ -437,7 +448,15 @@ __device__ __forceinline__ void warp_eval_block(double *sm, const JKArgs &a, int
                         }
                 }
         }
-        __syncwarp();
+        __syncwarp(gmask);
+}
+
+// group size (lanes per quartet) of the shared-memory family for a class
+template <int LA, int LB, int LC, int LD>
+__host__ __device__ constexpr int group_size()
+{
+        using K = Class4<LA, LB, LC, LD>;
+        return K::NG <= 100 ? 8 : (K::NG <= 400 ? 16 : 32);
 }
 
 template <int LA, int LB, int LC, int LD>
@@ -445,10 +464,14 @@ __global__ void __launch_bounds__(128) jk_warp_kernel(JKArgs a, int chunk_q)
 {
         using K = Class4<LA, LB, LC, LD>;
         using S = WarpSmem<LA, LB, LC, LD>;
+        constexpr int GS = group_size<LA, LB, LC, LD>();
+        constexpr int NGRP = 32 / GS;
         extern __shared__ double smem_dyn[];
         const int lane = threadIdx.x & 31;
+        const int grp = lane / GS, gl = lane % GS;
+        const unsigned gmask = GS == 32 ? 0xffffffffu : (((1u << GS) - 1u) << (grp * GS));
         const int wib = threadIdx.x >> 5;
-        double *sm = smem_dyn + (size_t)wib * S::SIZE;
+        double *sm = smem_dyn + (size_t)(wib * NGRP + grp) * S::SIZE;
         const int nseg = a.bra.n * B2_NBUCKET;
         const long long total = a.chunk_off[nseg];
         const long long nwarps = ((long long)gridDim.x * blockDim.x) >> 5;
@@ -468,7 +491,7 @@ __global__ void __launch_bounds__(128) jk_warp_kernel(JKArgs a, int chunk_q)
                 const double4 ABb = a.bra.AB[ij];
                 const double A[3] = {Ab.x, Ab.y, Ab.z}, AB[3] = {ABb.x, ABb.y, ABb.z};
                 const int ia = sb.x, ib = sb.y;
-                for (int kl = kl0; kl < kl1; kl++) {
+                for (int kl = kl0 + grp; kl < kl1; kl += NGRP) {
                         const int4 sk = a.ket.sh[kl];
                         if (!quartet_passes(a, sb, qij, sk, a.ket.q[kl])) continue;
                         const int2 pk = a.ket.pr[kl];
@@ -479,9 +502,11 @@ __global__ void __launch_bounds__(128) jk_warp_kernel(JKArgs a, int chunk_q)
                         if (Ak.w != 0.0) fac *= 0.5;
                         if (a.same && ij == kl) fac *= 0.5;
                         const double C[3] = {Ak.x, Ak.y, Ak.z}, CD[3] = {CDk.x, CDk.y, CDk.z};
-                        warp_eval_block<LA, LB, LC, LD>(sm, a, pb, pk, A, AB, C, CD, fac);
-                        nq++;
-                        npq += (unsigned long long)pb.y * pk.y;
+                        group_eval_block<LA, LB, LC, LD, GS>(sm, a, pb, pk, A, AB, C, CD, fac, gl, gmask);
+                        if (gl == 0) {
+                                nq++;
+                                npq += (unsigned long long)pb.y * pk.y;
+                        }
                         const double *G = sm + S::G;
                         const int ic = sk.x, id = sk.y;
                         for (int s = 0; s < a.n_dm; s++) {
@@ -489,20 +514,20 @@ __global__ void __launch_bounds__(128) jk_warp_kernel(JKArgs a, int chunk_q)
                                         const double *Ds = a.Ds + s * nn;
                                         double *J = a.Jacc + s * nn;
                                         double *dsab = sm + S::DSAB, *dscd = sm + S::DSCD;
-                                        for (int t = lane; t < K::NAB; t += 32) dsab[t] = __ldg(Ds + (ia + t / K::NB) * n + ib + t % K::NB);
-                                        for (int t = lane; t < K::NCD; t += 32) dscd[t] = __ldg(Ds + (ic + t / K::ND) * n + id + t % K::ND);
-                                        __syncwarp();
-                                        for (int t = lane; t < K::NCD; t += 32) {
+                                        for (int t = gl; t < K::NAB; t += GS) dsab[t] = __ldg(Ds + (ia + t / K::NB) * n + ib + t % K::NB);
+                                        for (int t = gl; t < K::NCD; t += GS) dscd[t] = __ldg(Ds + (ic + t / K::ND) * n + id + t % K::ND);
+                                        __syncwarp(gmask);
+                                        for (int t = gl; t < K::NCD; t += GS) {
                                                 double v = 0.0;
                                                 for (int u = 0; u < K::NAB; u++) v += G[u * K::NCD + t] * dsab[u];
                                                 atomicAdd(J + (ic + t / K::ND) * n + id + t % K::ND, v);
                                         }
-                                        for (int t = lane; t < K::NAB; t += 32) {
+                                        for (int t = gl; t < K::NAB; t += GS) {
                                                 double v = 0.0;
                                                 for (int u = 0; u < K::NCD; u++) v += G[t * K::NCD + u] * dscd[u];
                                                 atomicAdd(J + (ia + t / K::NB) * n + ib + t % K::NB, v);
                                         }
-                                        __syncwarp();
+                                        __syncwarp(gmask);
                                 }
                                 if (a.with_k) {
                                         for (int tk = 0; tk < a.nk; tk++) {
@@ -510,13 +535,13 @@ __global__ void __launch_bounds__(128) jk_warp_kernel(JKArgs a, int chunk_q)
                                                 double *Kt = a.Kacc + (s * a.nk + tk) * nn;
                                                 double *xbc = sm + S::XBC, *xbd = sm + S::XBD;
                                                 double *xac = sm + S::XAC, *xad = sm + S::XAD;
-                                                for (int t = lane; t < K::NB * K::NC; t += 32) xbc[t] = __ldg(X + (ib + t / K::NC) * n + ic + t % K::NC);
-                                                for (int t = lane; t < K::NB * K::ND; t += 32) xbd[t] = __ldg(X + (ib + t / K::ND) * n + id + t % K::ND);
-                                                for (int t = lane; t < K::NA * K::NC; t += 32) xac[t] = __ldg(X + (ia + t / K::NC) * n + ic + t % K::NC);
-                                                for (int t = lane; t < K::NA * K::ND; t += 32) xad[t] = __ldg(X + (ia + t / K::ND) * n + id + t % K::ND);
-                                                __syncwarp();
+                                                for (int t = gl; t < K::NB * K::NC; t += GS) xbc[t] = __ldg(X + (ib + t / K::NC) * n + ic + t % K::NC);
+                                                for (int t = gl; t < K::NB * K::ND; t += GS) xbd[t] = __ldg(X + (ib + t / K::ND) * n + id + t % K::ND);
+                                                for (int t = gl; t < K::NA * K::NC; t += GS) xac[t] = __ldg(X + (ia + t / K::NC) * n + ic + t % K::NC);
+                                                for (int t = gl; t < K::NA * K::ND; t += GS) xad[t] = __ldg(X + (ia + t / K::ND) * n + id + t % K::ND);
+                                                __syncwarp(gmask);
                                                 // K[a,d] += G X[b,c]
-                                                for (int t = lane; t < K::NA * K::ND; t += 32) {
+                                                for (int t = gl; t < K::NA * K::ND; t += GS) {
                                                         const int x = t / K::ND, d = t % K::ND;
                                                         double v = 0.0;
                                                         for (int b = 0; b < K::NB; b++)
@@ -525,7 +550,7 @@ __global__ void __launch_bounds__(128) jk_warp_kernel(JKArgs a, int chunk_q)
                                                         atomicAdd(Kt + (ia + x) * n + id + d, v);
                                                 }
                                                 // K[a,c] += G X[b,d]
-                                                for (int t = lane; t < K::NA * K::NC; t += 32) {
+                                                for (int t = gl; t < K::NA * K::NC; t += GS) {
                                                         const int x = t / K::NC, c = t % K::NC;
                                                         double v = 0.0;
                                                         for (int b = 0; b < K::NB; b++)
@@ -534,7 +559,7 @@ __global__ void __launch_bounds__(128) jk_warp_kernel(JKArgs a, int chunk_q)
                                                         atomicAdd(Kt + (ia + x) * n + ic + c, v);
                                                 }
                                                 // K[b,d] += G X[a,c]
-                                                for (int t = lane; t < K::NB * K::ND; t += 32) {
+                                                for (int t = gl; t < K::NB * K::ND; t += GS) {
                                                         const int b = t / K::ND, d = t % K::ND;
                                                         double v = 0.0;
                                                         for (int x = 0; x < K::NA; x++)
@@ -543,7 +568,7 @@ __global__ void __launch_bounds__(128) jk_warp_kernel(JKArgs a, int chunk_q)
                                                         atomicAdd(Kt + (ib + b) * n + id + d, v);
                                                 }
                                                 // K[b,c] += G X[a,d]
-                                                for (int t = lane; t < K::NB * K::NC; t += 32) {
+                                                for (int t = gl; t < K::NB * K::NC; t += GS) {
                                                         const int b = t / K::NC, c = t % K::NC;
                                                         double v = 0.0;
                                                         for (int x = 0; x < K::NA; x++)
@@ -551,13 +576,13 @@ __global__ void __launch_bounds__(128) jk_warp_kernel(JKArgs a, int chunk_q)
                                                                         v += G[((x * K::NB + b) * K::NC + c) * K::ND + d] * xad[x * K::ND + d];
                                                         atomicAdd(Kt + (ib + b) * n + ic + c, v);
                                                 }
-                                                __syncwarp();
+                                                __syncwarp(gmask);
                                         }
                                 }
                         }
                 }
         }
-        if (a.stats && lane == 0 && nq) {
+        if (a.stats && gl == 0 && nq) {
                 atomicAdd(a.stats + 0, nq);
                 atomicAdd(a.stats + 1, npq);
         }
@@ -598,7 +623,7 @@ __global__ void __launch_bounds__(32) qcond_kernel(QArgs q)
         const double4 Av = q.pairs.A[ij];
         const double4 ABv = q.pairs.AB[ij];
         const double A[3] = {Av.x, Av.y, Av.z}, AB[3] = {ABv.x, ABv.y, ABv.z};
-        warp_eval_block<LA, LB, LA, LB>(sm, a, pr, pr, A, AB, A, AB, 1.0);
+        group_eval_block<LA, LB, LA, LB, 32>(sm, a, pr, pr, A, AB, A, AB, 1.0, lane, 0xffffffffu);
         const double *G = sm + S::G;
         const int nsa = q.cart ? K::NA : 2 * LA + 1, nsb = q.cart ? K::NB : 2 * LB + 1;
         const double *ca = q.c2s + LA * 100, *cb = q.c2s + LB * 100;

@@ -15,7 +15,17 @@ inline int family_is_thread(int la, int lb, int lc, int ld)
         const int sa = (la + 1) * (lb + 1) * (lc + 1) * (ld + 1);
         return (ng + 3 * sa) <= 80;
 }
-inline int family_chunk(int la, int lb, int lc, int ld) { return family_is_thread(la, lb, lc, ld) ? 32 : 8; }
+// lanes per quartet of the shared-memory family (group_size<> in jk_kernels.cuh)
+inline int family_group(int la, int lb, int lc, int ld)
+{
+        const int ng = ncart(la) * ncart(lb) * ncart(lc) * ncart(ld);
+        return ng <= 100 ? 8 : (ng <= 400 ? 16 : 32);
+}
+// quartets per chunk: 32 (one per lane) or 8 per group of the warp
+inline int family_chunk(int la, int lb, int lc, int ld)
+{
+        return family_is_thread(la, lb, lc, ld) ? 32 : 8 * (32 / family_group(la, lb, lc, ld));
+}
 
 // one launcher per quartet class (la lb | lc ld), (lc, ld) <= (la, lb)
 int launch_jk_0000(const JKArgs &a, cudaStream_t s, int nsm, std::string &err);

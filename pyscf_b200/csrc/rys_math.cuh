@@ -125,6 +125,34 @@ B2_HD void rys_roots(double T, const double *__restrict__ table, double *u, doub
         }
 }
 
+// Root r (and its weight) of the order-NR rule only.
+template <int NR>
+B2_HD void rys_root_one(double T, const double *__restrict__ table, int r, double &u, double &w)
+{
+        if (!(T < (double)rys_t_asym(NR))) {
+                const double it = 1.0 / T;
+                double x2 = rys_herm_x2(NR * (NR - 1) / 2), wh = rys_herm_w(NR * (NR - 1) / 2);
+#pragma unroll
+                for (int i = 1; i < NR; i++)
+                        if (r == i) { x2 = rys_herm_x2(NR * (NR - 1) / 2 + i); wh = rys_herm_w(NR * (NR - 1) / 2 + i); }
+                u = x2 * it;
+                w = wh * sqrt(it);
+                return;
+        }
+        const int p = (int)T;
+        const double x = 2.0 * (T - (double)p) - 1.0;
+        const double *cu = table + rys_table_offset(NR) + p * (2 * NR * (RYS_DEG + 1)) + r * (RYS_DEG + 1);
+        const double *cw = cu + NR * (RYS_DEG + 1);
+        double a = B2_LDG(cu + RYS_DEG), b = B2_LDG(cw + RYS_DEG);
+#pragma unroll
+        for (int k = RYS_DEG - 1; k >= 0; k--) {
+                a = fma(a, x, B2_LDG(cu + k));
+                b = fma(b, x, B2_LDG(cw + k));
+        }
+        u = a;
+        w = b;
+}
+
 // 2D vertical recurrence: g[e*NF + f], e < NE, f < NF.
 template <int NE, int NF>
 B2_HD void vrr2d(double *g, double g00, double c00, double c00p, double b10, double b01, double b00)
