@@ -8,7 +8,7 @@
 //                 shell (nctr > 1) becomes nctr segments sharing its exponents;
 //   shell pairs   unordered segment pairs, oriented la >= lb, grouped into 10
 //                 angular classes, sorted by the parent-shell Schwarz bound;
-//   prim pairs    (P, p, K_ab c_a c_b, a) per surviving primitive pair
+//   prim pairs    (P, p, K_ab c_a c_b, 1/(2p)) per surviving primitive pair
 //                 (exp(-ab/(a+b) |AB|^2) >= e^-60, the libcint default cutoff);
 //   q_cond        CVHFnr_int2e_q_cond on parent shells, computed on the GPU.
 #include <cuda_runtime.h>
@@ -58,7 +58,7 @@ static const int LMAX = 3;
 static const int NPAIRCLASS = (LMAX + 1) * (LMAX + 2) / 2;
 static inline int pair_class(int la, int lb) { return la * (la + 1) / 2 + lb; }
 
-__device__ double d_rys_table[RYS_TABLE_SIZE];
+__device__ __align__(32) double d_rys_table[rys_padded_size()];
 
 // ---------------------------------------------------------------------------
 // real solid harmonics r^l Y_lm (unit-normalised Y_lm), rows m = -l..l
@@ -336,8 +336,10 @@ static int ensure_tables(int device)
 {
         if (device < 0 || device >= 64) return fail(B200JK_EINVAL, "device index out of range");
         std::call_once(g_table_once[device], [device]() {
-                g_table_status[device] = (cudaMemcpyToSymbol(d_rys_table, rys_table_data,
-                                                             sizeof(double) * RYS_TABLE_SIZE) == cudaSuccess)
+                std::vector<double> padded(rys_padded_size());
+                rys_pad_table(rys_table_data, padded.data());
+                g_table_status[device] = (cudaMemcpyToSymbol(d_rys_table, padded.data(),
+                                                             sizeof(double) * padded.size()) == cudaSuccess)
                                                  ? 0 : 1;
         });
         if (g_table_status[device]) return fail(B200JK_ECUDA, "could not upload the Rys tables");
@@ -521,7 +523,7 @@ int b200jk_plan_create(const int32_t *atm, int natm, const int32_t *bas, int nba
                                         P4.z = (a * A.R[2] + b * B.R[2]) / p;
                                         P4.w = p;
                                         hPP.push_back(P4);
-                                        hPK.push_back(make_double2(cc * exp(-mu * rr), a));
+                                        hPK.push_back(make_double2(cc * exp(-mu * rr), 0.5 / p));
                                         hp.nprim++;
                                 }
                         }

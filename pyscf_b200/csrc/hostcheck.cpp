@@ -20,7 +20,18 @@ namespace {
 
 enum { PTR_COORD = 1, ATM_SLOTS = 6 };
 enum { ATOM_OF = 0, ANG_OF = 1, NPRIM_OF = 2, NCTR_OF = 3, PTR_EXP = 5, PTR_COEFF = 6, BAS_SLOTS = 8 };
-constexpr double kTwoPi2p5 = 34.98683665524972497;   // 2 pi^{5/2}
+
+// the padded device layout, built once
+const double *padded_table()
+{
+        alignas(32) static double t[rys_padded_size()];
+        static bool done = false;
+        if (!done) {
+                rys_pad_table(rys_table_data, t);
+                done = true;
+        }
+        return t;
+}
 
 struct HSeg {
         int l, nprim;
@@ -50,8 +61,9 @@ void host_quartet(const HSeg *s, double *out)
                         const double c = s[2].exp[k], d = s[3].exp[l], q = c + d;
                         const double Q[3] = {(c * C[0] + d * D[0]) / q, (c * C[1] + d * D[1]) / q, (c * C[2] + d * D[2]) / q};
                         const double Kcd = s[2].coef[k] * s[3].coef[l] * exp(-c * d / q * rcd);
-                        const double pref = kTwoPi2p5 / (p * q * sqrt(p + q)) * Kab * Kcd;
-                        add_prim_quartet<LA, LB, LC, LD>(G.data(), rys_table_data, p, P, q, Q, A, C, AB, CD, pref);
+                        PrimQ sq;
+                        prim_setup(sq, p, 0.5 / p, P, q, 0.5 / q, Q, A, C, Kab * Kcd);
+                        add_prim_quartet<LA, LB, LC, LD>(G.data(), padded_table(), sq, AB, CD);
                 }
         }
         memcpy(out, G.data(), sizeof(double) * K::NG);

@@ -23,7 +23,8 @@ template <int LA, int LB, int LC, int LD>
 int launch_one(const JKArgs &a, cudaStream_t s, int nsm, std::string &err)
 {
         using K = Class4<LA, LB, LC, LD>;
-        constexpr bool thread = (K::NG + 3 * K::SA) <= 80;
+        constexpr int NP = thread_parts<LA, LB, LC, LD>();
+        constexpr bool thread = NP > 0;
         static LaunchCfg cfg;
         static std::mutex mu;
         {
@@ -33,7 +34,7 @@ int launch_one(const JKArgs &a, cudaStream_t s, int nsm, std::string &err)
                         if constexpr (thread) {
                                 cfg.block = 128;
                                 cfg.smem = 0;
-                                cfg.status = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, jk_thread_kernel<LA, LB, LC, LD>, 128, 0);
+                                cfg.status = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, jk_thread_kernel<LA, LB, LC, LD, (NP > 0 ? NP : 1)>, 128, 0);
                         } else {
                                 const size_t per_warp = sizeof(double) * WarpSmem<LA, LB, LC, LD>::SIZE *
                                                         (32 / group_size<LA, LB, LC, LD>());
@@ -55,7 +56,7 @@ int launch_one(const JKArgs &a, cudaStream_t s, int nsm, std::string &err)
                 return 1;
         }
         if constexpr (thread) {
-                jk_thread_kernel<LA, LB, LC, LD><<<cfg.grid, cfg.block, 0, s>>>(a);
+                jk_thread_kernel<LA, LB, LC, LD, NP><<<cfg.grid, cfg.block, 0, s>>>(a);
         } else {
                 jk_warp_kernel<LA, LB, LC, LD><<<cfg.grid, cfg.block, cfg.smem, s>>>(
                         a, 8 * (32 / group_size<LA, LB, LC, LD>()));

@@ -23,6 +23,8 @@
 // symmetric D).  These are the images PySCF's 'ji->s2kl' and 'li->s2kj' /
 // 'li->s1kj' scripts accumulate (pyscf/lib/vhf/nr_direct_dot.c:1293-1647).
 #pragma once
+#include <type_traits>
+#include <utility>
 #include "rys_math.cuh"
 
 namespace b200jk {
@@ -50,7 +52,7 @@ struct PairView {
 struct JKArgs {
         PairView bra, ket;
         const double4 *PP;           // primitive pair (P, p)
-        const double2 *PK;           // primitive pair (K_ab c_i c_j, a_i)
+        const double2 *PK;           // primitive pair (K_ab c_i c_j, 1/(2p))
         const long long *chunk_off;  // bra.n * B2_NBUCKET + 1 entries
         const int *nkl;              // per (bra pair, ket bucket)
         const double *dm_cond;       // nbas x nbas (parent shells)
@@ -133,11 +135,25 @@ static __global__ void count_kernel(PairView bra, PairView ket, int same, double
 }
 
 // ---------------------------------------------------------------------------
-// Thread-per-quartet family: the whole Cartesian block lives in registers.
-template <int LA, int LB, int LC, int LD>
+// Thread-per-quartet family: one quartet per lane, the Cartesian block in
+// registers.  Mid-size classes keep one part of the block at a time: the
+// block is cut into NP parts along the first (bra) index; each part re-runs
+// the primitive loop (roots and recurrences are cheap next to the assembly)
+// and is contracted before the next, so only NG/NP integrals are live.
+
+template <typename F, int... Ps>
+__device__ __forceinline__ void for_parts(F &&f, std::integer_sequence<int, Ps...>)
+{
+        (f(std::integral_constant<int, Ps>{}), ...);
+}
+
+template <int LA, int LB, int LC, int LD, int NP>
 __global__ void __launch_bounds__(128) jk_thread_kernel(JKArgs a)
 {
         using K = Class4<LA, LB, LC, LD>;
+        static_assert(K::NA % NP == 0, "parts must divide the bra components");
+        constexpr int NAP = K::NA / NP;            // bra components per part
+        constexpr int NGP = NAP * K::NB * K::NCD;  // integrals per part
         const int lane = threadIdx.x & 31;
         const int nseg = a.bra.n * B2_NBUCKET;
         const long long total = a.chunk_off[nseg];
@@ -157,161 +173,175 @@ __global__ void __launch_bounds__(128) jk_thread_kernel(JKArgs a)
                 const double4 ABb = a.bra.AB[ij];
                 bool active = pos < a.nkl[sgi];
                 int4 sk = make_int4(0, 0, 0, 0);
-                double G[K::NG];
-#pragma unroll
-                for (int t = 0; t < K::NG; t++) G[t] = 0.0;
                 if (active) {
                         sk = a.ket.sh[kl];
                         active = quartet_passes(a, sb, qij, sk, a.ket.q[kl]);
                 }
+                int2 pk = make_int2(0, 0);
+                double fac = 1.0;
+                double C[3] = {0, 0, 0}, CD[3] = {0, 0, 0};
+                const double A[3] = {Ab.x, Ab.y, Ab.z}, AB[3] = {ABb.x, ABb.y, ABb.z};
                 if (active) {
-                        const int2 pk = a.ket.pr[kl];
+                        pk = a.ket.pr[kl];
                         const double4 Ak = a.ket.A[kl];
                         const double4 CDk = a.ket.AB[kl];
-                        double fac = 1.0;
                         if (Ab.w != 0.0) fac *= 0.5;
                         if (Ak.w != 0.0) fac *= 0.5;
                         if (a.same && ij == kl) fac *= 0.5;
-                        const double A[3] = {Ab.x, Ab.y, Ab.z}, AB[3] = {ABb.x, ABb.y, ABb.z};
-                        const double C[3] = {Ak.x, Ak.y, Ak.z}, CD[3] = {CDk.x, CDk.y, CDk.z};
+                        C[0] = Ak.x; C[1] = Ak.y; C[2] = Ak.z;
+                        CD[0] = CDk.x; CD[1] = CDk.y; CD[2] = CDk.z;
                         nq++;
-                        for (int ip = 0; ip < pb.y; ip++) {
-                                const double4 P = a.PP[pb.x + ip];
-                                const double Kab = a.PK[pb.x + ip].x * fac;
-                                const double Pv[3] = {P.x, P.y, P.z};
-                                for (int kp = 0; kp < pk.y; kp++) {
-                                        const double4 Q = a.PP[pk.x + kp];
-                                        const double Kcd = a.PK[pk.x + kp].x;
-                                        const double Qv[3] = {Q.x, Q.y, Q.z};
-                                        const double pref = B2_TWO_PI_2P5 / (P.w * Q.w * sqrt(P.w + Q.w)) * Kab * Kcd;
-                                        add_prim_quartet<LA, LB, LC, LD>(G, a.table, P.w, Pv, Q.w, Qv, A, C, AB, CD, pref);
-                                }
-                        }
                         npq += (unsigned long long)pb.y * pk.y;
                 }
                 const int ia = sb.x, ib = sb.y, ic = sk.x, id = sk.y;
-                for (int s = 0; s < a.n_dm; s++) {
-                        if (a.with_j) {
-                                const double *Ds = a.Ds + s * nn;
-                                double *J = a.Jacc + s * nn;
-                                if (active) {
-                                        double dab[K::NAB];
+                for_parts([&](auto part_tag) {
+                        constexpr int PART = decltype(part_tag)::value;
+                        constexpr int A0 = PART * NAP;
+                        double Gp[NGP];
 #pragma unroll
-                                        for (int x = 0; x < K::NA; x++)
+                        for (int t = 0; t < NGP; t++) Gp[t] = 0.0;
+                        if (active) {
+                                for (int ip = 0; ip < pb.y; ip++) {
+                                        const double4 P = a.PP[pb.x + ip];
+                                        const double2 KP = a.PK[pb.x + ip];
+                                        const double Kab = KP.x * fac;
+                                        const double Pv[3] = {P.x, P.y, P.z};
+                                        for (int kp = 0; kp < pk.y; kp++) {
+                                                const double4 Q = a.PP[pk.x + kp];
+                                                const double2 KQ = a.PK[pk.x + kp];
+                                                const double Qv[3] = {Q.x, Q.y, Q.z};
+                                                PrimQ sq;
+                                                prim_setup(sq, P.w, KP.y, Pv, Q.w, KQ.y, Qv, A, C, Kab * KQ.x);
+                                                add_prim_quartet_part<LA, LB, LC, LD, PART * NGP, NGP>(Gp, a.table, sq, AB, CD);
+                                        }
+                                }
+                        }
+                        // Gp[((x*NB + b)*NC + c)*ND + d] holds bra component A0 + x
+                        for (int s = 0; s < a.n_dm; s++) {
+                                if (a.with_j) {
+                                        const double *Ds = a.Ds + s * nn;
+                                        double *J = a.Jacc + s * nn;
+                                        if (active) {
+                                                double dab[NAP * K::NB];
 #pragma unroll
-                                                for (int y = 0; y < K::NB; y++) dab[x * K::NB + y] = __ldg(Ds + (ia + x) * n + ib + y);
+                                                for (int x = 0; x < NAP; x++)
+#pragma unroll
+                                                        for (int y = 0; y < K::NB; y++)
+                                                                dab[x * K::NB + y] = __ldg(Ds + (ia + A0 + x) * n + ib + y);
+#pragma unroll
+                                                for (int x = 0; x < K::NC; x++)
+#pragma unroll
+                                                for (int y = 0; y < K::ND; y++) {
+                                                        double v = 0.0;
+#pragma unroll
+                                                        for (int t = 0; t < NAP * K::NB; t++) v += Gp[t * K::NCD + x * K::ND + y] * dab[t];
+                                                        atomicAdd(J + (ic + x) * n + id + y, v);
+                                                }
+                                        }
+                                        double dcd[K::NCD];
 #pragma unroll
                                         for (int x = 0; x < K::NC; x++)
 #pragma unroll
-                                        for (int y = 0; y < K::ND; y++) {
+                                                for (int y = 0; y < K::ND; y++)
+                                                        dcd[x * K::ND + y] = active ? __ldg(Ds + (ic + x) * n + id + y) : 0.0;
+#pragma unroll
+                                        for (int t = 0; t < NAP * K::NB; t++) {
                                                 double v = 0.0;
 #pragma unroll
-                                                for (int t = 0; t < K::NAB; t++) v += G[t * K::NCD + x * K::ND + y] * dab[t];
-                                                atomicAdd(J + (ic + x) * n + id + y, v);
+                                                for (int u = 0; u < K::NCD; u++) v += Gp[t * K::NCD + u] * dcd[u];
+                                                v = warp_sum(v);
+                                                if (lane == 0 && v != 0.0)
+                                                        atomicAdd(J + (ia + A0 + t / K::NB) * n + ib + t % K::NB, v);
                                         }
                                 }
-                                double dcd[K::NCD];
-#pragma unroll
-                                for (int x = 0; x < K::NC; x++)
-#pragma unroll
-                                        for (int y = 0; y < K::ND; y++)
-                                                dcd[x * K::ND + y] = active ? __ldg(Ds + (ic + x) * n + id + y) : 0.0;
-#pragma unroll
-                                for (int t = 0; t < K::NAB; t++) {
-                                        double v = 0.0;
-#pragma unroll
-                                        for (int u = 0; u < K::NCD; u++) v += G[t * K::NCD + u] * dcd[u];
-                                        v = warp_sum(v);
-                                        if (lane == 0 && v != 0.0) atomicAdd(J + (ia + t / K::NB) * n + ib + t % K::NB, v);
-                                }
-                        }
-                        if (a.with_k && active) {
-                                for (int t = 0; t < a.nk; t++) {
-                                        const double *X = a.Dk + (s * a.nk + t) * nn;
-                                        double *Kt = a.Kacc + (s * a.nk + t) * nn;
-                                        // K[a,d] += G X[b,c]
-                                        {
-                                                double x_[K::NB * K::NC];
-#pragma unroll
-                                                for (int b = 0; b < K::NB; b++)
-#pragma unroll
-                                                        for (int c = 0; c < K::NC; c++) x_[b * K::NC + c] = __ldg(X + (ib + b) * n + ic + c);
-#pragma unroll
-                                                for (int x = 0; x < K::NA; x++)
-#pragma unroll
-                                                for (int d = 0; d < K::ND; d++) {
-                                                        double v = 0.0;
+                                if (a.with_k && active) {
+                                        for (int tk = 0; tk < a.nk; tk++) {
+                                                const double *X = a.Dk + (s * a.nk + tk) * nn;
+                                                double *Kt = a.Kacc + (s * a.nk + tk) * nn;
+                                                // K[a,d] += G X[b,c]
+                                                {
+                                                        double x_[K::NB * K::NC];
 #pragma unroll
                                                         for (int b = 0; b < K::NB; b++)
 #pragma unroll
-                                                                for (int c = 0; c < K::NC; c++)
-                                                                        v += G[((x * K::NB + b) * K::NC + c) * K::ND + d] * x_[b * K::NC + c];
-                                                        atomicAdd(Kt + (ia + x) * n + id + d, v);
+                                                                for (int c = 0; c < K::NC; c++) x_[b * K::NC + c] = __ldg(X + (ib + b) * n + ic + c);
+#pragma unroll
+                                                        for (int x = 0; x < NAP; x++)
+#pragma unroll
+                                                        for (int d = 0; d < K::ND; d++) {
+                                                                double v = 0.0;
+#pragma unroll
+                                                                for (int b = 0; b < K::NB; b++)
+#pragma unroll
+                                                                        for (int c = 0; c < K::NC; c++)
+                                                                                v += Gp[((x * K::NB + b) * K::NC + c) * K::ND + d] * x_[b * K::NC + c];
+                                                                atomicAdd(Kt + (ia + A0 + x) * n + id + d, v);
+                                                        }
                                                 }
-                                        }
-                                        // K[a,c] += G X[b,d]
-                                        {
-                                                double x_[K::NB * K::ND];
-#pragma unroll
-                                                for (int b = 0; b < K::NB; b++)
-#pragma unroll
-                                                        for (int d = 0; d < K::ND; d++) x_[b * K::ND + d] = __ldg(X + (ib + b) * n + id + d);
-#pragma unroll
-                                                for (int x = 0; x < K::NA; x++)
-#pragma unroll
-                                                for (int c = 0; c < K::NC; c++) {
-                                                        double v = 0.0;
+                                                // K[a,c] += G X[b,d]
+                                                {
+                                                        double x_[K::NB * K::ND];
 #pragma unroll
                                                         for (int b = 0; b < K::NB; b++)
 #pragma unroll
-                                                                for (int d = 0; d < K::ND; d++)
-                                                                        v += G[((x * K::NB + b) * K::NC + c) * K::ND + d] * x_[b * K::ND + d];
-                                                        atomicAdd(Kt + (ia + x) * n + ic + c, v);
+                                                                for (int d = 0; d < K::ND; d++) x_[b * K::ND + d] = __ldg(X + (ib + b) * n + id + d);
+#pragma unroll
+                                                        for (int x = 0; x < NAP; x++)
+#pragma unroll
+                                                        for (int c = 0; c < K::NC; c++) {
+                                                                double v = 0.0;
+#pragma unroll
+                                                                for (int b = 0; b < K::NB; b++)
+#pragma unroll
+                                                                        for (int d = 0; d < K::ND; d++)
+                                                                                v += Gp[((x * K::NB + b) * K::NC + c) * K::ND + d] * x_[b * K::ND + d];
+                                                                atomicAdd(Kt + (ia + A0 + x) * n + ic + c, v);
+                                                        }
                                                 }
-                                        }
-                                        // K[b,d] += G X[a,c]
-                                        {
-                                                double x_[K::NA * K::NC];
+                                                // K[b,d] += G X[a,c]  (this part's a only)
+                                                {
+                                                        double x_[NAP * K::NC];
 #pragma unroll
-                                                for (int x = 0; x < K::NA; x++)
+                                                        for (int x = 0; x < NAP; x++)
 #pragma unroll
-                                                        for (int c = 0; c < K::NC; c++) x_[x * K::NC + c] = __ldg(X + (ia + x) * n + ic + c);
+                                                                for (int c = 0; c < K::NC; c++) x_[x * K::NC + c] = __ldg(X + (ia + A0 + x) * n + ic + c);
 #pragma unroll
-                                                for (int b = 0; b < K::NB; b++)
+                                                        for (int b = 0; b < K::NB; b++)
 #pragma unroll
-                                                for (int d = 0; d < K::ND; d++) {
-                                                        double v = 0.0;
+                                                        for (int d = 0; d < K::ND; d++) {
+                                                                double v = 0.0;
 #pragma unroll
-                                                        for (int x = 0; x < K::NA; x++)
+                                                                for (int x = 0; x < NAP; x++)
 #pragma unroll
-                                                                for (int c = 0; c < K::NC; c++)
-                                                                        v += G[((x * K::NB + b) * K::NC + c) * K::ND + d] * x_[x * K::NC + c];
-                                                        atomicAdd(Kt + (ib + b) * n + id + d, v);
+                                                                        for (int c = 0; c < K::NC; c++)
+                                                                                v += Gp[((x * K::NB + b) * K::NC + c) * K::ND + d] * x_[x * K::NC + c];
+                                                                atomicAdd(Kt + (ib + b) * n + id + d, v);
+                                                        }
                                                 }
-                                        }
-                                        // K[b,c] += G X[a,d]
-                                        {
-                                                double x_[K::NA * K::ND];
+                                                // K[b,c] += G X[a,d]  (this part's a only)
+                                                {
+                                                        double x_[NAP * K::ND];
 #pragma unroll
-                                                for (int x = 0; x < K::NA; x++)
+                                                        for (int x = 0; x < NAP; x++)
 #pragma unroll
-                                                        for (int d = 0; d < K::ND; d++) x_[x * K::ND + d] = __ldg(X + (ia + x) * n + id + d);
+                                                                for (int d = 0; d < K::ND; d++) x_[x * K::ND + d] = __ldg(X + (ia + A0 + x) * n + id + d);
 #pragma unroll
-                                                for (int b = 0; b < K::NB; b++)
+                                                        for (int b = 0; b < K::NB; b++)
 #pragma unroll
-                                                for (int c = 0; c < K::NC; c++) {
-                                                        double v = 0.0;
+                                                        for (int c = 0; c < K::NC; c++) {
+                                                                double v = 0.0;
 #pragma unroll
-                                                        for (int x = 0; x < K::NA; x++)
+                                                                for (int x = 0; x < NAP; x++)
 #pragma unroll
-                                                                for (int d = 0; d < K::ND; d++)
-                                                                        v += G[((x * K::NB + b) * K::NC + c) * K::ND + d] * x_[x * K::ND + d];
-                                                        atomicAdd(Kt + (ib + b) * n + ic + c, v);
+                                                                        for (int d = 0; d < K::ND; d++)
+                                                                                v += Gp[((x * K::NB + b) * K::NC + c) * K::ND + d] * x_[x * K::ND + d];
+                                                                atomicAdd(Kt + (ib + b) * n + ic + c, v);
+                                                        }
                                                 }
                                         }
                                 }
                         }
-                }
+                }, std::make_integer_sequence<int, NP>{});
         }
         if (a.stats) {
                 for (int o = 16; o > 0; o >>= 1) {
@@ -323,6 +353,19 @@ __global__ void __launch_bounds__(128) jk_thread_kernel(JKArgs a)
                         atomicAdd(a.stats + 1, npq);
                 }
         }
+}
+
+// Parts of the register family for a class: 0 = class goes to the shared-
+// memory family.  Budget: live integrals of a part plus the three 2D slices
+// of one root.
+template <int LA, int LB, int LC, int LD>
+__host__ __device__ constexpr int thread_parts()
+{
+        using K = Class4<LA, LB, LC, LD>;
+        if (K::SA > 18 || K::NR > 4) return (K::NG + 3 * K::SA <= 80) ? 1 : 0;
+        for (int np = 1; np <= K::NA && np <= 5; np++)
+                if (K::NA % np == 0 && K::NG / np + 3 * K::SA <= (np == 1 ? 80 : 72)) return np;
+        return 0;
 }
 
 // ---------------------------------------------------------------------------
@@ -403,10 +446,13 @@ __device__ __forceinline__ void group_eval_block(double *sm, const JKArgs &a, in
         for (int t = gl; t < K::NG; t += GS) G[t] = 0.0;
         for (int ip = 0; ip < pb.y; ip++) {
                 const double4 P = a.PP[pb.x + ip];
-                const double Kab = a.PK[pb.x + ip].x * fac;
+                const double2 KP = a.PK[pb.x + ip];
+                const double Kab = KP.x * fac;
+                const double Pv[3] = {P.x, P.y, P.z};
                 for (int kp = 0; kp < pk.y; kp++) {
                         const double4 Q = a.PP[pk.x + kp];
-                        const double Kcd = a.PK[pk.x + kp].x;
+                        const double2 KQ = a.PK[pk.x + kp];
+                        const double Qv[3] = {Q.x, Q.y, Q.z};
                         __syncwarp(gmask);
                         // one task per root (all three directions) when the slices
                         // are small, else one per (root, direction)
@@ -414,16 +460,13 @@ __device__ __forceinline__ void group_eval_block(double *sm, const JKArgs &a, in
                         constexpr int NTASK = PER_ROOT ? K::NR : 3 * K::NR;
                         for (int task = gl; task < NTASK; task += GS) {
                                 const int r = PER_ROOT ? task : task / 3;
-                                const double PA[3] = {P.x - A[0], P.y - A[1], P.z - A[2]};
-                                const double QC[3] = {Q.x - C[0], Q.y - C[1], Q.z - C[2]};
-                                const double PQ[3] = {P.x - Q.x, P.y - Q.y, P.z - Q.z};
-                                const double p = P.w, q = Q.w;
-                                const double T = p * q / (p + q) * (PQ[0] * PQ[0] + PQ[1] * PQ[1] + PQ[2] * PQ[2]);
+                                PrimQ sq;
+                                prim_setup(sq, P.w, KP.y, Pv, Q.w, KQ.y, Qv, A, C, Kab * KQ.x);
                                 double ur, wr;
-                                rys_root_one<K::NR>(T, a.table, r, ur, wr);
+                                rys_root_one<K::NR>(sq.T, a.table, r, ur, wr);
                                 RysCoef rc;
-                                rys_coef(rc, ur, p, q, PA, QC, PQ);
-                                const double pref = B2_TWO_PI_2P5 / (p * q * sqrt(p + q)) * Kab * Kcd;
+                                rys_coef(rc, ur, sq);
+                                const double pref = sq.pref;
                                 if constexpr (PER_ROOT) {
                                         warp_slice_to_smem<LA, LB, LC, LD>(H + (0 * K::NR + r) * K::SA, 1.0, rc, 0, AB[0], CD[0]);
                                         warp_slice_to_smem<LA, LB, LC, LD>(H + (1 * K::NR + r) * K::SA, 1.0, rc, 1, AB[1], CD[1]);

@@ -9,12 +9,20 @@
 namespace b200jk {
 
 // quartets per chunk of the kernel family used for class (la lb | lc ld)
-inline int family_is_thread(int la, int lb, int lc, int ld)
+// host twin of thread_parts<> (jk_kernels.cuh): parts of the register
+// family, 0 for the shared-memory family
+inline int family_thread_parts(int la, int lb, int lc, int ld)
 {
-        const int ng = ncart(la) * ncart(lb) * ncart(lc) * ncart(ld);
+        const int na = ncart(la);
+        const int ng = na * ncart(lb) * ncart(lc) * ncart(ld);
         const int sa = (la + 1) * (lb + 1) * (lc + 1) * (ld + 1);
-        return (ng + 3 * sa) <= 80;
+        const int nr = (la + lb + lc + ld) / 2 + 1;
+        if (sa > 18 || nr > 4) return (ng + 3 * sa <= 80) ? 1 : 0;
+        for (int np = 1; np <= na && np <= 5; np++)
+                if (na % np == 0 && ng / np + 3 * sa <= (np == 1 ? 80 : 72)) return np;
+        return 0;
 }
+inline int family_is_thread(int la, int lb, int lc, int ld) { return family_thread_parts(la, lb, lc, ld) > 0; }
 // lanes per quartet of the shared-memory family (group_size<> in jk_kernels.cuh)
 inline int family_group(int la, int lb, int lc, int ld)
 {

@@ -95,9 +95,50 @@ B2_HDC double rys_herm_w(int k)
         return t[k];
 }
 
-// Roots u[i] and weights w[i] of the order-NR Rys rule at argument T.
-// NaN or huge T take the asymptotic branch, so the table is never indexed
-// out of range.
+// Device layout of the tables: every polynomial row padded from RYS_DEG+1 to
+// RYS_ROW coefficients so that a row is four aligned 32-byte vectors.
+#define RYS_ROW 16
+B2_HDC int rys_padded_offset(int n)
+{
+        int o = 0;
+        for (int m = 1; m < n; m++) o += rys_t_asym(m) * 2 * m * RYS_ROW;
+        return o;
+}
+B2_HDC int rys_padded_size() { return rys_padded_offset(RYS_NMAX + 1); }
+
+// packed generator table -> padded layout
+inline void rys_pad_table(const double *packed, double *out)
+{
+        for (int n = 1; n <= RYS_NMAX; n++) {
+                const double *src = packed + rys_table_offset(n);
+                double *dst = out + rys_padded_offset(n);
+                for (int row = 0; row < rys_t_asym(n) * 2 * n; row++) {
+                        for (int k = 0; k < RYS_ROW; k++)
+                                dst[row * RYS_ROW + k] = k <= RYS_DEG ? src[row * (RYS_DEG + 1) + k] : 0.0;
+                }
+        }
+}
+
+struct alignas(32) RysRow4 {
+        double v[4];
+};
+
+// Horner evaluation of one padded row at x
+B2_HD double rys_poly(const double *__restrict__ row, double x)
+{
+        const RysRow4 *q = reinterpret_cast<const RysRow4 *>(row);
+        const RysRow4 q0 = q[0], q1 = q[1], q2 = q[2], q3 = q[3];
+        double r = q3.v[1];
+        r = fma(r, x, q3.v[0]);
+        r = fma(r, x, q2.v[3]); r = fma(r, x, q2.v[2]); r = fma(r, x, q2.v[1]); r = fma(r, x, q2.v[0]);
+        r = fma(r, x, q1.v[3]); r = fma(r, x, q1.v[2]); r = fma(r, x, q1.v[1]); r = fma(r, x, q1.v[0]);
+        r = fma(r, x, q0.v[3]); r = fma(r, x, q0.v[2]); r = fma(r, x, q0.v[1]); r = fma(r, x, q0.v[0]);
+        return r;
+}
+
+// Roots u[i] and weights w[i] of the order-NR Rys rule at argument T from the
+// padded table.  NaN or huge T take the asymptotic branch, so the table is
+// never indexed out of range.
 template <int NR>
 B2_HD void rys_roots(double T, const double *__restrict__ table, double *u, double *w)
 {
@@ -113,15 +154,11 @@ B2_HD void rys_roots(double T, const double *__restrict__ table, double *u, doub
         }
         const int p = (int)T;
         const double x = 2.0 * (T - (double)p) - 1.0;
-        const double *c = table + rys_table_offset(NR) + p * (2 * NR * (RYS_DEG + 1));
+        const double *c = table + rys_padded_offset(NR) + p * (2 * NR * RYS_ROW);
 #pragma unroll
-        for (int f = 0; f < 2 * NR; f++) {
-                const double *cf = c + f * (RYS_DEG + 1);
-                double r = B2_LDG(cf + RYS_DEG);
-#pragma unroll
-                for (int k = RYS_DEG - 1; k >= 0; k--) r = fma(r, x, B2_LDG(cf + k));
-                if (f < NR) u[f] = r;
-                else w[f - NR] = r;
+        for (int f = 0; f < NR; f++) {
+                u[f] = rys_poly(c + f * RYS_ROW, x);
+                w[f] = rys_poly(c + (NR + f) * RYS_ROW, x);
         }
 }
 
@@ -141,16 +178,9 @@ B2_HD void rys_root_one(double T, const double *__restrict__ table, int r, doubl
         }
         const int p = (int)T;
         const double x = 2.0 * (T - (double)p) - 1.0;
-        const double *cu = table + rys_table_offset(NR) + p * (2 * NR * (RYS_DEG + 1)) + r * (RYS_DEG + 1);
-        const double *cw = cu + NR * (RYS_DEG + 1);
-        double a = B2_LDG(cu + RYS_DEG), b = B2_LDG(cw + RYS_DEG);
-#pragma unroll
-        for (int k = RYS_DEG - 1; k >= 0; k--) {
-                a = fma(a, x, B2_LDG(cu + k));
-                b = fma(b, x, B2_LDG(cw + k));
-        }
-        u = a;
-        w = b;
+        const double *c = table + rys_padded_offset(NR) + p * (2 * NR * RYS_ROW);
+        u = rys_poly(c + r * RYS_ROW, x);
+        w = rys_poly(c + (NR + r) * RYS_ROW, x);
 }
 
 // 2D vertical recurrence: g[e*NF + f], e < NE, f < NF.
@@ -238,23 +268,50 @@ struct Class4 {
         }
 };
 
+// Scalars of one primitive quartet shared by all roots.  Primitive pairs
+// carry 1/(2p), so a quartet needs one division and one square root.
+struct PrimQ {
+        double PA[3], QC[3], PQ[3];
+        double ipq;          // 1/(p+q)
+        double qf0, pf0;     // q/(p+q), p/(p+q)
+        double i2p, i2q;     // 1/(2p), 1/(2q)
+        double T;            // rho |PQ|^2
+        double pref;         // 2 pi^{5/2} K_ab K_cd / (p q sqrt(p+q))
+};
+
+B2_HD void prim_setup(PrimQ &s, double p, double i2p, const double P[3], double q, double i2q,
+                      const double Q[3], const double A[3], const double C[3], double kk)
+{
+        s.ipq = 1.0 / (p + q);
+        s.qf0 = q * s.ipq;
+        s.pf0 = p * s.ipq;
+        s.i2p = i2p;
+        s.i2q = i2q;
+#pragma unroll
+        for (int x = 0; x < 3; x++) {
+                s.PA[x] = P[x] - A[x];
+                s.QC[x] = Q[x] - C[x];
+                s.PQ[x] = P[x] - Q[x];
+        }
+        s.T = p * s.qf0 * (s.PQ[0] * s.PQ[0] + s.PQ[1] * s.PQ[1] + s.PQ[2] * s.PQ[2]);
+        s.pref = 34.98683665524972497 * kk * (4.0 * i2p * i2q) * sqrt(s.ipq);
+}
+
 // Root-dependent recurrence coefficients of one primitive quartet.
 struct RysCoef {
         double c00[3], c00p[3], b10, b01, b00;
 };
 
-B2_HD void rys_coef(RysCoef &rc, double u, double p, double q, const double PA[3],
-                    const double QC[3], const double PQ[3])
+B2_HD void rys_coef(RysCoef &rc, double u, const PrimQ &s)
 {
-        const double ipq = 1.0 / (p + q);
-        const double qf = q * ipq * u, pf = p * ipq * u;
-        rc.b00 = 0.5 * u * ipq;
-        rc.b10 = 0.5 / p * (1.0 - qf);
-        rc.b01 = 0.5 / q * (1.0 - pf);
+        const double qf = s.qf0 * u, pf = s.pf0 * u;
+        rc.b00 = 0.5 * u * s.ipq;
+        rc.b10 = s.i2p * (1.0 - qf);
+        rc.b01 = s.i2q * (1.0 - pf);
 #pragma unroll
         for (int x = 0; x < 3; x++) {
-                rc.c00[x] = PA[x] - qf * PQ[x];
-                rc.c00p[x] = QC[x] + pf * PQ[x];
+                rc.c00[x] = s.PA[x] - qf * s.PQ[x];
+                rc.c00p[x] = s.QC[x] + pf * s.PQ[x];
         }
 }
 
@@ -279,36 +336,69 @@ B2_HD void assemble_all(double *G, const double *hx, const double *hy, const dou
         (assemble_one<LA, LB, LC, LD, Ts>(G, hx, hy, hz), ...);
 }
 
-// Add one primitive quartet to the Cartesian block G[((a*NB+b)*NC+c)*ND+d].
-// pref = 2 pi^{5/2}/(pq sqrt(p+q)) K_ab K_cd (coefficients included).
-template <int LA, int LB, int LC, int LD>
-B2_HD void add_prim_quartet(double *G, const double *table, double p, const double P[3],
-                            double q, const double Q[3], const double A[3], const double C[3],
-                            const double AB[3], const double CD[3], double pref)
+// Components [BASE, BASE + N) of the block only (register kernels that
+// keep one part of the block at a time), into Gp[0..N).
+template <int LA, int LB, int LC, int LD, int T>
+B2_HD void assemble_one_to(double &g, const double *hx, const double *hy, const double *hz)
 {
         using K = Class4<LA, LB, LC, LD>;
-        double PA[3], QC[3], PQ[3];
-#pragma unroll
-        for (int x = 0; x < 3; x++) {
-                PA[x] = P[x] - A[x];
-                QC[x] = Q[x] - C[x];
-                PQ[x] = P[x] - Q[x];
-        }
-        const double rho = p * q / (p + q);
-        const double T = rho * (PQ[0] * PQ[0] + PQ[1] * PQ[1] + PQ[2] * PQ[2]);
+        constexpr int id = T % K::ND, ic = (T / K::ND) % K::NC, ib = (T / K::NCD) % K::NB, ia = T / (K::NCD * K::NB);
+        constexpr int ox = K::hidx(cart_lx(LA, ia), cart_lx(LB, ib), cart_lx(LC, ic), cart_lx(LD, id));
+        constexpr int oy = K::hidx(cart_ly(LA, ia), cart_ly(LB, ib), cart_ly(LC, ic), cart_ly(LD, id));
+        constexpr int oz = K::hidx(cart_lz(LA, ia), cart_lz(LB, ib), cart_lz(LC, ic), cart_lz(LD, id));
+        g += hx[ox] * hy[oy] * hz[oz];
+}
+
+template <int LA, int LB, int LC, int LD, int BASE, int... Ts>
+B2_HD void assemble_part(double *Gp, const double *hx, const double *hy, const double *hz,
+                         std::integer_sequence<int, Ts...>)
+{
+        (assemble_one_to<LA, LB, LC, LD, BASE + Ts>(Gp[Ts], hx, hy, hz), ...);
+}
+
+// One primitive quartet into components [BASE, BASE + N) of the block.
+template <int LA, int LB, int LC, int LD, int BASE, int N>
+B2_HD void add_prim_quartet_part(double *Gp, const double *table, const PrimQ &s,
+                                 const double AB[3], const double CD[3])
+{
+        using K = Class4<LA, LB, LC, LD>;
         double u[K::NR], w[K::NR];
-        rys_roots<K::NR>(T, table, u, w);
+        rys_roots<K::NR>(s.T, table, u, w);
 #pragma unroll
         for (int r = 0; r < K::NR; r++) {
                 RysCoef rc;
-                rys_coef(rc, u[r], p, q, PA, QC, PQ);
+                rys_coef(rc, u[r], s);
                 double g[K::NE * K::NF];
                 double hx[K::SA], hy[K::SA], hz[K::SA];
                 vrr2d<K::NE, K::NF>(g, 1.0, rc.c00[0], rc.c00p[0], rc.b10, rc.b01, rc.b00);
                 hrr2d<LA, LB, LC, LD>(g, hx, AB[0], CD[0]);
                 vrr2d<K::NE, K::NF>(g, 1.0, rc.c00[1], rc.c00p[1], rc.b10, rc.b01, rc.b00);
                 hrr2d<LA, LB, LC, LD>(g, hy, AB[1], CD[1]);
-                vrr2d<K::NE, K::NF>(g, pref * w[r], rc.c00[2], rc.c00p[2], rc.b10, rc.b01, rc.b00);
+                vrr2d<K::NE, K::NF>(g, s.pref * w[r], rc.c00[2], rc.c00p[2], rc.b10, rc.b01, rc.b00);
+                hrr2d<LA, LB, LC, LD>(g, hz, AB[2], CD[2]);
+                assemble_part<LA, LB, LC, LD, BASE>(Gp, hx, hy, hz, std::make_integer_sequence<int, N>{});
+        }
+}
+
+// Add one primitive quartet to the Cartesian block G[((a*NB+b)*NC+c)*ND+d].
+template <int LA, int LB, int LC, int LD>
+B2_HD void add_prim_quartet(double *G, const double *table, const PrimQ &s, const double AB[3],
+                            const double CD[3])
+{
+        using K = Class4<LA, LB, LC, LD>;
+        double u[K::NR], w[K::NR];
+        rys_roots<K::NR>(s.T, table, u, w);
+#pragma unroll
+        for (int r = 0; r < K::NR; r++) {
+                RysCoef rc;
+                rys_coef(rc, u[r], s);
+                double g[K::NE * K::NF];
+                double hx[K::SA], hy[K::SA], hz[K::SA];
+                vrr2d<K::NE, K::NF>(g, 1.0, rc.c00[0], rc.c00p[0], rc.b10, rc.b01, rc.b00);
+                hrr2d<LA, LB, LC, LD>(g, hx, AB[0], CD[0]);
+                vrr2d<K::NE, K::NF>(g, 1.0, rc.c00[1], rc.c00p[1], rc.b10, rc.b01, rc.b00);
+                hrr2d<LA, LB, LC, LD>(g, hy, AB[1], CD[1]);
+                vrr2d<K::NE, K::NF>(g, s.pref * w[r], rc.c00[2], rc.c00p[2], rc.b10, rc.b01, rc.b00);
                 hrr2d<LA, LB, LC, LD>(g, hz, AB[2], CD[2]);
 #if defined(__CUDA_ARCH__)
                 if constexpr (K::NG <= 128) {
