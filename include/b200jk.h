@@ -48,6 +48,9 @@ extern "C" {
 #define B200JK_ENOTBUILT     5   /* library built without device code */
 
 #define B200JK_PREC_FP64     0   /* all quartets in float64 */
+#define B200JK_PREC_MIXED    1   /* quartets with q_ij q_kl max|D| < tau evaluated in
+                                    float32, all contraction and accumulation in
+                                    float64; tau set by b200jk_set_mixed_threshold */
 
 typedef struct b200jk_plan b200jk_plan;
 
@@ -60,6 +63,8 @@ typedef struct {
     double  last_build_ms;       /* device time of the last J/K build */
     int32_t nao, nao_cart, nbas, nseg;
     int64_t kernel_launches;     /* kernels this library launched in the last build */
+    int64_t fp32_quartets;       /* of quartets, those evaluated in float32 (mixed mode) */
+    int64_t fp32_prim_quartets;  /* of prim_quartets, those evaluated in float32 */
 } b200jk_stats_t;
 
 typedef struct {
@@ -69,6 +74,7 @@ typedef struct {
     double  ms;                  /* kernel time of the class (profiling on), else 0 */
     int32_t family;              /* 0 thread-per-quartet, 1 warp-per-quartet */
     int32_t pad;
+    int64_t fp32_quartets;       /* of quartets, those evaluated in float32 */
 } b200jk_class_stat_t;
 
 /* Library version, (major << 16) | minor. */
@@ -128,6 +134,14 @@ int b200jk_stats(const b200jk_plan *plan, b200jk_stats_t *stats);
  * each class kernel is bracketed by CUDA events and ms is filled in. */
 int b200jk_class_stats(const b200jk_plan *plan, b200jk_class_stat_t *out, int max, int *n);
 int b200jk_set_profiling(b200jk_plan *plan, int on);
+
+/* Threshold tau of B200JK_PREC_MIXED (default 1e-9): a shell quartet whose
+ * Schwarz bound times the largest density element, q_ij q_kl max|D|, is below
+ * tau is evaluated in float32.  The bound uses the density passed to each
+ * build, so incremental (difference-density) builds move more quartets to
+ * float32 as the SCF converges.  tau <= 0 makes mixed mode all-float64.
+ * No reference counterpart: PySCF evaluates every quartet in float64. */
+int b200jk_set_mixed_threshold(b200jk_plan *plan, double tau);
 
 /* Measured FP64 FMA throughput of device `device` (TFLOP/s), from a
  * register-resident FMA loop over all SMs: the denominator of the FP64

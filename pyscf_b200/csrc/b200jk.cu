@@ -59,6 +59,8 @@ static const int NPAIRCLASS = (LMAX + 1) * (LMAX + 2) / 2;
 static inline int pair_class(int la, int lb) { return la * (la + 1) / 2 + lb; }
 
 __device__ __align__(32) double d_rys_table[rys_padded_size()];
+// the same tables rounded to float32, for the float32 pass of mixed precision
+__device__ __align__(32) float d_rys_table_f[rys_padded_size()];
 
 // ---------------------------------------------------------------------------
 // real solid harmonics r^l Y_lm (unit-normalised Y_lm), rows m = -l..l
@@ -183,6 +185,8 @@ struct PairClassDev {
 struct b200jk_plan {
         int device = 0, cart = 0, natm = 0, nbas = 0, nao = 0, naoc = 0, nseg = 0;
         double tol = 0;
+        // mixed precision: quartets with q_ij q_kl max|D| below fp32_tau run in float32
+        double fp32_tau = 1e-9;
         std::vector<int> ao_loc;
         std::vector<double> h_qcond;
         PairClassDev pc[NPAIRCLASS];
@@ -197,7 +201,7 @@ struct b200jk_plan {
         int ws_ndm = 0;
         DevArr<double> D, Dc, Ds, Jacc, Kacc, outJ, outK;
         DevArr<unsigned long long> dmax, stats;
-        DevArr<int> nkl;
+        DevArr<int> nkl, kst;
         DevArr<long long> nchunk, chunk_off;
         DevArr<unsigned char> cub_tmp;
         cudaStream_t stream = nullptr;
@@ -215,7 +219,7 @@ struct b200jk_plan {
                 goff_all.release(); seg_info.release(); out_seg.release(); out_comp.release();
                 cart_seg.release(); cart_comp.release(); ao_loc_d.release();
                 D.release(); Dc.release(); Ds.release(); Jacc.release(); Kacc.release(); outJ.release(); outK.release();
-                dmax.release(); stats.release(); nkl.release(); nchunk.release(); chunk_off.release(); cub_tmp.release();
+                dmax.release(); stats.release(); nkl.release(); kst.release(); nchunk.release(); chunk_off.release(); cub_tmp.release();
                 for (auto e : cls_ev) cudaEventDestroy(e);
                 if (ev0) cudaEventDestroy(ev0);
                 if (ev1) cudaEventDestroy(ev1);
@@ -241,9 +245,9 @@ static void class_l(int X, int &la, int &lb)
                         if (pair_class(a, b) == X) { la = a; lb = b; return; }
 }
 
-typedef int (*jk_launcher_t)(const JKArgs &, cudaStream_t, int, std::string &);
+typedef int (*jk_launcher_t)(const JKArgs &, cudaStream_t, int, int, std::string &);
 
-static int dispatch_jk(b200jk_plan *P, int la, int lb, int lc, int ld, const JKArgs &a, cudaStream_t s)
+static int dispatch_jk(b200jk_plan *P, int la, int lb, int lc, int ld, const JKArgs &a, int fp32, cudaStream_t s)
 {
         struct Entry { int la, lb, lc, ld; jk_launcher_t fn; };
         static const Entry table[] = {
@@ -306,7 +310,7 @@ static int dispatch_jk(b200jk_plan *P, int la, int lb, int lc, int ld, const JKA
         for (const Entry &e : table) {
                 if (e.la == la && e.lb == lb && e.lc == lc && e.ld == ld) {
                         std::string err;
-                        if (e.fn(a, s, P->nsm, err)) return fail(B200JK_ECUDA, err);
+                        if (e.fn(a, s, P->nsm, fp32, err)) return fail(B200JK_ECUDA, err);
                         return B200JK_OK;
                 }
         }
@@ -338,9 +342,11 @@ static int ensure_tables(int device)
         std::call_once(g_table_once[device], [device]() {
                 std::vector<double> padded(rys_padded_size());
                 rys_pad_table(rys_table_data, padded.data());
-                g_table_status[device] = (cudaMemcpyToSymbol(d_rys_table, padded.data(),
-                                                             sizeof(double) * padded.size()) == cudaSuccess)
-                                                 ? 0 : 1;
+                std::vector<float> padded_f(padded.begin(), padded.end());
+                g_table_status[device] =
+                        (cudaMemcpyToSymbol(d_rys_table, padded.data(), sizeof(double) * padded.size()) == cudaSuccess &&
+                         cudaMemcpyToSymbol(d_rys_table_f, padded_f.data(), sizeof(float) * padded_f.size()) == cudaSuccess)
+                                ? 0 : 1;
         });
         if (g_table_status[device]) return fail(B200JK_ECUDA, "could not upload the Rys tables");
         return B200JK_OK;
@@ -365,6 +371,13 @@ static const double *table_ptr()
         void *p = nullptr;
         cudaGetSymbolAddress(&p, d_rys_table);
         return (const double *)p;
+}
+
+static const float *table_f_ptr()
+{
+        void *p = nullptr;
+        cudaGetSymbolAddress(&p, d_rys_table_f);
+        return (const float *)p;
 }
 
 // ---------------------------------------------------------------------------
@@ -649,11 +662,11 @@ static int ensure_workspace(b200jk_plan *P, int n_dm)
             (rc = dev_alloc(P->Ds, nc * n_dm)) || (rc = dev_alloc(P->Jacc, nc * n_dm)) ||
             (rc = dev_alloc(P->Kacc, nc * n_dm * 2)) || (rc = dev_alloc(P->outJ, nn * n_dm)) ||
             (rc = dev_alloc(P->outK, nn * n_dm)) || (rc = dev_alloc(P->dm_cond, (size_t)P->nbas * P->nbas)) ||
-            (rc = dev_alloc(P->dmax, 1)) || (rc = dev_alloc(P->stats, 2 * 64)))
+            (rc = dev_alloc(P->dmax, 1)) || (rc = dev_alloc(P->stats, 4 * 64)))
                 return rc;
         int maxn = 1;
         for (auto &c : P->pc) maxn = std::max(maxn, c.n * B2_NBUCKET);
-        if ((rc = dev_alloc(P->nkl, maxn)) || (rc = dev_alloc(P->nchunk, maxn + 1)) ||
+        if ((rc = dev_alloc(P->nkl, maxn)) || (rc = dev_alloc(P->kst, maxn)) || (rc = dev_alloc(P->nchunk, maxn + 1)) ||
             (rc = dev_alloc(P->chunk_off, maxn + 1)))
                 return rc;
         size_t tmp = 0;
@@ -673,7 +686,9 @@ int b200jk_get_jk(b200jk_plan *P, const double *dms, int n_dm, int hermi, int wi
         if (hermi < 0 || hermi > 2) return fail(B200JK_EINVAL, "hermi must be 0, 1 or 2");
         if (with_j && !vj) return fail(B200JK_EINVAL, "vj is NULL while with_j is set");
         if (with_k && !vk) return fail(B200JK_EINVAL, "vk is NULL while with_k is set");
-        if (precision_mode != B200JK_PREC_FP64) return fail(B200JK_EUNSUPPORTED, "only precision_mode 0 (FP64) is implemented");
+        if (precision_mode != B200JK_PREC_FP64 && precision_mode != B200JK_PREC_MIXED)
+                return fail(B200JK_EUNSUPPORTED, "precision_mode must be 0 (FP64) or 1 (mixed FP32/FP64)");
+        const int mixed = precision_mode == B200JK_PREC_MIXED && P->fp32_tau > 0;
         CUDA_TRY(cudaSetDevice(P->device));
         int rc = ensure_workspace(P, n_dm);
         if (rc) return rc;
@@ -688,7 +703,7 @@ int b200jk_get_jk(b200jk_plan *P, const double *dms, int n_dm, int hermi, int wi
         }
         // screening data
         CUDA_TRY(cudaMemsetAsync(P->dmax.p, 0, sizeof(unsigned long long), s));
-        CUDA_TRY(cudaMemsetAsync(P->stats.p, 0, 2 * 64 * sizeof(unsigned long long), s));
+        CUDA_TRY(cudaMemsetAsync(P->stats.p, 0, 4 * 64 * sizeof(unsigned long long), s));
         {
                 const long long npair = (long long)P->nbas * (P->nbas + 1) / 2;
                 dm_cond_kernel<<<grid_for(npair, 256), 256, 0, s>>>(dD, n_dm, P->nao, P->ao_loc_d.p, P->nbas,
@@ -709,6 +724,7 @@ int b200jk_get_jk(b200jk_plan *P, const double *dms, int n_dm, int hermi, int wi
         if (with_k) CUDA_TRY(cudaMemsetAsync(P->Kacc.p, 0, sizeof(double) * nc * n_dm * nk, s));
 
         const double *tbl = table_ptr();
+        const float *tbl_f = table_f_ptr();
         auto qcs = quartet_classes();
         int64_t launches = 1 + 2 * n_dm;   // dm_cond, to-Cartesian + symmetrise per density
         if (P->cls.size() != qcs.size()) {
@@ -735,34 +751,40 @@ int b200jk_get_jk(b200jk_plan *P, const double *dms, int n_dm, int hermi, int wi
                         // chunk size of the family the dispatcher will pick
                         const int chunk = family_chunk(la, lb, lc, ld);
                         const int nseg = bra.n * B2_NBUCKET;
-                        count_kernel<<<grid_for(nseg, 256), 256, 0, s>>>(bra.view(), ket.view(), same,
-                                                                        P->tol > 0 ? P->tol : 0.0,
-                                                                        (const double *)P->dmax.p, chunk,
-                                                                        P->nkl.p, P->nchunk.p);
-                        CUDA_TRY(cudaGetLastError());
-                        CUDA_TRY(cudaMemsetAsync(P->nchunk.p + nseg, 0, sizeof(long long), s));
-                        size_t tmp = P->cub_tmp.n;
-                        CUDA_TRY(cub::DeviceScan::ExclusiveSum(P->cub_tmp.p, tmp, P->nchunk.p, P->chunk_off.p, nseg + 1, s));
-                        JKArgs a;
-                        a.bra = bra.view();
-                        a.ket = ket.view();
-                        a.PP = P->PP.p; a.PK = P->PK.p;
-                        a.chunk_off = P->chunk_off.p;
-                        a.nkl = P->nkl.p;
-                        a.dm_cond = P->dm_cond.p;
-                        a.table = tbl;
-                        a.goff = P->goff_all.p + P->goff_at[t];
-                        a.Jacc = P->Jacc.p; a.Kacc = P->Kacc.p;
-                        a.Ds = P->Ds.p; a.Dk = P->Dc.p;
-                        a.stats = P->stats.p + 2 * t;
-                        a.tol = P->tol > 0 ? P->tol : -1.0;
-                        a.nbas = P->nbas; a.naoc = P->naoc; a.n_dm = n_dm; a.nk = nk;
-                        a.with_j = with_j; a.with_k = with_k; a.same = same;
                         if (P->profiling) CUDA_TRY(cudaEventRecord(P->cls_ev[2 * t], s));
-                        if ((rc = dispatch_jk(P, la, lb, lc, ld, a, s))) return rc;
+                        // pass 0: float64 quartets (all of them unless mixed);
+                        // pass 1: the float32 quartets of mixed precision
+                        for (int pass = 0; pass < (mixed ? 2 : 1); pass++) {
+                                count_kernel<<<grid_for(nseg, 256), 256, 0, s>>>(
+                                        bra.view(), ket.view(), same, P->tol > 0 ? P->tol : 0.0, (const double *)P->dmax.p,
+                                        chunk, mixed ? P->fp32_tau : 0.0, pass, P->nkl.p, P->kst.p, P->nchunk.p);
+                                CUDA_TRY(cudaGetLastError());
+                                CUDA_TRY(cudaMemsetAsync(P->nchunk.p + nseg, 0, sizeof(long long), s));
+                                size_t tmp = P->cub_tmp.n;
+                                CUDA_TRY(cub::DeviceScan::ExclusiveSum(P->cub_tmp.p, tmp, P->nchunk.p, P->chunk_off.p,
+                                                                       nseg + 1, s));
+                                JKArgs a;
+                                a.bra = bra.view();
+                                a.ket = ket.view();
+                                a.PP = P->PP.p; a.PK = P->PK.p;
+                                a.chunk_off = P->chunk_off.p;
+                                a.nkl = P->nkl.p;
+                                a.kst = P->kst.p;
+                                a.dm_cond = P->dm_cond.p;
+                                a.table = tbl;
+                                a.table_f = tbl_f;
+                                a.goff = P->goff_all.p + P->goff_at[t];
+                                a.Jacc = P->Jacc.p; a.Kacc = P->Kacc.p;
+                                a.Ds = P->Ds.p; a.Dk = P->Dc.p;
+                                a.stats = P->stats.p + 2 * (64 * pass + t);
+                                a.tol = P->tol > 0 ? P->tol : -1.0;
+                                a.nbas = P->nbas; a.naoc = P->naoc; a.n_dm = n_dm; a.nk = nk;
+                                a.with_j = with_j; a.with_k = with_k; a.same = same;
+                                if ((rc = dispatch_jk(P, la, lb, lc, ld, a, pass, s))) return rc;
+                                launches += 2;   // count + class kernel (the scan is a CUB library kernel)
+                        }
                         if (P->profiling) CUDA_TRY(cudaEventRecord(P->cls_ev[2 * t + 1], s));
                         ran[t] = 1;
-                        launches += 2;   // count + class kernel (the scan is a CUB library kernel)
                 }
         }
         // back to the output basis
@@ -791,18 +813,24 @@ int b200jk_get_jk(b200jk_plan *P, const double *dms, int n_dm, int hermi, int wi
                 if (with_j) CUDA_TRY(cudaMemcpyAsync(vj, P->outJ.p, sizeof(double) * nn * n_dm, cudaMemcpyDeviceToHost, s));
                 if (with_k) CUDA_TRY(cudaMemcpyAsync(vk, P->outK.p, sizeof(double) * nn * n_dm, cudaMemcpyDeviceToHost, s));
         }
-        unsigned long long hs[2 * 64];
+        unsigned long long hs[4 * 64];
         CUDA_TRY(cudaMemcpyAsync(hs, P->stats.p, sizeof(hs), cudaMemcpyDeviceToHost, s));
         CUDA_TRY(cudaStreamSynchronize(s));
         float ms = 0;
         CUDA_TRY(cudaEventElapsedTime(&ms, P->ev0, P->ev1));
         P->st.quartets = 0;
         P->st.prim_quartets = 0;
+        P->st.fp32_quartets = 0;
+        P->st.fp32_prim_quartets = 0;
         for (size_t t = 0; t < qcs.size(); t++) {
-                P->cls[t].quartets = (int64_t)hs[2 * t];
-                P->cls[t].prim_quartets = (int64_t)hs[2 * t + 1];
-                P->st.quartets += (int64_t)hs[2 * t];
-                P->st.prim_quartets += (int64_t)hs[2 * t + 1];
+                const unsigned long long *h64 = hs + 2 * t, *h32 = hs + 2 * (64 + t);
+                P->cls[t].quartets = (int64_t)(h64[0] + h32[0]);
+                P->cls[t].prim_quartets = (int64_t)(h64[1] + h32[1]);
+                P->cls[t].fp32_quartets = (int64_t)h32[0];
+                P->st.quartets += P->cls[t].quartets;
+                P->st.prim_quartets += P->cls[t].prim_quartets;
+                P->st.fp32_quartets += (int64_t)h32[0];
+                P->st.fp32_prim_quartets += (int64_t)h32[1];
                 P->cls[t].ms = 0;
                 if (P->profiling && ran[t]) {
                         float cm = 0;
@@ -812,6 +840,14 @@ int b200jk_get_jk(b200jk_plan *P, const double *dms, int n_dm, int hermi, int wi
         }
         P->st.last_build_ms = ms;
         P->st.kernel_launches = launches;
+        return B200JK_OK;
+}
+
+int b200jk_set_mixed_threshold(b200jk_plan *plan, double tau)
+{
+        if (!plan) return fail(B200JK_EINVAL, "plan is NULL");
+        if (!(tau == tau)) return fail(B200JK_EINVAL, "tau is NaN");
+        plan->fp32_tau = tau;
         return B200JK_OK;
 }
 
@@ -931,6 +967,7 @@ extern "C" int b200jk_get_jk_noalloc(b200jk_plan *P, const double *dms, int n_dm
         const size_t o_dmax = take(sizeof(unsigned long long));
         const size_t o_stats = take(sizeof(unsigned long long) * 2 * 64);
         const size_t o_nkl = take(sizeof(int) * (size_t)maxn);
+        const size_t o_kst = take(sizeof(int) * (size_t)maxn);
         const size_t o_nchunk = take(sizeof(long long) * (size_t)(maxn + 1));
         const size_t o_off = take(sizeof(long long) * (size_t)(maxn + 1));
         const size_t o_cub = take(cub_bytes + 16);
@@ -948,7 +985,7 @@ extern "C" int b200jk_get_jk_noalloc(b200jk_plan *P, const double *dms, int n_dm
         double *dmc = (double *)(base + o_dmc);
         unsigned long long *dmax = (unsigned long long *)(base + o_dmax);
         unsigned long long *stats = (unsigned long long *)(base + o_stats);
-        int *nkl = (int *)(base + o_nkl);
+        int *nkl = (int *)(base + o_nkl), *kst = (int *)(base + o_kst);
         long long *nchunk = (long long *)(base + o_nchunk), *chunk_off = (long long *)(base + o_off);
         void *cub_tmp = base + o_cub;
 
@@ -982,7 +1019,7 @@ extern "C" int b200jk_get_jk_noalloc(b200jk_plan *P, const double *dms, int n_dm
                 const int nseg = bra.n * B2_NBUCKET;
                 count_kernel<<<grid_for(nseg, 256), 256, 0, s>>>(bra.view(), ket.view(), same, P->tol > 0 ? P->tol : 0.0,
                                                                 (const double *)dmax, family_chunk(la, lb, lc, ld),
-                                                                nkl, nchunk);
+                                                                0.0, 0, nkl, kst, nchunk);
                 CUDA_TRY(cudaGetLastError());
                 CUDA_TRY(cudaMemsetAsync(nchunk + nseg, 0, sizeof(long long), s));
                 size_t tmp = cub_bytes;
@@ -993,6 +1030,7 @@ extern "C" int b200jk_get_jk_noalloc(b200jk_plan *P, const double *dms, int n_dm
                 a.PP = P->PP.p; a.PK = P->PK.p;
                 a.chunk_off = chunk_off;
                 a.nkl = nkl;
+                a.kst = kst;
                 a.dm_cond = dmc;
                 a.table = tbl;
                 a.goff = P->goff_all.p + P->goff_at[t];
@@ -1002,7 +1040,7 @@ extern "C" int b200jk_get_jk_noalloc(b200jk_plan *P, const double *dms, int n_dm
                 a.tol = P->tol > 0 ? P->tol : -1.0;
                 a.nbas = P->nbas; a.naoc = P->naoc; a.n_dm = n_dm; a.nk = nk;
                 a.with_j = with_j; a.with_k = with_k; a.same = same;
-                int rc = dispatch_jk(P, la, lb, lc, ld, a, s);
+                int rc = dispatch_jk(P, la, lb, lc, ld, a, 0, s);
                 if (rc) return rc;
         }
         for (int d = 0; d < n_dm; d++) {

@@ -61,7 +61,7 @@ void host_quartet(const HSeg *s, double *out)
                         const double c = s[2].exp[k], d = s[3].exp[l], q = c + d;
                         const double Q[3] = {(c * C[0] + d * D[0]) / q, (c * C[1] + d * D[1]) / q, (c * C[2] + d * D[2]) / q};
                         const double Kcd = s[2].coef[k] * s[3].coef[l] * exp(-c * d / q * rcd);
-                        PrimQ sq;
+                        PrimQ<double> sq;
                         prim_setup(sq, p, 0.5 / p, P, q, 0.5 / q, Q, A, C, Kab * Kcd);
                         add_prim_quartet<LA, LB, LC, LD>(G.data(), padded_table(), sq, AB, CD);
                 }

@@ -19,7 +19,9 @@ struct LaunchCfg {
         cudaError_t status = cudaSuccess;
 };
 
-template <int LA, int LB, int LC, int LD>
+// R is the evaluation type: double for the FP64 pass, float for the FP32 pass
+// of mixed precision (accumulation stays in float64 either way)
+template <int LA, int LB, int LC, int LD, typename R>
 int launch_one(const JKArgs &a, cudaStream_t s, int nsm, std::string &err)
 {
         using K = Class4<LA, LB, LC, LD>;
@@ -33,18 +35,22 @@ int launch_one(const JKArgs &a, cudaStream_t s, int nsm, std::string &err)
                         int nb = 0;
                         if constexpr (thread) {
                                 cfg.block = 128;
-                                cfg.smem = 0;
-                                cfg.status = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, jk_thread_kernel<LA, LB, LC, LD, (NP > 0 ? NP : 1)>, 128, 0);
+                                cfg.smem = K::NR <= 4 ? sizeof(R) * rys_slice_size(K::NR) : 0;
+                                cfg.status = cudaFuncSetAttribute(jk_thread_kernel<LA, LB, LC, LD, (NP > 0 ? NP : 1), R>,
+                                                                  cudaFuncAttributeMaxDynamicSharedMemorySize, (int)cfg.smem);
+                                if (cfg.status == cudaSuccess)
+                                        cfg.status = cudaOccupancyMaxActiveBlocksPerMultiprocessor(
+                                                &nb, jk_thread_kernel<LA, LB, LC, LD, (NP > 0 ? NP : 1), R>, 128, cfg.smem);
                         } else {
-                                const size_t per_warp = sizeof(double) * WarpSmem<LA, LB, LC, LD>::SIZE *
+                                const size_t per_warp = sizeof(double) * WarpSmem<LA, LB, LC, LD, R>::SIZE *
                                                         (32 / group_size<LA, LB, LC, LD>());
                                 const int wpb = (int)std::min<size_t>(4, std::max<size_t>(1, (200 * 1024) / per_warp));
                                 cfg.block = 32 * wpb;
                                 cfg.smem = per_warp * wpb;
-                                cfg.status = cudaFuncSetAttribute(jk_warp_kernel<LA, LB, LC, LD>,
+                                cfg.status = cudaFuncSetAttribute(jk_warp_kernel<LA, LB, LC, LD, R>,
                                                                   cudaFuncAttributeMaxDynamicSharedMemorySize, (int)cfg.smem);
                                 if (cfg.status == cudaSuccess)
-                                        cfg.status = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, jk_warp_kernel<LA, LB, LC, LD>,
+                                        cfg.status = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, jk_warp_kernel<LA, LB, LC, LD, R>,
                                                                                                    cfg.block, cfg.smem);
                         }
                         cfg.grid = (nb > 0 ? nb : 1) * nsm;
@@ -56,9 +62,9 @@ int launch_one(const JKArgs &a, cudaStream_t s, int nsm, std::string &err)
                 return 1;
         }
         if constexpr (thread) {
-                jk_thread_kernel<LA, LB, LC, LD, NP><<<cfg.grid, cfg.block, 0, s>>>(a);
+                jk_thread_kernel<LA, LB, LC, LD, NP, R><<<cfg.grid, cfg.block, cfg.smem, s>>>(a);
         } else {
-                jk_warp_kernel<LA, LB, LC, LD><<<cfg.grid, cfg.block, cfg.smem, s>>>(
+                jk_warp_kernel<LA, LB, LC, LD, R><<<cfg.grid, cfg.block, cfg.smem, s>>>(
                         a, 8 * (32 / group_size<LA, LB, LC, LD>()));
         }
         cudaError_t e = cudaGetLastError();
@@ -72,9 +78,10 @@ int launch_one(const JKArgs &a, cudaStream_t s, int nsm, std::string &err)
 } // namespace
 
 // B2_FN_NAME is launch_jk_<la><lb><lc><ld>, declared in jk_launch.h
-int B2_FN_NAME(const JKArgs &a, cudaStream_t s, int nsm, std::string &err)
+int B2_FN_NAME(const JKArgs &a, cudaStream_t s, int nsm, int fp32, std::string &err)
 {
-        return launch_one<B2_BRA_LA, B2_BRA_LB, B2_KET_LC, B2_KET_LD>(a, s, nsm, err);
+        if (fp32) return launch_one<B2_BRA_LA, B2_BRA_LB, B2_KET_LC, B2_KET_LD, float>(a, s, nsm, err);
+        return launch_one<B2_BRA_LA, B2_BRA_LB, B2_KET_LC, B2_KET_LD, double>(a, s, nsm, err);
 }
 
 } // namespace b200jk

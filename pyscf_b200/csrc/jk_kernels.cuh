@@ -56,7 +56,9 @@ struct JKArgs {
         const long long *chunk_off;  // bra.n * B2_NBUCKET + 1 entries
         const int *nkl;              // per (bra pair, ket bucket)
         const double *dm_cond;       // nbas x nbas (parent shells)
-        const double *table;         // Rys tables
+        const double *table;         // Rys tables (padded layout), float64
+        const float *table_f;        // the same tables in float32
+        const int *kst;              // per (bra pair, ket bucket): first ket of this pass
         const int *goff;             // packed (ox, oy, oz) per Cartesian component (warp family)
         double *Jacc, *Kacc;
         const double *Ds, *Dk;
@@ -101,18 +103,22 @@ __device__ __forceinline__ bool quartet_passes(const JKArgs &a, int4 sb, double 
 #define B2_TWO_PI_2P5 34.98683665524972497
 
 // ---------------------------------------------------------------------------
-// Count kernel: for bra pair ij and ket bucket b, the length of the prefix of
-// the bucket that can pass the screen, and its chunks of `chunk` quartets.
-// Same-class quartets keep kl <= ij in the (bucket, rank) order.
+// Count kernel: for bra pair ij and ket bucket b, the prefix of the bucket
+// that can pass the screen, split at the mixed-precision threshold: kets with
+// q_ij q_kl max|D| >= tau32 form the FP64 part [0, n64), the rest the FP32
+// part [n64, n).  pass 0 writes the FP64 part, pass 1 the FP32 part (start in
+// kst, length in nkl) with its chunks of `chunk` quartets.  tau32 = 0 keeps
+// every quartet in FP64.  Same-class quartets keep kl <= ij in the
+// (bucket, rank) order.
 static __global__ void count_kernel(PairView bra, PairView ket, int same, double tol, const double *dmax4,
-                                    int chunk, int *nkl, long long *nchunk)
+                                    int chunk, double tau32, int pass, int *nkl, int *kst, long long *nchunk)
 {
         const int t = blockIdx.x * blockDim.x + threadIdx.x;
         if (t >= bra.n * B2_NBUCKET) return;
         const int ij = t / B2_NBUCKET, b = t % B2_NBUCKET;
         const double qij = bra.q[ij];
         const double dm = *dmax4;
-        int cnt = 0;
+        int cnt = 0, n64 = 0;
         const int lo0 = ket.boff[b], hi0 = ket.boff[b + 1];
         if (dm > 0 && qij > 0 && hi0 > lo0) {
                 const double thr = tol / (qij * dm);
@@ -129,9 +135,24 @@ static __global__ void count_kernel(PairView bra, PairView ket, int same, double
                         if (b > bi) cnt = 0;
                         else if (b == bi) cnt = min(cnt, ij - lo0 + 1);
                 }
+                n64 = cnt;
+                if (tau32 > 0) {
+                        const double thr32 = tau32 / (qij * dm);
+                        lo = lo0;
+                        hi = lo0 + cnt;
+                        while (lo < hi) {
+                                int mid = (lo + hi) >> 1;
+                                if (ket.q[mid] >= thr32) lo = mid + 1;
+                                else hi = mid;
+                        }
+                        n64 = lo - lo0;
+                }
         }
-        nkl[t] = cnt;
-        nchunk[t] = (cnt + chunk - 1) / chunk;
+        const int start = pass == 0 ? 0 : n64;
+        const int len = pass == 0 ? n64 : cnt - n64;
+        nkl[t] = len;
+        kst[t] = start;
+        nchunk[t] = (len + chunk - 1) / chunk;
 }
 
 // ---------------------------------------------------------------------------
@@ -147,7 +168,11 @@ __device__ __forceinline__ void for_parts(F &&f, std::integer_sequence<int, Ps..
         (f(std::integral_constant<int, Ps>{}), ...);
 }
 
-template <int LA, int LB, int LC, int LD, int NP>
+template <typename R> __device__ __forceinline__ const R *table_of(const JKArgs &a);
+template <> __device__ __forceinline__ const double *table_of<double>(const JKArgs &a) { return a.table; }
+template <> __device__ __forceinline__ const float *table_of<float>(const JKArgs &a) { return a.table_f; }
+
+template <int LA, int LB, int LC, int LD, int NP, typename R>
 __global__ void __launch_bounds__(128) jk_thread_kernel(JKArgs a)
 {
         using K = Class4<LA, LB, LC, LD>;
@@ -155,6 +180,18 @@ __global__ void __launch_bounds__(128) jk_thread_kernel(JKArgs a)
         constexpr int NAP = K::NA / NP;            // bra components per part
         constexpr int NGP = NAP * K::NB * K::NCD;  // integrals per part
         const int lane = threadIdx.x & 31;
+        // the order-NR slice of the Rys table: staged in shared memory for up
+        // to four roots (<= 59 KB), read from global memory otherwise
+        extern __shared__ __align__(32) double smem_dyn[];
+        const R *tab = table_of<R>(a) + rys_padded_offset(K::NR);
+        if constexpr (K::NR <= 4) {
+                constexpr int NS = rys_slice_size(K::NR);
+                const RysVec4<R> *src = reinterpret_cast<const RysVec4<R> *>(tab);
+                RysVec4<R> *dst = reinterpret_cast<RysVec4<R> *>(smem_dyn);
+                for (int t = threadIdx.x; t < NS / 4; t += blockDim.x) dst[t] = src[t];
+                __syncthreads();
+                tab = reinterpret_cast<const R *>(smem_dyn);
+        }
         const int nseg = a.bra.n * B2_NBUCKET;
         const long long total = a.chunk_off[nseg];
         const long long nwarps = ((long long)gridDim.x * blockDim.x) >> 5;
@@ -165,7 +202,7 @@ __global__ void __launch_bounds__(128) jk_thread_kernel(JKArgs a)
                 const int sgi = find_bra(a.chunk_off, nseg, chunk);
                 const int ij = sgi / B2_NBUCKET;
                 const int pos = (int)(chunk - a.chunk_off[sgi]) * 32 + lane;
-                const int kl = a.ket.boff[sgi % B2_NBUCKET] + pos;
+                const int kl = a.ket.boff[sgi % B2_NBUCKET] + a.kst[sgi] + pos;
                 const int4 sb = a.bra.sh[ij];
                 const int2 pb = a.bra.pr[ij];
                 const double qij = a.bra.q[ij];
@@ -178,18 +215,21 @@ __global__ void __launch_bounds__(128) jk_thread_kernel(JKArgs a)
                         active = quartet_passes(a, sb, qij, sk, a.ket.q[kl]);
                 }
                 int2 pk = make_int2(0, 0);
-                double fac = 1.0;
-                double C[3] = {0, 0, 0}, CD[3] = {0, 0, 0};
-                const double A[3] = {Ab.x, Ab.y, Ab.z}, AB[3] = {ABb.x, ABb.y, ABb.z};
+                R fac = (R)1;
+                // coordinates relative to the bra centre A, differenced in
+                // float64: keeps the float32 pass accurate for quartets far
+                // from the origin
+                R C[3] = {0, 0, 0}, CD[3] = {0, 0, 0};
+                const R A[3] = {(R)0, (R)0, (R)0}, AB[3] = {(R)ABb.x, (R)ABb.y, (R)ABb.z};
                 if (active) {
                         pk = a.ket.pr[kl];
                         const double4 Ak = a.ket.A[kl];
                         const double4 CDk = a.ket.AB[kl];
-                        if (Ab.w != 0.0) fac *= 0.5;
-                        if (Ak.w != 0.0) fac *= 0.5;
-                        if (a.same && ij == kl) fac *= 0.5;
-                        C[0] = Ak.x; C[1] = Ak.y; C[2] = Ak.z;
-                        CD[0] = CDk.x; CD[1] = CDk.y; CD[2] = CDk.z;
+                        if (Ab.w != 0.0) fac *= (R)0.5;
+                        if (Ak.w != 0.0) fac *= (R)0.5;
+                        if (a.same && ij == kl) fac *= (R)0.5;
+                        C[0] = (R)(Ak.x - Ab.x); C[1] = (R)(Ak.y - Ab.y); C[2] = (R)(Ak.z - Ab.z);
+                        CD[0] = (R)CDk.x; CD[1] = (R)CDk.y; CD[2] = (R)CDk.z;
                         nq++;
                         npq += (unsigned long long)pb.y * pk.y;
                 }
@@ -197,22 +237,23 @@ __global__ void __launch_bounds__(128) jk_thread_kernel(JKArgs a)
                 for_parts([&](auto part_tag) {
                         constexpr int PART = decltype(part_tag)::value;
                         constexpr int A0 = PART * NAP;
-                        double Gp[NGP];
+                        R Gp[NGP];
 #pragma unroll
-                        for (int t = 0; t < NGP; t++) Gp[t] = 0.0;
+                        for (int t = 0; t < NGP; t++) Gp[t] = (R)0;
                         if (active) {
                                 for (int ip = 0; ip < pb.y; ip++) {
                                         const double4 P = a.PP[pb.x + ip];
                                         const double2 KP = a.PK[pb.x + ip];
-                                        const double Kab = KP.x * fac;
-                                        const double Pv[3] = {P.x, P.y, P.z};
+                                        const R Kab = (R)KP.x * fac;
+                                        const R Pv[3] = {(R)(P.x - Ab.x), (R)(P.y - Ab.y), (R)(P.z - Ab.z)};
                                         for (int kp = 0; kp < pk.y; kp++) {
                                                 const double4 Q = a.PP[pk.x + kp];
                                                 const double2 KQ = a.PK[pk.x + kp];
-                                                const double Qv[3] = {Q.x, Q.y, Q.z};
-                                                PrimQ sq;
-                                                prim_setup(sq, P.w, KP.y, Pv, Q.w, KQ.y, Qv, A, C, Kab * KQ.x);
-                                                add_prim_quartet_part<LA, LB, LC, LD, PART * NGP, NGP>(Gp, a.table, sq, AB, CD);
+                                                const R Qv[3] = {(R)(Q.x - Ab.x), (R)(Q.y - Ab.y), (R)(Q.z - Ab.z)};
+                                                PrimQ<R> sq;
+                                                prim_setup<R>(sq, (R)P.w, (R)KP.y, Pv, (R)Q.w, (R)KQ.y, Qv, A, C,
+                                                              Kab * (R)KQ.x);
+                                                add_prim_quartet_part<LA, LB, LC, LD, PART * NGP, NGP, R>(Gp, tab, sq, AB, CD);
                                         }
                                 }
                         }
@@ -234,7 +275,7 @@ __global__ void __launch_bounds__(128) jk_thread_kernel(JKArgs a)
                                                 for (int y = 0; y < K::ND; y++) {
                                                         double v = 0.0;
 #pragma unroll
-                                                        for (int t = 0; t < NAP * K::NB; t++) v += Gp[t * K::NCD + x * K::ND + y] * dab[t];
+                                                        for (int t = 0; t < NAP * K::NB; t++) v += (double)Gp[t * K::NCD + x * K::ND + y] * dab[t];
                                                         atomicAdd(J + (ic + x) * n + id + y, v);
                                                 }
                                         }
@@ -248,7 +289,7 @@ __global__ void __launch_bounds__(128) jk_thread_kernel(JKArgs a)
                                         for (int t = 0; t < NAP * K::NB; t++) {
                                                 double v = 0.0;
 #pragma unroll
-                                                for (int u = 0; u < K::NCD; u++) v += Gp[t * K::NCD + u] * dcd[u];
+                                                for (int u = 0; u < K::NCD; u++) v += (double)Gp[t * K::NCD + u] * dcd[u];
                                                 v = warp_sum(v);
                                                 if (lane == 0 && v != 0.0)
                                                         atomicAdd(J + (ia + A0 + t / K::NB) * n + ib + t % K::NB, v);
@@ -274,7 +315,7 @@ __global__ void __launch_bounds__(128) jk_thread_kernel(JKArgs a)
                                                                 for (int b = 0; b < K::NB; b++)
 #pragma unroll
                                                                         for (int c = 0; c < K::NC; c++)
-                                                                                v += Gp[((x * K::NB + b) * K::NC + c) * K::ND + d] * x_[b * K::NC + c];
+                                                                                v += (double)Gp[((x * K::NB + b) * K::NC + c) * K::ND + d] * x_[b * K::NC + c];
                                                                 atomicAdd(Kt + (ia + A0 + x) * n + id + d, v);
                                                         }
                                                 }
@@ -294,7 +335,7 @@ __global__ void __launch_bounds__(128) jk_thread_kernel(JKArgs a)
                                                                 for (int b = 0; b < K::NB; b++)
 #pragma unroll
                                                                         for (int d = 0; d < K::ND; d++)
-                                                                                v += Gp[((x * K::NB + b) * K::NC + c) * K::ND + d] * x_[b * K::ND + d];
+                                                                                v += (double)Gp[((x * K::NB + b) * K::NC + c) * K::ND + d] * x_[b * K::ND + d];
                                                                 atomicAdd(Kt + (ia + A0 + x) * n + ic + c, v);
                                                         }
                                                 }
@@ -314,7 +355,7 @@ __global__ void __launch_bounds__(128) jk_thread_kernel(JKArgs a)
                                                                 for (int x = 0; x < NAP; x++)
 #pragma unroll
                                                                         for (int c = 0; c < K::NC; c++)
-                                                                                v += Gp[((x * K::NB + b) * K::NC + c) * K::ND + d] * x_[x * K::NC + c];
+                                                                                v += (double)Gp[((x * K::NB + b) * K::NC + c) * K::ND + d] * x_[x * K::NC + c];
                                                                 atomicAdd(Kt + (ib + b) * n + id + d, v);
                                                         }
                                                 }
@@ -334,7 +375,7 @@ __global__ void __launch_bounds__(128) jk_thread_kernel(JKArgs a)
                                                                 for (int x = 0; x < NAP; x++)
 #pragma unroll
                                                                         for (int d = 0; d < K::ND; d++)
-                                                                                v += Gp[((x * K::NB + b) * K::NC + c) * K::ND + d] * x_[x * K::ND + d];
+                                                                                v += (double)Gp[((x * K::NB + b) * K::NC + c) * K::ND + d] * x_[x * K::ND + d];
                                                                 atomicAdd(Kt + (ib + b) * n + ic + c, v);
                                                         }
                                                 }
@@ -371,34 +412,35 @@ __host__ __device__ constexpr int thread_parts()
 // ---------------------------------------------------------------------------
 // Warp-per-quartet family: 2D integrals and the Cartesian block in shared
 // memory, components spread over the lanes.
-template <int LA, int LB, int LC, int LD>
+template <int LA, int LB, int LC, int LD, typename R = double>
 struct WarpSmem {
         using K = Class4<LA, LB, LC, LD>;
-        static constexpr int G = 0;
-        static constexpr int H = G + K::NG;                      // [3][NR][SA]
-        static constexpr int DSAB = H + 3 * K::NR * K::SA;
+        // G[NG] and H[3][NR][SA] in the compute type, then float64 staging
+        static constexpr int G = 0;                              // in R units
+        static constexpr int H = G + K::NG;                      // in R units
+        static constexpr int NRV = K::NG + 3 * K::NR * K::SA;
+        static constexpr int DSAB = (int)((NRV * sizeof(R) + 7) / 8);   // doubles from here
         static constexpr int DSCD = DSAB + K::NAB;
         static constexpr int XBC = DSCD + K::NCD;
         static constexpr int XBD = XBC + K::NB * K::NC;
         static constexpr int XAC = XBD + K::NB * K::ND;
         static constexpr int XAD = XAC + K::NA * K::NC;
-        static constexpr int SIZE = ((XAD + K::NA * K::ND) + 1) & ~1;   // doubles per warp
+        static constexpr int SIZE = ((XAD + K::NA * K::ND) + 3) & ~3;   // doubles per group
 };
 
-template <int LA, int LB, int LC, int LD>
-__device__ __forceinline__ void warp_slice_to_smem(double *h, double g00, const RysCoef &rc, int dir,
-                                                   double ab, double cd)
+template <int LA, int LB, int LC, int LD, typename R>
+__device__ __forceinline__ void warp_slice_to_smem(R *h, R g00, const RysCoef<R> &rc, int dir, R ab, R cd)
 {
         using K = Class4<LA, LB, LC, LD>;
-        double g[K::NE * K::NF];
-        const double c00 = dir == 0 ? rc.c00[0] : (dir == 1 ? rc.c00[1] : rc.c00[2]);
-        const double c00p = dir == 0 ? rc.c00p[0] : (dir == 1 ? rc.c00p[1] : rc.c00p[2]);
-        vrr2d<K::NE, K::NF>(g, g00, c00, c00p, rc.b10, rc.b01, rc.b00);
+        R g[K::NE * K::NF];
+        const R c00 = dir == 0 ? rc.c00[0] : (dir == 1 ? rc.c00[1] : rc.c00[2]);
+        const R c00p = dir == 0 ? rc.c00p[0] : (dir == 1 ? rc.c00p[1] : rc.c00p[2]);
+        vrr2d<K::NE, K::NF, R>(g, g00, c00, c00p, rc.b10, rc.b01, rc.b00);
         // ket transfer first: u[e][c][d]
         constexpr int NCD1 = (LC + 1) * (LD + 1);
-        double u[K::NE * NCD1];
-        double cdp[LD + 1];
-        cdp[0] = 1.0;
+        R u[K::NE * NCD1];
+        R cdp[LD + 1];
+        cdp[0] = (R)1;
 #pragma unroll
         for (int k = 1; k <= LD; k++) cdp[k] = cdp[k - 1] * cd;
 #pragma unroll
@@ -407,13 +449,13 @@ __device__ __forceinline__ void warp_slice_to_smem(double *h, double g00, const 
         for (int c = 0; c <= LC; c++)
 #pragma unroll
         for (int d = 0; d <= LD; d++) {
-                double v = 0.0;
+                R v = (R)0;
 #pragma unroll
-                for (int k = 0; k <= d; k++) v += (double)binom(d, k) * cdp[d - k] * g[e * K::NF + c + k];
+                for (int k = 0; k <= d; k++) v += (R)binom(d, k) * cdp[d - k] * g[e * K::NF + c + k];
                 u[e * NCD1 + c * (LD + 1) + d] = v;
         }
-        double abp[LB + 1];
-        abp[0] = 1.0;
+        R abp[LB + 1];
+        abp[0] = (R)1;
 #pragma unroll
         for (int k = 1; k <= LB; k++) abp[k] = abp[k - 1] * ab;
 #pragma unroll
@@ -422,9 +464,9 @@ __device__ __forceinline__ void warp_slice_to_smem(double *h, double g00, const 
         for (int b = 0; b <= LB; b++)
 #pragma unroll
         for (int t = 0; t < NCD1; t++) {
-                double v = 0.0;
+                R v = (R)0;
 #pragma unroll
-                for (int k = 0; k <= b; k++) v += (double)binom(b, k) * abp[b - k] * u[(x + k) * NCD1 + t];
+                for (int k = 0; k <= b; k++) v += (R)binom(b, k) * abp[b - k] * u[(x + k) * NCD1 + t];
                 h[(x * (LB + 1) + b) * NCD1 + t] = v;
         }
 }
@@ -433,26 +475,27 @@ __device__ __forceinline__ void warp_slice_to_smem(double *h, double g00, const 
 // the (root, direction) slices of the 2D integrals are spread over the group,
 // then the Cartesian block is accumulated with components spread over it.
 // `gl` is the lane index inside the group, `gmask` the group's lane mask.
-template <int LA, int LB, int LC, int LD, int GS>
-__device__ __forceinline__ void group_eval_block(double *sm, const JKArgs &a, int2 pb, int2 pk,
-                                                 const double A[3], const double AB[3],
-                                                 const double C[3], const double CD[3], double fac,
-                                                 int gl, unsigned gmask)
+// A, C, and the P, Q read here are relative to the origin O (the bra centre)
+template <int LA, int LB, int LC, int LD, int GS, typename R>
+__device__ __forceinline__ void group_eval_block(double *sm, const JKArgs &a, int2 pb, int2 pk, const double4 O,
+                                                 const R A[3], const R AB[3], const R C[3], const R CD[3],
+                                                 R fac, int gl, unsigned gmask)
 {
         using K = Class4<LA, LB, LC, LD>;
-        using S = WarpSmem<LA, LB, LC, LD>;
-        double *G = sm + S::G;
-        double *H = sm + S::H;
-        for (int t = gl; t < K::NG; t += GS) G[t] = 0.0;
+        using S = WarpSmem<LA, LB, LC, LD, R>;
+        R *G = reinterpret_cast<R *>(sm) + S::G;
+        R *H = reinterpret_cast<R *>(sm) + S::H;
+        const R *table = table_of<R>(a);
+        for (int t = gl; t < K::NG; t += GS) G[t] = (R)0;
         for (int ip = 0; ip < pb.y; ip++) {
                 const double4 P = a.PP[pb.x + ip];
                 const double2 KP = a.PK[pb.x + ip];
-                const double Kab = KP.x * fac;
-                const double Pv[3] = {P.x, P.y, P.z};
+                const R Kab = (R)KP.x * fac;
+                const R Pv[3] = {(R)(P.x - O.x), (R)(P.y - O.y), (R)(P.z - O.z)};
                 for (int kp = 0; kp < pk.y; kp++) {
                         const double4 Q = a.PP[pk.x + kp];
                         const double2 KQ = a.PK[pk.x + kp];
-                        const double Qv[3] = {Q.x, Q.y, Q.z};
+                        const R Qv[3] = {(R)(Q.x - O.x), (R)(Q.y - O.y), (R)(Q.z - O.z)};
                         __syncwarp(gmask);
                         // one task per root (all three directions) when the slices
                         // are small, else one per (root, direction)
@@ -460,30 +503,30 @@ __device__ __forceinline__ void group_eval_block(double *sm, const JKArgs &a, in
                         constexpr int NTASK = PER_ROOT ? K::NR : 3 * K::NR;
                         for (int task = gl; task < NTASK; task += GS) {
                                 const int r = PER_ROOT ? task : task / 3;
-                                PrimQ sq;
-                                prim_setup(sq, P.w, KP.y, Pv, Q.w, KQ.y, Qv, A, C, Kab * KQ.x);
-                                double ur, wr;
-                                rys_root_one<K::NR>(sq.T, a.table, r, ur, wr);
-                                RysCoef rc;
-                                rys_coef(rc, ur, sq);
-                                const double pref = sq.pref;
+                                PrimQ<R> sq;
+                                prim_setup<R>(sq, (R)P.w, (R)KP.y, Pv, (R)Q.w, (R)KQ.y, Qv, A, C, Kab * (R)KQ.x);
+                                R ur, wr;
+                                rys_root_one<K::NR, R>(sq.T, table, r, ur, wr);
+                                RysCoef<R> rc;
+                                rys_coef<R>(rc, ur, sq);
+                                const R pref = sq.pref;
                                 if constexpr (PER_ROOT) {
-                                        warp_slice_to_smem<LA, LB, LC, LD>(H + (0 * K::NR + r) * K::SA, 1.0, rc, 0, AB[0], CD[0]);
-                                        warp_slice_to_smem<LA, LB, LC, LD>(H + (1 * K::NR + r) * K::SA, 1.0, rc, 1, AB[1], CD[1]);
-                                        warp_slice_to_smem<LA, LB, LC, LD>(H + (2 * K::NR + r) * K::SA, pref * wr, rc, 2, AB[2], CD[2]);
+                                        warp_slice_to_smem<LA, LB, LC, LD, R>(H + (0 * K::NR + r) * K::SA, (R)1, rc, 0, AB[0], CD[0]);
+                                        warp_slice_to_smem<LA, LB, LC, LD, R>(H + (1 * K::NR + r) * K::SA, (R)1, rc, 1, AB[1], CD[1]);
+                                        warp_slice_to_smem<LA, LB, LC, LD, R>(H + (2 * K::NR + r) * K::SA, pref * wr, rc, 2, AB[2], CD[2]);
                                 } else {
                                         const int dir = task - 3 * r;
-                                        const double g00 = dir == 2 ? pref * wr : 1.0;
-                                        const double abx = dir == 0 ? AB[0] : (dir == 1 ? AB[1] : AB[2]);
-                                        const double cdx = dir == 0 ? CD[0] : (dir == 1 ? CD[1] : CD[2]);
-                                        warp_slice_to_smem<LA, LB, LC, LD>(H + (dir * K::NR + r) * K::SA, g00, rc, dir, abx, cdx);
+                                        const R g00 = dir == 2 ? pref * wr : (R)1;
+                                        const R abx = dir == 0 ? AB[0] : (dir == 1 ? AB[1] : AB[2]);
+                                        const R cdx = dir == 0 ? CD[0] : (dir == 1 ? CD[1] : CD[2]);
+                                        warp_slice_to_smem<LA, LB, LC, LD, R>(H + (dir * K::NR + r) * K::SA, g00, rc, dir, abx, cdx);
                                 }
                         }
                         __syncwarp(gmask);
                         for (int t = gl; t < K::NG; t += GS) {
                                 const int o = __ldg(a.goff + t);
                                 const int ox = o & 1023, oy = (o >> 10) & 1023, oz = o >> 20;
-                                double v = 0.0;
+                                R v = (R)0;
 #pragma unroll
                                 for (int r = 0; r < K::NR; r++)
                                         v += H[r * K::SA + ox] * H[(K::NR + r) * K::SA + oy] * H[(2 * K::NR + r) * K::SA + oz];
@@ -502,14 +545,14 @@ __host__ __device__ constexpr int group_size()
         return K::NG <= 100 ? 8 : (K::NG <= 400 ? 16 : 32);
 }
 
-template <int LA, int LB, int LC, int LD>
+template <int LA, int LB, int LC, int LD, typename R>
 __global__ void __launch_bounds__(128) jk_warp_kernel(JKArgs a, int chunk_q)
 {
         using K = Class4<LA, LB, LC, LD>;
-        using S = WarpSmem<LA, LB, LC, LD>;
+        using S = WarpSmem<LA, LB, LC, LD, R>;
         constexpr int GS = group_size<LA, LB, LC, LD>();
         constexpr int NGRP = 32 / GS;
-        extern __shared__ double smem_dyn[];
+        extern __shared__ __align__(32) double smem_dyn[];
         const int lane = threadIdx.x & 31;
         const int grp = lane / GS, gl = lane % GS;
         const unsigned gmask = GS == 32 ? 0xffffffffu : (((1u << GS) - 1u) << (grp * GS));
@@ -524,7 +567,7 @@ __global__ void __launch_bounds__(128) jk_warp_kernel(JKArgs a, int chunk_q)
              chunk += nwarps) {
                 const int sgi = find_bra(a.chunk_off, nseg, chunk);
                 const int ij = sgi / B2_NBUCKET;
-                const int kb = a.ket.boff[sgi % B2_NBUCKET];
+                const int kb = a.ket.boff[sgi % B2_NBUCKET] + a.kst[sgi];
                 const int kl0 = kb + (int)(chunk - a.chunk_off[sgi]) * chunk_q;
                 const int kl1 = kb + min((int)(chunk - a.chunk_off[sgi]) * chunk_q + chunk_q, a.nkl[sgi]);
                 const int4 sb = a.bra.sh[ij];
@@ -532,7 +575,7 @@ __global__ void __launch_bounds__(128) jk_warp_kernel(JKArgs a, int chunk_q)
                 const double qij = a.bra.q[ij];
                 const double4 Ab = a.bra.A[ij];
                 const double4 ABb = a.bra.AB[ij];
-                const double A[3] = {Ab.x, Ab.y, Ab.z}, AB[3] = {ABb.x, ABb.y, ABb.z};
+                const R A[3] = {(R)0, (R)0, (R)0}, AB[3] = {(R)ABb.x, (R)ABb.y, (R)ABb.z};
                 const int ia = sb.x, ib = sb.y;
                 for (int kl = kl0 + grp; kl < kl1; kl += NGRP) {
                         const int4 sk = a.ket.sh[kl];
@@ -540,17 +583,18 @@ __global__ void __launch_bounds__(128) jk_warp_kernel(JKArgs a, int chunk_q)
                         const int2 pk = a.ket.pr[kl];
                         const double4 Ak = a.ket.A[kl];
                         const double4 CDk = a.ket.AB[kl];
-                        double fac = 1.0;
-                        if (Ab.w != 0.0) fac *= 0.5;
-                        if (Ak.w != 0.0) fac *= 0.5;
-                        if (a.same && ij == kl) fac *= 0.5;
-                        const double C[3] = {Ak.x, Ak.y, Ak.z}, CD[3] = {CDk.x, CDk.y, CDk.z};
-                        group_eval_block<LA, LB, LC, LD, GS>(sm, a, pb, pk, A, AB, C, CD, fac, gl, gmask);
+                        R fac = (R)1;
+                        if (Ab.w != 0.0) fac *= (R)0.5;
+                        if (Ak.w != 0.0) fac *= (R)0.5;
+                        if (a.same && ij == kl) fac *= (R)0.5;
+                        const R C[3] = {(R)(Ak.x - Ab.x), (R)(Ak.y - Ab.y), (R)(Ak.z - Ab.z)};
+                        const R CD[3] = {(R)CDk.x, (R)CDk.y, (R)CDk.z};
+                        group_eval_block<LA, LB, LC, LD, GS, R>(sm, a, pb, pk, Ab, A, AB, C, CD, fac, gl, gmask);
                         if (gl == 0) {
                                 nq++;
                                 npq += (unsigned long long)pb.y * pk.y;
                         }
-                        const double *G = sm + S::G;
+                        const R *G = reinterpret_cast<const R *>(sm) + S::G;
                         const int ic = sk.x, id = sk.y;
                         for (int s = 0; s < a.n_dm; s++) {
                                 if (a.with_j) {
@@ -562,12 +606,12 @@ __global__ void __launch_bounds__(128) jk_warp_kernel(JKArgs a, int chunk_q)
                                         __syncwarp(gmask);
                                         for (int t = gl; t < K::NCD; t += GS) {
                                                 double v = 0.0;
-                                                for (int u = 0; u < K::NAB; u++) v += G[u * K::NCD + t] * dsab[u];
+                                                for (int u = 0; u < K::NAB; u++) v += (double)G[u * K::NCD + t] * dsab[u];
                                                 atomicAdd(J + (ic + t / K::ND) * n + id + t % K::ND, v);
                                         }
                                         for (int t = gl; t < K::NAB; t += GS) {
                                                 double v = 0.0;
-                                                for (int u = 0; u < K::NCD; u++) v += G[t * K::NCD + u] * dscd[u];
+                                                for (int u = 0; u < K::NCD; u++) v += (double)G[t * K::NCD + u] * dscd[u];
                                                 atomicAdd(J + (ia + t / K::NB) * n + ib + t % K::NB, v);
                                         }
                                         __syncwarp(gmask);
@@ -589,7 +633,7 @@ __global__ void __launch_bounds__(128) jk_warp_kernel(JKArgs a, int chunk_q)
                                                         double v = 0.0;
                                                         for (int b = 0; b < K::NB; b++)
                                                                 for (int c = 0; c < K::NC; c++)
-                                                                        v += G[((x * K::NB + b) * K::NC + c) * K::ND + d] * xbc[b * K::NC + c];
+                                                                        v += (double)G[((x * K::NB + b) * K::NC + c) * K::ND + d] * xbc[b * K::NC + c];
                                                         atomicAdd(Kt + (ia + x) * n + id + d, v);
                                                 }
                                                 // K[a,c] += G X[b,d]
@@ -598,7 +642,7 @@ __global__ void __launch_bounds__(128) jk_warp_kernel(JKArgs a, int chunk_q)
                                                         double v = 0.0;
                                                         for (int b = 0; b < K::NB; b++)
                                                                 for (int d = 0; d < K::ND; d++)
-                                                                        v += G[((x * K::NB + b) * K::NC + c) * K::ND + d] * xbd[b * K::ND + d];
+                                                                        v += (double)G[((x * K::NB + b) * K::NC + c) * K::ND + d] * xbd[b * K::ND + d];
                                                         atomicAdd(Kt + (ia + x) * n + ic + c, v);
                                                 }
                                                 // K[b,d] += G X[a,c]
@@ -607,7 +651,7 @@ __global__ void __launch_bounds__(128) jk_warp_kernel(JKArgs a, int chunk_q)
                                                         double v = 0.0;
                                                         for (int x = 0; x < K::NA; x++)
                                                                 for (int c = 0; c < K::NC; c++)
-                                                                        v += G[((x * K::NB + b) * K::NC + c) * K::ND + d] * xac[x * K::NC + c];
+                                                                        v += (double)G[((x * K::NB + b) * K::NC + c) * K::ND + d] * xac[x * K::NC + c];
                                                         atomicAdd(Kt + (ib + b) * n + id + d, v);
                                                 }
                                                 // K[b,c] += G X[a,d]
@@ -616,7 +660,7 @@ __global__ void __launch_bounds__(128) jk_warp_kernel(JKArgs a, int chunk_q)
                                                         double v = 0.0;
                                                         for (int x = 0; x < K::NA; x++)
                                                                 for (int d = 0; d < K::ND; d++)
-                                                                        v += G[((x * K::NB + b) * K::NC + c) * K::ND + d] * xad[x * K::ND + d];
+                                                                        v += (double)G[((x * K::NB + b) * K::NC + c) * K::ND + d] * xad[x * K::ND + d];
                                                         atomicAdd(Kt + (ib + b) * n + ic + c, v);
                                                 }
                                                 __syncwarp(gmask);
@@ -650,8 +694,8 @@ template <int LA, int LB>
 __global__ void __launch_bounds__(32) qcond_kernel(QArgs q)
 {
         using K = Class4<LA, LB, LA, LB>;
-        using S = WarpSmem<LA, LB, LA, LB>;
-        extern __shared__ double smem_dyn[];
+        using S = WarpSmem<LA, LB, LA, LB, double>;
+        extern __shared__ __align__(32) double smem_dyn[];
         double *sm = smem_dyn;
         const int lane = threadIdx.x & 31;
         const int ij = blockIdx.x;
@@ -665,8 +709,8 @@ __global__ void __launch_bounds__(32) qcond_kernel(QArgs q)
         const int2 pr = q.pairs.pr[ij];
         const double4 Av = q.pairs.A[ij];
         const double4 ABv = q.pairs.AB[ij];
-        const double A[3] = {Av.x, Av.y, Av.z}, AB[3] = {ABv.x, ABv.y, ABv.z};
-        group_eval_block<LA, LB, LA, LB, 32>(sm, a, pr, pr, A, AB, A, AB, 1.0, lane, 0xffffffffu);
+        const double A[3] = {0.0, 0.0, 0.0}, AB[3] = {ABv.x, ABv.y, ABv.z};
+        group_eval_block<LA, LB, LA, LB, 32, double>(sm, a, pr, pr, Av, A, AB, A, AB, 1.0, lane, 0xffffffffu);
         const double *G = sm + S::G;
         const int nsa = q.cart ? K::NA : 2 * LA + 1, nsb = q.cart ? K::NB : 2 * LB + 1;
         const double *ca = q.c2s + LA * 100, *cb = q.c2s + LB * 100;

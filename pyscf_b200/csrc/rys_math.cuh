@@ -47,6 +47,13 @@
 
 namespace b200jk {
 
+// arithmetic helpers for the two compute types (double: FP64 path, float:
+// FP32 evaluation of the mixed-precision path)
+B2_HD double b2fma(double a, double b, double c) { return fma(a, b, c); }
+B2_HD float b2fma(float a, float b, float c) { return fmaf(a, b, c); }
+B2_HD double b2sqrt(double a) { return sqrt(a); }
+B2_HD float b2sqrt(float a) { return sqrtf(a); }
+
 B2_HDC int ncart(int l) { return (l + 1) * (l + 2) / 2; }
 B2_HDC int nsph(int l) { return 2 * l + 1; }
 
@@ -119,91 +126,105 @@ inline void rys_pad_table(const double *packed, double *out)
         }
 }
 
-struct alignas(32) RysRow4 {
-        double v[4];
+template <typename R>
+struct alignas(4 * sizeof(R)) RysVec4 {
+        R v[4];
 };
 
-// Horner evaluation of one padded row at x
-B2_HD double rys_poly(const double *__restrict__ row, double x)
+// Horner evaluation of one padded row at x (double or float table)
+template <typename R>
+B2_HD R rys_poly(const R *__restrict__ row, R x)
 {
-        const RysRow4 *q = reinterpret_cast<const RysRow4 *>(row);
-        const RysRow4 q0 = q[0], q1 = q[1], q2 = q[2], q3 = q[3];
-        double r = q3.v[1];
-        r = fma(r, x, q3.v[0]);
-        r = fma(r, x, q2.v[3]); r = fma(r, x, q2.v[2]); r = fma(r, x, q2.v[1]); r = fma(r, x, q2.v[0]);
-        r = fma(r, x, q1.v[3]); r = fma(r, x, q1.v[2]); r = fma(r, x, q1.v[1]); r = fma(r, x, q1.v[0]);
-        r = fma(r, x, q0.v[3]); r = fma(r, x, q0.v[2]); r = fma(r, x, q0.v[1]); r = fma(r, x, q0.v[0]);
+        const RysVec4<R> *q = reinterpret_cast<const RysVec4<R> *>(row);
+        const RysVec4<R> q0 = q[0], q1 = q[1], q2 = q[2], q3 = q[3];
+        R r = q3.v[1];
+        r = b2fma(r, x, q3.v[0]);
+        r = b2fma(r, x, q2.v[3]); r = b2fma(r, x, q2.v[2]); r = b2fma(r, x, q2.v[1]); r = b2fma(r, x, q2.v[0]);
+        r = b2fma(r, x, q1.v[3]); r = b2fma(r, x, q1.v[2]); r = b2fma(r, x, q1.v[1]); r = b2fma(r, x, q1.v[0]);
+        r = b2fma(r, x, q0.v[3]); r = b2fma(r, x, q0.v[2]); r = b2fma(r, x, q0.v[1]); r = b2fma(r, x, q0.v[0]);
         return r;
 }
 
 // Roots u[i] and weights w[i] of the order-NR Rys rule at argument T from the
 // padded table.  NaN or huge T take the asymptotic branch, so the table is
 // never indexed out of range.
-template <int NR>
-B2_HD void rys_roots(double T, const double *__restrict__ table, double *u, double *w)
+// Same with `tab` pointing at the order-NR slice of the padded table (for
+// example a copy of that slice in shared memory).
+template <int NR, typename R>
+B2_HD void rys_roots_slice(R T, const R *__restrict__ tab, R *u, R *w)
 {
-        if (!(T < (double)rys_t_asym(NR))) {
-                const double it = 1.0 / T;
-                const double st = sqrt(it);
+        if (!(T < (R)rys_t_asym(NR))) {
+                const R it = (R)1 / T;
+                const R st = b2sqrt(it);
 #pragma unroll
                 for (int i = 0; i < NR; i++) {
-                        u[i] = rys_herm_x2(NR * (NR - 1) / 2 + i) * it;
-                        w[i] = rys_herm_w(NR * (NR - 1) / 2 + i) * st;
+                        u[i] = (R)rys_herm_x2(NR * (NR - 1) / 2 + i) * it;
+                        w[i] = (R)rys_herm_w(NR * (NR - 1) / 2 + i) * st;
                 }
                 return;
         }
         const int p = (int)T;
-        const double x = 2.0 * (T - (double)p) - 1.0;
-        const double *c = table + rys_padded_offset(NR) + p * (2 * NR * RYS_ROW);
+        const R x = (R)2 * (T - (R)p) - (R)1;
+        const R *c = tab + p * (2 * NR * RYS_ROW);
 #pragma unroll
         for (int f = 0; f < NR; f++) {
-                u[f] = rys_poly(c + f * RYS_ROW, x);
-                w[f] = rys_poly(c + (NR + f) * RYS_ROW, x);
+                u[f] = rys_poly<R>(c + f * RYS_ROW, x);
+                w[f] = rys_poly<R>(c + (NR + f) * RYS_ROW, x);
         }
 }
 
-// Root r (and its weight) of the order-NR rule only.
 template <int NR>
-B2_HD void rys_root_one(double T, const double *__restrict__ table, int r, double &u, double &w)
+B2_HD void rys_roots(double T, const double *__restrict__ table, double *u, double *w)
 {
-        if (!(T < (double)rys_t_asym(NR))) {
-                const double it = 1.0 / T;
+        rys_roots_slice<NR, double>(T, table + rys_padded_offset(NR), u, w);
+}
+
+// doubles in the order-NR slice of the padded table
+B2_HDC int rys_slice_size(int nr) { return rys_t_asym(nr) * 2 * nr * RYS_ROW; }
+
+// Root r (and its weight) of the order-NR rule only; `table` is the full
+// padded table of type R.
+template <int NR, typename R>
+B2_HD void rys_root_one(R T, const R *__restrict__ table, int r, R &u, R &w)
+{
+        if (!(T < (R)rys_t_asym(NR))) {
+                const R it = (R)1 / T;
                 double x2 = rys_herm_x2(NR * (NR - 1) / 2), wh = rys_herm_w(NR * (NR - 1) / 2);
 #pragma unroll
                 for (int i = 1; i < NR; i++)
                         if (r == i) { x2 = rys_herm_x2(NR * (NR - 1) / 2 + i); wh = rys_herm_w(NR * (NR - 1) / 2 + i); }
-                u = x2 * it;
-                w = wh * sqrt(it);
+                u = (R)x2 * it;
+                w = (R)wh * b2sqrt(it);
                 return;
         }
         const int p = (int)T;
-        const double x = 2.0 * (T - (double)p) - 1.0;
-        const double *c = table + rys_padded_offset(NR) + p * (2 * NR * RYS_ROW);
-        u = rys_poly(c + r * RYS_ROW, x);
-        w = rys_poly(c + (NR + r) * RYS_ROW, x);
+        const R x = (R)2 * (T - (R)p) - (R)1;
+        const R *c = table + rys_padded_offset(NR) + p * (2 * NR * RYS_ROW);
+        u = rys_poly<R>(c + r * RYS_ROW, x);
+        w = rys_poly<R>(c + (NR + r) * RYS_ROW, x);
 }
 
 // 2D vertical recurrence: g[e*NF + f], e < NE, f < NF.
-template <int NE, int NF>
-B2_HD void vrr2d(double *g, double g00, double c00, double c00p, double b10, double b01, double b00)
+template <int NE, int NF, typename R>
+B2_HD void vrr2d(R *g, R g00, R c00, R c00p, R b10, R b01, R b00)
 {
         g[0] = g00;
         if (NE > 1) g[NF] = c00 * g00;
 #pragma unroll
-        for (int e = 1; e < NE - 1; e++) g[(e + 1) * NF] = c00 * g[e * NF] + (double)e * b10 * g[(e - 1) * NF];
+        for (int e = 1; e < NE - 1; e++) g[(e + 1) * NF] = c00 * g[e * NF] + (R)e * b10 * g[(e - 1) * NF];
         if (NF > 1) {
 #pragma unroll
                 for (int e = 0; e < NE; e++) {
-                        double v = c00p * g[e * NF];
-                        if (e > 0) v += (double)e * b00 * g[(e - 1) * NF];
+                        R v = c00p * g[e * NF];
+                        if (e > 0) v += (R)e * b00 * g[(e - 1) * NF];
                         g[e * NF + 1] = v;
                 }
 #pragma unroll
                 for (int f = 1; f < NF - 1; f++) {
 #pragma unroll
                         for (int e = 0; e < NE; e++) {
-                                double v = c00p * g[e * NF + f] + (double)f * b01 * g[e * NF + f - 1];
-                                if (e > 0) v += (double)e * b00 * g[(e - 1) * NF + f];
+                                R v = c00p * g[e * NF + f] + (R)f * b01 * g[e * NF + f - 1];
+                                if (e > 0) v += (R)e * b00 * g[(e - 1) * NF + f];
                                 g[e * NF + f + 1] = v;
                         }
                 }
@@ -212,29 +233,29 @@ B2_HD void vrr2d(double *g, double g00, double c00, double c00p, double b10, dou
 
 // 2D horizontal transfer: from g[e][f] (e <= LA+LB, f <= LC+LD) to
 // h[((a*(LB+1) + b)*(LC+1) + c)*(LD+1) + d].
-template <int LA, int LB, int LC, int LD>
-B2_HD void hrr2d(const double *g, double *h, double ab, double cd)
+template <int LA, int LB, int LC, int LD, typename R>
+B2_HD void hrr2d(const R *g, R *h, R ab, R cd)
 {
         constexpr int NF = LC + LD + 1;
-        double abp[LB + 1], cdp[LD + 1];
-        abp[0] = 1.0;
+        R abp[LB + 1], cdp[LD + 1];
+        abp[0] = (R)1;
 #pragma unroll
         for (int k = 1; k <= LB; k++) abp[k] = abp[k - 1] * ab;
-        cdp[0] = 1.0;
+        cdp[0] = (R)1;
 #pragma unroll
         for (int k = 1; k <= LD; k++) cdp[k] = cdp[k - 1] * cd;
         // t[(a*(LB+1)+b)*NF + f]
-        double t[(LA + 1) * (LB + 1) * NF];
+        R t[(LA + 1) * (LB + 1) * NF];
 #pragma unroll
         for (int a = 0; a <= LA; a++) {
 #pragma unroll
                 for (int b = 0; b <= LB; b++) {
 #pragma unroll
                         for (int f = 0; f < NF; f++) {
-                                double v = 0.0;
+                                R v = (R)0;
 #pragma unroll
                                 for (int k = 0; k <= b; k++)
-                                        v += (double)binom(b, k) * abp[b - k] * g[(a + k) * NF + f];
+                                        v += (R)binom(b, k) * abp[b - k] * g[(a + k) * NF + f];
                                 t[(a * (LB + 1) + b) * NF + f] = v;
                         }
                 }
@@ -245,10 +266,10 @@ B2_HD void hrr2d(const double *g, double *h, double ab, double cd)
                 for (int c = 0; c <= LC; c++) {
 #pragma unroll
                         for (int d = 0; d <= LD; d++) {
-                                double v = 0.0;
+                                R v = (R)0;
 #pragma unroll
                                 for (int k = 0; k <= d; k++)
-                                        v += (double)binom(d, k) * cdp[d - k] * t[ab_ * NF + c + k];
+                                        v += (R)binom(d, k) * cdp[d - k] * t[ab_ * NF + c + k];
                                 h[(ab_ * (LC + 1) + c) * (LD + 1) + d] = v;
                         }
                 }
@@ -269,20 +290,23 @@ struct Class4 {
 };
 
 // Scalars of one primitive quartet shared by all roots.  Primitive pairs
-// carry 1/(2p), so a quartet needs one division and one square root.
+// carry 1/(2p), so a quartet needs one division and one square root.  R is
+// the compute type (double, or float for the FP32 quartets of the mixed path).
+template <typename R>
 struct PrimQ {
-        double PA[3], QC[3], PQ[3];
-        double ipq;          // 1/(p+q)
-        double qf0, pf0;     // q/(p+q), p/(p+q)
-        double i2p, i2q;     // 1/(2p), 1/(2q)
-        double T;            // rho |PQ|^2
-        double pref;         // 2 pi^{5/2} K_ab K_cd / (p q sqrt(p+q))
+        R PA[3], QC[3], PQ[3];
+        R ipq;          // 1/(p+q)
+        R qf0, pf0;     // q/(p+q), p/(p+q)
+        R i2p, i2q;     // 1/(2p), 1/(2q)
+        R T;            // rho |PQ|^2
+        R pref;         // 2 pi^{5/2} K_ab K_cd / (p q sqrt(p+q))
 };
 
-B2_HD void prim_setup(PrimQ &s, double p, double i2p, const double P[3], double q, double i2q,
-                      const double Q[3], const double A[3], const double C[3], double kk)
+template <typename R>
+B2_HD void prim_setup(PrimQ<R> &s, R p, R i2p, const R P[3], R q, R i2q, const R Q[3], const R A[3],
+                      const R C[3], R kk)
 {
-        s.ipq = 1.0 / (p + q);
+        s.ipq = (R)1 / (p + q);
         s.qf0 = q * s.ipq;
         s.pf0 = p * s.ipq;
         s.i2p = i2p;
@@ -294,20 +318,22 @@ B2_HD void prim_setup(PrimQ &s, double p, double i2p, const double P[3], double 
                 s.PQ[x] = P[x] - Q[x];
         }
         s.T = p * s.qf0 * (s.PQ[0] * s.PQ[0] + s.PQ[1] * s.PQ[1] + s.PQ[2] * s.PQ[2]);
-        s.pref = 34.98683665524972497 * kk * (4.0 * i2p * i2q) * sqrt(s.ipq);
+        s.pref = (R)34.98683665524972497 * kk * ((R)4 * i2p * i2q) * b2sqrt(s.ipq);
 }
 
 // Root-dependent recurrence coefficients of one primitive quartet.
+template <typename R>
 struct RysCoef {
-        double c00[3], c00p[3], b10, b01, b00;
+        R c00[3], c00p[3], b10, b01, b00;
 };
 
-B2_HD void rys_coef(RysCoef &rc, double u, const PrimQ &s)
+template <typename R>
+B2_HD void rys_coef(RysCoef<R> &rc, R u, const PrimQ<R> &s)
 {
-        const double qf = s.qf0 * u, pf = s.pf0 * u;
-        rc.b00 = 0.5 * u * s.ipq;
-        rc.b10 = s.i2p * (1.0 - qf);
-        rc.b01 = s.i2q * (1.0 - pf);
+        const R qf = s.qf0 * u, pf = s.pf0 * u;
+        rc.b00 = (R)0.5 * u * s.ipq;
+        rc.b10 = s.i2p * ((R)1 - qf);
+        rc.b01 = s.i2q * ((R)1 - pf);
 #pragma unroll
         for (int x = 0; x < 3; x++) {
                 rc.c00[x] = s.PA[x] - qf * s.PQ[x];
@@ -338,8 +364,8 @@ B2_HD void assemble_all(double *G, const double *hx, const double *hy, const dou
 
 // Components [BASE, BASE + N) of the block only (register kernels that
 // keep one part of the block at a time), into Gp[0..N).
-template <int LA, int LB, int LC, int LD, int T>
-B2_HD void assemble_one_to(double &g, const double *hx, const double *hy, const double *hz)
+template <int LA, int LB, int LC, int LD, int T, typename R>
+B2_HD void assemble_one_to(R &g, const R *hx, const R *hy, const R *hz)
 {
         using K = Class4<LA, LB, LC, LD>;
         constexpr int id = T % K::ND, ic = (T / K::ND) % K::NC, ib = (T / K::NCD) % K::NB, ia = T / (K::NCD * K::NB);
@@ -349,40 +375,39 @@ B2_HD void assemble_one_to(double &g, const double *hx, const double *hy, const 
         g += hx[ox] * hy[oy] * hz[oz];
 }
 
-template <int LA, int LB, int LC, int LD, int BASE, int... Ts>
-B2_HD void assemble_part(double *Gp, const double *hx, const double *hy, const double *hz,
-                         std::integer_sequence<int, Ts...>)
+template <int LA, int LB, int LC, int LD, int BASE, typename R, int... Ts>
+B2_HD void assemble_part(R *Gp, const R *hx, const R *hy, const R *hz, std::integer_sequence<int, Ts...>)
 {
-        (assemble_one_to<LA, LB, LC, LD, BASE + Ts>(Gp[Ts], hx, hy, hz), ...);
+        (assemble_one_to<LA, LB, LC, LD, BASE + Ts, R>(Gp[Ts], hx, hy, hz), ...);
 }
 
 // One primitive quartet into components [BASE, BASE + N) of the block.
-template <int LA, int LB, int LC, int LD, int BASE, int N>
-B2_HD void add_prim_quartet_part(double *Gp, const double *table, const PrimQ &s,
-                                 const double AB[3], const double CD[3])
+// `tab` is the order-NR slice of the padded table of type R.
+template <int LA, int LB, int LC, int LD, int BASE, int N, typename R>
+B2_HD void add_prim_quartet_part(R *Gp, const R *tab, const PrimQ<R> &s, const R AB[3], const R CD[3])
 {
         using K = Class4<LA, LB, LC, LD>;
-        double u[K::NR], w[K::NR];
-        rys_roots<K::NR>(s.T, table, u, w);
+        R u[K::NR], w[K::NR];
+        rys_roots_slice<K::NR, R>(s.T, tab, u, w);
 #pragma unroll
         for (int r = 0; r < K::NR; r++) {
-                RysCoef rc;
-                rys_coef(rc, u[r], s);
-                double g[K::NE * K::NF];
-                double hx[K::SA], hy[K::SA], hz[K::SA];
-                vrr2d<K::NE, K::NF>(g, 1.0, rc.c00[0], rc.c00p[0], rc.b10, rc.b01, rc.b00);
-                hrr2d<LA, LB, LC, LD>(g, hx, AB[0], CD[0]);
-                vrr2d<K::NE, K::NF>(g, 1.0, rc.c00[1], rc.c00p[1], rc.b10, rc.b01, rc.b00);
-                hrr2d<LA, LB, LC, LD>(g, hy, AB[1], CD[1]);
-                vrr2d<K::NE, K::NF>(g, s.pref * w[r], rc.c00[2], rc.c00p[2], rc.b10, rc.b01, rc.b00);
-                hrr2d<LA, LB, LC, LD>(g, hz, AB[2], CD[2]);
-                assemble_part<LA, LB, LC, LD, BASE>(Gp, hx, hy, hz, std::make_integer_sequence<int, N>{});
+                RysCoef<R> rc;
+                rys_coef<R>(rc, u[r], s);
+                R g[K::NE * K::NF];
+                R hx[K::SA], hy[K::SA], hz[K::SA];
+                vrr2d<K::NE, K::NF, R>(g, (R)1, rc.c00[0], rc.c00p[0], rc.b10, rc.b01, rc.b00);
+                hrr2d<LA, LB, LC, LD, R>(g, hx, AB[0], CD[0]);
+                vrr2d<K::NE, K::NF, R>(g, (R)1, rc.c00[1], rc.c00p[1], rc.b10, rc.b01, rc.b00);
+                hrr2d<LA, LB, LC, LD, R>(g, hy, AB[1], CD[1]);
+                vrr2d<K::NE, K::NF, R>(g, s.pref * w[r], rc.c00[2], rc.c00p[2], rc.b10, rc.b01, rc.b00);
+                hrr2d<LA, LB, LC, LD, R>(g, hz, AB[2], CD[2]);
+                assemble_part<LA, LB, LC, LD, BASE, R>(Gp, hx, hy, hz, std::make_integer_sequence<int, N>{});
         }
 }
 
 // Add one primitive quartet to the Cartesian block G[((a*NB+b)*NC+c)*ND+d].
 template <int LA, int LB, int LC, int LD>
-B2_HD void add_prim_quartet(double *G, const double *table, const PrimQ &s, const double AB[3],
+B2_HD void add_prim_quartet(double *G, const double *table, const PrimQ<double> &s, const double AB[3],
                             const double CD[3])
 {
         using K = Class4<LA, LB, LC, LD>;
@@ -390,8 +415,8 @@ B2_HD void add_prim_quartet(double *G, const double *table, const PrimQ &s, cons
         rys_roots<K::NR>(s.T, table, u, w);
 #pragma unroll
         for (int r = 0; r < K::NR; r++) {
-                RysCoef rc;
-                rys_coef(rc, u[r], s);
+                RysCoef<double> rc;
+                rys_coef<double>(rc, u[r], s);
                 double g[K::NE * K::NF];
                 double hx[K::SA], hy[K::SA], hz[K::SA];
                 vrr2d<K::NE, K::NF>(g, 1.0, rc.c00[0], rc.c00p[0], rc.b10, rc.b01, rc.b00);
@@ -422,13 +447,13 @@ B2_HD void add_prim_quartet(double *G, const double *table, const PrimQ &s, cons
 
 // One (root, direction) slice of the 2D integrals after the transfer,
 // written to h (used by the warp-cooperative kernels).
-template <int LA, int LB, int LC, int LD>
-B2_HD void rys_2d_slice(double *h, double g00, const RysCoef &rc, int dir, double ab, double cd)
+template <int LA, int LB, int LC, int LD, typename R>
+B2_HD void rys_2d_slice(R *h, R g00, const RysCoef<R> &rc, int dir, R ab, R cd)
 {
         using K = Class4<LA, LB, LC, LD>;
-        double g[K::NE * K::NF];
-        vrr2d<K::NE, K::NF>(g, g00, rc.c00[dir], rc.c00p[dir], rc.b10, rc.b01, rc.b00);
-        hrr2d<LA, LB, LC, LD>(g, h, ab, cd);
+        R g[K::NE * K::NF];
+        vrr2d<K::NE, K::NF, R>(g, g00, rc.c00[dir], rc.c00p[dir], rc.b10, rc.b01, rc.b00);
+        hrr2d<LA, LB, LC, LD, R>(g, h, ab, cd);
 }
 
 } // namespace b200jk

@@ -18,13 +18,14 @@ B200JK_EUNSUPPORTED = 2
 B200JK_ECUDA = 3
 B200JK_ENOMEM = 4
 PREC_FP64 = 0
+PREC_MIXED = 1
 
 # every entry point of include/b200jk.h
 EXPORTS = (
     'b200jk_version', 'b200jk_last_error', 'b200jk_device_count', 'b200jk_plan_create',
     'b200jk_plan_destroy', 'b200jk_plan_dims', 'b200jk_get_q_cond', 'b200jk_get_jk',
     'b200jk_stats', 'b200jk_hostcheck_cart_quartet', 'b200jk_class_stats', 'b200jk_set_profiling',
-    'b200jk_measure_fp64_peak', 'b200jk_get_jk_noalloc',
+    'b200jk_measure_fp64_peak', 'b200jk_get_jk_noalloc', 'b200jk_set_mixed_threshold',
 )
 
 
@@ -40,13 +41,14 @@ class Stats(ctypes.Structure):
                 ('flops', ctypes.c_double), ('last_build_ms', ctypes.c_double),
                 ('nao', ctypes.c_int32), ('nao_cart', ctypes.c_int32),
                 ('nbas', ctypes.c_int32), ('nseg', ctypes.c_int32),
-                ('kernel_launches', ctypes.c_int64)]
+                ('kernel_launches', ctypes.c_int64), ('fp32_quartets', ctypes.c_int64),
+                ('fp32_prim_quartets', ctypes.c_int64)]
 
 
 class ClassStat(ctypes.Structure):
     _fields_ = [('la', ctypes.c_int32), ('lb', ctypes.c_int32), ('lc', ctypes.c_int32), ('ld', ctypes.c_int32),
                 ('quartets', ctypes.c_int64), ('prim_quartets', ctypes.c_int64), ('ms', ctypes.c_double),
-                ('family', ctypes.c_int32), ('pad', ctypes.c_int32)]
+                ('family', ctypes.c_int32), ('pad', ctypes.c_int32), ('fp32_quartets', ctypes.c_int64)]
 
 
 _lib = None
@@ -77,6 +79,7 @@ def load(path=LIB_PATH):
         lib.b200jk_set_profiling.argtypes = [vp, ip]
         lib.b200jk_measure_fp64_peak.argtypes = [ip, ctypes.POINTER(dp)]
         lib.b200jk_get_jk_noalloc.argtypes = [vp, vp, ip, ip, ip, ip, vp, vp, vp]
+        lib.b200jk_set_mixed_threshold.argtypes = [vp, dp]
         _lib = lib
         return lib
 
@@ -149,6 +152,10 @@ class Plan:
 
     def set_profiling(self, on=True):
         check(load().b200jk_set_profiling(self._h, int(bool(on))))
+
+    def set_mixed_threshold(self, tau):
+        """tau of precision=PREC_MIXED: quartets with q_ij q_kl max|D| < tau run in float32."""
+        check(load().b200jk_set_mixed_threshold(self._h, float(tau)))
 
     def get_jk(self, dms, hermi=1, with_j=True, with_k=True, out_j=None, out_k=None,
                precision=PREC_FP64, stream=None):

@@ -1,0 +1,98 @@
+"""Mixed precision (B200JK_PREC_MIXED) of the CUDA J/K build.
+
+Quartets whose Schwarz bound times max|D| is below tau are evaluated in
+float32 (roots, recurrences, assembly) and contracted and accumulated in
+float64; the rest run the float64 kernels.  Reference values are the
+reference's own J/K (tests/golden, PySCF's direct-SCF drivers) and RHF
+energy.  The float64 path of the same plan is the baseline for the error.
+
+Tolerances: the RHF energy with mixed builds stays within 1e-6 Eh of the
+reference's (the accuracy target of the mixed mode); single builds are
+bounded relative to max|J|, max|K|.
+"""
+import numpy
+import pytest
+
+from conftest import load_fixture
+
+pytestmark = pytest.mark.gpu
+
+TOL_E_MIXED = 1e-6
+
+
+@pytest.fixture(scope='module')
+def b2():
+    from pyscf_b200 import lib
+    if lib.device_count() == 0:
+        pytest.fail('no CUDA device visible to libb200jk')
+    return lib
+
+
+def plan_for(b2, f, tol=1e-13):
+    return b2.Plan(f['atm'], f['bas'], f['env'], cart=bool(f['cart']), direct_scf_tol=tol)
+
+
+def test_mixed_tau_zero_is_fp64(b2):
+    f = load_fixture('h2o8_vdz')
+    p = plan_for(b2, f)
+    p.set_mixed_threshold(0.0)
+    vj, vk = p.get_jk(f['dm_conv'], hermi=1, precision=b2.PREC_MIXED)
+    assert p.stats()['fp32_quartets'] == 0
+    assert abs(vj - f['vj_conv']).max() < 1e-10
+    assert abs(vk - f['vk_conv']).max() < 1e-10
+
+
+@pytest.mark.parametrize('name', ['h2o8_vdz', 'h2o2_vtz'])
+def test_mixed_all_fp32(b2, name):
+    """tau above every bound: every quartet class (s..f) runs its float32
+    kernel; the result keeps float32 accuracy against the reference."""
+    f = load_fixture(name)
+    p = plan_for(b2, f)
+    p.set_mixed_threshold(1e30)
+    vj, vk = p.get_jk(f['dm_rand'], hermi=1, precision=b2.PREC_MIXED)
+    st = p.stats()
+    assert st['fp32_quartets'] == st['quartets'] > 0
+    assert abs(vj - f['vj_rand']).max() < 2e-5 * abs(f['vj_rand']).max()
+    assert abs(vk - f['vk_rand']).max() < 2e-5 * abs(f['vk_rand']).max()
+    # the split is exact: all quartets are still there
+    p.set_mixed_threshold(0.0)
+    p.get_jk(f['dm_rand'], hermi=1, precision=b2.PREC_MIXED)
+    assert p.stats()['quartets'] == st['quartets']
+
+
+def test_mixed_default_threshold(b2):
+    f = load_fixture('h2o8_vdz')
+    p = plan_for(b2, f)
+    vj, vk = p.get_jk(f['dm_conv'], hermi=1, precision=b2.PREC_MIXED)
+    st = p.stats()
+    assert 0 < st['fp32_quartets'] < st['quartets']
+    assert abs(vj - f['vj_conv']).max() < 1e-8
+    assert abs(vk - f['vk_conv']).max() < 1e-8
+
+
+def test_mixed_general_density(b2):
+    f = load_fixture('h2o2_vtz')
+    p = plan_for(b2, f)
+    p.set_mixed_threshold(1e30)
+    vj, vk = p.get_jk(f['dm_ns'], hermi=0, precision=b2.PREC_MIXED)
+    assert abs(vj - f['vj_ns']).max() < 2e-5 * abs(f['vj_ns']).max()
+    assert abs(vk - f['vk_ns']).max() < 2e-5 * abs(f['vk_ns']).max()
+
+
+def test_mixed_scf_energy(b2):
+    """RHF with incremental mixed-precision builds: as the density change
+    shrinks, more quartets move to float32; the energy stays within 1e-6 Eh."""
+    from pyscf_b200 import rhf
+    f = load_fixture('h2o8_vdz')
+    p = plan_for(b2, f)
+    frac = []
+
+    def get_jk(dm):
+        r = p.get_jk(dm, hermi=1, precision=b2.PREC_MIXED)
+        st = p.stats()
+        frac.append(st['fp32_quartets'] / st['quartets'])
+        return r
+    conv, e, *_ = rhf.kernel(f['hcore'], f['ovlp'], int(f['nelec']), float(f['e_nuc']), get_jk, conv_tol=1e-10)
+    assert conv
+    assert abs(e - float(f['e_rhf'])) < TOL_E_MIXED
+    assert frac[-1] > frac[0]
