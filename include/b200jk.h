@@ -156,6 +156,12 @@ int b200jk_measure_fp64_peak(int device, double *tflops);
 int b200jk_hostcheck_cart_quartet(const int32_t *atm, int natm, const int32_t *bas, int nbas,
                                   const double *env, const int32_t *shls, double *out);
 
+/* The same block evaluated in float32 with the float32 tables, as the float32
+ * pass of B200JK_PREC_MIXED does (coordinates relative to the first centre);
+ * out is float64.  No reference counterpart (validation only). */
+int b200jk_hostcheck_cart_quartet_fp32(const int32_t *atm, int natm, const int32_t *bas, int nbas,
+                                       const double *env, const int32_t *shls, double *out);
+
 #ifdef __cplusplus
 }
 #endif

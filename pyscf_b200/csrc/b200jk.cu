@@ -59,8 +59,9 @@ static const int NPAIRCLASS = (LMAX + 1) * (LMAX + 2) / 2;
 static inline int pair_class(int la, int lb) { return la * (la + 1) / 2 + lb; }
 
 __device__ __align__(32) double d_rys_table[rys_padded_size()];
-// the same tables rounded to float32, for the float32 pass of mixed precision
-__device__ __align__(32) float d_rys_table_f[rys_padded_size()];
+// the float32 tables (degree 7, earlier large-T limit) of the float32 pass of
+// mixed precision
+__device__ __align__(32) float d_rys_table_f[RYS_F_SIZE];
 
 // ---------------------------------------------------------------------------
 // real solid harmonics r^l Y_lm (unit-normalised Y_lm), rows m = -l..l
@@ -342,10 +343,9 @@ static int ensure_tables(int device)
         std::call_once(g_table_once[device], [device]() {
                 std::vector<double> padded(rys_padded_size());
                 rys_pad_table(rys_table_data, padded.data());
-                std::vector<float> padded_f(padded.begin(), padded.end());
                 g_table_status[device] =
                         (cudaMemcpyToSymbol(d_rys_table, padded.data(), sizeof(double) * padded.size()) == cudaSuccess &&
-                         cudaMemcpyToSymbol(d_rys_table_f, padded_f.data(), sizeof(float) * padded_f.size()) == cudaSuccess)
+                         cudaMemcpyToSymbol(d_rys_table_f, rys_table_f_data, sizeof(float) * RYS_F_SIZE) == cudaSuccess)
                                 ? 0 : 1;
         });
         if (g_table_status[device]) return fail(B200JK_ECUDA, "could not upload the Rys tables");

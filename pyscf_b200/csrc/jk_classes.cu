@@ -35,7 +35,7 @@ int launch_one(const JKArgs &a, cudaStream_t s, int nsm, std::string &err)
                         int nb = 0;
                         if constexpr (thread) {
                                 cfg.block = 128;
-                                cfg.smem = K::NR <= 4 ? sizeof(R) * rys_slice_size(K::NR) : 0;
+                                cfg.smem = stage_table<R>(K::NR) ? sizeof(R) * rys_slice_elems<R>(K::NR) : 0;
                                 cfg.status = cudaFuncSetAttribute(jk_thread_kernel<LA, LB, LC, LD, (NP > 0 ? NP : 1), R>,
                                                                   cudaFuncAttributeMaxDynamicSharedMemorySize, (int)cfg.smem);
                                 if (cfg.status == cudaSuccess)

@@ -169,6 +169,11 @@ __device__ __forceinline__ void for_parts(F &&f, std::integer_sequence<int, Ps..
 }
 
 template <typename R> __device__ __forceinline__ const R *table_of(const JKArgs &a);
+// whether the register family stages the order-nr table slice in shared memory
+template <typename R> __host__ __device__ constexpr bool stage_table(int nr)
+{
+        return sizeof(R) == 4 || nr <= 4;
+}
 template <> __device__ __forceinline__ const double *table_of<double>(const JKArgs &a) { return a.table; }
 template <> __device__ __forceinline__ const float *table_of<float>(const JKArgs &a) { return a.table_f; }
 
@@ -180,12 +185,13 @@ __global__ void __launch_bounds__(128) jk_thread_kernel(JKArgs a)
         constexpr int NAP = K::NA / NP;            // bra components per part
         constexpr int NGP = NAP * K::NB * K::NCD;  // integrals per part
         const int lane = threadIdx.x & 31;
-        // the order-NR slice of the Rys table: staged in shared memory for up
-        // to four roots (<= 59 KB), read from global memory otherwise
+        // the order-NR slice of the Rys table: staged in shared memory when
+        // small (float64 up to four roots, <= 59 KB; float32 always, <= 27 KB),
+        // read from global memory otherwise
         extern __shared__ __align__(32) double smem_dyn[];
-        const R *tab = table_of<R>(a) + rys_padded_offset(K::NR);
-        if constexpr (K::NR <= 4) {
-                constexpr int NS = rys_slice_size(K::NR);
+        const R *tab = table_of<R>(a) + RysLayout<R>::offset(K::NR);
+        if constexpr (stage_table<R>(K::NR)) {
+                constexpr int NS = rys_slice_elems<R>(K::NR);
                 const RysVec4<R> *src = reinterpret_cast<const RysVec4<R> *>(tab);
                 RysVec4<R> *dst = reinterpret_cast<RysVec4<R> *>(smem_dyn);
                 for (int t = threadIdx.x; t < NS / 4; t += blockDim.x) dst[t] = src[t];
@@ -485,7 +491,7 @@ __device__ __forceinline__ void group_eval_block(double *sm, const JKArgs &a, in
         using S = WarpSmem<LA, LB, LC, LD, R>;
         R *G = reinterpret_cast<R *>(sm) + S::G;
         R *H = reinterpret_cast<R *>(sm) + S::H;
-        const R *table = table_of<R>(a);
+        const R *table = table_of<R>(a) + RysLayout<R>::offset(K::NR);
         for (int t = gl; t < K::NG; t += GS) G[t] = (R)0;
         for (int ip = 0; ip < pb.y; ip++) {
                 const double4 P = a.PP[pb.x + ip];

@@ -44,6 +44,7 @@
 #endif
 
 #include "rys_table.inc"
+#include "rys_table_f.inc"
 
 namespace b200jk {
 
@@ -131,13 +132,47 @@ struct alignas(4 * sizeof(R)) RysVec4 {
         R v[4];
 };
 
-// Horner evaluation of one padded row at x (double or float table)
-template <typename R>
-B2_HD R rys_poly(const R *__restrict__ row, R x)
+// Layout of the device tables per compute type.  float64: rows of RYS_ROW
+// (degree RYS_DEG, padded), large-T limit from rys_t_asym(n).  float32 (the
+// float32 pass of mixed precision): rows of RYS_F_ROW (degree RYS_F_DEG),
+// large-T limit from the smaller rys_f_t_asym(n).
+B2_HDC int rys_f_t_asym(int n)
 {
-        const RysVec4<R> *q = reinterpret_cast<const RysVec4<R> *>(row);
-        const RysVec4<R> q0 = q[0], q1 = q[1], q2 = q[2], q3 = q[3];
-        R r = q3.v[1];
+        constexpr int t[] = {RYS_F_T_ASYM_LIST};
+        return t[n];
+}
+B2_HDC int rys_f_offset(int n)
+{
+        constexpr int t[] = {RYS_F_OFFSET_LIST};
+        return t[n];
+}
+
+template <typename R> struct RysLayout;
+template <> struct RysLayout<double> {
+        static constexpr int ROW = RYS_ROW;
+        static B2_HDC int t_asym(int n) { return rys_t_asym(n); }
+        static B2_HDC int offset(int n) { return rys_padded_offset(n); }
+};
+template <> struct RysLayout<float> {
+        static constexpr int ROW = RYS_F_ROW;
+        static B2_HDC int t_asym(int n) { return rys_f_t_asym(n); }
+        static B2_HDC int offset(int n) { return rys_f_offset(n); }
+};
+
+// elements of the order-n slice of the table of type R
+template <typename R>
+B2_HDC int rys_slice_elems(int n) { return RysLayout<R>::t_asym(n) * 2 * n * RysLayout<R>::ROW; }
+
+// Horner evaluation of one row at x
+template <typename R>
+B2_HD R rys_poly(const R *__restrict__ row, R x);
+
+template <>
+B2_HD double rys_poly<double>(const double *__restrict__ row, double x)
+{
+        const RysVec4<double> *q = reinterpret_cast<const RysVec4<double> *>(row);
+        const RysVec4<double> q0 = q[0], q1 = q[1], q2 = q[2], q3 = q[3];
+        double r = q3.v[1];
         r = b2fma(r, x, q3.v[0]);
         r = b2fma(r, x, q2.v[3]); r = b2fma(r, x, q2.v[2]); r = b2fma(r, x, q2.v[1]); r = b2fma(r, x, q2.v[0]);
         r = b2fma(r, x, q1.v[3]); r = b2fma(r, x, q1.v[2]); r = b2fma(r, x, q1.v[1]); r = b2fma(r, x, q1.v[0]);
@@ -145,15 +180,26 @@ B2_HD R rys_poly(const R *__restrict__ row, R x)
         return r;
 }
 
-// Roots u[i] and weights w[i] of the order-NR Rys rule at argument T from the
-// padded table.  NaN or huge T take the asymptotic branch, so the table is
-// never indexed out of range.
-// Same with `tab` pointing at the order-NR slice of the padded table (for
-// example a copy of that slice in shared memory).
+template <>
+B2_HD float rys_poly<float>(const float *__restrict__ row, float x)
+{
+        const RysVec4<float> *q = reinterpret_cast<const RysVec4<float> *>(row);
+        const RysVec4<float> q0 = q[0], q1 = q[1];
+        float r = q1.v[3];
+        r = b2fma(r, x, q1.v[2]); r = b2fma(r, x, q1.v[1]); r = b2fma(r, x, q1.v[0]);
+        r = b2fma(r, x, q0.v[3]); r = b2fma(r, x, q0.v[2]); r = b2fma(r, x, q0.v[1]); r = b2fma(r, x, q0.v[0]);
+        return r;
+}
+
+// Roots u[i] and weights w[i] of the order-NR Rys rule at argument T, with
+// `tab` pointing at the order-NR slice of the table of type R (global memory
+// or a copy in shared memory).  NaN or huge T take the asymptotic branch, so
+// the table is never indexed out of range.
 template <int NR, typename R>
 B2_HD void rys_roots_slice(R T, const R *__restrict__ tab, R *u, R *w)
 {
-        if (!(T < (R)rys_t_asym(NR))) {
+        using L = RysLayout<R>;
+        if (!(T < (R)L::t_asym(NR))) {
                 const R it = (R)1 / T;
                 const R st = b2sqrt(it);
 #pragma unroll
@@ -165,29 +211,24 @@ B2_HD void rys_roots_slice(R T, const R *__restrict__ tab, R *u, R *w)
         }
         const int p = (int)T;
         const R x = (R)2 * (T - (R)p) - (R)1;
-        const R *c = tab + p * (2 * NR * RYS_ROW);
+        const R *c = tab + p * (2 * NR * L::ROW);
 #pragma unroll
         for (int f = 0; f < NR; f++) {
-                u[f] = rys_poly<R>(c + f * RYS_ROW, x);
-                w[f] = rys_poly<R>(c + (NR + f) * RYS_ROW, x);
+                u[f] = rys_poly<R>(c + f * L::ROW, x);
+                w[f] = rys_poly<R>(c + (NR + f) * L::ROW, x);
         }
 }
 
-template <int NR>
-B2_HD void rys_roots(double T, const double *__restrict__ table, double *u, double *w)
-{
-        rys_roots_slice<NR, double>(T, table + rys_padded_offset(NR), u, w);
-}
+// doubles in the order-NR slice of the padded float64 table
+B2_HDC int rys_slice_size(int nr) { return rys_slice_elems<double>(nr); }
 
-// doubles in the order-NR slice of the padded table
-B2_HDC int rys_slice_size(int nr) { return rys_t_asym(nr) * 2 * nr * RYS_ROW; }
-
-// Root r (and its weight) of the order-NR rule only; `table` is the full
-// padded table of type R.
+// Root r (and its weight) of the order-NR rule only; `tab` points at the
+// order-NR slice of the table of type R.
 template <int NR, typename R>
-B2_HD void rys_root_one(R T, const R *__restrict__ table, int r, R &u, R &w)
+B2_HD void rys_root_one(R T, const R *__restrict__ tab, int r, R &u, R &w)
 {
-        if (!(T < (R)rys_t_asym(NR))) {
+        using L = RysLayout<R>;
+        if (!(T < (R)L::t_asym(NR))) {
                 const R it = (R)1 / T;
                 double x2 = rys_herm_x2(NR * (NR - 1) / 2), wh = rys_herm_w(NR * (NR - 1) / 2);
 #pragma unroll
@@ -199,9 +240,9 @@ B2_HD void rys_root_one(R T, const R *__restrict__ table, int r, R &u, R &w)
         }
         const int p = (int)T;
         const R x = (R)2 * (T - (R)p) - (R)1;
-        const R *c = table + rys_padded_offset(NR) + p * (2 * NR * RYS_ROW);
-        u = rys_poly<R>(c + r * RYS_ROW, x);
-        w = rys_poly<R>(c + (NR + r) * RYS_ROW, x);
+        const R *c = tab + p * (2 * NR * L::ROW);
+        u = rys_poly<R>(c + r * L::ROW, x);
+        w = rys_poly<R>(c + (NR + r) * L::ROW, x);
 }
 
 // 2D vertical recurrence: g[e*NF + f], e < NE, f < NF.
@@ -341,29 +382,9 @@ B2_HD void rys_coef(RysCoef<R> &rc, R u, const PrimQ<R> &s)
         }
 }
 
-// G[T] += I_x I_y I_z for Cartesian component T; the offsets into the 2D
-// integrals are constant expressions, so the whole assembly unrolls into
-// register operations.
-template <int LA, int LB, int LC, int LD, int T>
-B2_HD void assemble_one(double *G, const double *hx, const double *hy, const double *hz)
-{
-        using K = Class4<LA, LB, LC, LD>;
-        constexpr int id = T % K::ND, ic = (T / K::ND) % K::NC, ib = (T / K::NCD) % K::NB, ia = T / (K::NCD * K::NB);
-        constexpr int ox = K::hidx(cart_lx(LA, ia), cart_lx(LB, ib), cart_lx(LC, ic), cart_lx(LD, id));
-        constexpr int oy = K::hidx(cart_ly(LA, ia), cart_ly(LB, ib), cart_ly(LC, ic), cart_ly(LD, id));
-        constexpr int oz = K::hidx(cart_lz(LA, ia), cart_lz(LB, ib), cart_lz(LC, ic), cart_lz(LD, id));
-        G[T] += hx[ox] * hy[oy] * hz[oz];
-}
-
-template <int LA, int LB, int LC, int LD, int... Ts>
-B2_HD void assemble_all(double *G, const double *hx, const double *hy, const double *hz,
-                        std::integer_sequence<int, Ts...>)
-{
-        (assemble_one<LA, LB, LC, LD, Ts>(G, hx, hy, hz), ...);
-}
-
-// Components [BASE, BASE + N) of the block only (register kernels that
-// keep one part of the block at a time), into Gp[0..N).
+// Components [BASE, BASE + N) of the block, into Gp[0..N): G[T] += I_x I_y I_z
+// for Cartesian component T.  The offsets into the 2D integrals are constant
+// expressions, so the whole assembly unrolls into register operations.
 template <int LA, int LB, int LC, int LD, int T, typename R>
 B2_HD void assemble_one_to(R &g, const R *hx, const R *hy, const R *hz)
 {
@@ -405,42 +426,35 @@ B2_HD void add_prim_quartet_part(R *Gp, const R *tab, const PrimQ<R> &s, const R
         }
 }
 
-// Add one primitive quartet to the Cartesian block G[((a*NB+b)*NC+c)*ND+d].
-template <int LA, int LB, int LC, int LD>
-B2_HD void add_prim_quartet(double *G, const double *table, const PrimQ<double> &s, const double AB[3],
-                            const double CD[3])
+// Add one primitive quartet to the Cartesian block G[((a*NB+b)*NC+c)*ND+d]
+// (host replay of the kernels' arithmetic); `tab` is the order-NR slice of
+// the table of type R.
+template <int LA, int LB, int LC, int LD, typename R>
+B2_HD void add_prim_quartet(R *G, const R *tab, const PrimQ<R> &s, const R AB[3], const R CD[3])
 {
         using K = Class4<LA, LB, LC, LD>;
-        double u[K::NR], w[K::NR];
-        rys_roots<K::NR>(s.T, table, u, w);
-#pragma unroll
+        R u[K::NR], w[K::NR];
+        rys_roots_slice<K::NR, R>(s.T, tab, u, w);
         for (int r = 0; r < K::NR; r++) {
-                RysCoef<double> rc;
-                rys_coef<double>(rc, u[r], s);
-                double g[K::NE * K::NF];
-                double hx[K::SA], hy[K::SA], hz[K::SA];
-                vrr2d<K::NE, K::NF>(g, 1.0, rc.c00[0], rc.c00p[0], rc.b10, rc.b01, rc.b00);
-                hrr2d<LA, LB, LC, LD>(g, hx, AB[0], CD[0]);
-                vrr2d<K::NE, K::NF>(g, 1.0, rc.c00[1], rc.c00p[1], rc.b10, rc.b01, rc.b00);
-                hrr2d<LA, LB, LC, LD>(g, hy, AB[1], CD[1]);
-                vrr2d<K::NE, K::NF>(g, s.pref * w[r], rc.c00[2], rc.c00p[2], rc.b10, rc.b01, rc.b00);
-                hrr2d<LA, LB, LC, LD>(g, hz, AB[2], CD[2]);
-#if defined(__CUDA_ARCH__)
-                if constexpr (K::NG <= 128) {
-                        assemble_all<LA, LB, LC, LD>(G, hx, hy, hz, std::make_integer_sequence<int, K::NG>{});
-                } else
-#endif
-                {
-                        // same operations in the same order as assemble_all
-                        for (int ia = 0; ia < K::NA; ia++)
-                        for (int ib = 0; ib < K::NB; ib++)
-                        for (int ic = 0; ic < K::NC; ic++)
-                        for (int id = 0; id < K::ND; id++) {
-                                const int ox = K::hidx(cart_lx(LA, ia), cart_lx(LB, ib), cart_lx(LC, ic), cart_lx(LD, id));
-                                const int oy = K::hidx(cart_ly(LA, ia), cart_ly(LB, ib), cart_ly(LC, ic), cart_ly(LD, id));
-                                const int oz = K::hidx(cart_lz(LA, ia), cart_lz(LB, ib), cart_lz(LC, ic), cart_lz(LD, id));
-                                G[((ia * K::NB + ib) * K::NC + ic) * K::ND + id] += hx[ox] * hy[oy] * hz[oz];
-                        }
+                RysCoef<R> rc;
+                rys_coef<R>(rc, u[r], s);
+                R g[K::NE * K::NF];
+                R hx[K::SA], hy[K::SA], hz[K::SA];
+                vrr2d<K::NE, K::NF, R>(g, (R)1, rc.c00[0], rc.c00p[0], rc.b10, rc.b01, rc.b00);
+                hrr2d<LA, LB, LC, LD, R>(g, hx, AB[0], CD[0]);
+                vrr2d<K::NE, K::NF, R>(g, (R)1, rc.c00[1], rc.c00p[1], rc.b10, rc.b01, rc.b00);
+                hrr2d<LA, LB, LC, LD, R>(g, hy, AB[1], CD[1]);
+                vrr2d<K::NE, K::NF, R>(g, s.pref * w[r], rc.c00[2], rc.c00p[2], rc.b10, rc.b01, rc.b00);
+                hrr2d<LA, LB, LC, LD, R>(g, hz, AB[2], CD[2]);
+                // same operations in the same order as assemble_one_to
+                for (int ia = 0; ia < K::NA; ia++)
+                for (int ib = 0; ib < K::NB; ib++)
+                for (int ic = 0; ic < K::NC; ic++)
+                for (int id = 0; id < K::ND; id++) {
+                        const int ox = K::hidx(cart_lx(LA, ia), cart_lx(LB, ib), cart_lx(LC, ic), cart_lx(LD, id));
+                        const int oy = K::hidx(cart_ly(LA, ia), cart_ly(LB, ib), cart_ly(LC, ic), cart_ly(LD, id));
+                        const int oz = K::hidx(cart_lz(LA, ia), cart_lz(LB, ib), cart_lz(LC, ic), cart_lz(LD, id));
+                        G[((ia * K::NB + ib) * K::NC + ic) * K::ND + id] += hx[ox] * hy[oy] * hz[oz];
                 }
         }
 }

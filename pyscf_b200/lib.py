@@ -26,6 +26,7 @@ EXPORTS = (
     'b200jk_plan_destroy', 'b200jk_plan_dims', 'b200jk_get_q_cond', 'b200jk_get_jk',
     'b200jk_stats', 'b200jk_hostcheck_cart_quartet', 'b200jk_class_stats', 'b200jk_set_profiling',
     'b200jk_measure_fp64_peak', 'b200jk_get_jk_noalloc', 'b200jk_set_mixed_threshold',
+    'b200jk_hostcheck_cart_quartet_fp32',
 )
 
 
@@ -75,6 +76,7 @@ def load(path=LIB_PATH):
         lib.b200jk_get_jk.argtypes = [vp, vp, ip, ip, ip, ip, vp, vp, ip, ip, vp]
         lib.b200jk_stats.argtypes = [vp, ctypes.POINTER(Stats)]
         lib.b200jk_hostcheck_cart_quartet.argtypes = [vp, ip, vp, ip, vp, vp, vp]
+        lib.b200jk_hostcheck_cart_quartet_fp32.argtypes = [vp, ip, vp, ip, vp, vp, vp]
         lib.b200jk_class_stats.argtypes = [vp, ctypes.POINTER(ClassStat), ip, ctypes.POINTER(ip)]
         lib.b200jk_set_profiling.argtypes = [vp, ip]
         lib.b200jk_measure_fp64_peak.argtypes = [ip, ctypes.POINTER(dp)]
@@ -210,9 +212,10 @@ def measure_fp64_peak(device=0):
     return t.value
 
 
-def hostcheck_cart_quartet(atm, bas, env, shls):
+def hostcheck_cart_quartet(atm, bas, env, shls, fp32=False):
     """Host replay of the kernels' integral arithmetic for one quartet of
-    segmented shells; returns the Cartesian block [a][b][c][d]."""
+    segmented shells; returns the Cartesian block [a][b][c][d].  fp32=True
+    replays the float32 pass of mixed precision."""
     lib = load()
     atm = numpy.asarray(atm, dtype=numpy.int32, order='C')
     bas = numpy.asarray(bas, dtype=numpy.int32, order='C')
@@ -220,6 +223,6 @@ def hostcheck_cart_quartet(atm, bas, env, shls):
     shls = numpy.asarray(shls, dtype=numpy.int32)
     nc = [(int(bas[s, 1]) + 1) * (int(bas[s, 1]) + 2) // 2 for s in shls]
     out = numpy.zeros(nc)
-    check(lib.b200jk_hostcheck_cart_quartet(_ptr(atm), atm.shape[0], _ptr(bas), bas.shape[0],
-                                            _ptr(env), _ptr(shls), _ptr(out)))
+    fn = lib.b200jk_hostcheck_cart_quartet_fp32 if fp32 else lib.b200jk_hostcheck_cart_quartet
+    check(fn(_ptr(atm), atm.shape[0], _ptr(bas), bas.shape[0], _ptr(env), _ptr(shls), _ptr(out)))
     return out
