@@ -135,6 +135,32 @@ int b200jk_stats(const b200jk_plan *plan, b200jk_stats_t *stats);
 int b200jk_class_stats(const b200jk_plan *plan, b200jk_class_stat_t *out, int max, int *n);
 int b200jk_set_profiling(b200jk_plan *plan, int on);
 
+/* Nuclear-gradient J/K: the drop-in for pyscf.grad.rhf.get_jk(mol, dm)
+ * (pyscf/grad/rhf.py:149-178, i.e. _vhf.direct_mapdm('int2e_ip1', 's2kl',
+ * ('lk->s1ij', 'jk->s1il'), dm, 3, ...) with CVHFgrad_jk_prescreen,
+ * pyscf/lib/vhf/hessian_screen.c:44-123).  For each of the n_dm densities
+ * (nao x nao, C order, need not be symmetric)
+ *     vj[s][x][i][j] = -sum_kl (d_x i j|kl) D[l][k]
+ *     vk[s][x][i][l] = -sum_jk (d_x i j|kl) D[j][k]
+ * with d_x the x derivative acting on function i (libcint's int2e_ip1,
+ * nabla on the electron coordinate); outputs (n_dm, 3, nao, nao)
+ * are overwritten.  direct_scf_tol is the gradient screen's threshold (the
+ * reference uses 1e-14); <= 0 disables screening.  dev_ptrs: 0 host arrays,
+ * 1 device arrays on the plan's GPU.  The first call builds the derivative
+ * Schwarz bound of the plan (int2e_ip1ip2 diagonal) on the GPU. */
+int b200jk_grad_jk(b200jk_plan *plan, const double *dms, int n_dm, int with_j, int with_k,
+                   double *vj, double *vk, int dev_ptrs, double direct_scf_tol, void *stream);
+
+/* Counters of the last gradient build: shell quartets (bra sides), primitive
+ * quartets, device time (ms), kernels launched by this library. */
+int b200jk_grad_stats(const b200jk_plan *plan, int64_t *quartets, int64_t *prim_quartets, double *ms,
+                      int64_t *kernel_launches);
+
+/* The two screening planes of the gradient (2, nbas, nbas): plane 0 the
+ * derivative bound sqrt(max |(d_x i j|d_x i j)|) with the derivative on the
+ * row shell (CVHFnr_int2e_pp_q_cond), plane 1 q_cond. */
+int b200jk_get_grad_q_cond(b200jk_plan *plan, double *q_cond);
+
 /* Threshold tau of B200JK_PREC_MIXED (default 1e-9): a shell quartet whose
  * Schwarz bound times the largest density element, q_ij q_kl max|D|, is below
  * tau is evaluated in float32.  The bound uses the density passed to each

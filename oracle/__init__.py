@@ -129,3 +129,49 @@ def int2e_cart(atm, bas, env, shls):
     lib.int2e_cart(_p(out), None, _p(shls), _p(atm), ctypes.c_int(atm.shape[0]), _p(bas),
                    ctypes.c_int(bas.shape[0]), _p(env), None, None)
     return out.reshape(dims, order='F')
+
+
+def grad_q_cond(atm, bas, env, cart=False, direct_scf_tol=1e-14):
+    """The two screening planes of grad.rhf.get_jk: (2, nbas, nbas), plane 0
+    from int2e_ip1ip2 (CVHFnr_int2e_pp_q_cond), plane 1 from int2e, both under
+    mol.with_integral_screen(tol**2) (pyscf/grad/rhf.py:155-169)."""
+    lib = load()
+    atm, bas, env = _arrays(atm, bas, env)
+    nbas = bas.shape[0]
+    q = numpy.empty((2, nbas, nbas))
+    cut = -numpy.log(direct_scf_tol ** 2)
+    lib.oracle_grad_q_cond(_p(q), _p(atm), ctypes.c_int(atm.shape[0]), _p(bas), ctypes.c_int(nbas), _p(env),
+                           ctypes.c_int(int(cart)), ctypes.c_double(cut))
+    return q
+
+
+def dm_cond1(dm, bas, cart=False):
+    """CVHFnr_dm_cond1: max |D| over each shell block, not symmetrised."""
+    lib = load()
+    bas = numpy.ascontiguousarray(bas, dtype=numpy.int32)
+    dm = numpy.ascontiguousarray(dm, dtype=numpy.double)
+    out = numpy.empty((bas.shape[0], bas.shape[0]))
+    lib.oracle_dm_cond1(_p(out), _p(dm), ctypes.c_int(1), _p(bas), ctypes.c_int(bas.shape[0]),
+                        ctypes.c_int(int(cart)))
+    return out
+
+
+def grad_jk(dm, atm, bas, env, cart=False, direct_scf_tol=1e-14, screen=True):
+    """grad.rhf.get_jk restated: (vj, vk), each (3, nao, nao), already negated
+    as the reference returns them (pyscf/grad/rhf.py:149-178)."""
+    lib = load()
+    atm, bas, env = _arrays(atm, bas, env)
+    dm = numpy.ascontiguousarray(dm, dtype=numpy.double)
+    n = dm.shape[-1]
+    vj = numpy.empty((3, n, n))
+    vk = numpy.empty((3, n, n))
+    qc = dc = None
+    if screen:
+        qc = grad_q_cond(atm, bas, env, cart, direct_scf_tol)
+        dc = dm_cond1(dm, bas, cart)
+    rc = lib.oracle_grad_jk(_p(dm), _p(vj), _p(vk), _p(atm), ctypes.c_int(atm.shape[0]), _p(bas),
+                            ctypes.c_int(bas.shape[0]), _p(env), ctypes.c_int(int(cart)),
+                            _p(qc) if screen else None, _p(dc) if screen else None, ctypes.c_double(direct_scf_tol))
+    if rc != 0:
+        raise RuntimeError('oracle_grad_jk failed')
+    return vj, vk

@@ -70,22 +70,31 @@ int oracle_nao(const int *bas, int nbas, int cart)
 }
 
 /* shared diagonal-quartet conditioner: q[ij] = sqrt(max over comps in
- * comp_sel of |(ij|ij)|), floor 1e-100 */
+ * comp_sel of |(ij|ij)|), floor 1e-100.  ordered=0: pairs i >= j, mirrored
+ * (CVHFnr_int2e_q_cond); ordered=1: every (i, j) on its own, not mirrored, as
+ * the derivative conditioner is not symmetric (CVHFnr_int2e_pp_q_cond,
+ * hessian_screen.c:70-123) */
 static void q_cond_generic(double *q_cond, intor_t intor, int ncomp, const int *comp_sel, int nsel,
-                           int *atm, int natm, int *bas, int nbas, double *env, int cart)
+                           int *atm, int natm, int *bas, int nbas, double *env, int cart, int ordered)
 {
         int *ao_loc = malloc(sizeof(int) * (nbas + 1));
         make_ao_loc(ao_loc, bas, nbas, cart);
         int dmax = 0;
         for (int i = 0; i < nbas; i++) dmax = MAX(dmax, ao_loc[i + 1] - ao_loc[i]);
-        size_t npair = (size_t)nbas * (nbas + 1) / 2;
+        size_t npair = ordered ? (size_t)nbas * nbas : (size_t)nbas * (nbas + 1) / 2;
 #pragma omp parallel
 {
         double *buf = malloc(sizeof(double) * (size_t)dmax * dmax * dmax * dmax * ncomp);
 #pragma omp for schedule(dynamic, 4)
         for (size_t ij = 0; ij < npair; ij++) {
-                int ish = (int)(sqrt(2 * (double)ij + .25) - .5 + 1e-7);
-                int jsh = (int)(ij - (size_t)ish * (ish + 1) / 2);
+                int ish, jsh;
+                if (ordered) {
+                        ish = (int)(ij / nbas);
+                        jsh = (int)(ij - (size_t)ish * nbas);
+                } else {
+                        ish = (int)(sqrt(2 * (double)ij + .25) - .5 + 1e-7);
+                        jsh = (int)(ij - (size_t)ish * (ish + 1) / 2);
+                }
                 int di = ao_loc[ish + 1] - ao_loc[ish];
                 int dj = ao_loc[jsh + 1] - ao_loc[jsh];
                 int shls[4] = {ish, jsh, ish, jsh};
@@ -103,7 +112,7 @@ static void q_cond_generic(double *q_cond, intor_t intor, int ncomp, const int *
                         qtmp = sqrt(qtmp);
                 }
                 q_cond[(size_t)ish * nbas + jsh] = qtmp;
-                q_cond[(size_t)jsh * nbas + ish] = qtmp;
+                if (!ordered) q_cond[(size_t)jsh * nbas + ish] = qtmp;
         }
         free(buf);
 }
@@ -119,7 +128,7 @@ void oracle_q_cond(double *q_cond, int *atm, int natm, int *bas, int nbas, doubl
         env[PTR_EXPCUTOFF] = expcutoff;
         int sel0[1] = {0};
         q_cond_generic(q_cond, cart ? int2e_cart : int2e_sph, 1, sel0, 1,
-                       atm, natm, bas, nbas, env, cart);
+                       atm, natm, bas, nbas, env, cart, 0);
         env[PTR_EXPCUTOFF] = saved;
 }
 
@@ -132,10 +141,10 @@ void oracle_grad_q_cond(double *q_cond, int *atm, int natm, int *bas, int nbas, 
         env[PTR_EXPCUTOFF] = expcutoff;
         int seld[3] = {0, 4, 8};
         q_cond_generic(q_cond, cart ? int2e_ip1ip2_cart : int2e_ip1ip2_sph, 9, seld, 3,
-                       atm, natm, bas, nbas, env, cart);
+                       atm, natm, bas, nbas, env, cart, 1);
         int sel0[1] = {0};
         q_cond_generic(q_cond + (size_t)nbas * nbas, cart ? int2e_cart : int2e_sph, 1, sel0, 1,
-                       atm, natm, bas, nbas, env, cart);
+                       atm, natm, bas, nbas, env, cart, 0);
         env[PTR_EXPCUTOFF] = saved;
 }
 

@@ -5,7 +5,8 @@
 The library is a plain shared object with a C ABI (include/b200jk.h); the
 Python package loads it with ctypes.  It is built next to the sources so it
 travels with the repository snapshot.  The per-class kernels are split into
-one translation unit per quartet class (jk_classes.cu compiled 55 times) and
+one translation unit per quartet class (jk_classes.cu compiled 55 times), the
+gradient kernels into one per bra class (grad_classes.cu, 10 times), all
 compiled in parallel.
 """
 import os
@@ -19,7 +20,8 @@ ROOT = os.path.dirname(HERE)
 CSRC = os.path.join(HERE, 'csrc')
 OBJ = os.path.join(HERE, '_build')
 LIB = os.path.join(HERE, 'libb200jk.so')
-HEADERS = ['rys_math.cuh', 'jk_kernels.cuh', 'jk_launch.h', 'rys_table.inc']
+HEADERS = ['rys_math.cuh', 'jk_kernels.cuh', 'jk_launch.h', 'rys_table.inc', 'rys_table_f.inc',
+           'grad_kernels.cuh', 'grad_launch.h']
 ARCH = ['-gencode', 'arch=compute_100a,code=sm_100a']
 PAIR_CLASSES = [(la, lb) for la in range(4) for lb in range(la + 1)]
 QUARTET_CLASSES = [(la, lb, lc, ld) for x, (la, lb) in enumerate(PAIR_CLASSES)
@@ -35,7 +37,7 @@ def nvcc_path():
 
 def _deps():
     files = [os.path.join(CSRC, f) for f in
-             ['b200jk.cu', 'jk_classes.cu', 'jk_qcond.cu', 'hostcheck.cpp'] + HEADERS]
+             ['b200jk.cu', 'jk_classes.cu', 'jk_qcond.cu', 'grad_classes.cu', 'hostcheck.cpp'] + HEADERS]
     files.append(os.path.join(ROOT, 'include', 'b200jk.h'))
     files.append(os.path.abspath(__file__))
     return files
@@ -63,6 +65,10 @@ def _units():
         units.append((common + ['-DB2_BRA_LA=%d' % la, '-DB2_BRA_LB=%d' % lb, '-DB2_KET_LC=%d' % lc,
                                 '-DB2_KET_LD=%d' % ld, '-DB2_FN_NAME=launch_jk_%s' % tag,
                                 os.path.join(CSRC, 'jk_classes.cu'), '-o', o], o))
+    for la, lb in PAIR_CLASSES:
+        o = os.path.join(OBJ, 'grad_%d%d.o' % (la, lb))
+        units.append((common + ['-DB2_BRA_LA=%d' % la, '-DB2_BRA_LB=%d' % lb,
+                                os.path.join(CSRC, 'grad_classes.cu'), '-o', o], o))
     o = os.path.join(OBJ, 'hostcheck.o')
     units.append((['g++', '-O2', '-std=c++17', '-fPIC', '-I', os.path.join(ROOT, 'include'), '-I', CSRC,
                    '-c', os.path.join(CSRC, 'hostcheck.cpp'), '-o', o], o))

@@ -26,6 +26,7 @@
 #define RYS_TABLE_QUALIFIER static const
 #include "rys_math.cuh"
 #include "jk_launch.h"
+#include "grad_launch.h"
 #include "../../include/b200jk.h"
 
 using namespace b200jk;
@@ -183,6 +184,44 @@ struct PairClassDev {
         void release() { sh.release(); pr.release(); q.release(); A.release(); AB.release(); n = 0; }
 };
 
+// what the gradient set-up keeps of the planner's segments and pairs
+struct SegLite {
+        int parent, l, cart_off;
+        double R[3];
+};
+struct PairLite {
+        int i, j;              // segments, l_i >= l_j
+        int prim0, nprim;      // primitive pairs
+};
+
+// Gradient J/K state of a plan (built on the first gradient call): the
+// derivative Schwarz bound q0 and the bra/ket pair lists of the gradient
+// screen, plus the per-call workspace.
+struct GradPlan {
+        bool q0_ready = false, lists_ready = false;
+        double tol = 0;
+        PairClassDev bra[NPAIRCLASS], ket[NPAIRCLASS];
+        DevArr<double> q0;
+        DevArr<int2> goff;
+        std::vector<size_t> goff_at;   // [X * NPAIRCLASS + Y], then NPAIRCLASS^2 + X for q0
+        std::vector<double> h_q0;
+        DevArr<double> D, Dc, Ds, V, out, dmc, fac;
+        DevArr<unsigned long long> dmax, stats;
+        DevArr<int> nkl, kst;
+        DevArr<long long> nchunk, chunk_off;
+        DevArr<unsigned char> cub_tmp;
+        int64_t quartets = 0, prim_quartets = 0, launches = 0;
+        double last_ms = 0;
+        void release()
+        {
+                for (auto &c : bra) c.release();
+                for (auto &c : ket) c.release();
+                q0.release(); goff.release(); D.release(); Dc.release(); Ds.release(); V.release(); out.release();
+                dmc.release(); fac.release(); dmax.release(); stats.release(); nkl.release(); kst.release();
+                nchunk.release(); chunk_off.release(); cub_tmp.release();
+        }
+};
+
 struct b200jk_plan {
         int device = 0, cart = 0, natm = 0, nbas = 0, nao = 0, naoc = 0, nseg = 0;
         double tol = 0;
@@ -193,6 +232,10 @@ struct b200jk_plan {
         PairClassDev pc[NPAIRCLASS];
         DevArr<double4> PP;
         DevArr<double2> PK;
+        DevArr<double2> PE;            // primitive exponents (alpha of i, beta of j) per primitive pair
+        std::vector<SegLite> segl;
+        std::vector<PairLite> all_pairs[NPAIRCLASS];   // before screening
+        GradPlan grad;
         DevArr<double> c2s, qcond, dm_cond;
         DevArr<int> goff_all;
         std::vector<size_t> goff_at;   // per quartet class
@@ -216,7 +259,7 @@ struct b200jk_plan {
         ~b200jk_plan()
         {
                 for (auto &c : pc) c.release();
-                PP.release(); PK.release(); c2s.release(); qcond.release(); dm_cond.release();
+                PP.release(); PK.release(); PE.release(); grad.release(); c2s.release(); qcond.release(); dm_cond.release();
                 goff_all.release(); seg_info.release(); out_seg.release(); out_comp.release();
                 cart_seg.release(); cart_comp.release(); ao_loc_d.release();
                 D.release(); Dc.release(); Ds.release(); Jacc.release(); Kacc.release(); outJ.release(); outK.release();
@@ -512,7 +555,7 @@ int b200jk_plan_create(const int32_t *atm, int natm, const int32_t *bas, int nba
         // shell pairs and primitive pairs
         std::vector<HostPair> pairs[NPAIRCLASS];
         std::vector<double4> hPP;
-        std::vector<double2> hPK;
+        std::vector<double2> hPK, hPE;
         const double expcut = 60.0;
         for (int si = 0; si < (int)segs.size(); si++) {
                 for (int sj = 0; sj <= si; sj++) {
@@ -537,6 +580,7 @@ int b200jk_plan_create(const int32_t *atm, int natm, const int32_t *bas, int nba
                                         P4.w = p;
                                         hPP.push_back(P4);
                                         hPK.push_back(make_double2(cc * exp(-mu * rr), 0.5 / p));
+                                        hPE.push_back(make_double2(a, b));
                                         hp.nprim++;
                                 }
                         }
@@ -545,7 +589,20 @@ int b200jk_plan_create(const int32_t *atm, int natm, const int32_t *bas, int nba
                 }
         }
         P->prim_pairs = (int64_t)hPP.size();
-        if ((rc = dev_upload(P->PP, hPP)) || (rc = dev_upload(P->PK, hPK))) return bail(rc);
+        if ((rc = dev_upload(P->PP, hPP)) || (rc = dev_upload(P->PK, hPK)) || (rc = dev_upload(P->PE, hPE)))
+                return bail(rc);
+        // the gradient set-up re-screens the unpruned pairs with its own bounds
+        P->segl.resize(segs.size());
+        for (size_t t = 0; t < segs.size(); t++) {
+                P->segl[t].parent = segs[t].parent;
+                P->segl[t].l = segs[t].l;
+                P->segl[t].cart_off = segs[t].cart_off;
+                for (int x = 0; x < 3; x++) P->segl[t].R[x] = segs[t].R[x];
+        }
+        for (int X = 0; X < NPAIRCLASS; X++) {
+                P->all_pairs[X].clear();
+                for (const HostPair &h : pairs[X]) P->all_pairs[X].push_back({h.i, h.j, h.prim0, h.nprim});
+        }
 
         // Cartesian offset tables of all quartet classes (also used by q_cond)
         {
@@ -903,6 +960,305 @@ int b200jk_stats(const b200jk_plan *plan, b200jk_stats_t *stats)
 }
 
 } // extern "C"
+
+// ---------------------------------------------------------------------------
+// Nuclear-gradient J/K (pyscf/grad/rhf.py:149-178).
+
+// packed offsets/exponents of the gradient classes (GClass in grad_kernels.cuh)
+static void grad_goff(int la, int lb, int lc, int ld, int mode, std::vector<int2> &out)
+{
+        const int EB = lb + 2, EC = lc + 1 + mode, ED = ld + 1 + mode;
+        auto eidx = [&](int a, int b, int c, int d) { return ((a * EB + b) * EC + c) * ED + d; };
+        auto ex = [](int l, int n) { return cart_lx(l, n) | (cart_ly(l, n) << 2) | (cart_lz(l, n) << 4); };
+        const int na = ncart(la), nb = ncart(lb), nc = ncart(lc), nd = ncart(ld);
+        for (int a = 0; a < na; a++)
+                for (int b = 0; b < nb; b++)
+                        for (int c = 0; c < nc; c++)
+                                for (int d = 0; d < nd; d++) {
+                                        const int ox = eidx(cart_lx(la, a), cart_lx(lb, b), cart_lx(lc, c), cart_lx(ld, d));
+                                        const int oy = eidx(cart_ly(la, a), cart_ly(lb, b), cart_ly(lc, c), cart_ly(ld, d));
+                                        const int oz = eidx(cart_lz(la, a), cart_lz(lb, b), cart_lz(lc, c), cart_lz(ld, d));
+                                        out.push_back(make_int2(ox | (oy << 10) | (oz << 20),
+                                                                ex(la, a) | (ex(lb, b) << 6) | (ex(lc, c) << 12) | (ex(ld, d) << 18)));
+                                }
+}
+
+typedef int (*grad_launcher_t)(int, int, const GradArgs &, cudaStream_t, int, std::string &);
+typedef int (*gq0_launcher_t)(const GradQArgs &, cudaStream_t, std::string &);
+static const grad_launcher_t g_grad_launch[NPAIRCLASS] = {
+        launch_grad_00, launch_grad_10, launch_grad_11, launch_grad_20, launch_grad_21,
+        launch_grad_22, launch_grad_30, launch_grad_31, launch_grad_32, launch_grad_33};
+static const gq0_launcher_t g_gq0_launch[NPAIRCLASS] = {
+        launch_gq0_00, launch_gq0_10, launch_gq0_11, launch_gq0_20, launch_gq0_21,
+        launch_gq0_22, launch_gq0_30, launch_gq0_31, launch_gq0_32, launch_gq0_33};
+
+// upload one class of pairs in the given order, q per pair
+static int upload_pairs(const b200jk_plan *P, PairClassDev &c, int X, const std::vector<PairLite> &hv,
+                        const std::vector<double> &q)
+{
+        class_l(X, c.la, c.lb);
+        c.n = (int)hv.size();
+        for (int b = 0; b <= B2_NBUCKET; b++) c.boff[b] = 0;
+        for (const PairLite &p : hv) c.boff[prim_bucket(p.nprim) + 1]++;
+        for (int b = 0; b < B2_NBUCKET; b++) c.boff[b + 1] += c.boff[b];
+        std::vector<int4> sh(hv.size());
+        std::vector<int2> pr(hv.size());
+        std::vector<double4> Av(hv.size()), ABv(hv.size());
+        for (size_t t = 0; t < hv.size(); t++) {
+                const SegLite &A = P->segl[hv[t].i], &B = P->segl[hv[t].j];
+                sh[t] = make_int4(A.cart_off, B.cart_off, A.parent, B.parent);
+                pr[t] = make_int2(hv[t].prim0, hv[t].nprim);
+                Av[t] = make_double4(A.R[0], A.R[1], A.R[2], hv[t].i == hv[t].j ? 1.0 : 0.0);
+                ABv[t] = make_double4(A.R[0] - B.R[0], A.R[1] - B.R[1], A.R[2] - B.R[2], 0.0);
+        }
+        int r;
+        if ((r = dev_upload(c.sh, sh)) || (r = dev_upload(c.pr, pr)) || (r = dev_upload(c.q, q)) ||
+            (r = dev_upload(c.A, Av)) || (r = dev_upload(c.AB, ABv)))
+                return r;
+        return B200JK_OK;
+}
+
+// q0 (once per plan) and the gradient pair lists (per screening tolerance)
+static int ensure_grad(b200jk_plan *P, double tol)
+{
+        GradPlan &g = P->grad;
+        const int nbas = P->nbas;
+        const size_t n2 = (size_t)nbas * nbas;
+        int rc;
+        if (!g.q0_ready) {
+                std::vector<int2> all;
+                g.goff_at.assign(NPAIRCLASS * NPAIRCLASS + NPAIRCLASS, 0);
+                for (int X = 0; X < NPAIRCLASS; X++) {
+                        int la, lb;
+                        class_l(X, la, lb);
+                        for (int Y = 0; Y < NPAIRCLASS; Y++) {
+                                int lc, ld;
+                                class_l(Y, lc, ld);
+                                g.goff_at[X * NPAIRCLASS + Y] = all.size();
+                                grad_goff(la, lb, lc, ld, 0, all);
+                        }
+                }
+                for (int X = 0; X < NPAIRCLASS; X++) {
+                        int la, lb;
+                        class_l(X, la, lb);
+                        g.goff_at[NPAIRCLASS * NPAIRCLASS + X] = all.size();
+                        grad_goff(la, lb, la, lb, 1, all);
+                }
+                if ((rc = dev_upload(g.goff, all))) return rc;
+                std::vector<double> init(n2, 1e-100);
+                if ((rc = dev_upload(g.q0, init))) return rc;
+                for (int X = 0; X < NPAIRCLASS; X++) {
+                        const std::vector<PairLite> &hv = P->all_pairs[X];
+                        if (hv.empty()) continue;
+                        PairClassDev tmp;
+                        if ((rc = upload_pairs(P, tmp, X, hv, std::vector<double>(hv.size(), 0.0)))) return rc;
+                        GradQArgs q;
+                        q.pairs = tmp.view();
+                        q.PP = P->PP.p; q.PK = P->PK.p; q.PE = P->PE.p;
+                        q.table = table_ptr();
+                        q.goff = g.goff.p + g.goff_at[NPAIRCLASS * NPAIRCLASS + X];
+                        q.c2s = P->c2s.p;
+                        q.q0 = (unsigned long long *)g.q0.p;
+                        q.nbas = nbas;
+                        q.cart = P->cart;
+                        std::string err;
+                        if (g_gq0_launch[X](q, P->stream, err)) { tmp.release(); return fail(B200JK_ECUDA, err); }
+                        const cudaError_t e = cudaStreamSynchronize(P->stream);
+                        tmp.release();
+                        if (e != cudaSuccess) return fail(B200JK_ECUDA, std::string("gradient q_cond: ") + cudaGetErrorString(e));
+                }
+                g.h_q0.resize(n2);
+                CUDA_TRY(cudaMemcpy(g.h_q0.data(), g.q0.p, sizeof(double) * n2, cudaMemcpyDeviceToHost));
+                g.q0_ready = true;
+                g.lists_ready = false;
+        }
+        if (g.lists_ready && g.tol == tol) return B200JK_OK;
+        const std::vector<double> &q1 = P->h_qcond, &q0 = g.h_q0;
+        double q0max = 0, q1max = 0;
+        for (size_t t = 0; t < n2; t++) { q0max = std::max(q0max, q0[t]); q1max = std::max(q1max, q1[t]); }
+        for (int X = 0; X < NPAIRCLASS; X++) {
+                std::vector<PairLite> hb, hk;
+                std::vector<double> qb, qk;
+                for (const PairLite &p : P->all_pairs[X]) {
+                        const size_t pi = P->segl[p.i].parent, pj = P->segl[p.j].parent;
+                        const double b = std::max(q0[pi * nbas + pj], q0[pj * nbas + pi]);
+                        const double k = q1[pi * nbas + pj];
+                        if (!(tol > 0) || b * q1max > tol) { hb.push_back(p); qb.push_back(b); }
+                        if (!(tol > 0) || k * q0max > tol) { hk.push_back(p); qk.push_back(k); }
+                }
+                // bucket-major, descending bound inside a bucket
+                auto order = [](std::vector<PairLite> &v, std::vector<double> &q) {
+                        std::vector<size_t> idx(v.size());
+                        std::iota(idx.begin(), idx.end(), 0);
+                        std::stable_sort(idx.begin(), idx.end(), [&](size_t a, size_t b) {
+                                const int ba = prim_bucket(v[a].nprim), bb = prim_bucket(v[b].nprim);
+                                if (ba != bb) return ba < bb;
+                                return q[a] > q[b];
+                        });
+                        std::vector<PairLite> v2(v.size());
+                        std::vector<double> q2(v.size());
+                        for (size_t t = 0; t < idx.size(); t++) { v2[t] = v[idx[t]]; q2[t] = q[idx[t]]; }
+                        v.swap(v2);
+                        q.swap(q2);
+                };
+                order(hb, qb);
+                order(hk, qk);
+                g.bra[X].release();
+                g.ket[X].release();
+                if ((rc = upload_pairs(P, g.bra[X], X, hb, qb)) || (rc = upload_pairs(P, g.ket[X], X, hk, qk))) return rc;
+        }
+        g.tol = tol;
+        g.lists_ready = true;
+        return B200JK_OK;
+}
+
+extern "C" int b200jk_grad_jk(b200jk_plan *P, const double *dms, int n_dm, int with_j, int with_k, double *vj,
+                              double *vk, int dev_ptrs, double direct_scf_tol, void *stream)
+{
+        if (!P) return fail(B200JK_EINVAL, "plan is NULL");
+        if (!dms || n_dm <= 0) return fail(B200JK_EINVAL, "no density matrices");
+        if (with_j && !vj) return fail(B200JK_EINVAL, "vj is NULL while with_j is set");
+        if (with_k && !vk) return fail(B200JK_EINVAL, "vk is NULL while with_k is set");
+        if (!(direct_scf_tol == direct_scf_tol)) return fail(B200JK_EINVAL, "direct_scf_tol is NaN");
+        CUDA_TRY(cudaSetDevice(P->device));
+        const double tol = direct_scf_tol > 0 ? direct_scf_tol : 0.0;
+        int rc = ensure_grad(P, tol);
+        if (rc) return rc;
+        GradPlan &g = P->grad;
+        const size_t nn = (size_t)P->nao * P->nao, nc = (size_t)P->naoc * P->naoc;
+        int maxn = 1;
+        for (auto &c : g.bra) maxn = std::max(maxn, c.n * B2_NBUCKET);
+        if ((rc = dev_alloc(g.D, nn * n_dm)) || (rc = dev_alloc(g.Dc, nc * n_dm)) || (rc = dev_alloc(g.Ds, nc * n_dm)) ||
+            (rc = dev_alloc(g.V, 6 * nc * n_dm)) || (rc = dev_alloc(g.out, dev_ptrs ? 1 : 6 * nn * n_dm)) ||
+            (rc = dev_alloc(g.dmc, (size_t)P->nbas * P->nbas)) || (rc = dev_alloc(g.fac, 1)) ||
+            (rc = dev_alloc(g.dmax, 1)) || (rc = dev_alloc(g.stats, 2)) || (rc = dev_alloc(g.nkl, maxn)) ||
+            (rc = dev_alloc(g.kst, maxn)) || (rc = dev_alloc(g.nchunk, maxn + 1)) || (rc = dev_alloc(g.chunk_off, maxn + 1)))
+                return rc;
+        size_t cub_bytes = 0;
+        cub::DeviceScan::ExclusiveSum(nullptr, cub_bytes, g.nchunk.p, g.chunk_off.p, maxn + 1);
+        if ((rc = dev_alloc(g.cub_tmp, cub_bytes + 16))) return rc;
+
+        cudaStream_t s = stream ? (cudaStream_t)stream : P->stream;
+        CUDA_TRY(cudaEventRecord(P->ev0, s));
+        const double *dD = dms;
+        if (!dev_ptrs) {
+                CUDA_TRY(cudaMemcpyAsync(g.D.p, dms, sizeof(double) * nn * n_dm, cudaMemcpyHostToDevice, s));
+                dD = g.D.p;
+        }
+        CUDA_TRY(cudaMemsetAsync(g.dmax.p, 0, sizeof(unsigned long long), s));
+        CUDA_TRY(cudaMemsetAsync(g.stats.p, 0, 2 * sizeof(unsigned long long), s));
+        int64_t launches = 0;
+        dm_cond1_kernel<<<grid_for((long long)P->nbas * P->nbas, 256), 256, 0, s>>>(dD, n_dm, P->nao, P->ao_loc_d.p,
+                                                                                  P->nbas, g.dmc.p, g.dmax.p);
+        CUDA_TRY(cudaGetLastError());
+        grad_dm_factor_kernel<<<1, 1, 0, s>>>(g.dmax.p, g.fac.p);
+        CUDA_TRY(cudaGetLastError());
+        launches += 2;
+        for (int d = 0; d < n_dm; d++) {
+                double *Dc = g.Dc.p + (size_t)d * nc;
+                out_to_cart_kernel<<<grid_for((long long)nc, 256), 256, 0, s>>>(
+                        dD + (size_t)d * nn, P->nao, P->naoc, P->cart_seg.p, P->cart_comp.p, P->seg_info.p, P->c2s.p,
+                        P->cart, Dc, nullptr, nullptr);
+                CUDA_TRY(cudaGetLastError());
+                sym_sum_kernel<<<grid_for((long long)nc, 256), 256, 0, s>>>(Dc, P->naoc, g.Ds.p + (size_t)d * nc);
+                CUDA_TRY(cudaGetLastError());
+                launches += 2;
+        }
+        CUDA_TRY(cudaMemsetAsync(g.V.p, 0, sizeof(double) * 6 * nc * n_dm, s));
+        double *Vj = g.V.p, *Vk = g.V.p + 3 * nc * n_dm;
+        for (int X = 0; X < NPAIRCLASS; X++) {
+                const PairClassDev &bra = g.bra[X];
+                if (bra.n == 0) continue;
+                for (int Y = 0; Y < NPAIRCLASS; Y++) {
+                        const PairClassDev &ket = g.ket[Y];
+                        if (ket.n == 0) continue;
+                        const int nseg = bra.n * B2_NBUCKET;
+                        const int chunk = grad_chunk(bra.la, bra.lb, ket.la, ket.lb);
+                        count_kernel<<<grid_for(nseg, 256), 256, 0, s>>>(bra.view(), ket.view(), 0, tol, g.fac.p, chunk,
+                                                                        0.0, 0, g.nkl.p, g.kst.p, g.nchunk.p);
+                        CUDA_TRY(cudaGetLastError());
+                        CUDA_TRY(cudaMemsetAsync(g.nchunk.p + nseg, 0, sizeof(long long), s));
+                        size_t tmp = g.cub_tmp.n;
+                        CUDA_TRY(cub::DeviceScan::ExclusiveSum(g.cub_tmp.p, tmp, g.nchunk.p, g.chunk_off.p, nseg + 1, s));
+                        GradArgs a;
+                        a.bra = bra.view();
+                        a.ket = ket.view();
+                        a.PP = P->PP.p; a.PK = P->PK.p; a.PE = P->PE.p;
+                        a.chunk_off = g.chunk_off.p;
+                        a.nkl = g.nkl.p;
+                        a.kst = g.kst.p;
+                        a.q0 = g.q0.p;
+                        a.q1 = P->qcond.p;
+                        a.dmc = g.dmc.p;
+                        a.table = table_ptr();
+                        a.goff = g.goff.p + g.goff_at[X * NPAIRCLASS + Y];
+                        a.Vj = Vj; a.Vk = Vk;
+                        a.Ds = g.Ds.p; a.Dc = g.Dc.p;
+                        a.stats = g.stats.p;
+                        a.tol = tol > 0 ? tol : -1.0;
+                        a.nbas = P->nbas; a.naoc = P->naoc; a.n_dm = n_dm;
+                        a.with_j = with_j; a.with_k = with_k;
+                        std::string err;
+                        if (g_grad_launch[X](ket.la, ket.lb, a, s, P->nsm, err)) return fail(B200JK_ECUDA, err);
+                        launches += 2;   // count + class kernel (the scan is a CUB library kernel)
+                }
+        }
+        // to the output basis.  The kernels differentiate with respect to the
+        // centre (d/dA = -nabla_r of int2e_ip1), so the accumulators already
+        // hold the negated contraction grad.rhf.get_jk returns
+        double *oj = dev_ptrs ? vj : g.out.p, *ok = dev_ptrs ? vk : g.out.p + 3 * nn * n_dm;
+        const long long nout = (long long)3 * n_dm * nn;
+        if (with_j) {
+                grad_cart_to_out_kernel<<<grid_for(nout, 256), 256, 0, s>>>(Vj, 3 * n_dm, P->nao, P->naoc, P->out_seg.p,
+                                                                          P->out_comp.p, P->seg_info.p, P->c2s.p, 1.0, oj);
+                CUDA_TRY(cudaGetLastError());
+                launches++;
+        }
+        if (with_k) {
+                grad_cart_to_out_kernel<<<grid_for(nout, 256), 256, 0, s>>>(Vk, 3 * n_dm, P->nao, P->naoc, P->out_seg.p,
+                                                                          P->out_comp.p, P->seg_info.p, P->c2s.p, 1.0, ok);
+                CUDA_TRY(cudaGetLastError());
+                launches++;
+        }
+        CUDA_TRY(cudaEventRecord(P->ev1, s));
+        if (!dev_ptrs) {
+                if (with_j) CUDA_TRY(cudaMemcpyAsync(vj, oj, sizeof(double) * nout, cudaMemcpyDeviceToHost, s));
+                if (with_k) CUDA_TRY(cudaMemcpyAsync(vk, ok, sizeof(double) * nout, cudaMemcpyDeviceToHost, s));
+        }
+        unsigned long long hs[2];
+        CUDA_TRY(cudaMemcpyAsync(hs, g.stats.p, sizeof(hs), cudaMemcpyDeviceToHost, s));
+        CUDA_TRY(cudaStreamSynchronize(s));
+        float ms = 0;
+        CUDA_TRY(cudaEventElapsedTime(&ms, P->ev0, P->ev1));
+        g.quartets = (int64_t)hs[0];
+        g.prim_quartets = (int64_t)hs[1];
+        g.last_ms = ms;
+        g.launches = launches;
+        return B200JK_OK;
+}
+
+extern "C" int b200jk_grad_stats(const b200jk_plan *P, int64_t *quartets, int64_t *prim_quartets, double *ms,
+                                 int64_t *kernel_launches)
+{
+        if (!P) return fail(B200JK_EINVAL, "plan is NULL");
+        if (quartets) *quartets = P->grad.quartets;
+        if (prim_quartets) *prim_quartets = P->grad.prim_quartets;
+        if (ms) *ms = P->grad.last_ms;
+        if (kernel_launches) *kernel_launches = P->grad.launches;
+        return B200JK_OK;
+}
+
+extern "C" int b200jk_get_grad_q_cond(b200jk_plan *P, double *q_cond)
+{
+        if (!P || !q_cond) return fail(B200JK_EINVAL, "NULL argument");
+        CUDA_TRY(cudaSetDevice(P->device));
+        int rc = ensure_grad(P, P->grad.lists_ready ? P->grad.tol : 1e-14);
+        if (rc) return rc;
+        const size_t n2 = (size_t)P->nbas * P->nbas;
+        memcpy(q_cond, P->grad.h_q0.data(), sizeof(double) * n2);
+        memcpy(q_cond + n2, P->h_qcond.data(), sizeof(double) * n2);
+        return B200JK_OK;
+}
 
 
 // ---------------------------------------------------------------------------

@@ -1,0 +1,541 @@
+// grad_kernels.cuh — sm_100a kernels of the nuclear-gradient J/K build.
+//
+// The reference path is pyscf.grad.rhf.get_jk (pyscf/grad/rhf.py:149-178):
+//     vj_x[i,j] = -sum_kl (d_x i j|kl) D[l,k],   vk_x[i,l] = -sum_jk (d_x i j|kl) D[j,k]
+// over all ordered bra shell pairs (i,j) and ket pairs k >= l ('s2kl'), with
+// libcint's int2e_ip1 (derivative of the first bra function) and the screen
+// CVHFgrad_jk_prescreen (pyscf/lib/vhf/hessian_screen.c:44-68).
+//
+// Work decomposition.  Bra pairs are the planner's unordered segment pairs
+// (A,B); one evaluation of the quartet (AB|CD) yields both bra derivatives,
+// side A = (d A, B|CD) and side B = (A, d B|CD) = the reference's (d B, A|CD),
+// so the ordered pairs (i,j) and (j,i) share roots and recurrences.  A pair
+// of one segment has side A only.  Ket pairs are the unordered segment pairs
+// with both images (CD) and (DC) (weight 1/2 for a pair of one segment), as in
+// the energy build.  Classes: every bra class X with every ket class Y.
+//
+// Arithmetic.  The 2D Rys integrals are built with the bra indices extended by
+// one (a <= la+1, b <= lb+1), then per primitive quartet
+//     d/dA_x : 2 alpha I_x(a+1, b) - a_x I_x(a-1, b)
+//     d/dB_x : 2 beta  I_x(a, b+1) - b_x I_x(a, b-1)
+// replace the x factor of the product I_x I_y I_z (alpha, beta the bra
+// primitive exponents).  These are derivatives with respect to the centres,
+// d/dA = -nabla_r on the function (libcint's ip1 is nabla_r), so the
+// accumulated contraction is the negated one grad.rhf.get_jk returns.
+// Mode 1 of the same machinery also extends the ket indices and
+// differentiates bra and ket together, which gives the diagonal blocks
+// (d_x a b|d_x a b) of int2e_ip1ip2 for the derivative Schwarz bound
+// (CVHFnr_int2e_pp_q_cond, hessian_screen.c:70-123).
+#pragma once
+#include "jk_kernels.cuh"
+
+namespace b200jk {
+
+template <int LA, int LB, int LC, int LD, int MODE>
+struct GClass {
+        using K = Class4<LA, LB, LC, LD>;
+        // extended 2D integral dimensions
+        static constexpr int EA = LA + 2, EB = LB + 2, EC = LC + 1 + MODE, ED = LD + 1 + MODE;
+        static constexpr int SE = EA * EB * EC * ED;
+        static constexpr int STEP_A = EB * EC * ED, STEP_B = EC * ED, STEP_C = ED, STEP_D = 1;
+        static constexpr int NE = LA + LB + 2, NF = LC + LD + 1 + MODE;
+        static constexpr int NR = rys_nroots(LA + LB + LC + LD + 1 + MODE);
+        static constexpr int NG = K::NG;
+        // derivative components: side A x,y,z then side B x,y,z; NCP of them
+        // are accumulated per pass over the primitives (all six when they fit)
+        static constexpr int NCP = 6 * NG <= 8192 ? 6 : (3 * NG <= 8192 ? 3 : 1);
+        static constexpr int NPASS = 6 / NCP;
+        B2_HD static constexpr int eidx(int a, int b, int c, int d) { return ((a * EB + b) * EC + c) * ED + d; }
+};
+
+// shared-memory layout of one group (doubles)
+template <int LA, int LB, int LC, int LD, int MODE>
+struct GradSmem {
+        using GC = GClass<LA, LB, LC, LD, MODE>;
+        using K = Class4<LA, LB, LC, LD>;
+        static constexpr int G = 0;                                  // [NCP][NG]
+        static constexpr int E = G + GC::NCP * GC::NG;               // [3][NR][SE]
+        static constexpr int DSAB = E + 3 * GC::NR * GC::SE;
+        static constexpr int DSCD = DSAB + K::NAB;
+        static constexpr int XBC = DSCD + K::NCD;
+        static constexpr int XBD = XBC + K::NB * K::NC;
+        static constexpr int XAC = XBD + K::NB * K::ND;
+        static constexpr int XAD = XAC + K::NA * K::NC;
+        static constexpr int SIZE = ((XAD + K::NA * K::ND) + 3) & ~3;
+};
+
+// One (root, direction) slice of the extended 2D integrals:
+// h[((a*EB + b)*EC + c)*ED + d] for a < EA, b < EB, c < EC, d < ED with
+// a + b < NE and c + d < NF (the other entries are never read).
+template <int LA, int LB, int LC, int LD, int MODE>
+__device__ __forceinline__ void grad_slice(double *h, double g00, const RysCoef<double> &rc, int dir, double ab,
+                                           double cd)
+{
+        using GC = GClass<LA, LB, LC, LD, MODE>;
+        constexpr int NE = GC::NE, NF = GC::NF, EA = GC::EA, EB = GC::EB, EC = GC::EC, ED = GC::ED;
+        double g[NE * NF];
+        const double c00 = dir == 0 ? rc.c00[0] : (dir == 1 ? rc.c00[1] : rc.c00[2]);
+        const double c00p = dir == 0 ? rc.c00p[0] : (dir == 1 ? rc.c00p[1] : rc.c00p[2]);
+        vrr2d<NE, NF, double>(g, g00, c00, c00p, rc.b10, rc.b01, rc.b00);
+        constexpr int NCD1 = EC * ED;
+        double u[NE * NCD1];
+        double cdp[ED];
+        cdp[0] = 1.0;
+#pragma unroll
+        for (int k = 1; k < ED; k++) cdp[k] = cdp[k - 1] * cd;
+#pragma unroll
+        for (int e = 0; e < NE; e++)
+#pragma unroll
+        for (int c = 0; c < EC; c++)
+#pragma unroll
+        for (int d = 0; d < ED; d++) {
+                double v = 0.0;
+                if (c + d < NF) {
+#pragma unroll
+                        for (int k = 0; k <= d; k++) v += (double)binom(d, k) * cdp[d - k] * g[e * NF + c + k];
+                }
+                u[e * NCD1 + c * ED + d] = v;
+        }
+        double abp[EB];
+        abp[0] = 1.0;
+#pragma unroll
+        for (int k = 1; k < EB; k++) abp[k] = abp[k - 1] * ab;
+#pragma unroll
+        for (int a = 0; a < EA; a++)
+#pragma unroll
+        for (int b = 0; b < EB; b++)
+#pragma unroll
+        for (int t = 0; t < NCD1; t++) {
+                double v = 0.0;
+                if (a + b < NE) {
+#pragma unroll
+                        for (int k = 0; k <= b; k++) v += (double)binom(b, k) * abp[b - k] * u[(a + k) * NCD1 + t];
+                }
+                h[(a * EB + b) * NCD1 + t] = v;
+        }
+}
+
+// Per Cartesian component of a class, packed by the planner:
+//   x: extended offsets ox | oy << 10 | oz << 20
+//   y: exponents of a, b, c, d, 6 bits each (x | y << 2 | z << 4)
+__device__ __forceinline__ int gexp(int packed, int fn, int dir) { return (packed >> (6 * fn + 2 * dir)) & 3; }
+
+struct GradArgs {
+        PairView bra, ket;
+        const double4 *PP;           // primitive pair (P, p)
+        const double2 *PK;           // primitive pair (K_ab c_i c_j, 1/(2p))
+        const double2 *PE;           // primitive pair exponents (alpha of A, beta of B)
+        const long long *chunk_off;
+        const int *nkl, *kst;
+        const double *q0;            // nbas x nbas derivative Schwarz bound (ordered, derivative on the row shell)
+        const double *q1;            // nbas x nbas Schwarz bound
+        const double *dmc;           // nbas x nbas max |D| per block (not symmetrised)
+        const double *table;
+        const int2 *goff;
+        double *Vj, *Vk;             // [n_dm][3][naoc][naoc] Cartesian accumulators
+        const double *Ds, *Dc;       // [n_dm][naoc][naoc]: D + D^T and D (Cartesian)
+        unsigned long long *stats;   // [0] quartets (sides), [1] primitive quartets
+        double tol;
+        int nbas, naoc, n_dm, with_j, with_k;
+};
+
+// CVHFgrad_jk_prescreen for bra shells (i, j) (derivative on i) and ket
+// shells k >= l
+__device__ __forceinline__ bool grad_side_passes(const GradArgs &a, int i, int j, int k, int l)
+{
+        const size_t n = (size_t)a.nbas;
+        const double qq = __ldg(a.q0 + i * n + j) * __ldg(a.q1 + k * n + l);
+        if (!(qq > a.tol)) return false;
+        const double dmin = a.tol / qq;
+        return 2 * __ldg(a.dmc + l * n + k) > dmin || __ldg(a.dmc + j * n + k) > dmin || __ldg(a.dmc + j * n + l) > dmin;
+}
+
+// Accumulate derivative components [c0, c0 + GC::NCP) of one quartet into G.
+// Mode 0: components 0..2 = d/dA_{x,y,z}, 3..5 = d/dB_{x,y,z}.  Mode 1 (bra =
+// ket pair): components 0..2 = d/dA_x d/dC_x (same x), 3..5 = d/dB_x d/dD_x.
+// P and Q are taken relative to the origin O; A = 0, C relative to O.
+template <int LA, int LB, int LC, int LD, int MODE, int GS>
+__device__ __forceinline__ void grad_eval_pass(double *sm, const GradArgs &a, int2 pb, int2 pk, const double4 O,
+                                               const double AB[3], const double C[3], const double CD[3], double fac,
+                                               int c0, int gl, unsigned gmask)
+{
+        using GC = GClass<LA, LB, LC, LD, MODE>;
+        using S = GradSmem<LA, LB, LC, LD, MODE>;
+        constexpr int NR = GC::NR, SE = GC::SE, NG = GC::NG, NCP = GC::NCP;
+        double *G = sm + S::G;
+        double *E = sm + S::E;
+        const double *table = a.table + rys_padded_offset(NR);
+        const double A[3] = {0.0, 0.0, 0.0};
+        for (int t = gl; t < NCP * NG; t += GS) G[t] = 0.0;
+        for (int ip = 0; ip < pb.y; ip++) {
+                const double4 P = a.PP[pb.x + ip];
+                const double2 KP = a.PK[pb.x + ip];
+                const double2 EP = a.PE[pb.x + ip];
+                const double Kab = KP.x * fac;
+                const double Pv[3] = {P.x - O.x, P.y - O.y, P.z - O.z};
+                const double ta = 2.0 * EP.x, tb = 2.0 * EP.y;
+                for (int kp = 0; kp < pk.y; kp++) {
+                        const double4 Q = a.PP[pk.x + kp];
+                        const double2 KQ = a.PK[pk.x + kp];
+                        const double2 EQ = a.PE[pk.x + kp];
+                        const double Qv[3] = {Q.x - O.x, Q.y - O.y, Q.z - O.z};
+                        const double tc = 2.0 * EQ.x, td = 2.0 * EQ.y;
+                        __syncwarp(gmask);
+                        for (int task = gl; task < 3 * NR; task += GS) {
+                                const int r = task / 3, dir = task - 3 * r;
+                                PrimQ<double> sq;
+                                prim_setup<double>(sq, P.w, KP.y, Pv, Q.w, KQ.y, Qv, A, C, Kab * KQ.x);
+                                double ur, wr;
+                                rys_root_one<NR, double>(sq.T, table, r, ur, wr);
+                                RysCoef<double> rc;
+                                rys_coef<double>(rc, ur, sq);
+                                const double g00 = dir == 2 ? sq.pref * wr : 1.0;
+                                const double abx = dir == 0 ? AB[0] : (dir == 1 ? AB[1] : AB[2]);
+                                const double cdx = dir == 0 ? CD[0] : (dir == 1 ? CD[1] : CD[2]);
+                                grad_slice<LA, LB, LC, LD, MODE>(E + (dir * NR + r) * SE, g00, rc, dir, abx, cdx);
+                        }
+                        __syncwarp(gmask);
+                        for (int t = gl; t < NG; t += GS) {
+                                const int2 o = __ldg(a.goff + t);
+                                const int oo[3] = {o.x & 1023, (o.x >> 10) & 1023, o.x >> 20};
+                                for (int cc = 0; cc < NCP; cc++) {
+                                        const int comp = c0 + cc;
+                                        const int side = comp / 3, dir = comp - 3 * side;
+                                        const int d1 = dir == 0 ? 1 : 0, d2 = dir == 2 ? 1 : 2;
+                                        const int od = oo[dir], o1 = oo[d1], o2 = oo[d2];
+                                        double v = 0.0;
+                                        if (MODE == 0) {
+                                                const int n = gexp(o.y, side, dir);   // a_x (side A) or b_x (side B)
+                                                const int st = side == 0 ? GC::STEP_A : GC::STEP_B;
+                                                const double tw = side == 0 ? ta : tb;
+                                                for (int r = 0; r < NR; r++) {
+                                                        const double *Ed = E + (dir * NR + r) * SE;
+                                                        double dv = tw * Ed[od + st];
+                                                        if (n) dv -= n * Ed[od - st];
+                                                        v += dv * E[(d1 * NR + r) * SE + o1] * E[(d2 * NR + r) * SE + o2];
+                                                }
+                                        } else {
+                                                // bra function (a or b) and its ket partner (c or d)
+                                                const int n1 = gexp(o.y, side, dir), n2 = gexp(o.y, 2 + side, dir);
+                                                const int s1 = side == 0 ? GC::STEP_A : GC::STEP_B;
+                                                const int s2 = side == 0 ? GC::STEP_C : GC::STEP_D;
+                                                const double w1 = side == 0 ? ta : tb, w2 = side == 0 ? tc : td;
+                                                for (int r = 0; r < NR; r++) {
+                                                        const double *Ed = E + (dir * NR + r) * SE;
+                                                        double dv = w1 * w2 * Ed[od + s1 + s2];
+                                                        if (n2) dv -= w1 * n2 * Ed[od + s1 - s2];
+                                                        if (n1) dv -= n1 * w2 * Ed[od - s1 + s2];
+                                                        if (n1 && n2) dv += n1 * n2 * Ed[od - s1 - s2];
+                                                        v += dv * E[(d1 * NR + r) * SE + o1] * E[(d2 * NR + r) * SE + o2];
+                                                }
+                                        }
+                                        G[cc * NG + t] += v;
+                                }
+                        }
+                }
+        }
+        __syncwarp(gmask);
+}
+
+template <int LA, int LB, int LC, int LD>
+__host__ __device__ constexpr int grad_group_size()
+{
+        using K = Class4<LA, LB, LC, LD>;
+        return K::NG <= 100 ? 8 : (K::NG <= 400 ? 16 : 32);
+}
+
+// The gradient J/K kernel of class (LA LB | LC LD): groups of GS lanes walk
+// chunks of chunk_q quartets of one bra pair.
+template <int LA, int LB, int LC, int LD>
+__global__ void __launch_bounds__(128) grad_jk_kernel(GradArgs a, int chunk_q)
+{
+        using K = Class4<LA, LB, LC, LD>;
+        using GC = GClass<LA, LB, LC, LD, 0>;
+        using S = GradSmem<LA, LB, LC, LD, 0>;
+        constexpr int GS = grad_group_size<LA, LB, LC, LD>();
+        constexpr int NGRP = 32 / GS;
+        constexpr int NG = K::NG;
+        extern __shared__ __align__(32) double smem_dyn[];
+        const int lane = threadIdx.x & 31;
+        const int grp = lane / GS, gl = lane % GS;
+        const unsigned gmask = GS == 32 ? 0xffffffffu : (((1u << GS) - 1u) << (grp * GS));
+        const int wib = threadIdx.x >> 5;
+        double *sm = smem_dyn + (size_t)(wib * NGRP + grp) * S::SIZE;
+        const int nseg = a.bra.n * B2_NBUCKET;
+        const long long total = a.chunk_off[nseg];
+        const long long nwarps = ((long long)gridDim.x * blockDim.x) >> 5;
+        const size_t n = (size_t)a.naoc, nn = n * n;
+        unsigned long long nq = 0, npq = 0;
+        for (long long chunk = ((long long)blockIdx.x * blockDim.x + threadIdx.x) >> 5; chunk < total;
+             chunk += nwarps) {
+                const int sgi = find_bra(a.chunk_off, nseg, chunk);
+                const int ij = sgi / B2_NBUCKET;
+                const int kb = a.ket.boff[sgi % B2_NBUCKET] + a.kst[sgi];
+                const int kl0 = kb + (int)(chunk - a.chunk_off[sgi]) * chunk_q;
+                const int kl1 = kb + min((int)(chunk - a.chunk_off[sgi]) * chunk_q + chunk_q, a.nkl[sgi]);
+                const int4 sb = a.bra.sh[ij];
+                const int2 pb = a.bra.pr[ij];
+                const double4 Ab = a.bra.A[ij];
+                const double4 ABb = a.bra.AB[ij];
+                const double AB[3] = {ABb.x, ABb.y, ABb.z};
+                const int ia = sb.x, ib = sb.y;
+                const bool bra_one_segment = Ab.w != 0.0;
+                for (int kl = kl0 + grp; kl < kl1; kl += NGRP) {
+                        const int4 sk = a.ket.sh[kl];
+                        const int kk = max(sk.z, sk.w), ll = min(sk.z, sk.w);
+                        const bool sideA = grad_side_passes(a, sb.z, sb.w, kk, ll);
+                        const bool sideB = !bra_one_segment && grad_side_passes(a, sb.w, sb.z, kk, ll);
+                        if (!sideA && !sideB) continue;
+                        const int2 pk = a.ket.pr[kl];
+                        const double4 Ak = a.ket.A[kl];
+                        const double4 CDk = a.ket.AB[kl];
+                        const double fac = Ak.w != 0.0 ? 0.5 : 1.0;
+                        const double C[3] = {Ak.x - Ab.x, Ak.y - Ab.y, Ak.z - Ab.z};
+                        const double CD[3] = {CDk.x, CDk.y, CDk.z};
+                        if (gl == 0) {
+                                nq += (unsigned long long)sideA + (unsigned long long)sideB;
+                                npq += (unsigned long long)pb.y * pk.y;
+                        }
+                        const int ic = sk.x, id = sk.y;
+                        for (int pass = 0; pass < GC::NPASS; pass++) {
+                                const int c0 = pass * GC::NCP;
+                                // skip a pass whose components all belong to a failing side
+                                const bool needA = sideA && c0 < 3, needB = sideB && c0 + GC::NCP > 3;
+                                if (!needA && !needB) continue;
+                                grad_eval_pass<LA, LB, LC, LD, 0, GS>(sm, a, pb, pk, Ab, AB, C, CD, fac, c0, gl, gmask);
+                                const double *G = sm + S::G;
+                                for (int s = 0; s < a.n_dm; s++) {
+                                        const double *Ds = a.Ds + s * nn;
+                                        const double *X = a.Dc + s * nn;
+                                        double *dsab = sm + S::DSAB, *dscd = sm + S::DSCD;
+                                        double *xbc = sm + S::XBC, *xbd = sm + S::XBD;
+                                        double *xac = sm + S::XAC, *xad = sm + S::XAD;
+                                        for (int t = gl; t < K::NCD; t += GS) dscd[t] = __ldg(Ds + (ic + t / K::ND) * n + id + t % K::ND);
+                                        for (int t = gl; t < K::NB * K::NC; t += GS) xbc[t] = __ldg(X + (ib + t / K::NC) * n + ic + t % K::NC);
+                                        for (int t = gl; t < K::NB * K::ND; t += GS) xbd[t] = __ldg(X + (ib + t / K::ND) * n + id + t % K::ND);
+                                        for (int t = gl; t < K::NA * K::NC; t += GS) xac[t] = __ldg(X + (ia + t / K::NC) * n + ic + t % K::NC);
+                                        for (int t = gl; t < K::NA * K::ND; t += GS) xad[t] = __ldg(X + (ia + t / K::ND) * n + id + t % K::ND);
+                                        (void)dsab;
+                                        __syncwarp(gmask);
+                                        for (int cc = 0; cc < GC::NCP; cc++) {
+                                                const int comp = c0 + cc;
+                                                const int side = comp / 3, x = comp - 3 * side;
+                                                if (side == 0 ? !sideA : !sideB) continue;
+                                                const double *Gc = G + cc * NG;
+                                                double *Vj = a.Vj + ((size_t)s * 3 + x) * nn;
+                                                double *Vk = a.Vk + ((size_t)s * 3 + x) * nn;
+                                                if (a.with_j) {
+                                                        // side A: Vj[a,b];  side B: Vj[b,a]
+                                                        for (int t = gl; t < K::NAB; t += GS) {
+                                                                double v = 0.0;
+                                                                for (int u = 0; u < K::NCD; u++) v += Gc[t * K::NCD + u] * dscd[u];
+                                                                const int xa = t / K::NB, yb = t % K::NB;
+                                                                if (side == 0) atomicAdd(Vj + (ia + xa) * n + ib + yb, v);
+                                                                else atomicAdd(Vj + (ib + yb) * n + ia + xa, v);
+                                                        }
+                                                }
+                                                if (a.with_k) {
+                                                        if (side == 0) {
+                                                                // Vk[a,d] += G X[b,c];  Vk[a,c] += G X[b,d]
+                                                                for (int t = gl; t < K::NA * K::ND; t += GS) {
+                                                                        const int xa = t / K::ND, d = t % K::ND;
+                                                                        double v = 0.0;
+                                                                        for (int b = 0; b < K::NB; b++)
+                                                                                for (int c = 0; c < K::NC; c++)
+                                                                                        v += Gc[((xa * K::NB + b) * K::NC + c) * K::ND + d] * xbc[b * K::NC + c];
+                                                                        atomicAdd(Vk + (ia + xa) * n + id + d, v);
+                                                                }
+                                                                for (int t = gl; t < K::NA * K::NC; t += GS) {
+                                                                        const int xa = t / K::NC, c = t % K::NC;
+                                                                        double v = 0.0;
+                                                                        for (int b = 0; b < K::NB; b++)
+                                                                                for (int d = 0; d < K::ND; d++)
+                                                                                        v += Gc[((xa * K::NB + b) * K::NC + c) * K::ND + d] * xbd[b * K::ND + d];
+                                                                        atomicAdd(Vk + (ia + xa) * n + ic + c, v);
+                                                                }
+                                                        } else {
+                                                                // Vk[b,d] += G X[a,c];  Vk[b,c] += G X[a,d]
+                                                                for (int t = gl; t < K::NB * K::ND; t += GS) {
+                                                                        const int b = t / K::ND, d = t % K::ND;
+                                                                        double v = 0.0;
+                                                                        for (int xa = 0; xa < K::NA; xa++)
+                                                                                for (int c = 0; c < K::NC; c++)
+                                                                                        v += Gc[((xa * K::NB + b) * K::NC + c) * K::ND + d] * xac[xa * K::NC + c];
+                                                                        atomicAdd(Vk + (ib + b) * n + id + d, v);
+                                                                }
+                                                                for (int t = gl; t < K::NB * K::NC; t += GS) {
+                                                                        const int b = t / K::NC, c = t % K::NC;
+                                                                        double v = 0.0;
+                                                                        for (int xa = 0; xa < K::NA; xa++)
+                                                                                for (int d = 0; d < K::ND; d++)
+                                                                                        v += Gc[((xa * K::NB + b) * K::NC + c) * K::ND + d] * xad[xa * K::ND + d];
+                                                                        atomicAdd(Vk + (ib + b) * n + ic + c, v);
+                                                                }
+                                                        }
+                                                }
+                                        }
+                                        __syncwarp(gmask);
+                                }
+                        }
+                }
+        }
+        if (a.stats && gl == 0 && nq) {
+                atomicAdd(a.stats + 0, nq);
+                atomicAdd(a.stats + 1, npq);
+        }
+}
+
+// ---------------------------------------------------------------------------
+// Derivative Schwarz bound: one warp per shell pair evaluates the diagonal
+// blocks (d_x a b|d_x a b) (derivative on the first function of bra and ket,
+// x = y = z components of int2e_ip1ip2) for both orientations of the pair,
+// transforms them to the output basis and folds sqrt(max |.|) into the
+// parent-shell entries q0[A,B] (derivative on A) and q0[B,A].
+struct GradQArgs {
+        PairView pairs;
+        const double4 *PP;
+        const double2 *PK;
+        const double2 *PE;
+        const double *table;
+        const int2 *goff;
+        const double *c2s;
+        unsigned long long *q0;
+        int nbas, cart;
+};
+
+template <int LA, int LB>
+__global__ void __launch_bounds__(32) grad_q0_kernel(GradQArgs q)
+{
+        using K = Class4<LA, LB, LA, LB>;
+        using GC = GClass<LA, LB, LA, LB, 1>;
+        using S = GradSmem<LA, LB, LA, LB, 1>;
+        extern __shared__ __align__(32) double smem_dyn[];
+        double *sm = smem_dyn;
+        const int lane = threadIdx.x & 31;
+        const int ij = blockIdx.x;
+        if (ij >= q.pairs.n) return;
+        GradArgs a;
+        a.PP = q.PP;
+        a.PK = q.PK;
+        a.PE = q.PE;
+        a.table = q.table;
+        a.goff = q.goff;
+        const int4 sh = q.pairs.sh[ij];
+        const int2 pr = q.pairs.pr[ij];
+        const double4 Av = q.pairs.A[ij];
+        const double4 ABv = q.pairs.AB[ij];
+        const double AB[3] = {ABv.x, ABv.y, ABv.z}, C0[3] = {0.0, 0.0, 0.0};
+        const int nsa = q.cart ? K::NA : 2 * LA + 1, nsb = q.cart ? K::NB : 2 * LB + 1;
+        const double *ca = q.c2s + LA * 100, *cb = q.c2s + LB * 100;
+        double mA = 0.0, mB = 0.0;
+        for (int pass = 0; pass < GC::NPASS; pass++) {
+                const int c0 = pass * GC::NCP;
+                grad_eval_pass<LA, LB, LA, LB, 1, 32>(sm, a, pr, pr, Av, AB, C0, AB, 1.0, c0, lane, 0xffffffffu);
+                const double *G = sm + S::G;
+                for (int cc = 0; cc < GC::NCP; cc++) {
+                        const int side = (c0 + cc) / 3;
+                        const double *Gc = G + cc * GC::NG;
+                        double m = 0.0;
+                        for (int t = lane; t < nsa * nsb; t += 32) {
+                                const int mi = t / nsb, ni = t % nsb;
+                                double v = 0.0;
+                                for (int x = 0; x < K::NA; x++) {
+                                        const double c1 = ca[mi * 10 + x];
+                                        if (c1 == 0.0) continue;
+                                        for (int y = 0; y < K::NB; y++) {
+                                                const double c2 = cb[ni * 10 + y];
+                                                if (c2 == 0.0) continue;
+                                                for (int x2 = 0; x2 < K::NA; x2++) {
+                                                        const double c3 = ca[mi * 10 + x2];
+                                                        if (c3 == 0.0) continue;
+                                                        for (int y2 = 0; y2 < K::NB; y2++) {
+                                                                const double c4 = cb[ni * 10 + y2];
+                                                                if (c4 == 0.0) continue;
+                                                                v += c1 * c2 * c3 * c4 * Gc[((x * K::NB + y) * K::NA + x2) * K::NB + y2];
+                                                        }
+                                                }
+                                        }
+                                }
+                                m = fmax(m, fabs(v));
+                        }
+                        if (side == 0) mA = fmax(mA, m);
+                        else mB = fmax(mB, m);
+                }
+                __syncwarp();
+        }
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) {
+                mA = fmax(mA, __shfl_xor_sync(0xffffffffu, mA, o));
+                mB = fmax(mB, __shfl_xor_sync(0xffffffffu, mB, o));
+        }
+        if (lane == 0) {
+                const unsigned long long bA = (unsigned long long)__double_as_longlong(sqrt(fmax(mA, 1e-100)));
+                const unsigned long long bB = (unsigned long long)__double_as_longlong(sqrt(fmax(mB, 1e-100)));
+                atomicMax(q.q0 + (size_t)sh.z * q.nbas + sh.w, bA);
+                atomicMax(q.q0 + (size_t)sh.w * q.nbas + sh.z, bB);
+        }
+}
+
+// ---------------------------------------------------------------------------
+// helpers of the gradient build
+
+// CVHFnr_dm_cond1 (pyscf/lib/vhf/optimizer.c:472-492): max |D| over each
+// parent-shell block, all n_dm densities, not symmetrised; and the global max.
+static __global__ void dm_cond1_kernel(const double *dms, int n_dm, int nao, const int *ao_loc, int nbas,
+                                       double *dm_cond, unsigned long long *dmax_bits)
+{
+        const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+        if (t >= (long long)nbas * nbas) return;
+        const int I = (int)(t / nbas), J = (int)(t % nbas);
+        const size_t n = nao;
+        double m = 0.0;
+        for (int s = 0; s < n_dm; s++) {
+                const double *D = dms + (size_t)s * n * n;
+                for (int a = ao_loc[I]; a < ao_loc[I + 1]; a++)
+                        for (int b = ao_loc[J]; b < ao_loc[J + 1]; b++) m = fmax(m, fabs(D[a * n + b]));
+        }
+        dm_cond[t] = m;
+        atomicMax(dmax_bits, (unsigned long long)__double_as_longlong(m));
+}
+
+// density factor of the ket-prefix bound: the screen needs
+// q0 q1 > tol and q0 q1 max(2 D_lk, D_jk, D_jl) > tol, so q1 > tol / (q0 min(1, 2 max|D|))
+static __global__ void grad_dm_factor_kernel(const unsigned long long *dmax_bits, double *factor)
+{
+        const double m = __longlong_as_double((long long)*dmax_bits);
+        *factor = fmin(1.0, 2.0 * m);
+}
+
+// out[x][mu][nu] = scale sum_ab C[mu,a] V[x][a,b] C[nu,b], for nv blocks
+static __global__ void grad_cart_to_out_kernel(const double *V, int nv, int nao, int naoc, const int *out_seg,
+                                               const int *out_comp, const int4 *seg_info, const double *c2s,
+                                               double scale, double *out)
+{
+        const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+        const long long nn = (long long)nao * nao;
+        if (t >= nn * nv) return;
+        const long long blk = t / nn, r = t - blk * nn;
+        const int mu = (int)(r / nao), nu = (int)(r % nao);
+        const double *A = V + (size_t)blk * naoc * naoc;
+        const int sm = out_seg[mu], sn = out_seg[nu];
+        const int4 im = seg_info[sm], in_ = seg_info[sn];
+        const int km = out_comp[mu], kn = out_comp[nu];
+        const int ncm = (im.x + 1) * (im.x + 2) / 2, ncn = (in_.x + 1) * (in_.x + 2) / 2;
+        const double *cm = c2s + im.x * 100 + km * 10, *cn = c2s + in_.x * 100 + kn * 10;
+        double v = 0.0;
+        for (int x = 0; x < ncm; x++) {
+                const double f1 = cm[x];
+                if (f1 == 0.0) continue;
+                const size_t a = im.z + x;
+                double s = 0.0;
+                for (int y = 0; y < ncn; y++) {
+                        const double f2 = cn[y];
+                        if (f2 == 0.0) continue;
+                        s += f2 * A[a * naoc + in_.z + y];
+                }
+                v += f1 * s;
+        }
+        out[t] = scale * v;
+}
+
+} // namespace b200jk

@@ -1,0 +1,36 @@
+// grad_launch.h — interface between the host planner (b200jk.cu) and the
+// translation units of the gradient kernels (grad_classes.cu, compiled once
+// per bra angular class).
+#pragma once
+#include <cuda_runtime.h>
+#include <string>
+#include "grad_kernels.cuh"
+
+namespace b200jk {
+
+// quartets per chunk of a warp for class (la lb | lc ld): 8 per group
+inline int grad_chunk(int la, int lb, int lc, int ld)
+{
+        const int ng = ncart(la) * ncart(lb) * ncart(lc) * ncart(ld);
+        const int gs = ng <= 100 ? 8 : (ng <= 400 ? 16 : 32);
+        return 8 * (32 / gs);
+}
+
+// one launcher per bra class (la, lb), la >= lb; the ket class (lc, ld),
+// lc >= ld, is a run-time argument
+#define B2_GRAD_DECL(LA, LB)                                                                              \
+        int launch_grad_##LA##LB(int lc, int ld, const GradArgs &a, cudaStream_t s, int nsm, std::string &err); \
+        int launch_gq0_##LA##LB(const GradQArgs &q, cudaStream_t s, std::string &err);
+B2_GRAD_DECL(0, 0)
+B2_GRAD_DECL(1, 0)
+B2_GRAD_DECL(1, 1)
+B2_GRAD_DECL(2, 0)
+B2_GRAD_DECL(2, 1)
+B2_GRAD_DECL(2, 2)
+B2_GRAD_DECL(3, 0)
+B2_GRAD_DECL(3, 1)
+B2_GRAD_DECL(3, 2)
+B2_GRAD_DECL(3, 3)
+#undef B2_GRAD_DECL
+
+} // namespace b200jk

@@ -1,0 +1,157 @@
+"""Nuclear gradients of the two-electron energy on the GPU.
+
+``get_jk(mol, dm)`` is the drop-in for ``pyscf.grad.rhf.get_jk``
+(pyscf/grad/rhf.py:149-178): J/K with the first bra function differentiated
+(libcint's int2e_ip1), screened as CVHFgrad_jk_prescreen does with the
+reference's threshold 1e-14, returned negated, shape (3, nao, nao) per
+density.  ``patch_pyscf_grad()`` rebinds it in an unmodified PySCF, where
+``GradientsBase.get_jk`` looks it up through the module (pyscf/grad/rhf.py:321).
+
+``grad_2e(plan, dm, aoslice)`` contracts the result into the two-electron part
+of the RHF gradient, the term grad_elec adds (pyscf/grad/rhf.py:67-69):
+    de[A] = 2 sum_x sum_{i in A} sum_j (vj - vk/2)[x, i, j] D[i, j].
+
+``TwoElectronEnergy`` is a torch.autograd.Function of the nuclear coordinates
+(and the density): forward builds J/K on the GPU for the geometry and returns
+E2 = 1/2 tr(D J) - 1/4 tr(D K); backward runs the int2e_ip1 kernel and
+returns dE2/dR (at fixed AO density) and dE2/dD = J - K/2.
+"""
+import numpy
+
+from . import lib
+
+GRAD_SCREEN_TOL = 1e-14     # _VHFOpt's default threshold in grad.rhf.get_jk
+PTR_COORD = 1
+
+
+def aoslice_by_atom(atm, bas, cart=False):
+    """(natm, 2) AO ranges of every atom (shells of an atom are contiguous in _bas)."""
+    bas = numpy.asarray(bas)
+    l = bas[:, 1]
+    nf = ((l + 1) * (l + 2) // 2 if cart else 2 * l + 1) * bas[:, 3]
+    ao_loc = numpy.concatenate([[0], numpy.cumsum(nf)])
+    natm = len(atm)
+    out = numpy.zeros((natm, 2), dtype=numpy.int64)
+    for a in range(natm):
+        idx = numpy.where(bas[:, 0] == a)[0]
+        if len(idx):
+            out[a] = ao_loc[idx[0]], ao_loc[idx[-1] + 1]
+        else:
+            out[a] = ao_loc[-1], ao_loc[-1]
+    return out
+
+
+_plans = {}
+
+
+def _plan_for(mol):
+    key = (id(mol), mol._env.tobytes(), mol._bas.tobytes(), mol._atm.tobytes(), bool(mol.cart))
+    p = _plans.get(key)
+    if p is None:
+        _plans.clear()
+        p = lib.Plan(mol._atm, mol._bas, mol._env, cart=bool(mol.cart), direct_scf_tol=1e-13)
+        _plans[key] = p
+    return p
+
+
+def get_jk(mol, dm):
+    """pyscf.grad.rhf.get_jk(mol, dm) on the GPU: (vj, vk), each (3, nao, nao)
+    for one density or (n_dm, 3, nao, nao) for a stack."""
+    dm = numpy.asarray(dm, dtype=numpy.double)
+    return _plan_for(mol).grad_jk(dm, direct_scf_tol=GRAD_SCREEN_TOL)
+
+
+def grad_2e(vj, vk, dm, aoslice):
+    """Two-electron part of the RHF nuclear gradient from grad_jk's output."""
+    vhf = vj - 0.5 * vk
+    return numpy.array([2.0 * numpy.einsum('xij,ij->x', vhf[:, p0:p1], dm[p0:p1]) for p0, p1 in aoslice])
+
+
+_saved = {}
+
+
+def patch_pyscf_grad():
+    """Route pyscf.grad.rhf.get_jk (RHF/RKS nuclear gradients) through the GPU."""
+    import pyscf.grad.rhf as ref
+    if _saved:
+        return
+    _saved['get_jk'] = ref.get_jk
+    ref.get_jk = get_jk
+
+
+def unpatch_pyscf_grad():
+    import pyscf.grad.rhf as ref
+    if not _saved:
+        return
+    ref.get_jk = _saved.pop('get_jk')
+
+
+def _env_with_coords(atm, env, coords):
+    env = numpy.array(env, dtype=numpy.double, copy=True)
+    for a, row in enumerate(numpy.asarray(atm)):
+        p = int(row[PTR_COORD])
+        env[p:p + 3] = coords[a]
+    return env
+
+
+def _torch_function():
+    import torch
+
+    class TwoElectronEnergy(torch.autograd.Function):
+        """E2(R, D) = 1/2 tr(D J[D]) - 1/4 tr(D K[D]) for a symmetric AO density
+        D at nuclear coordinates R (Bohr, (natm, 3)); J/K and the ip1 backward
+        run on the GPU.  Usage:
+            E2 = TwoElectronEnergy.apply(coords, dm, atm, bas, env, cart)
+        """
+
+        @staticmethod
+        def forward(ctx, coords, dm, atm, bas, env, cart=False):
+            c = coords.detach().cpu().numpy().astype(numpy.double)
+            env2 = _env_with_coords(atm, env, c)
+            plan = lib.Plan(atm, bas, env2, cart=bool(cart), direct_scf_tol=1e-13,
+                            device=dm.device.index if dm.is_cuda else 0)
+            d = dm.detach()
+            if d.is_cuda:
+                vj, vk = plan.get_jk_device(d.contiguous(), hermi=1)
+            else:
+                vj, vk = plan.get_jk(d.numpy(), hermi=1)
+                vj, vk = torch.from_numpy(vj), torch.from_numpy(vk)
+            veff = vj - 0.5 * vk
+            e2 = 0.5 * torch.sum(d * veff)
+            ctx.plan = plan
+            ctx.aoslice = aoslice_by_atom(atm, bas, cart)
+            ctx.save_for_backward(d, veff)
+            return e2.to(coords.dtype).to(coords.device)
+
+        @staticmethod
+        def backward(ctx, grad_out):
+            d, veff = ctx.saved_tensors
+            g_coords = g_dm = None
+            if ctx.needs_input_grad[0]:
+                if d.is_cuda:
+                    gj, gk = ctx.plan.grad_jk_device(d.contiguous(), direct_scf_tol=GRAD_SCREEN_TOL)
+                    vhf = gj - 0.5 * gk
+                    rows = []
+                    for p0, p1 in ctx.aoslice:
+                        rows.append(2.0 * torch.einsum('xij,ij->x', vhf[:, p0:p1], d[p0:p1]))
+                    g = torch.stack(rows)
+                else:
+                    gj, gk = ctx.plan.grad_jk(d.numpy(), direct_scf_tol=GRAD_SCREEN_TOL)
+                    g = torch.from_numpy(grad_2e(gj, gk, d.numpy(), ctx.aoslice))
+                g_coords = (grad_out.to(g.device) * g).to(grad_out.device)
+            if ctx.needs_input_grad[1]:
+                g_dm = grad_out.to(veff.device) * veff
+            return g_coords, g_dm, None, None, None, None
+
+    return TwoElectronEnergy
+
+
+_fn = None
+
+
+def two_electron_energy(coords, dm, atm, bas, env, cart=False):
+    """E2(coords, dm) as a differentiable torch scalar (see TwoElectronEnergy)."""
+    global _fn
+    if _fn is None:
+        _fn = _torch_function()
+    return _fn.apply(coords, dm, atm, bas, env, cart)

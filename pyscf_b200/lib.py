@@ -26,7 +26,7 @@ EXPORTS = (
     'b200jk_plan_destroy', 'b200jk_plan_dims', 'b200jk_get_q_cond', 'b200jk_get_jk',
     'b200jk_stats', 'b200jk_hostcheck_cart_quartet', 'b200jk_class_stats', 'b200jk_set_profiling',
     'b200jk_measure_fp64_peak', 'b200jk_get_jk_noalloc', 'b200jk_set_mixed_threshold',
-    'b200jk_hostcheck_cart_quartet_fp32',
+    'b200jk_hostcheck_cart_quartet_fp32', 'b200jk_grad_jk', 'b200jk_grad_stats', 'b200jk_get_grad_q_cond',
 )
 
 
@@ -82,6 +82,10 @@ def load(path=LIB_PATH):
         lib.b200jk_measure_fp64_peak.argtypes = [ip, ctypes.POINTER(dp)]
         lib.b200jk_get_jk_noalloc.argtypes = [vp, vp, ip, ip, ip, ip, vp, vp, vp]
         lib.b200jk_set_mixed_threshold.argtypes = [vp, dp]
+        lib.b200jk_grad_jk.argtypes = [vp, vp, ip, ip, ip, vp, vp, ip, dp, vp]
+        lib.b200jk_grad_stats.argtypes = [vp, ctypes.POINTER(ctypes.c_int64), ctypes.POINTER(ctypes.c_int64),
+                                          ctypes.POINTER(dp), ctypes.POINTER(ctypes.c_int64)]
+        lib.b200jk_get_grad_q_cond.argtypes = [vp, vp]
         _lib = lib
         return lib
 
@@ -203,6 +207,55 @@ class Plan:
                                    ctypes.c_void_p(vk.data_ptr()) if with_k else None,
                                    1, int(precision), ctypes.c_void_p(stream)))
         return (vj.reshape(shape) if with_j else None), (vk.reshape(shape) if with_k else None)
+
+    def grad_jk(self, dms, with_j=True, with_k=True, direct_scf_tol=1e-14):
+        """pyscf.grad.rhf.get_jk of host densities: (vj, vk) with shape
+        (3, nao, nao) per density (leading n_dm axis kept if given)."""
+        dms = numpy.asarray(dms, dtype=numpy.double, order='C')
+        nao = dms.shape[-1]
+        if nao != self.nao or dms.shape[-2] != nao:
+            raise ValueError('density shape %s does not match nao=%d' % (dms.shape, self.nao))
+        d = dms.reshape(-1, nao, nao)
+        n_dm = d.shape[0]
+        vj = numpy.empty((n_dm, 3, nao, nao)) if with_j else None
+        vk = numpy.empty((n_dm, 3, nao, nao)) if with_k else None
+        check(load().b200jk_grad_jk(self._h, _ptr(d), n_dm, int(bool(with_j)), int(bool(with_k)),
+                                    _ptr(vj) if with_j else None, _ptr(vk) if with_k else None,
+                                    0, float(direct_scf_tol), None))
+        shape = dms.shape[:-2] + (3, nao, nao)
+        return (vj.reshape(shape) if with_j else None), (vk.reshape(shape) if with_k else None)
+
+    def grad_jk_device(self, dms, with_j=True, with_k=True, direct_scf_tol=1e-14):
+        """grad_jk of a float64 CUDA tensor (..., nao, nao) -> CUDA tensors (..., 3, nao, nao)."""
+        import torch
+        if not (isinstance(dms, torch.Tensor) and dms.is_cuda and dms.dtype == torch.float64):
+            raise TypeError('dms must be a float64 CUDA tensor')
+        nao = dms.shape[-1]
+        d = dms.reshape(-1, nao, nao).contiguous()
+        n_dm = d.shape[0]
+        vj = torch.empty((n_dm, 3, nao, nao), dtype=torch.float64, device=d.device) if with_j else None
+        vk = torch.empty((n_dm, 3, nao, nao), dtype=torch.float64, device=d.device) if with_k else None
+        stream = torch.cuda.current_stream(d.device).cuda_stream
+        check(load().b200jk_grad_jk(self._h, ctypes.c_void_p(d.data_ptr()), n_dm, int(bool(with_j)),
+                                    int(bool(with_k)), ctypes.c_void_p(vj.data_ptr()) if with_j else None,
+                                    ctypes.c_void_p(vk.data_ptr()) if with_k else None, 1,
+                                    float(direct_scf_tol), ctypes.c_void_p(stream)))
+        shape = tuple(dms.shape[:-2]) + (3, nao, nao)
+        return (vj.reshape(shape) if with_j else None), (vk.reshape(shape) if with_k else None)
+
+    def grad_stats(self):
+        q, pq, n = ctypes.c_int64(0), ctypes.c_int64(0), ctypes.c_int64(0)
+        ms = ctypes.c_double(0)
+        check(load().b200jk_grad_stats(self._h, ctypes.byref(q), ctypes.byref(pq), ctypes.byref(ms), ctypes.byref(n)))
+        return {'quartets': q.value, 'prim_quartets': pq.value, 'last_build_ms': ms.value, 'kernel_launches': n.value}
+
+    @property
+    def grad_q_cond(self):
+        """(2, nbas, nbas): derivative Schwarz bound and q_cond of the gradient screen."""
+        nbas = self.nbas
+        q = numpy.empty((2, nbas, nbas))
+        check(load().b200jk_get_grad_q_cond(self._h, _ptr(q)))
+        return q
 
 
 def measure_fp64_peak(device=0):

@@ -74,3 +74,32 @@ def test_reference_energies_in_fixture():
     f = load_fixture('h2o_vdz')
     assert abs(float(f['e_rhf']) - -76.026765673120565) < 1e-9
     assert abs(float(f['e_rhf']) - -76.026765673119627) < 1e-9
+
+
+def _grad_fixture(name):
+    import os
+    path = os.path.join(os.path.dirname(os.path.abspath(__file__)), 'golden', 'grad_%s.npz' % name)
+    return dict(numpy.load(path))
+
+
+@pytest.mark.parametrize('name', ['h2o_631g', 'h2o2_vtz'])
+def test_grad_oracle_matches_reference(name):
+    """The oracle's restatement of grad.rhf.get_jk (driver, screen, derivative
+    conditioner) against the reference's own output."""
+    f = _grad_fixture(name)
+    q = oracle.grad_q_cond(f['atm'], f['bas'], f['env'])
+    assert abs(q - f['gq_cond']).max() <= 1e-12 * abs(f['gq_cond']).max()
+    vj, vk = oracle.grad_jk(f['dm0'], f['atm'], f['bas'], f['env'])
+    assert abs(vj - f['gvj']).max() < 1e-11
+    assert abs(vk - f['gvk']).max() < 1e-11
+
+
+def test_grad_reference_fingerprint():
+    """The fixture's RHF gradient reproduces the reference test's value
+    (pyscf/grad/test/test_rhf.py:148-153, 6 places) and its own finite
+    differences."""
+    f = _grad_fixture('h2o_631g')
+    assert abs(lib_fp(f['de']) - 0.0055115512502467556) < 5e-7
+    h = float(f['fd_h'])
+    fd = (f['fd_energies'][:, 0] - f['fd_energies'][:, 1]) / (2 * h)
+    assert abs(f['de'].ravel()[f['fd_coords']] - fd).max() < 1e-6
