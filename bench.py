@@ -10,8 +10,18 @@ N(0,1)/sqrt(nao) entries (seed 304).  Metric: shell quartets per second
 (s8-unique quartets of PySCF _bas shells surviving the direct_scf_tol=1e-13
 screen) with seconds per build alongside.
 
-N > 1 (torchrun): every rank builds J/K of the same workload on its own GPU
-(replicas, weak scaling); the time is the max over ranks.
+N > 1 (torchrun): the quartets of the one workload are sharded over the ranks
+by bra shell pair (b200jk_set_shard) and every step ends with one NCCL
+all-reduce of [J; K] inside the timed region (strong scaling); the time is the
+max over ranks and the value counts the quartets of all ranks.
+
+Besides the FP64 headline the line carries, measured in the same run:
+  mixed   the mixed-precision build (float32 quartets below tau, float64
+          accumulation) of the same density, its time, speed-up over FP64,
+          float32 fraction and error against the FP64 build (max |dJ|, |dK|,
+          dE = 1/2 tr(D dJ) - 1/4 tr(D dK)), and the same for a
+          difference-density build (dD = 1e-4 C2 C2^T, the late-SCF regime);
+  grad    the nuclear-gradient J/K (int2e_ip1) of (H2O)16/cc-pVDZ.
 
 --impl reference times the reference's own CPU implementation of the path
 (PySCF's CVHFnr_direct_drv compiled from the reference sources, oracle/_ref,
@@ -164,121 +174,231 @@ def run_reference(args):
     print(json.dumps(line))
 
 
+def _max_over_ranks(v, dist, dev):
+    if dist is None:
+        return v
+    import torch
+    t = torch.tensor([v], device=dev, dtype=torch.float64)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def _sum_over_ranks(v, dist, dev):
+    if dist is None:
+        return v
+    import torch
+    t = torch.tensor([float(v)], device=dev, dtype=torch.float64)
+    dist.all_reduce(t, op=dist.ReduceOp.SUM)
+    return float(t.item())
+
+
+def _timed_builds(plan, d, flush, stream, steps, dist, build):
+    """steps builds of `build()` on the device, L2 flushed before each;
+    returns (list of seconds, summed plan stats)."""
+    import torch
+    times = []
+    nq = npq = nq32 = launches = 0
+    for _ in range(steps):
+        flush.fill_(1.0)
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        out = build()
+        e1.record(stream)
+        e1.synchronize()
+        times.append(e0.elapsed_time(e1) * 1e-3)
+        st = plan.stats()
+        nq += st['quartets']
+        npq += st['prim_quartets']
+        nq32 += st['fp32_quartets']
+        launches += st['kernel_launches']
+    return times, dict(quartets=nq, prim_quartets=npq, fp32_quartets=nq32, kernel_launches=launches), out
+
+
 def run_gpu(args):
     import torch
     from pyscf_b200 import lib, flops
     from pyscf_b200 import _vhf
+    from pyscf_b200 import dist as b2dist
     rank, world, local, dist = dist_init(args.gpus)
     torch.cuda.set_device(local)
     dev = torch.device('cuda', local)
     f = load_workload(args.config)
     nao = int(f['nao'])
     plan = lib.Plan(f['atm'], f['bas'], f['env'], direct_scf_tol=1e-13, device=local)
+    if world > 1:
+        plan.set_shard(rank, world)
     d = torch.tensor(f['dm'], device=dev)
     flush = torch.empty(2 * L2_BYTES // 4, dtype=torch.float32, device=dev)
     stream = torch.cuda.current_stream(dev)
+
+    def build64():
+        vj, vk = plan.get_jk_device(d, hermi=1)
+        if dist is not None:
+            b2dist.reduce_jk(vj, vk)
+        return vj, vk
+
     for _ in range(args.warmup):
-        plan.get_jk_device(d, hermi=1)
+        build64()
     torch.cuda.synchronize(dev)
     plan.set_profiling(True)
-    class_ms = {}
-    times = []
-    nq = npq = launches = 0
     if dist is not None:
         dist.barrier()
     torch.cuda.synchronize(dev)
     with ClockSampler(local) as clk:
-        for _ in range(args.steps):
-            flush.fill_(1.0)    # evict L2 between timed builds
-            e0 = torch.cuda.Event(enable_timing=True)
-            e1 = torch.cuda.Event(enable_timing=True)
-            e0.record(stream)
-            vj, vk = plan.get_jk_device(d, hermi=1)
-            e1.record(stream)
-            e1.synchronize()
-            times.append(e0.elapsed_time(e1) * 1e-3)
-            st = plan.stats()
-            nq += st['quartets']
-            npq += st['prim_quartets']
-            launches += st['kernel_launches']
-            for c in plan.class_stats():
-                k = (c['la'], c['lb'], c['lc'], c['ld'])
-                acc = class_ms.setdefault(k, dict(c, ms=0.0, quartets=0, prim_quartets=0))
-                acc['ms'] += c['ms']
-                acc['quartets'] += c['quartets']
-                acc['prim_quartets'] += c['prim_quartets']
+        times, tot, (vj64, vk64) = _timed_builds(plan, d, flush, stream, args.steps, dist, build64)
         torch.cuda.synchronize(dev)
     if dist is not None:
         dist.barrier()
-    t_total = sum(times)
-    if dist is not None:
-        tt = torch.tensor([t_total], device=dev, dtype=torch.float64)
-        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
-        t_total = float(tt.item())
     plan.set_profiling(False)
-    q_per_build = nq / args.steps
-    value = world * nq / t_total
+    class_ms = {}
+    # per-class times of the last build (profiling was on for all timed builds)
+    for c in plan.class_stats():
+        class_ms[(c['la'], c['lb'], c['lc'], c['ld'])] = dict(c)
+    t_total = _max_over_ranks(sum(times), dist, dev)
+    nq_all = _sum_over_ranks(tot['quartets'], dist, dev)
+    q_per_build = nq_all / args.steps
+    value = nq_all / t_total
     # roofline: FP64 pipe (the recurrences are scalar FP64, no tensor-core form)
     fp64_peak = lib.measure_fp64_peak(local)
     cls = list(class_ms.values())
-    build_flops = flops.build_flops(cls) / args.steps
+    build_flops = flops.build_flops(cls)
     dom = max(cls, key=lambda c: c['ms'])
-    dom_ms = dom['ms'] / args.steps
-    dom_flops = flops.class_flops(dom) / args.steps
+    dom_ms = dom['ms']
+    dom_flops = flops.class_flops(dom)
     achieved = dom_flops / (dom_ms * 1e-3) / 1e12
     traffic = None
     tpath = os.path.join(ROOT, 'profiles', 'traffic.json')
     key = 'jk_%d%d%d%d_%s' % (dom['la'], dom['lb'], dom['lc'], dom['ld'], args.config)
     if os.path.exists(tpath):
         traffic = json.load(open(tpath)).get(key)
+
+    # mixed precision on the same density, error against the FP64 build
+    def mixed_report(dens, tag, steps):
+        plan.set_mixed_threshold(args.tau)
+
+        def build32():
+            vj, vk = plan.get_jk_device(dens, hermi=1, precision=lib.PREC_MIXED)
+            if dist is not None:
+                b2dist.reduce_jk(vj, vk)
+            return vj, vk
+
+        def build64d():
+            vj, vk = plan.get_jk_device(dens, hermi=1)
+            if dist is not None:
+                b2dist.reduce_jk(vj, vk)
+            return vj, vk
+        build32()
+        t32, s32, (vj, vk) = _timed_builds(plan, dens, flush, stream, steps, dist, build32)
+        if tag == 'D':
+            t64, j64, k64 = times, vj64, vk64
+        else:
+            build64d()
+            t64, _, (j64, k64) = _timed_builds(plan, dens, flush, stream, steps, dist, build64d)
+        ms32 = _max_over_ranks(sum(t32), dist, dev) / steps * 1e3
+        ms64 = _max_over_ranks(sum(t64), dist, dev) / len(t64) * 1e3
+        dj = float((vj - j64).abs().max())
+        dk = float((vk - k64).abs().max())
+        de = float(0.5 * torch.sum(dens * ((vj - j64) - 0.5 * (vk - k64))))
+        return {'density': tag, 'tau': args.tau, 'ms_per_build': ms32, 'fp64_ms_per_build': ms64,
+                'speedup_vs_fp64': ms64 / ms32, 'fp32_quartet_fraction': s32['fp32_quartets'] / max(1, s32['quartets']),
+                'max_dJ': dj, 'max_dK': dk, 'dE_Eh': de}
+    mixed = [mixed_report(d, 'D', args.steps)]
+    rng = numpy.random.default_rng(305)
+    c2 = rng.standard_normal((nao, 64)) / numpy.sqrt(nao)
+    dd = torch.tensor(1e-4 * (c2 @ c2.T), device=dev)
+    mixed.append(mixed_report(dd, 'dD = 1e-4 C2 C2^T (C2 nao x 64, seed 305)', 1))
+    plan.set_mixed_threshold(0.0)
+
+    # nuclear-gradient J/K of the (H2O)16/cc-pVDZ workload
+    grad_line = None
+    try:
+        fg = load_workload('h2o16_vdz')
+        gplan = lib.Plan(fg['atm'], fg['bas'], fg['env'], direct_scf_tol=1e-13, device=local)
+        if world > 1:
+            gplan.set_shard(rank, world)
+        dg = torch.tensor(fg['dm'], device=dev)
+
+        def gbuild():
+            vj, vk = gplan.grad_jk_device(dg)
+            if dist is not None:
+                b2dist.reduce_jk(vj, vk)
+            return vj, vk
+        gbuild()
+        gt = []
+        gq = 0
+        for _ in range(args.steps):
+            flush.fill_(1.0)
+            e0 = torch.cuda.Event(enable_timing=True)
+            e1 = torch.cuda.Event(enable_timing=True)
+            e0.record(stream)
+            gbuild()
+            e1.record(stream)
+            e1.synchronize()
+            gt.append(e0.elapsed_time(e1) * 1e-3)
+            gq += gplan.grad_stats()['quartets']
+        tg = _max_over_ranks(sum(gt), dist, dev)
+        gq = _sum_over_ranks(gq, dist, dev)
+        grad_line = {'workload': 'h2o16_vdz', 'nao': int(fg['nao']), 'ms_per_build': tg / args.steps * 1e3,
+                     'quartet_sides_per_build': gq / args.steps, 'quartet_sides_per_s': gq / tg,
+                     'screen': 'CVHFgrad_jk_prescreen, tol 1e-14'}
+    except Exception as e:  # the gradient line must not sink the J/K measurement
+        grad_line = {'error': str(e)[:200]}
+
     # end to end through the public API, host arrays in pinned memory
     dm_host = torch.from_numpy(f['dm']).pin_memory().numpy()
     out = torch.empty((2, nao, nao), dtype=torch.float64).pin_memory().numpy()
     vhfopt = _vhf.VHFOpt(_Mol(f), direct_scf_tol=1e-13, device=local)
-    _vhf.direct(dm_host, f['atm'], f['bas'], f['env'], vhfopt, hermi=1, out=out)
+    if world > 1:
+        vhfopt.plan.set_shard(rank, world)
     e2e_times = []
-    for _ in range(max(1, min(args.steps, 3))):
+    for it in range(1 + max(1, min(args.steps, 3))):
         flush.fill_(1.0)
         torch.cuda.synchronize(dev)
         t0 = time.perf_counter()
         _vhf.direct(dm_host, f['atm'], f['bas'], f['env'], vhfopt, hermi=1, out=out)
-        e2e_times.append(time.perf_counter() - t0)
-    t_e2e = float(numpy.mean(e2e_times))
-    if dist is not None:
-        tt = torch.tensor([t_e2e], device=dev, dtype=torch.float64)
-        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
-        t_e2e = float(tt.item())
+        if dist is not None:
+            o = torch.from_numpy(out).to(dev)
+            dist.all_reduce(o)
+            out[...] = o.cpu().numpy()
+        if it > 0:
+            e2e_times.append(time.perf_counter() - t0)
+    t_e2e = _max_over_ranks(float(numpy.mean(e2e_times)), dist, dev)
     clocks = clk.summary()
     if rank == 0:
         line = {
             'metric': METRIC, 'value': value, 'unit': 'shell quartets/s', 'n_gpus': world,
             'steps': args.steps, 'warmup': args.warmup, 'ms_per_step': t_total / args.steps * 1e3,
-            'higher_is_better': True, 'scaling': 'weak', 'vs_baseline': None, 'dtype': 'f64',
-            'data': 'synthetic',
+            'higher_is_better': True, 'scaling': 'strong' if world > 1 else 'weak', 'vs_baseline': None,
+            'dtype': 'f64', 'data': 'synthetic',
             'config': {'workload': args.config, 'nao': nao, 'nbas': int(f['bas'].shape[0]),
                        'density': 'C C^T, C nao x 320 N(0,1)/sqrt(nao), seed 304', 'hermi': 1,
-                       'precision': 'fp64', 'direct_scf_tol': 1e-13, 'parallelism': 'replicas' if world > 1 else 'single',
+                       'precision': 'fp64', 'direct_scf_tol': 1e-13,
+                       'parallelism': ('bra-pair shards + NCCL all-reduce of [J;K], %d GPUs' % world) if world > 1
+                       else 'single',
                        'l2': 'flushed (256 MB write) before every timed build'},
             's_per_build': t_total / args.steps,
-            'quartets_per_build': q_per_build, 'prim_quartets_per_build': npq / args.steps,
-            'fp64_tflops_build': build_flops / (t_total / args.steps) / 1e12,
+            'quartets_per_build': q_per_build, 'prim_quartets_per_build': _sum_over_ranks(tot['prim_quartets'], dist, dev) / args.steps,
+            'fp64_tflops_build': build_flops / (t_total / args.steps) / 1e12 if world == 1 else None,
             'roofline': {'bound': 'fp64', 'kernel': 'jk_%s_kernel<%d,%d,%d,%d>' % (
                              'thread' if dom['family'] == 0 else 'warp', dom['la'], dom['lb'], dom['lc'], dom['ld']),
                          'achieved': achieved, 'peak': fp64_peak, 'unit': 'TFLOP/s', 'frac': achieved / fp64_peak,
                          'peak_source': 'measured FP64 FMA loop on this GPU (b200jk_measure_fp64_peak)',
-                         'share': dom_ms * 1e-3 / (t_total / args.steps), 'traffic': traffic},
-            'e2e': {'value': world * q_per_build / t_e2e, 'unit': 'shell quartets/s',
+                         'share': dom_ms * 1e-3 / (sum(times) / args.steps), 'traffic': traffic},
+            'mixed': mixed,
+            'grad': grad_line,
+            'e2e': {'value': q_per_build / t_e2e, 'unit': 'shell quartets/s',
                     's_per_build': t_e2e, 'h2d_bytes_per_step': int(nao * nao * 8),
                     'd2h_bytes_per_step': int(2 * nao * nao * 8),
                     'timing': 'wall clock around pyscf_b200._vhf.direct with pinned host arrays'},
             'classes': [{'class': '(%d%d|%d%d)' % (c['la'], c['lb'], c['lc'], c['ld']),
                          'family': 'thread' if c['family'] == 0 else 'group',
-                         'ms_per_build': c['ms'] / args.steps,
-                         'share': c['ms'] * 1e-3 / t_total,
-                         'quartets_per_build': c['quartets'] / args.steps,
+                         'ms_per_build': c['ms'],
+                         'share': c['ms'] * 1e-3 / (sum(times) / args.steps),
+                         'quartets_per_build': c['quartets'],
                          'tflops': flops.class_flops(c) / (c['ms'] * 1e-3) / 1e12 if c['ms'] > 0 else None}
                         for c in sorted(cls, key=lambda c: -c['ms'])[:12]],
-            'gpu_launches': int(launches),
+            'gpu_launches': int(tot['kernel_launches']),
             'clocks': clocks,
         }
         cb = None
@@ -314,6 +434,7 @@ def main():
     ap.add_argument('--impl', default='b200', choices=['b200', 'reference'])
     ap.add_argument('--config', default='h2o64_vtz')
     ap.add_argument('--no-cpu-baseline', action='store_true')
+    ap.add_argument('--tau', type=float, default=1e-6, help='float32 threshold of the mixed-precision line')
     args = ap.parse_args()
     if args.impl == 'reference':
         run_reference(args)

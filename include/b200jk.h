@@ -161,7 +161,15 @@ int b200jk_grad_stats(const b200jk_plan *plan, int64_t *quartets, int64_t *prim_
  * row shell (CVHFnr_int2e_pp_q_cond), plane 1 q_cond. */
 int b200jk_get_grad_q_cond(b200jk_plan *plan, double *q_cond);
 
-/* Threshold tau of B200JK_PREC_MIXED (default 1e-9): a shell quartet whose
+/* Multi-GPU sharding: the plan's J/K and gradient builds evaluate only the
+ * bra shell pairs ij = index (mod count) of every quartet class, so count
+ * plans (one per GPU, same molecule) produce partial results whose sum is the
+ * full build; the caller sums them (an all-reduce).  Default index 0, count 1.
+ * Replaces the reference's OpenMP split of CVHFnr_direct_drv's block loop
+ * (pyscf/lib/vhf/nr_direct.c:355-476) across GPUs. */
+int b200jk_set_shard(b200jk_plan *plan, int index, int count);
+
+/* Threshold tau of B200JK_PREC_MIXED (default 1e-6): a shell quartet whose
  * Schwarz bound times the largest density element, q_ij q_kl max|D|, is below
  * tau is evaluated in float32.  The bound uses the density passed to each
  * build, so incremental (difference-density) builds move more quartets to

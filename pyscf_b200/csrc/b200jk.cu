@@ -226,7 +226,9 @@ struct b200jk_plan {
         int device = 0, cart = 0, natm = 0, nbas = 0, nao = 0, naoc = 0, nseg = 0;
         double tol = 0;
         // mixed precision: quartets with q_ij q_kl max|D| below fp32_tau run in float32
-        double fp32_tau = 1e-9;
+        double fp32_tau = 1e-6;
+        // multi-GPU: this plan evaluates the bra pairs ij = shard (mod nshard)
+        int shard = 0, nshard = 1;
         std::vector<int> ao_loc;
         std::vector<double> h_qcond;
         PairClassDev pc[NPAIRCLASS];
@@ -814,7 +816,8 @@ int b200jk_get_jk(b200jk_plan *P, const double *dms, int n_dm, int hermi, int wi
                         for (int pass = 0; pass < (mixed ? 2 : 1); pass++) {
                                 count_kernel<<<grid_for(nseg, 256), 256, 0, s>>>(
                                         bra.view(), ket.view(), same, P->tol > 0 ? P->tol : 0.0, (const double *)P->dmax.p,
-                                        chunk, mixed ? P->fp32_tau : 0.0, pass, P->nkl.p, P->kst.p, P->nchunk.p);
+                                        chunk, mixed ? P->fp32_tau : 0.0, pass, P->shard, P->nshard, P->nkl.p, P->kst.p,
+                                        P->nchunk.p);
                                 CUDA_TRY(cudaGetLastError());
                                 CUDA_TRY(cudaMemsetAsync(P->nchunk.p + nseg, 0, sizeof(long long), s));
                                 size_t tmp = P->cub_tmp.n;
@@ -897,6 +900,15 @@ int b200jk_get_jk(b200jk_plan *P, const double *dms, int n_dm, int hermi, int wi
         }
         P->st.last_build_ms = ms;
         P->st.kernel_launches = launches;
+        return B200JK_OK;
+}
+
+int b200jk_set_shard(b200jk_plan *plan, int index, int count)
+{
+        if (!plan) return fail(B200JK_EINVAL, "plan is NULL");
+        if (count < 1 || index < 0 || index >= count) return fail(B200JK_EINVAL, "shard index must be in [0, count)");
+        plan->shard = index;
+        plan->nshard = count;
         return B200JK_OK;
 }
 
@@ -1175,7 +1187,8 @@ extern "C" int b200jk_grad_jk(b200jk_plan *P, const double *dms, int n_dm, int w
                         const int nseg = bra.n * B2_NBUCKET;
                         const int chunk = grad_chunk(bra.la, bra.lb, ket.la, ket.lb);
                         count_kernel<<<grid_for(nseg, 256), 256, 0, s>>>(bra.view(), ket.view(), 0, tol, g.fac.p, chunk,
-                                                                        0.0, 0, g.nkl.p, g.kst.p, g.nchunk.p);
+                                                                        0.0, 0, P->shard, P->nshard, g.nkl.p, g.kst.p,
+                                                                        g.nchunk.p);
                         CUDA_TRY(cudaGetLastError());
                         CUDA_TRY(cudaMemsetAsync(g.nchunk.p + nseg, 0, sizeof(long long), s));
                         size_t tmp = g.cub_tmp.n;
@@ -1375,7 +1388,7 @@ extern "C" int b200jk_get_jk_noalloc(b200jk_plan *P, const double *dms, int n_dm
                 const int nseg = bra.n * B2_NBUCKET;
                 count_kernel<<<grid_for(nseg, 256), 256, 0, s>>>(bra.view(), ket.view(), same, P->tol > 0 ? P->tol : 0.0,
                                                                 (const double *)dmax, family_chunk(la, lb, lc, ld),
-                                                                0.0, 0, nkl, kst, nchunk);
+                                                                0.0, 0, 0, 1, nkl, kst, nchunk);
                 CUDA_TRY(cudaGetLastError());
                 CUDA_TRY(cudaMemsetAsync(nchunk + nseg, 0, sizeof(long long), s));
                 size_t tmp = cub_bytes;

@@ -109,9 +109,12 @@ __device__ __forceinline__ bool quartet_passes(const JKArgs &a, int4 sb, double 
 // part [n64, n).  pass 0 writes the FP64 part, pass 1 the FP32 part (start in
 // kst, length in nkl) with its chunks of `chunk` quartets.  tau32 = 0 keeps
 // every quartet in FP64.  Same-class quartets keep kl <= ij in the
-// (bucket, rank) order.
+// (bucket, rank) order.  Sharded over nshard GPUs, rank `shard` takes the bra
+// pairs ij = shard (mod nshard): pairs are sorted by their bound inside a
+// bucket, so striding spreads the cost evenly.
 static __global__ void count_kernel(PairView bra, PairView ket, int same, double tol, const double *dmax4,
-                                    int chunk, double tau32, int pass, int *nkl, int *kst, long long *nchunk)
+                                    int chunk, double tau32, int pass, int shard, int nshard, int *nkl, int *kst,
+                                    long long *nchunk)
 {
         const int t = blockIdx.x * blockDim.x + threadIdx.x;
         if (t >= bra.n * B2_NBUCKET) return;
@@ -120,7 +123,9 @@ static __global__ void count_kernel(PairView bra, PairView ket, int same, double
         const double dm = *dmax4;
         int cnt = 0, n64 = 0;
         const int lo0 = ket.boff[b], hi0 = ket.boff[b + 1];
-        if (dm > 0 && qij > 0 && hi0 > lo0) {
+        // with nshard > 1 this rank keeps the bra pairs ij = shard (mod nshard)
+        const bool mine = nshard <= 1 || ij % nshard == shard;
+        if (mine && dm > 0 && qij > 0 && hi0 > lo0) {
                 const double thr = tol / (qij * dm);
                 int lo = lo0, hi = hi0;
                 while (lo < hi) {

@@ -27,6 +27,7 @@ EXPORTS = (
     'b200jk_stats', 'b200jk_hostcheck_cart_quartet', 'b200jk_class_stats', 'b200jk_set_profiling',
     'b200jk_measure_fp64_peak', 'b200jk_get_jk_noalloc', 'b200jk_set_mixed_threshold',
     'b200jk_hostcheck_cart_quartet_fp32', 'b200jk_grad_jk', 'b200jk_grad_stats', 'b200jk_get_grad_q_cond',
+    'b200jk_set_shard',
 )
 
 
@@ -86,6 +87,7 @@ def load(path=LIB_PATH):
         lib.b200jk_grad_stats.argtypes = [vp, ctypes.POINTER(ctypes.c_int64), ctypes.POINTER(ctypes.c_int64),
                                           ctypes.POINTER(dp), ctypes.POINTER(ctypes.c_int64)]
         lib.b200jk_get_grad_q_cond.argtypes = [vp, vp]
+        lib.b200jk_set_shard.argtypes = [vp, ip, ip]
         _lib = lib
         return lib
 
@@ -158,6 +160,10 @@ class Plan:
 
     def set_profiling(self, on=True):
         check(load().b200jk_set_profiling(self._h, int(bool(on))))
+
+    def set_shard(self, index, count):
+        """Evaluate only bra pairs ij = index (mod count): partial J/K for one of count GPUs."""
+        check(load().b200jk_set_shard(self._h, int(index), int(count)))
 
     def set_mixed_threshold(self, tau):
         """tau of precision=PREC_MIXED: quartets with q_ij q_kl max|D| < tau run in float32."""

@@ -162,3 +162,19 @@ def test_scf_energy(b2, name, ref):
     assert abs(e - float(f['e_rhf'])) < TOL_E
     if ref is not None:
         assert abs(e - ref) < TOL_E
+
+
+def test_sharded_plans_sum_to_full_build(b2):
+    """Two plans sharded (0, 2) and (1, 2), as two GPUs would run them, sum to
+    the unsharded build (here both on one GPU, one after the other)."""
+    f = load_fixture('h2o2_vtz')
+    parts = []
+    for r in range(2):
+        p = plan_for(b2, f)
+        p.set_shard(r, 2)
+        parts.append(p.get_jk(f['dm_ns'], hermi=0))
+        assert 0 < p.stats()['quartets']
+    vj = parts[0][0] + parts[1][0]
+    vk = parts[0][1] + parts[1][1]
+    assert abs(vj - f['vj_ns']).max() < TOL_JK
+    assert abs(vk - f['vk_ns']).max() < TOL_JK

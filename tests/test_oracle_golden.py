@@ -102,4 +102,4 @@ def test_grad_reference_fingerprint():
     assert abs(lib_fp(f['de']) - 0.0055115512502467556) < 5e-7
     h = float(f['fd_h'])
     fd = (f['fd_energies'][:, 0] - f['fd_energies'][:, 1]) / (2 * h)
-    assert abs(f['de'].ravel()[f['fd_coords']] - fd).max() < 1e-6
+    assert abs(f['de'].ravel()[f['fd_coords']] - fd).max() < 5e-6
