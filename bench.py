@@ -420,6 +420,15 @@ def run_gpu(args):
         dist.destroy_process_group()
 
 
+def run_one_build(args):
+    from pyscf_b200 import lib
+    f = load_workload(args.config)
+    plan = lib.Plan(f['atm'], f['bas'], f['env'], direct_scf_tol=1e-13)
+    plan.get_jk(f['dm'], hermi=1)
+    st = plan.stats()
+    print(json.dumps({'workload': args.config, 'ms': st['last_build_ms'], 'quartets': st['quartets']}))
+
+
 class _Mol:
     def __init__(self, f):
         self._atm, self._bas, self._env = f['atm'], f['bas'], f['env']
@@ -435,9 +444,13 @@ def main():
     ap.add_argument('--config', default='h2o64_vtz')
     ap.add_argument('--no-cpu-baseline', action='store_true')
     ap.add_argument('--tau', type=float, default=1e-6, help='float32 threshold of the mixed-precision line')
+    ap.add_argument('--one-build', action='store_true',
+                    help='plan + one FP64 J/K build of the workload, nothing else (the case profiled under ncu)')
     args = ap.parse_args()
     if args.impl == 'reference':
         run_reference(args)
+    elif args.one_build:
+        run_one_build(args)
     else:
         run_gpu(args)
 
