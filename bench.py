@@ -21,7 +21,11 @@ Besides the FP64 headline the line carries, measured in the same run:
           float32 fraction and error against the FP64 build (max |dJ|, |dK|,
           dE = 1/2 tr(D dJ) - 1/4 tr(D dK)), and the same for a
           difference-density build (dD = 1e-4 C2 C2^T, the late-SCF regime);
-  grad    the nuclear-gradient J/K (int2e_ip1) of (H2O)16/cc-pVDZ.
+  grad    the nuclear-gradient J/K (int2e_ip1) of (H2O)16/cc-pVDZ;
+  batch   512 molecules (H2O)n, n ~ U{1..16}, cc-pVDZ (tests/golden/
+          batch_h2o_vdz512.npz) in one batched build (one launch per quartet
+          class for all molecules), FP64 and mixed, against the same 512
+          builds run one molecule after another.
 
 --impl reference times the reference's own CPU implementation of the path
 (PySCF's CVHFnr_direct_drv compiled from the reference sources, oracle/_ref,
@@ -215,6 +219,59 @@ def _timed_builds(plan, d, flush, stream, steps, dist, build):
     return times, dict(quartets=nq, prim_quartets=npq, fp32_quartets=nq32, kernel_launches=launches), out
 
 
+def batch_report(local, flush, stream, steps, tau):
+    """Batched J/K of the 512-molecule workload vs one-by-one builds."""
+    import torch
+    from pyscf_b200 import lib
+    f = dict(numpy.load(os.path.join(GOLDEN, 'batch_h2o_vdz512.npz')))
+    dev = torch.device('cuda', local)
+    plans, dms = [], []
+    rng = numpy.random.default_rng(405)
+    for m in range(len(f['nao'])):
+        a0, a1 = f['atm_off'][m], f['atm_off'][m + 1]
+        b0, b1 = f['bas_off'][m], f['bas_off'][m + 1]
+        e0, e1 = f['env_off'][m], f['env_off'][m + 1]
+        p = lib.Plan(f['atm'][a0:a1], f['bas'][b0:b1], f['env'][e0:e1], direct_scf_tol=1e-13, device=local)
+        p.set_mixed_threshold(tau)
+        plans.append(p)
+        nao, nocc = int(f['nao'][m]), 5 * int(f['nwater'][m])
+        c = rng.standard_normal((nao, nocc)) / numpy.sqrt(nao)
+        dms.append(torch.tensor(c @ c.T, device=dev))
+    batch = lib.Batch(plans)
+
+    def timed(fn, n):
+        fn()
+        t = []
+        for _ in range(n):
+            flush.fill_(1.0)
+            torch.cuda.synchronize(dev)
+            e0 = torch.cuda.Event(enable_timing=True)
+            e1 = torch.cuda.Event(enable_timing=True)
+            e0.record(stream)
+            fn()
+            e1.record(stream)
+            e1.synchronize()
+            t.append(e0.elapsed_time(e1))
+        return float(numpy.median(t))
+    ms_b64 = timed(lambda: batch.get_jk_device(dms, hermi=1), steps)
+    q = batch.stats()['quartets']
+    launches = batch.stats()['kernel_launches']
+    ms_b32 = timed(lambda: batch.get_jk_device(dms, hermi=1, precision=lib.PREC_MIXED), steps)
+    f32 = batch.stats()['fp32_quartets'] / max(1, batch.stats()['quartets'])
+
+    def one_by_one():
+        for p, d in zip(plans, dms):
+            p.get_jk_device(d, hermi=1)
+    ms_seq = timed(one_by_one, 1)
+    return {'workload': '512 x (H2O)n, n ~ U{1..16} (seed 404), 3x3x2 lattice sites, cc-pVDZ',
+            'molecules': len(plans), 'total_nao': int(f['nao'].sum()), 'quartets_per_build': q,
+            'batched_fp64_ms': ms_b64, 'batched_fp64_quartets_per_s': q / (ms_b64 * 1e-3),
+            'batched_mixed_ms': ms_b32, 'mixed_tau': tau, 'mixed_fp32_fraction': f32,
+            'one_by_one_fp64_ms': ms_seq, 'batching_speedup': ms_seq / ms_b64,
+            'kernel_launches_per_batched_build': launches,
+            'density': 'per molecule C C^T, C nao x 5n N(0,1)/sqrt(nao), seed 405'}
+
+
 def run_gpu(args):
     import torch
     from pyscf_b200 import lib, flops
@@ -345,6 +402,13 @@ def run_gpu(args):
     except Exception as e:  # the gradient line must not sink the J/K measurement
         grad_line = {'error': str(e)[:200]}
 
+    batch_line = None
+    if world == 1:
+        try:
+            batch_line = batch_report(local, flush, stream, args.steps, args.tau)
+        except Exception as e:  # the batch line must not sink the J/K measurement
+            batch_line = {'error': str(e)[:200]}
+
     # end to end through the public API, host arrays in pinned memory
     dm_host = torch.from_numpy(f['dm']).pin_memory().numpy()
     out = torch.empty((2, nao, nao), dtype=torch.float64).pin_memory().numpy()
@@ -387,6 +451,7 @@ def run_gpu(args):
                          'share': dom_ms * 1e-3 / (sum(times) / args.steps), 'traffic': traffic},
             'mixed': mixed,
             'grad': grad_line,
+            'batch': batch_line,
             'e2e': {'value': q_per_build / t_e2e, 'unit': 'shell quartets/s',
                     's_per_build': t_e2e, 'h2d_bytes_per_step': int(nao * nao * 8),
                     'd2h_bytes_per_step': int(2 * nao * nao * 8),

@@ -53,6 +53,7 @@ extern "C" {
                                     float64; tau set by b200jk_set_mixed_threshold */
 
 typedef struct b200jk_plan b200jk_plan;
+typedef struct b200jk_batch b200jk_batch;
 
 typedef struct {
     int64_t quartets;            /* shell quartets evaluated by the last build */
@@ -160,6 +161,26 @@ int b200jk_grad_stats(const b200jk_plan *plan, int64_t *quartets, int64_t *prim_
  * derivative bound sqrt(max |(d_x i j|d_x i j)|) with the derivative on the
  * row shell (CVHFnr_int2e_pp_q_cond), plane 1 q_cond. */
 int b200jk_get_grad_q_cond(b200jk_plan *plan, double *q_cond);
+
+/* Batches of molecules: the J/K builds of many plans (one per molecule, all
+ * on one GPU, not sharded) in one launch per quartet class over a global
+ * quartet queue, instead of one set of launches per molecule.  No reference
+ * counterpart: PySCF builds J/K one molecule at a time.  The plans must
+ * outlive the batch. */
+int b200jk_batch_create(b200jk_plan *const *plans, int nmol, b200jk_batch **out);
+int b200jk_batch_destroy(b200jk_batch *batch);
+
+/* J/K of one density per molecule: dms[m], vj[m], vk[m] are DEVICE pointers to
+ * C-ordered (nao_m, nao_m) float64 arrays (outputs overwritten; vj or vk may
+ * be NULL with with_j / with_k 0).  hermi and precision_mode as in
+ * b200jk_get_jk; the mixed threshold is the first plan's. */
+int b200jk_batch_get_jk(b200jk_batch *batch, const double *const *dms, int hermi, int with_j, int with_k,
+                        double *const *vj, double *const *vk, int precision_mode, void *stream);
+
+/* Counters of the last batched build: quartets (all molecules), of them in
+ * float32, device time (ms), kernels launched by this library. */
+int b200jk_batch_stats(const b200jk_batch *batch, int64_t *quartets, int64_t *fp32_quartets, double *ms,
+                       int64_t *kernel_launches);
 
 /* Multi-GPU sharding: the plan's J/K and gradient builds evaluate only the
  * bra shell pairs ij = index (mod count) of every quartet class, so count

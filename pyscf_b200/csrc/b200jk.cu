@@ -291,9 +291,11 @@ static void class_l(int X, int &la, int &lb)
                         if (pair_class(a, b) == X) { la = a; lb = b; return; }
 }
 
-typedef int (*jk_launcher_t)(const JKArgs &, cudaStream_t, int, int, std::string &);
+typedef int (*jk_launcher_t)(const JKArgs &, cudaStream_t, int, int, const JKArgs *, const long long *, int,
+                             std::string &);
 
-static int dispatch_jk(b200jk_plan *P, int la, int lb, int lc, int ld, const JKArgs &a, int fp32, cudaStream_t s)
+static int dispatch_jk(b200jk_plan *P, int la, int lb, int lc, int ld, const JKArgs &a, int fp32, cudaStream_t s,
+                       const JKArgs *margs = nullptr, const long long *mchunk = nullptr, int nmol = 0)
 {
         struct Entry { int la, lb, lc, ld; jk_launcher_t fn; };
         static const Entry table[] = {
@@ -356,7 +358,7 @@ static int dispatch_jk(b200jk_plan *P, int la, int lb, int lc, int ld, const JKA
         for (const Entry &e : table) {
                 if (e.la == la && e.lb == lb && e.lc == lc && e.ld == ld) {
                         std::string err;
-                        if (e.fn(a, s, P->nsm, fp32, err)) return fail(B200JK_ECUDA, err);
+                        if (e.fn(a, s, P->nsm, fp32, margs, mchunk, nmol, err)) return fail(B200JK_ECUDA, err);
                         return B200JK_OK;
                 }
         }
@@ -1273,6 +1275,266 @@ extern "C" int b200jk_get_grad_q_cond(b200jk_plan *P, double *q_cond)
         return B200JK_OK;
 }
 
+
+// ---------------------------------------------------------------------------
+// Batches of molecules (one launch per quartet class for all of them).
+
+struct b200jk_batch {
+        std::vector<b200jk_plan *> plans;
+        int device = 0, nsm = 148;
+        cudaStream_t stream = nullptr;
+        cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+        DevArr<JKArgs> args;
+        DevArr<int> segoff, nkl, kst;
+        DevArr<long long> nchunk, chunk_off, mchunk;
+        DevArr<unsigned char> cub_tmp;
+        DevArr<unsigned long long> stats;
+        JKArgs *h_args = nullptr;       // pinned staging of the per-class argument arrays
+        int *h_segoff = nullptr;
+        size_t h_cap_args = 0, h_cap_seg = 0;
+        int64_t quartets = 0, prim_quartets = 0, fp32_quartets = 0, launches = 0;
+        double last_ms = 0;
+        ~b200jk_batch()
+        {
+                args.release(); segoff.release(); nkl.release(); kst.release(); nchunk.release();
+                chunk_off.release(); mchunk.release(); cub_tmp.release(); stats.release();
+                if (h_args) cudaFreeHost(h_args);
+                if (h_segoff) cudaFreeHost(h_segoff);
+                if (ev0) cudaEventDestroy(ev0);
+                if (ev1) cudaEventDestroy(ev1);
+                if (stream) cudaStreamDestroy(stream);
+        }
+};
+
+extern "C" int b200jk_batch_create(b200jk_plan *const *plans, int nmol, b200jk_batch **out)
+{
+        if (!out) return fail(B200JK_EINVAL, "out is NULL");
+        *out = nullptr;
+        if (!plans || nmol <= 0) return fail(B200JK_EINVAL, "no plans");
+        for (int m = 0; m < nmol; m++) {
+                if (!plans[m]) return fail(B200JK_EINVAL, "a plan of the batch is NULL");
+                if (plans[m]->device != plans[0]->device) return fail(B200JK_EINVAL, "the plans of a batch must share one GPU");
+                if (plans[m]->nshard != 1) return fail(B200JK_EUNSUPPORTED, "sharded plans cannot be batched");
+        }
+        CUDA_TRY(cudaSetDevice(plans[0]->device));
+        b200jk_batch *B = new b200jk_batch();
+        B->plans.assign(plans, plans + nmol);
+        B->device = plans[0]->device;
+        B->nsm = plans[0]->nsm;
+        if (cudaStreamCreateWithFlags(&B->stream, cudaStreamNonBlocking) != cudaSuccess ||
+            cudaEventCreate(&B->ev0) != cudaSuccess || cudaEventCreate(&B->ev1) != cudaSuccess) {
+                delete B;
+                return fail(B200JK_ECUDA, "stream/event creation failed");
+        }
+        *out = B;
+        return B200JK_OK;
+}
+
+extern "C" int b200jk_batch_destroy(b200jk_batch *B)
+{
+        delete B;
+        return B200JK_OK;
+}
+
+extern "C" int b200jk_batch_get_jk(b200jk_batch *B, const double *const *dms, int hermi, int with_j, int with_k,
+                                   double *const *vj, double *const *vk, int precision_mode, void *stream)
+{
+        if (!B) return fail(B200JK_EINVAL, "batch is NULL");
+        if (!dms) return fail(B200JK_EINVAL, "dms is NULL");
+        if (hermi < 0 || hermi > 2) return fail(B200JK_EINVAL, "hermi must be 0, 1 or 2");
+        if ((with_j && !vj) || (with_k && !vk)) return fail(B200JK_EINVAL, "output pointer array is NULL");
+        if (precision_mode != B200JK_PREC_FP64 && precision_mode != B200JK_PREC_MIXED)
+                return fail(B200JK_EUNSUPPORTED, "precision_mode must be 0 (FP64) or 1 (mixed FP32/FP64)");
+        const int nmol = (int)B->plans.size();
+        for (int m = 0; m < nmol; m++)
+                if (!dms[m] || (with_j && !vj[m]) || (with_k && !vk[m])) return fail(B200JK_EINVAL, "NULL device pointer in the batch");
+        const double tau = B->plans[0]->fp32_tau;
+        const int mixed = precision_mode == B200JK_PREC_MIXED && tau > 0;
+        CUDA_TRY(cudaSetDevice(B->device));
+        cudaStream_t s = stream ? (cudaStream_t)stream : B->stream;
+        const int nk = hermi == 1 ? 1 : 2;
+        int rc;
+        for (int m = 0; m < nmol; m++)
+                if ((rc = ensure_workspace(B->plans[m], 1))) return rc;
+        auto qcs = quartet_classes();
+        const int nclass = (int)qcs.size();
+        // argument arrays of every (class, pass): only molecules with work in the class
+        std::vector<size_t> at(2 * nclass + 1, 0), sat(2 * nclass + 1, 0);
+        std::vector<int> ncnt(2 * nclass, 0);
+        size_t tot_args = 0, tot_seg = 0;
+        int max_segs = 1;
+        for (int t = 0; t < nclass; t++) {
+                int cnt = 0, segs = 0;
+                for (int m = 0; m < nmol; m++) {
+                        const PairClassDev &bra = B->plans[m]->pc[qcs[t].X], &ket = B->plans[m]->pc[qcs[t].Y];
+                        if (bra.n == 0 || ket.n == 0) continue;
+                        cnt++;
+                        segs += bra.n * B2_NBUCKET;
+                }
+                max_segs = std::max(max_segs, segs);
+                for (int pass = 0; pass < 2; pass++) {
+                        at[2 * t + pass] = tot_args;
+                        sat[2 * t + pass] = tot_seg;
+                        ncnt[2 * t + pass] = cnt;
+                        tot_args += cnt;
+                        tot_seg += cnt + 1;
+                }
+        }
+        if (tot_args > B->h_cap_args) {
+                if (B->h_args) cudaFreeHost(B->h_args);
+                B->h_args = nullptr;
+                CUDA_TRY(cudaMallocHost(&B->h_args, sizeof(JKArgs) * tot_args));
+                B->h_cap_args = tot_args;
+        }
+        if (tot_seg > B->h_cap_seg) {
+                if (B->h_segoff) cudaFreeHost(B->h_segoff);
+                B->h_segoff = nullptr;
+                CUDA_TRY(cudaMallocHost(&B->h_segoff, sizeof(int) * tot_seg));
+                B->h_cap_seg = tot_seg;
+        }
+        if ((rc = dev_alloc(B->args, std::max<size_t>(1, tot_args))) || (rc = dev_alloc(B->segoff, std::max<size_t>(1, tot_seg))) ||
+            (rc = dev_alloc(B->nkl, max_segs)) || (rc = dev_alloc(B->kst, max_segs)) ||
+            (rc = dev_alloc(B->nchunk, max_segs + 1)) || (rc = dev_alloc(B->chunk_off, max_segs + 1)) ||
+            (rc = dev_alloc(B->mchunk, nmol + 1)) || (rc = dev_alloc(B->stats, 4 * 64)))
+                return rc;
+        size_t cub_bytes = 0;
+        cub::DeviceScan::ExclusiveSum(nullptr, cub_bytes, B->nchunk.p, B->chunk_off.p, max_segs + 1);
+        if ((rc = dev_alloc(B->cub_tmp, cub_bytes + 16))) return rc;
+
+        CUDA_TRY(cudaEventRecord(B->ev0, s));
+        int64_t launches = 0;
+        // per molecule: screening data, Cartesian densities, cleared accumulators
+        for (int m = 0; m < nmol; m++) {
+                b200jk_plan *P = B->plans[m];
+                const size_t nc = (size_t)P->naoc * P->naoc;
+                CUDA_TRY(cudaMemsetAsync(P->dmax.p, 0, sizeof(unsigned long long), s));
+                const long long npair = (long long)P->nbas * (P->nbas + 1) / 2;
+                dm_cond_kernel<<<grid_for(npair, 256), 256, 0, s>>>(dms[m], 1, P->nao, P->ao_loc_d.p, P->nbas,
+                                                                  P->dm_cond.p, P->dmax.p);
+                CUDA_TRY(cudaGetLastError());
+                out_to_cart_kernel<<<grid_for((long long)nc, 256), 256, 0, s>>>(
+                        dms[m], P->nao, P->naoc, P->cart_seg.p, P->cart_comp.p, P->seg_info.p, P->c2s.p, P->cart,
+                        P->Dc.p, nk == 2 ? P->Dc.p + nc : nullptr, nullptr);
+                CUDA_TRY(cudaGetLastError());
+                sym_sum_kernel<<<grid_for((long long)nc, 256), 256, 0, s>>>(P->Dc.p, P->naoc, P->Ds.p);
+                CUDA_TRY(cudaGetLastError());
+                if (with_j) CUDA_TRY(cudaMemsetAsync(P->Jacc.p, 0, sizeof(double) * nc, s));
+                if (with_k) CUDA_TRY(cudaMemsetAsync(P->Kacc.p, 0, sizeof(double) * nc * nk, s));
+                launches += 3;
+        }
+        CUDA_TRY(cudaMemsetAsync(B->stats.p, 0, 4 * 64 * sizeof(unsigned long long), s));
+        const double *tbl = table_ptr();
+        const float *tbl_f = table_f_ptr();
+        // argument arrays (pointers only depend on the workspaces): fill and upload once
+        for (int t = 0; t < nclass; t++) {
+                for (int pass = 0; pass < 2; pass++) {
+                        JKArgs *ha = B->h_args + at[2 * t + pass];
+                        int *hs = B->h_segoff + sat[2 * t + pass];
+                        int k = 0, seg = 0;
+                        for (int m = 0; m < nmol; m++) {
+                                b200jk_plan *P = B->plans[m];
+                                const PairClassDev &bra = P->pc[qcs[t].X], &ket = P->pc[qcs[t].Y];
+                                if (bra.n == 0 || ket.n == 0) continue;
+                                JKArgs a;
+                                memset(&a, 0, sizeof(a));
+                                a.bra = bra.view();
+                                a.ket = ket.view();
+                                a.PP = P->PP.p; a.PK = P->PK.p;
+                                a.chunk_off = B->chunk_off.p + seg;
+                                a.nkl = B->nkl.p + seg;
+                                a.kst = B->kst.p + seg;
+                                a.dm_cond = P->dm_cond.p;
+                                a.table = tbl;
+                                a.table_f = tbl_f;
+                                a.goff = P->goff_all.p + P->goff_at[t];
+                                a.Jacc = P->Jacc.p; a.Kacc = P->Kacc.p;
+                                a.Ds = P->Ds.p; a.Dk = P->Dc.p;
+                                a.stats = B->stats.p + 2 * (64 * pass + t);
+                                a.dmax4 = (const double *)P->dmax.p;
+                                a.tol = P->tol > 0 ? P->tol : -1.0;
+                                a.nbas = P->nbas; a.naoc = P->naoc; a.n_dm = 1; a.nk = nk;
+                                a.with_j = with_j; a.with_k = with_k; a.same = qcs[t].X == qcs[t].Y;
+                                ha[k] = a;
+                                hs[k] = seg;
+                                k++;
+                                seg += bra.n * B2_NBUCKET;
+                        }
+                        hs[k] = seg;
+                }
+        }
+        CUDA_TRY(cudaMemcpyAsync(B->args.p, B->h_args, sizeof(JKArgs) * tot_args, cudaMemcpyHostToDevice, s));
+        CUDA_TRY(cudaMemcpyAsync(B->segoff.p, B->h_segoff, sizeof(int) * tot_seg, cudaMemcpyHostToDevice, s));
+        for (int t = 0; t < nclass; t++) {
+                int la, lb, lc, ld;
+                class_l(qcs[t].X, la, lb);
+                class_l(qcs[t].Y, lc, ld);
+                const int chunk = family_chunk(la, lb, lc, ld);
+                for (int pass = 0; pass < (mixed ? 2 : 1); pass++) {
+                        const int nm = ncnt[2 * t + pass];
+                        if (nm == 0) continue;
+                        const JKArgs *dargs = B->args.p + at[2 * t + pass];
+                        const int *dseg = B->segoff.p + sat[2 * t + pass];
+                        const int segs = B->h_segoff[sat[2 * t + pass] + nm];
+                        count_kernel_multi<<<grid_for(segs, 256), 256, 0, s>>>(dargs, dseg, nm, chunk, mixed ? tau : 0.0,
+                                                                              pass, B->nkl.p, B->kst.p, B->nchunk.p);
+                        CUDA_TRY(cudaGetLastError());
+                        CUDA_TRY(cudaMemsetAsync(B->nchunk.p + segs, 0, sizeof(long long), s));
+                        size_t tmp = B->cub_tmp.n;
+                        CUDA_TRY(cub::DeviceScan::ExclusiveSum(B->cub_tmp.p, tmp, B->nchunk.p, B->chunk_off.p, segs + 1, s));
+                        batch_chunk_starts<<<grid_for(nm + 1, 128), 128, 0, s>>>(B->chunk_off.p, dseg, nm, B->mchunk.p);
+                        CUDA_TRY(cudaGetLastError());
+                        const JKArgs &a0 = B->h_args[at[2 * t + pass]];
+                        if ((rc = dispatch_jk(B->plans[0], la, lb, lc, ld, a0, pass, s, dargs, B->mchunk.p, nm))) return rc;
+                        launches += 3;
+                }
+        }
+        // back to the output basis, per molecule
+        for (int m = 0; m < nmol; m++) {
+                b200jk_plan *P = B->plans[m];
+                const size_t nn = (size_t)P->nao * P->nao, nc = (size_t)P->naoc * P->naoc;
+                if (with_j) {
+                        cart_to_out_kernel<<<grid_for((long long)nn, 256), 256, 0, s>>>(
+                                P->Jacc.p, P->Jacc.p, P->nao, P->naoc, P->out_seg.p, P->out_comp.p, P->seg_info.p, P->c2s.p,
+                                P->cart, 1, vj[m]);
+                        CUDA_TRY(cudaGetLastError());
+                        launches++;
+                }
+                if (with_k) {
+                        const double *K2 = nk == 2 ? P->Kacc.p + nc : P->Kacc.p;
+                        cart_to_out_kernel<<<grid_for((long long)nn, 256), 256, 0, s>>>(
+                                P->Kacc.p, K2, P->nao, P->naoc, P->out_seg.p, P->out_comp.p, P->seg_info.p, P->c2s.p,
+                                P->cart, hermi, vk[m]);
+                        CUDA_TRY(cudaGetLastError());
+                        launches++;
+                }
+        }
+        CUDA_TRY(cudaEventRecord(B->ev1, s));
+        unsigned long long hs[4 * 64];
+        CUDA_TRY(cudaMemcpyAsync(hs, B->stats.p, sizeof(hs), cudaMemcpyDeviceToHost, s));
+        CUDA_TRY(cudaStreamSynchronize(s));
+        float ms = 0;
+        CUDA_TRY(cudaEventElapsedTime(&ms, B->ev0, B->ev1));
+        B->quartets = B->prim_quartets = B->fp32_quartets = 0;
+        for (int t = 0; t < nclass; t++) {
+                B->quartets += (int64_t)(hs[2 * t] + hs[2 * (64 + t)]);
+                B->prim_quartets += (int64_t)(hs[2 * t + 1] + hs[2 * (64 + t) + 1]);
+                B->fp32_quartets += (int64_t)hs[2 * (64 + t)];
+        }
+        B->last_ms = ms;
+        B->launches = launches;
+        return B200JK_OK;
+}
+
+extern "C" int b200jk_batch_stats(const b200jk_batch *B, int64_t *quartets, int64_t *fp32_quartets, double *ms,
+                                  int64_t *kernel_launches)
+{
+        if (!B) return fail(B200JK_EINVAL, "batch is NULL");
+        if (quartets) *quartets = B->quartets;
+        if (fp32_quartets) *fp32_quartets = B->fp32_quartets;
+        if (ms) *ms = B->last_ms;
+        if (kernel_launches) *kernel_launches = B->launches;
+        return B200JK_OK;
+}
 
 // ---------------------------------------------------------------------------
 // Allocation-free J/K build.

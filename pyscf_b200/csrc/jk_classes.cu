@@ -20,9 +20,11 @@ struct LaunchCfg {
 };
 
 // R is the evaluation type: double for the FP64 pass, float for the FP32 pass
-// of mixed precision (accumulation stays in float64 either way)
-template <int LA, int LB, int LC, int LD, typename R>
-int launch_one(const JKArgs &a, cudaStream_t s, int nsm, std::string &err)
+// of mixed precision (accumulation stays in float64 either way).  MULTI: one
+// launch over a batch of molecules (margs, mchunk, nmol on the device).
+template <int LA, int LB, int LC, int LD, typename R, bool MULTI>
+int launch_one(const JKArgs &a, const JKArgs *margs, const long long *mchunk, int nmol, cudaStream_t s, int nsm,
+               std::string &err)
 {
         using K = Class4<LA, LB, LC, LD>;
         constexpr int NP = thread_parts<LA, LB, LC, LD>();
@@ -36,21 +38,21 @@ int launch_one(const JKArgs &a, cudaStream_t s, int nsm, std::string &err)
                         if constexpr (thread) {
                                 cfg.block = 128;
                                 cfg.smem = stage_table<R>(K::NR) ? sizeof(R) * rys_slice_elems<R>(K::NR) : 0;
-                                cfg.status = cudaFuncSetAttribute(jk_thread_kernel<LA, LB, LC, LD, (NP > 0 ? NP : 1), R>,
+                                cfg.status = cudaFuncSetAttribute(jk_thread_kernel<LA, LB, LC, LD, (NP > 0 ? NP : 1), R, MULTI>,
                                                                   cudaFuncAttributeMaxDynamicSharedMemorySize, (int)cfg.smem);
                                 if (cfg.status == cudaSuccess)
                                         cfg.status = cudaOccupancyMaxActiveBlocksPerMultiprocessor(
-                                                &nb, jk_thread_kernel<LA, LB, LC, LD, (NP > 0 ? NP : 1), R>, 128, cfg.smem);
+                                                &nb, jk_thread_kernel<LA, LB, LC, LD, (NP > 0 ? NP : 1), R, MULTI>, 128, cfg.smem);
                         } else {
                                 const size_t per_warp = sizeof(double) * WarpSmem<LA, LB, LC, LD, R>::SIZE *
                                                         (32 / group_size<LA, LB, LC, LD>());
                                 const int wpb = (int)std::min<size_t>(4, std::max<size_t>(1, (200 * 1024) / per_warp));
                                 cfg.block = 32 * wpb;
                                 cfg.smem = per_warp * wpb;
-                                cfg.status = cudaFuncSetAttribute(jk_warp_kernel<LA, LB, LC, LD, R>,
+                                cfg.status = cudaFuncSetAttribute(jk_warp_kernel<LA, LB, LC, LD, R, MULTI>,
                                                                   cudaFuncAttributeMaxDynamicSharedMemorySize, (int)cfg.smem);
                                 if (cfg.status == cudaSuccess)
-                                        cfg.status = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, jk_warp_kernel<LA, LB, LC, LD, R>,
+                                        cfg.status = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, jk_warp_kernel<LA, LB, LC, LD, R, MULTI>,
                                                                                                    cfg.block, cfg.smem);
                         }
                         cfg.grid = (nb > 0 ? nb : 1) * nsm;
@@ -62,10 +64,10 @@ int launch_one(const JKArgs &a, cudaStream_t s, int nsm, std::string &err)
                 return 1;
         }
         if constexpr (thread) {
-                jk_thread_kernel<LA, LB, LC, LD, NP, R><<<cfg.grid, cfg.block, cfg.smem, s>>>(a);
+                jk_thread_kernel<LA, LB, LC, LD, NP, R, MULTI><<<cfg.grid, cfg.block, cfg.smem, s>>>(a, margs, mchunk, nmol);
         } else {
-                jk_warp_kernel<LA, LB, LC, LD, R><<<cfg.grid, cfg.block, cfg.smem, s>>>(
-                        a, 8 * (32 / group_size<LA, LB, LC, LD>()));
+                jk_warp_kernel<LA, LB, LC, LD, R, MULTI><<<cfg.grid, cfg.block, cfg.smem, s>>>(
+                        a, 8 * (32 / group_size<LA, LB, LC, LD>()), margs, mchunk, nmol);
         }
         cudaError_t e = cudaGetLastError();
         if (e != cudaSuccess) {
@@ -78,10 +80,13 @@ int launch_one(const JKArgs &a, cudaStream_t s, int nsm, std::string &err)
 } // namespace
 
 // B2_FN_NAME is launch_jk_<la><lb><lc><ld>, declared in jk_launch.h
-int B2_FN_NAME(const JKArgs &a, cudaStream_t s, int nsm, int fp32, std::string &err)
+int B2_FN_NAME(const JKArgs &a, cudaStream_t s, int nsm, int fp32, const JKArgs *margs, const long long *mchunk,
+               int nmol, std::string &err)
 {
-        if (fp32) return launch_one<B2_BRA_LA, B2_BRA_LB, B2_KET_LC, B2_KET_LD, float>(a, s, nsm, err);
-        return launch_one<B2_BRA_LA, B2_BRA_LB, B2_KET_LC, B2_KET_LD, double>(a, s, nsm, err);
+#define B2_L(R, M) launch_one<B2_BRA_LA, B2_BRA_LB, B2_KET_LC, B2_KET_LD, R, M>(a, margs, mchunk, nmol, s, nsm, err)
+        if (nmol > 0) return fp32 ? B2_L(float, true) : B2_L(double, true);
+        return fp32 ? B2_L(float, false) : B2_L(double, false);
+#undef B2_L
 }
 
 } // namespace b200jk

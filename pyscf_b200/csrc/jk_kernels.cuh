@@ -63,6 +63,7 @@ struct JKArgs {
         double *Jacc, *Kacc;
         const double *Ds, *Dk;
         unsigned long long *stats;   // [0] quartets, [1] primitive quartets
+        const double *dmax4;         // 4 max|D| of the molecule (count kernel of a batch)
         double tol;
         int nbas, naoc, n_dm, nk;
         int with_j, with_k, same;
@@ -112,15 +113,13 @@ __device__ __forceinline__ bool quartet_passes(const JKArgs &a, int4 sb, double 
 // (bucket, rank) order.  Sharded over nshard GPUs, rank `shard` takes the bra
 // pairs ij = shard (mod nshard): pairs are sorted by their bound inside a
 // bucket, so striding spreads the cost evenly.
-static __global__ void count_kernel(PairView bra, PairView ket, int same, double tol, const double *dmax4,
-                                    int chunk, double tau32, int pass, int shard, int nshard, int *nkl, int *kst,
-                                    long long *nchunk)
+// one (bra pair, ket bucket) segment t of a class: its ket range and chunks
+__device__ __forceinline__ void count_segment(const PairView &bra, const PairView &ket, int same, double tol,
+                                              double dm, int chunk, double tau32, int pass, int shard, int nshard,
+                                              int t, int &nkl_out, int &kst_out, long long &nchunk_out)
 {
-        const int t = blockIdx.x * blockDim.x + threadIdx.x;
-        if (t >= bra.n * B2_NBUCKET) return;
         const int ij = t / B2_NBUCKET, b = t % B2_NBUCKET;
         const double qij = bra.q[ij];
-        const double dm = *dmax4;
         int cnt = 0, n64 = 0;
         const int lo0 = ket.boff[b], hi0 = ket.boff[b + 1];
         // with nshard > 1 this rank keeps the bra pairs ij = shard (mod nshard)
@@ -155,9 +154,44 @@ static __global__ void count_kernel(PairView bra, PairView ket, int same, double
         }
         const int start = pass == 0 ? 0 : n64;
         const int len = pass == 0 ? n64 : cnt - n64;
-        nkl[t] = len;
-        kst[t] = start;
-        nchunk[t] = (len + chunk - 1) / chunk;
+        nkl_out = len;
+        kst_out = start;
+        nchunk_out = (len + chunk - 1) / chunk;
+}
+
+static __global__ void count_kernel(PairView bra, PairView ket, int same, double tol, const double *dmax4,
+                                    int chunk, double tau32, int pass, int shard, int nshard, int *nkl, int *kst,
+                                    long long *nchunk)
+{
+        const int t = blockIdx.x * blockDim.x + threadIdx.x;
+        if (t >= bra.n * B2_NBUCKET) return;
+        count_segment(bra, ket, same, tol, *dmax4, chunk, tau32, pass, shard, nshard, t, nkl[t], kst[t], nchunk[t]);
+}
+
+// Count kernel of a batch of molecules: one thread per segment of the batch;
+// molecule m owns segments [segoff[m], segoff[m+1]) of the concatenated
+// nkl/kst/nchunk arrays.
+static __global__ void count_kernel_multi(const JKArgs *__restrict__ margs, const int *__restrict__ segoff, int nmol,
+                                          int chunk, double tau32, int pass, int *nkl, int *kst, long long *nchunk)
+{
+        const int t = blockIdx.x * blockDim.x + threadIdx.x;
+        if (t >= segoff[nmol]) return;
+        int lo = 0, hi = nmol;   // segoff[lo] <= t < segoff[hi]
+        while (hi - lo > 1) {
+                const int mid = (lo + hi) >> 1;
+                if (segoff[mid] <= t) lo = mid;
+                else hi = mid;
+        }
+        const JKArgs &a = margs[lo];
+        count_segment(a.bra, a.ket, a.same, a.tol > 0 ? a.tol : 0.0, *a.dmax4, chunk, tau32, pass, 0, 1,
+                      t - segoff[lo], nkl[t], kst[t], nchunk[t]);
+}
+
+// first chunk of every molecule of a batch: mchunk[m] = chunk_off[segoff[m]]
+static __global__ void batch_chunk_starts(const long long *chunk_off, const int *segoff, int nmol, long long *mchunk)
+{
+        const int m = blockIdx.x * blockDim.x + threadIdx.x;
+        if (m <= nmol) mchunk[m] = chunk_off[segoff[m]];
 }
 
 // ---------------------------------------------------------------------------
@@ -182,8 +216,14 @@ template <typename R> __host__ __device__ constexpr bool stage_table(int nr)
 template <> __device__ __forceinline__ const double *table_of<double>(const JKArgs &a) { return a.table; }
 template <> __device__ __forceinline__ const float *table_of<float>(const JKArgs &a) { return a.table_f; }
 
-template <int LA, int LB, int LC, int LD, int NP, typename R>
-__global__ void __launch_bounds__(128) jk_thread_kernel(JKArgs a)
+// MULTI: one launch for a batch of molecules (b200jk_batch_get_jk).
+// margs[m] holds the arguments of molecule m (its pair tables, matrices and
+// slices of the batch's chunk arrays, whose chunk numbers are global) and
+// mchunk[m] its first chunk in the batch's chunk queue, mchunk[nmol] the end;
+// a0 carries the shared fields (tables, statistics).
+template <int LA, int LB, int LC, int LD, int NP, typename R, bool MULTI>
+__global__ void __launch_bounds__(128) jk_thread_kernel(JKArgs a0, const JKArgs *__restrict__ margs,
+                                                        const long long *__restrict__ mchunk, int nmol)
 {
         using K = Class4<LA, LB, LC, LD>;
         static_assert(K::NA % NP == 0, "parts must divide the bra components");
@@ -194,7 +234,7 @@ __global__ void __launch_bounds__(128) jk_thread_kernel(JKArgs a)
         // small (float64 up to four roots, <= 59 KB; float32 always, <= 27 KB),
         // read from global memory otherwise
         extern __shared__ __align__(32) double smem_dyn[];
-        const R *tab = table_of<R>(a) + RysLayout<R>::offset(K::NR);
+        const R *tab = table_of<R>(a0) + RysLayout<R>::offset(K::NR);
         if constexpr (stage_table<R>(K::NR)) {
                 constexpr int NS = rys_slice_elems<R>(K::NR);
                 const RysVec4<R> *src = reinterpret_cast<const RysVec4<R> *>(tab);
@@ -203,13 +243,14 @@ __global__ void __launch_bounds__(128) jk_thread_kernel(JKArgs a)
                 __syncthreads();
                 tab = reinterpret_cast<const R *>(smem_dyn);
         }
-        const int nseg = a.bra.n * B2_NBUCKET;
-        const long long total = a.chunk_off[nseg];
+        const long long total = MULTI ? mchunk[nmol] : a0.chunk_off[a0.bra.n * B2_NBUCKET];
         const long long nwarps = ((long long)gridDim.x * blockDim.x) >> 5;
-        const size_t n = (size_t)a.naoc, nn = n * n;
         unsigned long long nq = 0, npq = 0;
         for (long long chunk = ((long long)blockIdx.x * blockDim.x + threadIdx.x) >> 5; chunk < total;
              chunk += nwarps) {
+              auto body = [&](const JKArgs &a) {
+                const int nseg = a.bra.n * B2_NBUCKET;
+                const size_t n = (size_t)a.naoc, nn = n * n;
                 const int sgi = find_bra(a.chunk_off, nseg, chunk);
                 const int ij = sgi / B2_NBUCKET;
                 const int pos = (int)(chunk - a.chunk_off[sgi]) * 32 + lane;
@@ -394,15 +435,18 @@ __global__ void __launch_bounds__(128) jk_thread_kernel(JKArgs a)
                                 }
                         }
                 }, std::make_integer_sequence<int, NP>{});
+              };
+                if constexpr (MULTI) body(margs[find_bra(mchunk, nmol, chunk)]);
+                else body(a0);
         }
-        if (a.stats) {
+        if (a0.stats) {
                 for (int o = 16; o > 0; o >>= 1) {
                         nq += __shfl_xor_sync(0xffffffffu, nq, o);
                         npq += __shfl_xor_sync(0xffffffffu, npq, o);
                 }
                 if (lane == 0 && nq) {
-                        atomicAdd(a.stats + 0, nq);
-                        atomicAdd(a.stats + 1, npq);
+                        atomicAdd(a0.stats + 0, nq);
+                        atomicAdd(a0.stats + 1, npq);
                 }
         }
 }
@@ -556,8 +600,9 @@ __host__ __device__ constexpr int group_size()
         return K::NG <= 100 ? 8 : (K::NG <= 400 ? 16 : 32);
 }
 
-template <int LA, int LB, int LC, int LD, typename R>
-__global__ void __launch_bounds__(128) jk_warp_kernel(JKArgs a, int chunk_q)
+template <int LA, int LB, int LC, int LD, typename R, bool MULTI>
+__global__ void __launch_bounds__(128) jk_warp_kernel(JKArgs a0, int chunk_q, const JKArgs *__restrict__ margs,
+                                                      const long long *__restrict__ mchunk, int nmol)
 {
         using K = Class4<LA, LB, LC, LD>;
         using S = WarpSmem<LA, LB, LC, LD, R>;
@@ -569,13 +614,14 @@ __global__ void __launch_bounds__(128) jk_warp_kernel(JKArgs a, int chunk_q)
         const unsigned gmask = GS == 32 ? 0xffffffffu : (((1u << GS) - 1u) << (grp * GS));
         const int wib = threadIdx.x >> 5;
         double *sm = smem_dyn + (size_t)(wib * NGRP + grp) * S::SIZE;
-        const int nseg = a.bra.n * B2_NBUCKET;
-        const long long total = a.chunk_off[nseg];
+        const long long total = MULTI ? mchunk[nmol] : a0.chunk_off[a0.bra.n * B2_NBUCKET];
         const long long nwarps = ((long long)gridDim.x * blockDim.x) >> 5;
-        const size_t n = (size_t)a.naoc, nn = n * n;
         unsigned long long nq = 0, npq = 0;
         for (long long chunk = ((long long)blockIdx.x * blockDim.x + threadIdx.x) >> 5; chunk < total;
              chunk += nwarps) {
+              auto body = [&](const JKArgs &a) {
+                const int nseg = a.bra.n * B2_NBUCKET;
+                const size_t n = (size_t)a.naoc, nn = n * n;
                 const int sgi = find_bra(a.chunk_off, nseg, chunk);
                 const int ij = sgi / B2_NBUCKET;
                 const int kb = a.ket.boff[sgi % B2_NBUCKET] + a.kst[sgi];
@@ -679,10 +725,13 @@ __global__ void __launch_bounds__(128) jk_warp_kernel(JKArgs a, int chunk_q)
                                 }
                         }
                 }
+              };
+                if constexpr (MULTI) body(margs[find_bra(mchunk, nmol, chunk)]);
+                else body(a0);
         }
-        if (a.stats && gl == 0 && nq) {
-                atomicAdd(a.stats + 0, nq);
-                atomicAdd(a.stats + 1, npq);
+        if (a0.stats && gl == 0 && nq) {
+                atomicAdd(a0.stats + 0, nq);
+                atomicAdd(a0.stats + 1, npq);
         }
 }
 

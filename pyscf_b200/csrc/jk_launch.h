@@ -36,61 +36,116 @@ inline int family_chunk(int la, int lb, int lc, int ld)
 }
 
 // one launcher per quartet class (la lb | lc ld), (lc, ld) <= (la, lb)
-int launch_jk_0000(const JKArgs &a, cudaStream_t s, int nsm, int fp32, std::string &err);
-int launch_jk_1000(const JKArgs &a, cudaStream_t s, int nsm, int fp32, std::string &err);
-int launch_jk_1010(const JKArgs &a, cudaStream_t s, int nsm, int fp32, std::string &err);
-int launch_jk_1100(const JKArgs &a, cudaStream_t s, int nsm, int fp32, std::string &err);
-int launch_jk_1110(const JKArgs &a, cudaStream_t s, int nsm, int fp32, std::string &err);
-int launch_jk_1111(const JKArgs &a, cudaStream_t s, int nsm, int fp32, std::string &err);
-int launch_jk_2000(const JKArgs &a, cudaStream_t s, int nsm, int fp32, std::string &err);
-int launch_jk_2010(const JKArgs &a, cudaStream_t s, int nsm, int fp32, std::string &err);
-int launch_jk_2011(const JKArgs &a, cudaStream_t s, int nsm, int fp32, std::string &err);
-int launch_jk_2020(const JKArgs &a, cudaStream_t s, int nsm, int fp32, std::string &err);
-int launch_jk_2100(const JKArgs &a, cudaStream_t s, int nsm, int fp32, std::string &err);
-int launch_jk_2110(const JKArgs &a, cudaStream_t s, int nsm, int fp32, std::string &err);
-int launch_jk_2111(const JKArgs &a, cudaStream_t s, int nsm, int fp32, std::string &err);
-int launch_jk_2120(const JKArgs &a, cudaStream_t s, int nsm, int fp32, std::string &err);
-int launch_jk_2121(const JKArgs &a, cudaStream_t s, int nsm, int fp32, std::string &err);
-int launch_jk_2200(const JKArgs &a, cudaStream_t s, int nsm, int fp32, std::string &err);
-int launch_jk_2210(const JKArgs &a, cudaStream_t s, int nsm, int fp32, std::string &err);
-int launch_jk_2211(const JKArgs &a, cudaStream_t s, int nsm, int fp32, std::string &err);
-int launch_jk_2220(const JKArgs &a, cudaStream_t s, int nsm, int fp32, std::string &err);
-int launch_jk_2221(const JKArgs &a, cudaStream_t s, int nsm, int fp32, std::string &err);
-int launch_jk_2222(const JKArgs &a, cudaStream_t s, int nsm, int fp32, std::string &err);
-int launch_jk_3000(const JKArgs &a, cudaStream_t s, int nsm, int fp32, std::string &err);
-int launch_jk_3010(const JKArgs &a, cudaStream_t s, int nsm, int fp32, std::string &err);
-int launch_jk_3011(const JKArgs &a, cudaStream_t s, int nsm, int fp32, std::string &err);
-int launch_jk_3020(const JKArgs &a, cudaStream_t s, int nsm, int fp32, std::string &err);
-int launch_jk_3021(const JKArgs &a, cudaStream_t s, int nsm, int fp32, std::string &err);
-int launch_jk_3022(const JKArgs &a, cudaStream_t s, int nsm, int fp32, std::string &err);
-int launch_jk_3030(const JKArgs &a, cudaStream_t s, int nsm, int fp32, std::string &err);
-int launch_jk_3100(const JKArgs &a, cudaStream_t s, int nsm, int fp32, std::string &err);
-int launch_jk_3110(const JKArgs &a, cudaStream_t s, int nsm, int fp32, std::string &err);
-int launch_jk_3111(const JKArgs &a, cudaStream_t s, int nsm, int fp32, std::string &err);
-int launch_jk_3120(const JKArgs &a, cudaStream_t s, int nsm, int fp32, std::string &err);
-int launch_jk_3121(const JKArgs &a, cudaStream_t s, int nsm, int fp32, std::string &err);
-int launch_jk_3122(const JKArgs &a, cudaStream_t s, int nsm, int fp32, std::string &err);
-int launch_jk_3130(const JKArgs &a, cudaStream_t s, int nsm, int fp32, std::string &err);
-int launch_jk_3131(const JKArgs &a, cudaStream_t s, int nsm, int fp32, std::string &err);
-int launch_jk_3200(const JKArgs &a, cudaStream_t s, int nsm, int fp32, std::string &err);
-int launch_jk_3210(const JKArgs &a, cudaStream_t s, int nsm, int fp32, std::string &err);
-int launch_jk_3211(const JKArgs &a, cudaStream_t s, int nsm, int fp32, std::string &err);
-int launch_jk_3220(const JKArgs &a, cudaStream_t s, int nsm, int fp32, std::string &err);
-int launch_jk_3221(const JKArgs &a, cudaStream_t s, int nsm, int fp32, std::string &err);
-int launch_jk_3222(const JKArgs &a, cudaStream_t s, int nsm, int fp32, std::string &err);
-int launch_jk_3230(const JKArgs &a, cudaStream_t s, int nsm, int fp32, std::string &err);
-int launch_jk_3231(const JKArgs &a, cudaStream_t s, int nsm, int fp32, std::string &err);
-int launch_jk_3232(const JKArgs &a, cudaStream_t s, int nsm, int fp32, std::string &err);
-int launch_jk_3300(const JKArgs &a, cudaStream_t s, int nsm, int fp32, std::string &err);
-int launch_jk_3310(const JKArgs &a, cudaStream_t s, int nsm, int fp32, std::string &err);
-int launch_jk_3311(const JKArgs &a, cudaStream_t s, int nsm, int fp32, std::string &err);
-int launch_jk_3320(const JKArgs &a, cudaStream_t s, int nsm, int fp32, std::string &err);
-int launch_jk_3321(const JKArgs &a, cudaStream_t s, int nsm, int fp32, std::string &err);
-int launch_jk_3322(const JKArgs &a, cudaStream_t s, int nsm, int fp32, std::string &err);
-int launch_jk_3330(const JKArgs &a, cudaStream_t s, int nsm, int fp32, std::string &err);
-int launch_jk_3331(const JKArgs &a, cudaStream_t s, int nsm, int fp32, std::string &err);
-int launch_jk_3332(const JKArgs &a, cudaStream_t s, int nsm, int fp32, std::string &err);
-int launch_jk_3333(const JKArgs &a, cudaStream_t s, int nsm, int fp32, std::string &err);
+int launch_jk_0000(const JKArgs &a, cudaStream_t s, int nsm, int fp32, const JKArgs *margs,
+                   const long long *mchunk, int nmol, std::string &err);
+int launch_jk_1000(const JKArgs &a, cudaStream_t s, int nsm, int fp32, const JKArgs *margs,
+                   const long long *mchunk, int nmol, std::string &err);
+int launch_jk_1010(const JKArgs &a, cudaStream_t s, int nsm, int fp32, const JKArgs *margs,
+                   const long long *mchunk, int nmol, std::string &err);
+int launch_jk_1100(const JKArgs &a, cudaStream_t s, int nsm, int fp32, const JKArgs *margs,
+                   const long long *mchunk, int nmol, std::string &err);
+int launch_jk_1110(const JKArgs &a, cudaStream_t s, int nsm, int fp32, const JKArgs *margs,
+                   const long long *mchunk, int nmol, std::string &err);
+int launch_jk_1111(const JKArgs &a, cudaStream_t s, int nsm, int fp32, const JKArgs *margs,
+                   const long long *mchunk, int nmol, std::string &err);
+int launch_jk_2000(const JKArgs &a, cudaStream_t s, int nsm, int fp32, const JKArgs *margs,
+                   const long long *mchunk, int nmol, std::string &err);
+int launch_jk_2010(const JKArgs &a, cudaStream_t s, int nsm, int fp32, const JKArgs *margs,
+                   const long long *mchunk, int nmol, std::string &err);
+int launch_jk_2011(const JKArgs &a, cudaStream_t s, int nsm, int fp32, const JKArgs *margs,
+                   const long long *mchunk, int nmol, std::string &err);
+int launch_jk_2020(const JKArgs &a, cudaStream_t s, int nsm, int fp32, const JKArgs *margs,
+                   const long long *mchunk, int nmol, std::string &err);
+int launch_jk_2100(const JKArgs &a, cudaStream_t s, int nsm, int fp32, const JKArgs *margs,
+                   const long long *mchunk, int nmol, std::string &err);
+int launch_jk_2110(const JKArgs &a, cudaStream_t s, int nsm, int fp32, const JKArgs *margs,
+                   const long long *mchunk, int nmol, std::string &err);
+int launch_jk_2111(const JKArgs &a, cudaStream_t s, int nsm, int fp32, const JKArgs *margs,
+                   const long long *mchunk, int nmol, std::string &err);
+int launch_jk_2120(const JKArgs &a, cudaStream_t s, int nsm, int fp32, const JKArgs *margs,
+                   const long long *mchunk, int nmol, std::string &err);
+int launch_jk_2121(const JKArgs &a, cudaStream_t s, int nsm, int fp32, const JKArgs *margs,
+                   const long long *mchunk, int nmol, std::string &err);
+int launch_jk_2200(const JKArgs &a, cudaStream_t s, int nsm, int fp32, const JKArgs *margs,
+                   const long long *mchunk, int nmol, std::string &err);
+int launch_jk_2210(const JKArgs &a, cudaStream_t s, int nsm, int fp32, const JKArgs *margs,
+                   const long long *mchunk, int nmol, std::string &err);
+int launch_jk_2211(const JKArgs &a, cudaStream_t s, int nsm, int fp32, const JKArgs *margs,
+                   const long long *mchunk, int nmol, std::string &err);
+int launch_jk_2220(const JKArgs &a, cudaStream_t s, int nsm, int fp32, const JKArgs *margs,
+                   const long long *mchunk, int nmol, std::string &err);
+int launch_jk_2221(const JKArgs &a, cudaStream_t s, int nsm, int fp32, const JKArgs *margs,
+                   const long long *mchunk, int nmol, std::string &err);
+int launch_jk_2222(const JKArgs &a, cudaStream_t s, int nsm, int fp32, const JKArgs *margs,
+                   const long long *mchunk, int nmol, std::string &err);
+int launch_jk_3000(const JKArgs &a, cudaStream_t s, int nsm, int fp32, const JKArgs *margs,
+                   const long long *mchunk, int nmol, std::string &err);
+int launch_jk_3010(const JKArgs &a, cudaStream_t s, int nsm, int fp32, const JKArgs *margs,
+                   const long long *mchunk, int nmol, std::string &err);
+int launch_jk_3011(const JKArgs &a, cudaStream_t s, int nsm, int fp32, const JKArgs *margs,
+                   const long long *mchunk, int nmol, std::string &err);
+int launch_jk_3020(const JKArgs &a, cudaStream_t s, int nsm, int fp32, const JKArgs *margs,
+                   const long long *mchunk, int nmol, std::string &err);
+int launch_jk_3021(const JKArgs &a, cudaStream_t s, int nsm, int fp32, const JKArgs *margs,
+                   const long long *mchunk, int nmol, std::string &err);
+int launch_jk_3022(const JKArgs &a, cudaStream_t s, int nsm, int fp32, const JKArgs *margs,
+                   const long long *mchunk, int nmol, std::string &err);
+int launch_jk_3030(const JKArgs &a, cudaStream_t s, int nsm, int fp32, const JKArgs *margs,
+                   const long long *mchunk, int nmol, std::string &err);
+int launch_jk_3100(const JKArgs &a, cudaStream_t s, int nsm, int fp32, const JKArgs *margs,
+                   const long long *mchunk, int nmol, std::string &err);
+int launch_jk_3110(const JKArgs &a, cudaStream_t s, int nsm, int fp32, const JKArgs *margs,
+                   const long long *mchunk, int nmol, std::string &err);
+int launch_jk_3111(const JKArgs &a, cudaStream_t s, int nsm, int fp32, const JKArgs *margs,
+                   const long long *mchunk, int nmol, std::string &err);
+int launch_jk_3120(const JKArgs &a, cudaStream_t s, int nsm, int fp32, const JKArgs *margs,
+                   const long long *mchunk, int nmol, std::string &err);
+int launch_jk_3121(const JKArgs &a, cudaStream_t s, int nsm, int fp32, const JKArgs *margs,
+                   const long long *mchunk, int nmol, std::string &err);
+int launch_jk_3122(const JKArgs &a, cudaStream_t s, int nsm, int fp32, const JKArgs *margs,
+                   const long long *mchunk, int nmol, std::string &err);
+int launch_jk_3130(const JKArgs &a, cudaStream_t s, int nsm, int fp32, const JKArgs *margs,
+                   const long long *mchunk, int nmol, std::string &err);
+int launch_jk_3131(const JKArgs &a, cudaStream_t s, int nsm, int fp32, const JKArgs *margs,
+                   const long long *mchunk, int nmol, std::string &err);
+int launch_jk_3200(const JKArgs &a, cudaStream_t s, int nsm, int fp32, const JKArgs *margs,
+                   const long long *mchunk, int nmol, std::string &err);
+int launch_jk_3210(const JKArgs &a, cudaStream_t s, int nsm, int fp32, const JKArgs *margs,
+                   const long long *mchunk, int nmol, std::string &err);
+int launch_jk_3211(const JKArgs &a, cudaStream_t s, int nsm, int fp32, const JKArgs *margs,
+                   const long long *mchunk, int nmol, std::string &err);
+int launch_jk_3220(const JKArgs &a, cudaStream_t s, int nsm, int fp32, const JKArgs *margs,
+                   const long long *mchunk, int nmol, std::string &err);
+int launch_jk_3221(const JKArgs &a, cudaStream_t s, int nsm, int fp32, const JKArgs *margs,
+                   const long long *mchunk, int nmol, std::string &err);
+int launch_jk_3222(const JKArgs &a, cudaStream_t s, int nsm, int fp32, const JKArgs *margs,
+                   const long long *mchunk, int nmol, std::string &err);
+int launch_jk_3230(const JKArgs &a, cudaStream_t s, int nsm, int fp32, const JKArgs *margs,
+                   const long long *mchunk, int nmol, std::string &err);
+int launch_jk_3231(const JKArgs &a, cudaStream_t s, int nsm, int fp32, const JKArgs *margs,
+                   const long long *mchunk, int nmol, std::string &err);
+int launch_jk_3232(const JKArgs &a, cudaStream_t s, int nsm, int fp32, const JKArgs *margs,
+                   const long long *mchunk, int nmol, std::string &err);
+int launch_jk_3300(const JKArgs &a, cudaStream_t s, int nsm, int fp32, const JKArgs *margs,
+                   const long long *mchunk, int nmol, std::string &err);
+int launch_jk_3310(const JKArgs &a, cudaStream_t s, int nsm, int fp32, const JKArgs *margs,
+                   const long long *mchunk, int nmol, std::string &err);
+int launch_jk_3311(const JKArgs &a, cudaStream_t s, int nsm, int fp32, const JKArgs *margs,
+                   const long long *mchunk, int nmol, std::string &err);
+int launch_jk_3320(const JKArgs &a, cudaStream_t s, int nsm, int fp32, const JKArgs *margs,
+                   const long long *mchunk, int nmol, std::string &err);
+int launch_jk_3321(const JKArgs &a, cudaStream_t s, int nsm, int fp32, const JKArgs *margs,
+                   const long long *mchunk, int nmol, std::string &err);
+int launch_jk_3322(const JKArgs &a, cudaStream_t s, int nsm, int fp32, const JKArgs *margs,
+                   const long long *mchunk, int nmol, std::string &err);
+int launch_jk_3330(const JKArgs &a, cudaStream_t s, int nsm, int fp32, const JKArgs *margs,
+                   const long long *mchunk, int nmol, std::string &err);
+int launch_jk_3331(const JKArgs &a, cudaStream_t s, int nsm, int fp32, const JKArgs *margs,
+                   const long long *mchunk, int nmol, std::string &err);
+int launch_jk_3332(const JKArgs &a, cudaStream_t s, int nsm, int fp32, const JKArgs *margs,
+                   const long long *mchunk, int nmol, std::string &err);
+int launch_jk_3333(const JKArgs &a, cudaStream_t s, int nsm, int fp32, const JKArgs *margs,
+                   const long long *mchunk, int nmol, std::string &err);
 
 int launch_qcond(int la, int lb, const QArgs &q, cudaStream_t s, std::string &err);
 

@@ -27,7 +27,7 @@ EXPORTS = (
     'b200jk_stats', 'b200jk_hostcheck_cart_quartet', 'b200jk_class_stats', 'b200jk_set_profiling',
     'b200jk_measure_fp64_peak', 'b200jk_get_jk_noalloc', 'b200jk_set_mixed_threshold',
     'b200jk_hostcheck_cart_quartet_fp32', 'b200jk_grad_jk', 'b200jk_grad_stats', 'b200jk_get_grad_q_cond',
-    'b200jk_set_shard',
+    'b200jk_set_shard', 'b200jk_batch_create', 'b200jk_batch_destroy', 'b200jk_batch_get_jk', 'b200jk_batch_stats',
 )
 
 
@@ -88,6 +88,11 @@ def load(path=LIB_PATH):
                                           ctypes.POINTER(dp), ctypes.POINTER(ctypes.c_int64)]
         lib.b200jk_get_grad_q_cond.argtypes = [vp, vp]
         lib.b200jk_set_shard.argtypes = [vp, ip, ip]
+        lib.b200jk_batch_create.argtypes = [vp, ip, ctypes.POINTER(vp)]
+        lib.b200jk_batch_destroy.argtypes = [vp]
+        lib.b200jk_batch_get_jk.argtypes = [vp, vp, ip, ip, ip, vp, vp, ip, vp]
+        lib.b200jk_batch_stats.argtypes = [vp, ctypes.POINTER(ctypes.c_int64), ctypes.POINTER(ctypes.c_int64),
+                                           ctypes.POINTER(dp), ctypes.POINTER(ctypes.c_int64)]
         _lib = lib
         return lib
 
@@ -262,6 +267,49 @@ class Plan:
         q = numpy.empty((2, nbas, nbas))
         check(load().b200jk_get_grad_q_cond(self._h, _ptr(q)))
         return q
+
+
+class Batch:
+    """J/K of many molecules (one Plan each, same GPU) in one launch per quartet class."""
+
+    def __init__(self, plans):
+        self.plans = list(plans)
+        arr = (ctypes.c_void_p * len(self.plans))(*[p._h for p in self.plans])
+        h = ctypes.c_void_p()
+        check(load().b200jk_batch_create(arr, len(self.plans), ctypes.byref(h)))
+        self._h = h
+
+    def __del__(self):
+        h = getattr(self, '_h', None)
+        if h and _lib is not None:
+            _lib.b200jk_batch_destroy(h)
+            self._h = None
+
+    def get_jk_device(self, dms, hermi=1, with_j=True, with_k=True, precision=PREC_FP64):
+        """dms: list of float64 CUDA tensors (nao_m, nao_m) -> lists vj, vk."""
+        import torch
+        if len(dms) != len(self.plans):
+            raise ValueError('one density per molecule of the batch')
+        ds = [d.contiguous() for d in dms]
+        for d, p in zip(ds, self.plans):
+            if not (d.is_cuda and d.dtype == torch.float64 and tuple(d.shape) == (p.nao, p.nao)):
+                raise ValueError('density must be a float64 CUDA tensor (nao, nao) of its molecule')
+        vj = [torch.empty_like(d) for d in ds] if with_j else None
+        vk = [torch.empty_like(d) for d in ds] if with_k else None
+        P = ctypes.c_void_p * len(ds)
+        pd = P(*[d.data_ptr() for d in ds])
+        pj = P(*[t.data_ptr() for t in vj]) if with_j else None
+        pk = P(*[t.data_ptr() for t in vk]) if with_k else None
+        stream = torch.cuda.current_stream(ds[0].device).cuda_stream
+        check(load().b200jk_batch_get_jk(self._h, pd, int(hermi), int(bool(with_j)), int(bool(with_k)),
+                                         pj, pk, int(precision), ctypes.c_void_p(stream)))
+        return vj, vk
+
+    def stats(self):
+        q, q32, n = ctypes.c_int64(0), ctypes.c_int64(0), ctypes.c_int64(0)
+        ms = ctypes.c_double(0)
+        check(load().b200jk_batch_stats(self._h, ctypes.byref(q), ctypes.byref(q32), ctypes.byref(ms), ctypes.byref(n)))
+        return {'quartets': q.value, 'fp32_quartets': q32.value, 'last_build_ms': ms.value, 'kernel_launches': n.value}
 
 
 def measure_fp64_peak(device=0):
