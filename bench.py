@@ -25,7 +25,11 @@ Besides the FP64 headline the line carries, measured in the same run:
   batch   512 molecules (H2O)n, n ~ U{1..16}, cc-pVDZ (tests/golden/
           batch_h2o_vdz512.npz) in one batched build (one launch per quartet
           class for all molecules), FP64 and mixed, against the same 512
-          builds run one molecule after another.
+          builds run one molecule after another;
+  scf     C20H42/cc-pVDZ RHF with incremental builds, FP64 and mixed: per
+          build the mixed J/K against the FP64 J/K of the same density change
+          and per iteration the energy against the FP64 SCF; final energies
+          against the reference's RHF energy (tests/golden/mol_c20h42_vdz.npz).
 
 --impl reference times the reference's own CPU implementation of the path
 (PySCF's CVHFnr_direct_drv compiled from the reference sources, oracle/_ref,
@@ -272,6 +276,25 @@ def batch_report(local, flush, stream, steps, tau):
             'density': 'per molecule C C^T, C nao x 5n N(0,1)/sqrt(nao), seed 405'}
 
 
+def scf_report(local, tau):
+    """Per-iteration errors of a mixed-precision RHF on C20H42/cc-pVDZ."""
+    from pyscf_b200 import lib, rhf
+    f = dict(numpy.load(os.path.join(GOLDEN, 'mol_c20h42_vdz.npz')))
+    if 'hcore' not in f:
+        return {'error': 'fixture without hcore'}
+    plan = lib.Plan(f['atm'], f['bas'], f['env'], direct_scf_tol=1e-13, device=local)
+    t0 = time.perf_counter()
+    rows, e64, e32, c64, c32 = rhf.mixed_precision_report(f['hcore'], f['ovlp'], int(f['nelec']), float(f['e_nuc']),
+                                                          plan, tau=tau, conv_tol=1e-10)
+    ref = float(f['e_rhf'])
+    return {'workload': 'C20H42/cc-pVDZ RHF, conv_tol 1e-10, incremental builds on dD', 'tau': tau,
+            'converged': [bool(c64), bool(c32)], 'e_reference': ref,
+            'dE_fp64_vs_reference': e64 - ref, 'dE_mixed_vs_reference': e32 - ref,
+            'builds': len(rows), 'wall_s': time.perf_counter() - t0,
+            'per_build': [{k: (round(v, 15) if isinstance(v, float) else v) for k, v in r.items()
+                           if k in ('build', 'max_dJ', 'max_dK', 'fp32_fraction', 'dE')} for r in rows]}
+
+
 def run_gpu(args):
     import torch
     from pyscf_b200 import lib, flops
@@ -409,6 +432,13 @@ def run_gpu(args):
         except Exception as e:  # the batch line must not sink the J/K measurement
             batch_line = {'error': str(e)[:200]}
 
+    scf_line = None
+    if world == 1:
+        try:
+            scf_line = scf_report(local, args.tau)
+        except Exception as e:  # the SCF line must not sink the J/K measurement
+            scf_line = {'error': str(e)[:200]}
+
     # end to end through the public API, host arrays in pinned memory
     dm_host = torch.from_numpy(f['dm']).pin_memory().numpy()
     out = torch.empty((2, nao, nao), dtype=torch.float64).pin_memory().numpy()
@@ -452,6 +482,7 @@ def run_gpu(args):
             'mixed': mixed,
             'grad': grad_line,
             'batch': batch_line,
+            'scf': scf_line,
             'e2e': {'value': q_per_build / t_e2e, 'unit': 'shell quartets/s',
                     's_per_build': t_e2e, 'h2d_bytes_per_step': int(nao * nao * 8),
                     'd2h_bytes_per_step': int(2 * nao * nao * 8),

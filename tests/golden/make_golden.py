@@ -15,7 +15,9 @@ atm/bas/env arrays; for the small ones also
              vhfopt=None) (unscreened), and a non-symmetric density with hermi=0;
   * the converged RHF density and energy (max_memory=0, i.e. the direct path,
     as pyscf/scf/test/test_h2o_vdz.py:94-98), hcore and overlap, so that an
-    SCF can be replayed on the GPU box without PySCF.
+    SCF can be replayed on the GPU box without PySCF;
+and for the SCF_ONLY workloads (C20H42/cc-pVDZ) the RHF energy, hcore and
+overlap only.
 
     python tests/golden/make_golden.py [names...]
 """
@@ -45,7 +47,9 @@ from pyscf.scf import _vhf  # noqa: E402
 import geometry  # noqa: E402
 
 SMALL = ('h2o_631g', 'h2o_vdz', 'h2o2_vtz', 'h2o8_vdz')
-SCF_TOL = {'h2o_631g': 1e-11, 'h2o_vdz': 1e-11, 'h2o2_vtz': 1e-10, 'h2o8_vdz': 1e-10}
+# workloads that get an SCF replay (energy, hcore, overlap) but no J/K matrices
+SCF_ONLY = ('c20h42_vdz',)
+SCF_TOL = {'h2o_631g': 1e-11, 'h2o_vdz': 1e-11, 'h2o2_vtz': 1e-10, 'h2o8_vdz': 1e-10, 'c20h42_vdz': 1e-10}
 
 
 def build_mol(name):
@@ -79,6 +83,13 @@ def make(name):
                    dm_ns=dm_ns, vj_ns=vjn, vk_ns=vkn, dm_conv=dm_conv, vj_conv=vjc, vk_conv=vkc,
                    e_rhf=e, hcore=mf.get_hcore(), ovlp=mf.get_ovlp(), q_cond=opt.q_cond,
                    scf_conv_tol=SCF_TOL[name])
+    if name in SCF_ONLY:
+        mf = scf.RHF(mol)
+        mf.max_memory = 0
+        mf.conv_tol = SCF_TOL[name]
+        e = mf.kernel()
+        assert mf.converged
+        out.update(e_rhf=e, hcore=mf.get_hcore(), ovlp=mf.get_ovlp(), scf_conv_tol=SCF_TOL[name])
     path = os.path.join(HERE, 'mol_%s.npz' % name)
     numpy.savez_compressed(path, **out)
     print('%-12s nao=%4d nbas=%4d  %.1fs -> %s' % (name, mol.nao, mol.nbas, time.time() - t0, path))

@@ -96,3 +96,23 @@ def test_mixed_scf_energy(b2):
     assert conv
     assert abs(e - float(f['e_rhf'])) < TOL_E_MIXED
     assert frac[-1] > frac[0]
+
+
+def test_c20h42_mixed_scf_report(b2):
+    """C20H42/cc-pVDZ: FP64 and mixed-precision RHF with incremental builds;
+    per build the mixed J/K against the FP64 J/K of the same density change,
+    per iteration the energy against the FP64 SCF, and both final energies
+    against the reference's RHF energy."""
+    from pyscf_b200 import rhf
+    f = load_fixture('c20h42_vdz')
+    if 'hcore' not in f:
+        pytest.skip('fixture without hcore (run tests/golden/make_golden.py c20h42_vdz)')
+    p = plan_for(b2, f)
+    rows, e64, e32, c64, c32 = rhf.mixed_precision_report(f['hcore'], f['ovlp'], int(f['nelec']), float(f['e_nuc']),
+                                                          p, tau=1e-6, conv_tol=1e-10)
+    assert c64 and c32
+    assert abs(e64 - float(f['e_rhf'])) < 1e-9
+    assert abs(e32 - float(f['e_rhf'])) < TOL_E_MIXED
+    assert max(r['max_dJ'] for r in rows) < 1e-8
+    assert max(r['max_dK'] for r in rows) < 1e-8
+    assert rows[-1]['fp32_fraction'] > rows[0]['fp32_fraction']
