@@ -229,6 +229,13 @@ struct b200jk_plan {
         double fp32_tau = 1e-6;
         // multi-GPU: this plan evaluates the bra pairs ij = shard (mod nshard)
         int shard = 0, nshard = 1;
+        // packed ket blocks for the J contraction: class X's blocks start at
+        // pk_off[X] (entries, in ket-list order); pk_src maps entries to the
+        // Cartesian matrix
+        std::vector<long long> pk_off;
+        long long pk_total = 0;
+        DevArr<long long> pk_src;
+        DevArr<double> Dpk, Jpk;
         std::vector<int> ao_loc;
         std::vector<double> h_qcond;
         PairClassDev pc[NPAIRCLASS];
@@ -261,7 +268,8 @@ struct b200jk_plan {
         ~b200jk_plan()
         {
                 for (auto &c : pc) c.release();
-                PP.release(); PK.release(); PE.release(); grad.release(); c2s.release(); qcond.release(); dm_cond.release();
+                PP.release(); PK.release(); PE.release(); grad.release(); c2s.release();
+                pk_src.release(); Dpk.release(); Jpk.release(); qcond.release(); dm_cond.release();
                 goff_all.release(); seg_info.release(); out_seg.release(); out_comp.release();
                 cart_seg.release(); cart_comp.release(); ao_loc_d.release();
                 D.release(); Dc.release(); Ds.release(); Jacc.release(); Kacc.release(); outJ.release(); outK.release();
@@ -701,6 +709,23 @@ int b200jk_plan_create(const int32_t *atm, int natm, const int32_t *bas, int nba
                 P->shell_pairs += (int64_t)hv.size();
                 if ((rc = upload_class(X, hv))) return bail(rc);
         }
+        {
+                std::vector<long long> src;
+                P->pk_off.assign(NPAIRCLASS + 1, 0);
+                for (int X = 0; X < NPAIRCLASS; X++) {
+                        P->pk_off[X] = (long long)src.size();
+                        for (const HostPair &hp : pairs[X]) {
+                                const Seg &A = segs[hp.i], &B = segs[hp.j];
+                                const int na = ncart(A.l), nb = ncart(B.l);
+                                for (int x = 0; x < na; x++)
+                                        for (int y = 0; y < nb; y++)
+                                                src.push_back((long long)(A.cart_off + x) * P->naoc + B.cart_off + y);
+                        }
+                }
+                P->pk_off[NPAIRCLASS] = (long long)src.size();
+                P->pk_total = (long long)src.size();
+                if ((rc = dev_upload(P->pk_src, src))) return bail(rc);
+        }
         memset(&P->st, 0, sizeof(P->st));
         P->st.nao = P->nao; P->st.nao_cart = P->naoc; P->st.nbas = nbas; P->st.nseg = P->nseg;
         P->st.shell_pairs = P->shell_pairs; P->st.prim_pairs = P->prim_pairs;
@@ -723,7 +748,9 @@ static int ensure_workspace(b200jk_plan *P, int n_dm)
             (rc = dev_alloc(P->Ds, nc * n_dm)) || (rc = dev_alloc(P->Jacc, nc * n_dm)) ||
             (rc = dev_alloc(P->Kacc, nc * n_dm * 2)) || (rc = dev_alloc(P->outJ, nn * n_dm)) ||
             (rc = dev_alloc(P->outK, nn * n_dm)) || (rc = dev_alloc(P->dm_cond, (size_t)P->nbas * P->nbas)) ||
-            (rc = dev_alloc(P->dmax, 1)) || (rc = dev_alloc(P->stats, 4 * 64)))
+            (rc = dev_alloc(P->dmax, 1)) || (rc = dev_alloc(P->stats, 4 * 64)) ||
+            (rc = dev_alloc(P->Dpk, (size_t)std::max<long long>(1, P->pk_total) * n_dm)) ||
+            (rc = dev_alloc(P->Jpk, (size_t)std::max<long long>(1, P->pk_total) * n_dm)))
                 return rc;
         int maxn = 1;
         for (auto &c : P->pc) maxn = std::max(maxn, c.n * B2_NBUCKET);
@@ -780,14 +807,22 @@ int b200jk_get_jk(b200jk_plan *P, const double *dms, int n_dm, int hermi, int wi
                 CUDA_TRY(cudaGetLastError());
                 sym_sum_kernel<<<grid_for((long long)nc, 256), 256, 0, s>>>(Dc, P->naoc, P->Ds.p + (size_t)d * nc);
                 CUDA_TRY(cudaGetLastError());
+                if (with_j && P->pk_total > 0) {
+                        pack_gather_kernel<<<grid_for(P->pk_total, 256), 256, 0, s>>>(
+                                P->Ds.p + (size_t)d * nc, P->pk_src.p, P->pk_total, P->Dpk.p + (size_t)d * P->pk_total);
+                        CUDA_TRY(cudaGetLastError());
+                }
         }
+        if (with_j && P->pk_total > 0)
+                CUDA_TRY(cudaMemsetAsync(P->Jpk.p, 0, sizeof(double) * P->pk_total * n_dm, s));
         if (with_j) CUDA_TRY(cudaMemsetAsync(P->Jacc.p, 0, sizeof(double) * nc * n_dm, s));
         if (with_k) CUDA_TRY(cudaMemsetAsync(P->Kacc.p, 0, sizeof(double) * nc * n_dm * nk, s));
 
         const double *tbl = table_ptr();
         const float *tbl_f = table_f_ptr();
         auto qcs = quartet_classes();
-        int64_t launches = 1 + 2 * n_dm;   // dm_cond, to-Cartesian + symmetrise per density
+        // dm_cond, to-Cartesian + symmetrise (+ J block gather) per density
+        int64_t launches = 1 + (2 + (with_j && P->pk_total > 0 ? 1 : 0)) * n_dm;
         if (P->cls.size() != qcs.size()) {
                 P->cls.assign(qcs.size(), b200jk_class_stat_t());
                 for (size_t t = 0; t < qcs.size(); t++) {
@@ -838,6 +873,9 @@ int b200jk_get_jk(b200jk_plan *P, const double *dms, int n_dm, int hermi, int wi
                                 a.goff = P->goff_all.p + P->goff_at[t];
                                 a.Jacc = P->Jacc.p; a.Kacc = P->Kacc.p;
                                 a.Ds = P->Ds.p; a.Dk = P->Dc.p;
+                                a.Dpk = P->Dpk.p + P->pk_off[qcs[t].Y];
+                                a.Jpk = P->Jpk.p + P->pk_off[qcs[t].Y];
+                                a.pk_stride = P->pk_total;
                                 a.stats = P->stats.p + 2 * (64 * pass + t);
                                 a.tol = P->tol > 0 ? P->tol : -1.0;
                                 a.nbas = P->nbas; a.naoc = P->naoc; a.n_dm = n_dm; a.nk = nk;
@@ -849,7 +887,15 @@ int b200jk_get_jk(b200jk_plan *P, const double *dms, int n_dm, int hermi, int wi
                         ran[t] = 1;
                 }
         }
-        // back to the output basis
+        // ket-side J from the packed blocks, then back to the output basis
+        if (with_j && P->pk_total > 0) {
+                for (int d = 0; d < n_dm; d++) {
+                        pack_scatter_add_kernel<<<grid_for(P->pk_total, 256), 256, 0, s>>>(
+                                P->Jpk.p + (size_t)d * P->pk_total, P->pk_src.p, P->pk_total, P->Jacc.p + (size_t)d * nc);
+                        CUDA_TRY(cudaGetLastError());
+                        launches++;
+                }
+        }
         for (int d = 0; d < n_dm; d++) {
                 if (with_j) {
                         const double *J = P->Jacc.p + (size_t)d * nc;
@@ -1418,6 +1464,13 @@ extern "C" int b200jk_batch_get_jk(b200jk_batch *B, const double *const *dms, in
                 CUDA_TRY(cudaGetLastError());
                 sym_sum_kernel<<<grid_for((long long)nc, 256), 256, 0, s>>>(P->Dc.p, P->naoc, P->Ds.p);
                 CUDA_TRY(cudaGetLastError());
+                if (with_j && P->pk_total > 0) {
+                        pack_gather_kernel<<<grid_for(P->pk_total, 256), 256, 0, s>>>(P->Ds.p, P->pk_src.p, P->pk_total,
+                                                                                   P->Dpk.p);
+                        CUDA_TRY(cudaGetLastError());
+                        CUDA_TRY(cudaMemsetAsync(P->Jpk.p, 0, sizeof(double) * P->pk_total, s));
+                        launches++;
+                }
                 if (with_j) CUDA_TRY(cudaMemsetAsync(P->Jacc.p, 0, sizeof(double) * nc, s));
                 if (with_k) CUDA_TRY(cudaMemsetAsync(P->Kacc.p, 0, sizeof(double) * nc * nk, s));
                 launches += 3;
@@ -1435,8 +1488,7 @@ extern "C" int b200jk_batch_get_jk(b200jk_batch *B, const double *const *dms, in
                                 b200jk_plan *P = B->plans[m];
                                 const PairClassDev &bra = P->pc[qcs[t].X], &ket = P->pc[qcs[t].Y];
                                 if (bra.n == 0 || ket.n == 0) continue;
-                                JKArgs a;
-                                memset(&a, 0, sizeof(a));
+                                JKArgs a{};
                                 a.bra = bra.view();
                                 a.ket = ket.view();
                                 a.PP = P->PP.p; a.PK = P->PK.p;
@@ -1449,6 +1501,9 @@ extern "C" int b200jk_batch_get_jk(b200jk_batch *B, const double *const *dms, in
                                 a.goff = P->goff_all.p + P->goff_at[t];
                                 a.Jacc = P->Jacc.p; a.Kacc = P->Kacc.p;
                                 a.Ds = P->Ds.p; a.Dk = P->Dc.p;
+                                a.Dpk = P->Dpk.p + P->pk_off[qcs[t].Y];
+                                a.Jpk = P->Jpk.p + P->pk_off[qcs[t].Y];
+                                a.pk_stride = P->pk_total;
                                 a.stats = B->stats.p + 2 * (64 * pass + t);
                                 a.dmax4 = (const double *)P->dmax.p;
                                 a.tol = P->tol > 0 ? P->tol : -1.0;
@@ -1492,6 +1547,12 @@ extern "C" int b200jk_batch_get_jk(b200jk_batch *B, const double *const *dms, in
         for (int m = 0; m < nmol; m++) {
                 b200jk_plan *P = B->plans[m];
                 const size_t nn = (size_t)P->nao * P->nao, nc = (size_t)P->naoc * P->naoc;
+                if (with_j && P->pk_total > 0) {
+                        pack_scatter_add_kernel<<<grid_for(P->pk_total, 256), 256, 0, s>>>(P->Jpk.p, P->pk_src.p,
+                                                                                        P->pk_total, P->Jacc.p);
+                        CUDA_TRY(cudaGetLastError());
+                        launches++;
+                }
                 if (with_j) {
                         cart_to_out_kernel<<<grid_for((long long)nn, 256), 256, 0, s>>>(
                                 P->Jacc.p, P->Jacc.p, P->nao, P->naoc, P->out_seg.p, P->out_comp.p, P->seg_info.p, P->c2s.p,

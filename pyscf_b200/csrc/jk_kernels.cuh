@@ -64,10 +64,34 @@ struct JKArgs {
         const double *Ds, *Dk;
         unsigned long long *stats;   // [0] quartets, [1] primitive quartets
         const double *dmax4;         // 4 max|D| of the molecule (count kernel of a batch)
+        // Ket-side J in packed form (optional): Dpk[kl*NCD + t] holds Ds of ket
+        // pair kl's block and Jpk[kl*NCD + t] accumulates its J, density s at
+        // + s*pk_stride.  Consecutive lanes work on consecutive kets, so the
+        // reads and atomics are contiguous and the arrays stay in L2; nullptr
+        // = read Ds and add into Jacc directly.
+        const double *Dpk = nullptr;
+        double *Jpk = nullptr;
+        long long pk_stride = 0;
         double tol;
         int nbas, naoc, n_dm, nk;
         int with_j, with_k, same;
 };
+
+// Packed ket blocks: src[e] is the Cartesian matrix offset of packed entry e
+// (ket pair blocks of every class, in ket-list order).
+static __global__ void pack_gather_kernel(const double *__restrict__ Ds, const long long *__restrict__ src,
+                                          long long ne, double *__restrict__ Dpk)
+{
+        const long long e = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+        if (e < ne) Dpk[e] = Ds[src[e]];
+}
+
+static __global__ void pack_scatter_add_kernel(const double *__restrict__ Jpk, const long long *__restrict__ src,
+                                               long long ne, double *__restrict__ Jacc)
+{
+        const long long e = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+        if (e < ne) Jacc[src[e]] += Jpk[e];   // entries are distinct: no atomics
+}
 
 __device__ __forceinline__ double warp_sum(double v)
 {
@@ -328,7 +352,8 @@ __global__ void __launch_bounds__(128) jk_thread_kernel(JKArgs a0, const JKArgs 
                                                         double v = 0.0;
 #pragma unroll
                                                         for (int t = 0; t < NAP * K::NB; t++) v += (double)Gp[t * K::NCD + x * K::ND + y] * dab[t];
-                                                        atomicAdd(J + (ic + x) * n + id + y, v);
+                                                        if (a.Jpk) atomicAdd(a.Jpk + s * a.pk_stride + (long long)kl * K::NCD + x * K::ND + y, v);
+                                                        else atomicAdd(J + (ic + x) * n + id + y, v);
                                                 }
                                         }
                                         double dcd[K::NCD];
@@ -336,7 +361,9 @@ __global__ void __launch_bounds__(128) jk_thread_kernel(JKArgs a0, const JKArgs 
                                         for (int x = 0; x < K::NC; x++)
 #pragma unroll
                                                 for (int y = 0; y < K::ND; y++)
-                                                        dcd[x * K::ND + y] = active ? __ldg(Ds + (ic + x) * n + id + y) : 0.0;
+                                                        dcd[x * K::ND + y] = !active ? 0.0
+                                                                : (a.Dpk ? __ldg(a.Dpk + s * a.pk_stride + (long long)kl * K::NCD + x * K::ND + y)
+                                                                         : __ldg(Ds + (ic + x) * n + id + y));
 #pragma unroll
                                         for (int t = 0; t < NAP * K::NB; t++) {
                                                 double v = 0.0;
@@ -659,12 +686,15 @@ __global__ void __launch_bounds__(128) jk_warp_kernel(JKArgs a0, int chunk_q, co
                                         double *J = a.Jacc + s * nn;
                                         double *dsab = sm + S::DSAB, *dscd = sm + S::DSCD;
                                         for (int t = gl; t < K::NAB; t += GS) dsab[t] = __ldg(Ds + (ia + t / K::NB) * n + ib + t % K::NB);
-                                        for (int t = gl; t < K::NCD; t += GS) dscd[t] = __ldg(Ds + (ic + t / K::ND) * n + id + t % K::ND);
+                                        for (int t = gl; t < K::NCD; t += GS)
+                                                dscd[t] = a.Dpk ? __ldg(a.Dpk + s * a.pk_stride + (long long)kl * K::NCD + t)
+                                                                : __ldg(Ds + (ic + t / K::ND) * n + id + t % K::ND);
                                         __syncwarp(gmask);
                                         for (int t = gl; t < K::NCD; t += GS) {
                                                 double v = 0.0;
                                                 for (int u = 0; u < K::NAB; u++) v += (double)G[u * K::NCD + t] * dsab[u];
-                                                atomicAdd(J + (ic + t / K::ND) * n + id + t % K::ND, v);
+                                                if (a.Jpk) atomicAdd(a.Jpk + s * a.pk_stride + (long long)kl * K::NCD + t, v);
+                                                else atomicAdd(J + (ic + t / K::ND) * n + id + t % K::ND, v);
                                         }
                                         for (int t = gl; t < K::NAB; t += GS) {
                                                 double v = 0.0;
