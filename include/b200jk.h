@@ -157,6 +157,10 @@ int b200jk_grad_jk(b200jk_plan *plan, const double *dms, int n_dm, int with_j, i
 int b200jk_grad_stats(const b200jk_plan *plan, int64_t *quartets, int64_t *prim_quartets, double *ms,
                       int64_t *kernel_launches);
 
+/* Per (bra class, ket class) counters of the last gradient build (100
+ * entries; quartets = bra sides), with kernel times when profiling is on. */
+int b200jk_grad_class_stats(const b200jk_plan *plan, b200jk_class_stat_t *out, int max, int *n);
+
 /* The two screening planes of the gradient (2, nbas, nbas): plane 0 the
  * derivative bound sqrt(max |(d_x i j|d_x i j)|) with the derivative on the
  * row shell (CVHFnr_int2e_pp_q_cond), plane 1 q_cond. */

@@ -212,8 +212,12 @@ struct GradPlan {
         DevArr<unsigned char> cub_tmp;
         int64_t quartets = 0, prim_quartets = 0, launches = 0;
         double last_ms = 0;
+        std::vector<b200jk_class_stat_t> cls;   // per (bra class, ket class)
+        std::vector<cudaEvent_t> cls_ev;
         void release()
         {
+                for (auto e : cls_ev) cudaEventDestroy(e);
+                cls_ev.clear();
                 for (auto &c : bra) c.release();
                 for (auto &c : ket) c.release();
                 q0.release(); goff.release(); D.release(); Dc.release(); Ds.release(); V.release(); out.release();
@@ -1191,7 +1195,7 @@ extern "C" int b200jk_grad_jk(b200jk_plan *P, const double *dms, int n_dm, int w
         if ((rc = dev_alloc(g.D, nn * n_dm)) || (rc = dev_alloc(g.Dc, nc * n_dm)) || (rc = dev_alloc(g.Ds, nc * n_dm)) ||
             (rc = dev_alloc(g.V, 6 * nc * n_dm)) || (rc = dev_alloc(g.out, dev_ptrs ? 1 : 6 * nn * n_dm)) ||
             (rc = dev_alloc(g.dmc, (size_t)P->nbas * P->nbas)) || (rc = dev_alloc(g.fac, 1)) ||
-            (rc = dev_alloc(g.dmax, 1)) || (rc = dev_alloc(g.stats, 2)) || (rc = dev_alloc(g.nkl, maxn)) ||
+            (rc = dev_alloc(g.dmax, 1)) || (rc = dev_alloc(g.stats, 2 * NPAIRCLASS * NPAIRCLASS)) || (rc = dev_alloc(g.nkl, maxn)) ||
             (rc = dev_alloc(g.kst, maxn)) || (rc = dev_alloc(g.nchunk, maxn + 1)) || (rc = dev_alloc(g.chunk_off, maxn + 1)))
                 return rc;
         size_t cub_bytes = 0;
@@ -1206,7 +1210,12 @@ extern "C" int b200jk_grad_jk(b200jk_plan *P, const double *dms, int n_dm, int w
                 dD = g.D.p;
         }
         CUDA_TRY(cudaMemsetAsync(g.dmax.p, 0, sizeof(unsigned long long), s));
-        CUDA_TRY(cudaMemsetAsync(g.stats.p, 0, 2 * sizeof(unsigned long long), s));
+        CUDA_TRY(cudaMemsetAsync(g.stats.p, 0, 2 * NPAIRCLASS * NPAIRCLASS * sizeof(unsigned long long), s));
+        if (P->profiling && g.cls_ev.empty()) {
+                g.cls_ev.resize(2 * NPAIRCLASS * NPAIRCLASS);
+                for (auto &e : g.cls_ev) CUDA_TRY(cudaEventCreate(&e));
+        }
+        std::vector<char> ran(NPAIRCLASS * NPAIRCLASS, 0);
         int64_t launches = 0;
         dm_cond1_kernel<<<grid_for((long long)P->nbas * P->nbas, 256), 256, 0, s>>>(dD, n_dm, P->nao, P->ao_loc_d.p,
                                                                                   P->nbas, g.dmc.p, g.dmax.p);
@@ -1255,12 +1264,15 @@ extern "C" int b200jk_grad_jk(b200jk_plan *P, const double *dms, int n_dm, int w
                         a.goff = g.goff.p + g.goff_at[X * NPAIRCLASS + Y];
                         a.Vj = Vj; a.Vk = Vk;
                         a.Ds = g.Ds.p; a.Dc = g.Dc.p;
-                        a.stats = g.stats.p;
+                        a.stats = g.stats.p + 2 * (X * NPAIRCLASS + Y);
                         a.tol = tol > 0 ? tol : -1.0;
                         a.nbas = P->nbas; a.naoc = P->naoc; a.n_dm = n_dm;
                         a.with_j = with_j; a.with_k = with_k;
                         std::string err;
+                        if (P->profiling) CUDA_TRY(cudaEventRecord(g.cls_ev[2 * (X * NPAIRCLASS + Y)], s));
                         if (g_grad_launch[X](ket.la, ket.lb, a, s, P->nsm, err)) return fail(B200JK_ECUDA, err);
+                        if (P->profiling) CUDA_TRY(cudaEventRecord(g.cls_ev[2 * (X * NPAIRCLASS + Y) + 1], s));
+                        ran[X * NPAIRCLASS + Y] = 1;
                         launches += 2;   // count + class kernel (the scan is a CUB library kernel)
                 }
         }
@@ -1286,13 +1298,31 @@ extern "C" int b200jk_grad_jk(b200jk_plan *P, const double *dms, int n_dm, int w
                 if (with_j) CUDA_TRY(cudaMemcpyAsync(vj, oj, sizeof(double) * nout, cudaMemcpyDeviceToHost, s));
                 if (with_k) CUDA_TRY(cudaMemcpyAsync(vk, ok, sizeof(double) * nout, cudaMemcpyDeviceToHost, s));
         }
-        unsigned long long hs[2];
-        CUDA_TRY(cudaMemcpyAsync(hs, g.stats.p, sizeof(hs), cudaMemcpyDeviceToHost, s));
+        std::vector<unsigned long long> hs(2 * NPAIRCLASS * NPAIRCLASS);
+        CUDA_TRY(cudaMemcpyAsync(hs.data(), g.stats.p, sizeof(unsigned long long) * hs.size(), cudaMemcpyDeviceToHost, s));
         CUDA_TRY(cudaStreamSynchronize(s));
         float ms = 0;
         CUDA_TRY(cudaEventElapsedTime(&ms, P->ev0, P->ev1));
-        g.quartets = (int64_t)hs[0];
-        g.prim_quartets = (int64_t)hs[1];
+        g.quartets = g.prim_quartets = 0;
+        g.cls.assign(NPAIRCLASS * NPAIRCLASS, b200jk_class_stat_t());
+        for (int X = 0; X < NPAIRCLASS; X++)
+                for (int Y = 0; Y < NPAIRCLASS; Y++) {
+                        const int t = X * NPAIRCLASS + Y;
+                        b200jk_class_stat_t &c = g.cls[t];
+                        class_l(X, c.la, c.lb);
+                        class_l(Y, c.lc, c.ld);
+                        c.quartets = (int64_t)hs[2 * t];
+                        c.prim_quartets = (int64_t)hs[2 * t + 1];
+                        c.family = 1;
+                        c.ms = 0;
+                        if (P->profiling && ran[t]) {
+                                float cm = 0;
+                                CUDA_TRY(cudaEventElapsedTime(&cm, g.cls_ev[2 * t], g.cls_ev[2 * t + 1]));
+                                c.ms = cm;
+                        }
+                        g.quartets += c.quartets;
+                        g.prim_quartets += c.prim_quartets;
+                }
         g.last_ms = ms;
         g.launches = launches;
         return B200JK_OK;
@@ -1306,6 +1336,14 @@ extern "C" int b200jk_grad_stats(const b200jk_plan *P, int64_t *quartets, int64_
         if (prim_quartets) *prim_quartets = P->grad.prim_quartets;
         if (ms) *ms = P->grad.last_ms;
         if (kernel_launches) *kernel_launches = P->grad.launches;
+        return B200JK_OK;
+}
+
+extern "C" int b200jk_grad_class_stats(const b200jk_plan *P, b200jk_class_stat_t *out, int max, int *n)
+{
+        if (!P || !n) return fail(B200JK_EINVAL, "NULL argument");
+        *n = (int)P->grad.cls.size();
+        for (int t = 0; t < *n && t < max && out; t++) out[t] = P->grad.cls[t];
         return B200JK_OK;
 }
 

@@ -386,6 +386,231 @@ __global__ void __launch_bounds__(128) grad_jk_kernel(GradArgs a, int chunk_q)
 }
 
 // ---------------------------------------------------------------------------
+// Register family of the gradient for small classes: one ket per lane, the
+// six derivative blocks in registers, assembly offsets at compile time.
+
+template <int LA, int LB, int LC, int LD>
+__host__ __device__ constexpr bool grad_thread_family()
+{
+        using GC = GClass<LA, LB, LC, LD, 0>;
+        return 6 * GC::NG + 3 * GC::SE <= 104;
+}
+
+// component T of the block: G[c*NG + T] += (derivative c of) I_x I_y I_z
+template <int LA, int LB, int LC, int LD, int T>
+__device__ __forceinline__ void grad_assemble_one(double *G, const double *Ex, const double *Ey, const double *Ez,
+                                                  double ta, double tb)
+{
+        using K = Class4<LA, LB, LC, LD>;
+        using GC = GClass<LA, LB, LC, LD, 0>;
+        constexpr int NG = K::NG;
+        constexpr int id = T % K::ND, ic = (T / K::ND) % K::NC, ib = (T / K::NCD) % K::NB, ia = T / (K::NCD * K::NB);
+        constexpr int ax = cart_lx(LA, ia), ay = cart_ly(LA, ia), az = cart_lz(LA, ia);
+        constexpr int bx = cart_lx(LB, ib), by = cart_ly(LB, ib), bz = cart_lz(LB, ib);
+        constexpr int ox = GC::eidx(ax, bx, cart_lx(LC, ic), cart_lx(LD, id));
+        constexpr int oy = GC::eidx(ay, by, cart_ly(LC, ic), cart_ly(LD, id));
+        constexpr int oz = GC::eidx(az, bz, cart_lz(LC, ic), cart_lz(LD, id));
+        constexpr int SA = GC::STEP_A, SB = GC::STEP_B;
+        const double ex = Ex[ox], ey = Ey[oy], ez = Ez[oz];
+        double dax = ta * Ex[ox + SA], day = ta * Ey[oy + SA], daz = ta * Ez[oz + SA];
+        if constexpr (ax > 0) dax -= ax * Ex[ox - SA];
+        if constexpr (ay > 0) day -= ay * Ey[oy - SA];
+        if constexpr (az > 0) daz -= az * Ez[oz - SA];
+        double dbx = tb * Ex[ox + SB], dby = tb * Ey[oy + SB], dbz = tb * Ez[oz + SB];
+        if constexpr (bx > 0) dbx -= bx * Ex[ox - SB];
+        if constexpr (by > 0) dby -= by * Ey[oy - SB];
+        if constexpr (bz > 0) dbz -= bz * Ez[oz - SB];
+        G[0 * NG + T] += dax * ey * ez;
+        G[1 * NG + T] += ex * day * ez;
+        G[2 * NG + T] += ex * ey * daz;
+        G[3 * NG + T] += dbx * ey * ez;
+        G[4 * NG + T] += ex * dby * ez;
+        G[5 * NG + T] += ex * ey * dbz;
+}
+
+template <int LA, int LB, int LC, int LD, int... Ts>
+__device__ __forceinline__ void grad_assemble(double *G, const double *Ex, const double *Ey, const double *Ez,
+                                              double ta, double tb, std::integer_sequence<int, Ts...>)
+{
+        (grad_assemble_one<LA, LB, LC, LD, Ts>(G, Ex, Ey, Ez, ta, tb), ...);
+}
+
+template <int LA, int LB, int LC, int LD>
+__global__ void __launch_bounds__(128) grad_thread_kernel(GradArgs a)
+{
+        using K = Class4<LA, LB, LC, LD>;
+        using GC = GClass<LA, LB, LC, LD, 0>;
+        constexpr int NG = K::NG, NR = GC::NR, SE = GC::SE;
+        const int lane = threadIdx.x & 31;
+        const int nseg = a.bra.n * B2_NBUCKET;
+        const long long total = a.chunk_off[nseg];
+        const long long nwarps = ((long long)gridDim.x * blockDim.x) >> 5;
+        const size_t n = (size_t)a.naoc, nn = n * n;
+        const double *table = a.table + rys_padded_offset(NR);
+        unsigned long long nq = 0, npq = 0;
+        for (long long chunk = ((long long)blockIdx.x * blockDim.x + threadIdx.x) >> 5; chunk < total;
+             chunk += nwarps) {
+                const int sgi = find_bra(a.chunk_off, nseg, chunk);
+                const int ij = sgi / B2_NBUCKET;
+                const int pos = (int)(chunk - a.chunk_off[sgi]) * 32 + lane;
+                const int kl = a.ket.boff[sgi % B2_NBUCKET] + a.kst[sgi] + pos;
+                const int4 sb = a.bra.sh[ij];
+                const int2 pb = a.bra.pr[ij];
+                const double4 Ab = a.bra.A[ij];
+                const double4 ABb = a.bra.AB[ij];
+                const double AB[3] = {ABb.x, ABb.y, ABb.z};
+                int4 sk = make_int4(0, 0, 0, 0);
+                bool sideA = false, sideB = false;
+                if (pos < a.nkl[sgi]) {
+                        sk = a.ket.sh[kl];
+                        const int kk = max(sk.z, sk.w), ll = min(sk.z, sk.w);
+                        sideA = grad_side_passes(a, sb.z, sb.w, kk, ll);
+                        sideB = Ab.w == 0.0 && grad_side_passes(a, sb.w, sb.z, kk, ll);
+                }
+                const bool active = sideA || sideB;
+                double G[6 * NG];
+#pragma unroll
+                for (int t = 0; t < 6 * NG; t++) G[t] = 0.0;
+                if (active) {
+                        const int2 pk = a.ket.pr[kl];
+                        const double4 Ak = a.ket.A[kl];
+                        const double4 CDk = a.ket.AB[kl];
+                        const double fac = Ak.w != 0.0 ? 0.5 : 1.0;
+                        const double A0[3] = {0.0, 0.0, 0.0};
+                        const double C[3] = {Ak.x - Ab.x, Ak.y - Ab.y, Ak.z - Ab.z};
+                        const double CD[3] = {CDk.x, CDk.y, CDk.z};
+                        nq += (unsigned long long)sideA + (unsigned long long)sideB;
+                        npq += (unsigned long long)pb.y * pk.y;
+                        for (int ip = 0; ip < pb.y; ip++) {
+                                const double4 P = a.PP[pb.x + ip];
+                                const double2 KP = a.PK[pb.x + ip];
+                                const double2 EP = a.PE[pb.x + ip];
+                                const double Kab = KP.x * fac;
+                                const double Pv[3] = {P.x - Ab.x, P.y - Ab.y, P.z - Ab.z};
+                                const double ta = 2.0 * EP.x, tb = 2.0 * EP.y;
+                                for (int kp = 0; kp < pk.y; kp++) {
+                                        const double4 Q = a.PP[pk.x + kp];
+                                        const double2 KQ = a.PK[pk.x + kp];
+                                        const double Qv[3] = {Q.x - Ab.x, Q.y - Ab.y, Q.z - Ab.z};
+                                        PrimQ<double> sq;
+                                        prim_setup<double>(sq, P.w, KP.y, Pv, Q.w, KQ.y, Qv, A0, C, Kab * KQ.x);
+                                        double u[NR], w[NR];
+                                        rys_roots_slice<NR, double>(sq.T, table, u, w);
+#pragma unroll
+                                        for (int r = 0; r < NR; r++) {
+                                                RysCoef<double> rc;
+                                                rys_coef<double>(rc, u[r], sq);
+                                                double Ex[SE], Ey[SE], Ez[SE];
+                                                grad_slice<LA, LB, LC, LD, 0>(Ex, 1.0, rc, 0, AB[0], CD[0]);
+                                                grad_slice<LA, LB, LC, LD, 0>(Ey, 1.0, rc, 1, AB[1], CD[1]);
+                                                grad_slice<LA, LB, LC, LD, 0>(Ez, sq.pref * w[r], rc, 2, AB[2], CD[2]);
+                                                grad_assemble<LA, LB, LC, LD>(G, Ex, Ey, Ez, ta, tb,
+                                                                              std::make_integer_sequence<int, NG>{});
+                                        }
+                                }
+                        }
+                }
+                const int ia = sb.x, ib = sb.y, ic = sk.x, id = sk.y;
+                for (int s = 0; s < a.n_dm; s++) {
+                        const double *Ds = a.Ds + s * nn;
+                        const double *X = a.Dc + s * nn;
+                        double dcd[K::NCD];
+#pragma unroll
+                        for (int t = 0; t < K::NCD; t++)
+                                dcd[t] = active ? __ldg(Ds + (ic + t / K::ND) * n + id + t % K::ND) : 0.0;
+#pragma unroll
+                        for (int x = 0; x < 3; x++) {
+                                double *Vj = a.Vj + ((size_t)s * 3 + x) * nn;
+                                double *Vk = a.Vk + ((size_t)s * 3 + x) * nn;
+                                if (a.with_j) {
+                                        // the bra block is the warp's: sum over the lanes, one atomic
+#pragma unroll
+                                        for (int t = 0; t < K::NAB; t++) {
+                                                double vA = 0.0, vB = 0.0;
+#pragma unroll
+                                                for (int u = 0; u < K::NCD; u++) {
+                                                        vA += G[x * NG + t * K::NCD + u] * dcd[u];
+                                                        vB += G[(3 + x) * NG + t * K::NCD + u] * dcd[u];
+                                                }
+                                                vA = warp_sum(sideA ? vA : 0.0);
+                                                vB = warp_sum(sideB ? vB : 0.0);
+                                                const int xa = t / K::NB, yb = t % K::NB;
+                                                if (lane == 0 && vA != 0.0) atomicAdd(Vj + (ia + xa) * n + ib + yb, vA);
+                                                if (lane == 0 && vB != 0.0) atomicAdd(Vj + (ib + yb) * n + ia + xa, vB);
+                                        }
+                                }
+                                if (a.with_k && sideA) {
+                                        // Vk[a,d] += G X[b,c];  Vk[a,c] += G X[b,d]
+#pragma unroll
+                                        for (int xa = 0; xa < K::NA; xa++) {
+#pragma unroll
+                                                for (int d = 0; d < K::ND; d++) {
+                                                        double v = 0.0;
+#pragma unroll
+                                                        for (int b = 0; b < K::NB; b++)
+#pragma unroll
+                                                                for (int c = 0; c < K::NC; c++)
+                                                                        v += G[x * NG + ((xa * K::NB + b) * K::NC + c) * K::ND + d] *
+                                                                             __ldg(X + (ib + b) * n + ic + c);
+                                                        atomicAdd(Vk + (ia + xa) * n + id + d, v);
+                                                }
+#pragma unroll
+                                                for (int c = 0; c < K::NC; c++) {
+                                                        double v = 0.0;
+#pragma unroll
+                                                        for (int b = 0; b < K::NB; b++)
+#pragma unroll
+                                                                for (int d = 0; d < K::ND; d++)
+                                                                        v += G[x * NG + ((xa * K::NB + b) * K::NC + c) * K::ND + d] *
+                                                                             __ldg(X + (ib + b) * n + id + d);
+                                                        atomicAdd(Vk + (ia + xa) * n + ic + c, v);
+                                                }
+                                        }
+                                }
+                                if (a.with_k && sideB) {
+                                        // Vk[b,d] += G X[a,c];  Vk[b,c] += G X[a,d]
+#pragma unroll
+                                        for (int b = 0; b < K::NB; b++) {
+#pragma unroll
+                                                for (int d = 0; d < K::ND; d++) {
+                                                        double v = 0.0;
+#pragma unroll
+                                                        for (int xa = 0; xa < K::NA; xa++)
+#pragma unroll
+                                                                for (int c = 0; c < K::NC; c++)
+                                                                        v += G[(3 + x) * NG + ((xa * K::NB + b) * K::NC + c) * K::ND + d] *
+                                                                             __ldg(X + (ia + xa) * n + ic + c);
+                                                        atomicAdd(Vk + (ib + b) * n + id + d, v);
+                                                }
+#pragma unroll
+                                                for (int c = 0; c < K::NC; c++) {
+                                                        double v = 0.0;
+#pragma unroll
+                                                        for (int xa = 0; xa < K::NA; xa++)
+#pragma unroll
+                                                                for (int d = 0; d < K::ND; d++)
+                                                                        v += G[(3 + x) * NG + ((xa * K::NB + b) * K::NC + c) * K::ND + d] *
+                                                                             __ldg(X + (ia + xa) * n + id + d);
+                                                        atomicAdd(Vk + (ib + b) * n + ic + c, v);
+                                                }
+                                        }
+                                }
+                        }
+                }
+        }
+        if (a.stats) {
+                for (int o = 16; o > 0; o >>= 1) {
+                        nq += __shfl_xor_sync(0xffffffffu, nq, o);
+                        npq += __shfl_xor_sync(0xffffffffu, npq, o);
+                }
+                if (lane == 0 && nq) {
+                        atomicAdd(a.stats + 0, nq);
+                        atomicAdd(a.stats + 1, npq);
+                }
+        }
+}
+
+// ---------------------------------------------------------------------------
 // Derivative Schwarz bound: one warp per shell pair evaluates the diagonal
 // blocks (d_x a b|d_x a b) (derivative on the first function of bra and ket,
 // x = y = z components of int2e_ip1ip2) for both orientations of the pair,

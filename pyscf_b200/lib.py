@@ -27,7 +27,7 @@ EXPORTS = (
     'b200jk_stats', 'b200jk_hostcheck_cart_quartet', 'b200jk_class_stats', 'b200jk_set_profiling',
     'b200jk_measure_fp64_peak', 'b200jk_get_jk_noalloc', 'b200jk_set_mixed_threshold',
     'b200jk_hostcheck_cart_quartet_fp32', 'b200jk_grad_jk', 'b200jk_grad_stats', 'b200jk_get_grad_q_cond',
-    'b200jk_set_shard', 'b200jk_batch_create', 'b200jk_batch_destroy', 'b200jk_batch_get_jk', 'b200jk_batch_stats',
+    'b200jk_set_shard', 'b200jk_grad_class_stats', 'b200jk_batch_create', 'b200jk_batch_destroy', 'b200jk_batch_get_jk', 'b200jk_batch_stats',
 )
 
 
@@ -88,6 +88,7 @@ def load(path=LIB_PATH):
                                           ctypes.POINTER(dp), ctypes.POINTER(ctypes.c_int64)]
         lib.b200jk_get_grad_q_cond.argtypes = [vp, vp]
         lib.b200jk_set_shard.argtypes = [vp, ip, ip]
+        lib.b200jk_grad_class_stats.argtypes = [vp, ctypes.POINTER(ClassStat), ip, ctypes.POINTER(ip)]
         lib.b200jk_batch_create.argtypes = [vp, ip, ctypes.POINTER(vp)]
         lib.b200jk_batch_destroy.argtypes = [vp]
         lib.b200jk_batch_get_jk.argtypes = [vp, vp, ip, ip, ip, vp, vp, ip, vp]
@@ -259,6 +260,12 @@ class Plan:
         ms = ctypes.c_double(0)
         check(load().b200jk_grad_stats(self._h, ctypes.byref(q), ctypes.byref(pq), ctypes.byref(ms), ctypes.byref(n)))
         return {'quartets': q.value, 'prim_quartets': pq.value, 'last_build_ms': ms.value, 'kernel_launches': n.value}
+
+    def grad_class_stats(self):
+        n = ctypes.c_int(0)
+        buf = (ClassStat * 100)()
+        check(load().b200jk_grad_class_stats(self._h, buf, 100, ctypes.byref(n)))
+        return [{k: getattr(buf[i], k) for k, _ in ClassStat._fields_} for i in range(n.value)]
 
     @property
     def grad_q_cond(self):
