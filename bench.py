@@ -318,6 +318,9 @@ def run_gpu(args):
             b2dist.reduce_jk(vj, vk)
         return vj, vk
 
+    # the per-class launch variants (kets per lane of the register family)
+    # are tuned once per plan on the workload's density, like the planning
+    tuning = plan.autotune(d)
     for _ in range(args.warmup):
         build64()
     torch.cuda.synchronize(dev)
@@ -470,7 +473,8 @@ def run_gpu(args):
                        'precision': 'fp64', 'direct_scf_tol': 1e-13,
                        'parallelism': ('bra-pair shards + NCCL all-reduce of [J;K], %d GPUs' % world) if world > 1
                        else 'single',
-                       'l2': 'flushed (256 MB write) before every timed build'},
+                       'l2': 'flushed (256 MB write) before every timed build',
+                       'autotuned_classes': int(sum(tuning))},
             's_per_build': t_total / args.steps,
             'quartets_per_build': q_per_build, 'prim_quartets_per_build': _sum_over_ranks(tot['prim_quartets'], dist, dev) / args.steps,
             'fp64_tflops_build': build_flops / (t_total / args.steps) / 1e12 if world == 1 else None,

@@ -136,6 +136,17 @@ int b200jk_stats(const b200jk_plan *plan, b200jk_stats_t *stats);
 int b200jk_class_stats(const b200jk_plan *plan, b200jk_class_stat_t *out, int max, int *n);
 int b200jk_set_profiling(b200jk_plan *plan, int on);
 
+/* Autotuner: for every quartet class with more than one launch variant (the
+ * register family with 1 or 4 kets per lane), time each variant on one FP64
+ * J/K build of the density dm (nao x nao, symmetric; host array, or device
+ * array with dev_ptrs = 1) and keep the faster for later builds of this plan
+ * (and of batches whose first plan it is).  Three builds.  No reference
+ * counterpart (PySCF has no kernel variants to tune). */
+int b200jk_autotune(b200jk_plan *plan, const double *dm, int dev_ptrs, void *stream);
+
+/* The chosen variant per quartet class (55 classes, bra class >= ket class). */
+int b200jk_get_tuning(const b200jk_plan *plan, int *variants, int max, int *n);
+
 /* Nuclear-gradient J/K: the drop-in for pyscf.grad.rhf.get_jk(mol, dm)
  * (pyscf/grad/rhf.py:149-178, i.e. _vhf.direct_mapdm('int2e_ip1', 's2kl',
  * ('lk->s1ij', 'jk->s1il'), dm, 3, ...) with CVHFgrad_jk_prescreen,

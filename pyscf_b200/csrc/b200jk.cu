@@ -172,16 +172,16 @@ struct PairClassDev {
         int boff[B2_NBUCKET + 1] = {0, 0, 0, 0, 0};
         DevArr<int4> sh;
         DevArr<int2> pr;
-        DevArr<double> q;
+        DevArr<double> q, qs;
         DevArr<double4> A, AB;
         PairView view() const
         {
                 PairView v;
-                v.sh = sh.p; v.pr = pr.p; v.q = q.p; v.A = A.p; v.AB = AB.p; v.n = n;
+                v.sh = sh.p; v.pr = pr.p; v.q = q.p; v.qs = qs.p; v.A = A.p; v.AB = AB.p; v.n = n;
                 for (int b = 0; b <= B2_NBUCKET; b++) v.boff[b] = boff[b];
                 return v;
         }
-        void release() { sh.release(); pr.release(); q.release(); A.release(); AB.release(); n = 0; }
+        void release() { sh.release(); pr.release(); q.release(); qs.release(); A.release(); AB.release(); n = 0; }
 };
 
 // what the gradient set-up keeps of the planner's segments and pairs
@@ -233,6 +233,9 @@ struct b200jk_plan {
         double fp32_tau = 1e-6;
         // multi-GPU: this plan evaluates the bra pairs ij = shard (mod nshard)
         int shard = 0, nshard = 1;
+        // launch variant per quartet class (register family: 0 = one ket per
+        // lane, 1 = family_ket_run kets per lane), chosen by b200jk_autotune
+        std::vector<int> kvar;
         // packed ket blocks for the J contraction: class X's blocks start at
         // pk_off[X] (entries, in ket-list order); pk_src maps entries to the
         // Cartesian matrix
@@ -303,11 +306,11 @@ static void class_l(int X, int &la, int &lb)
                         if (pair_class(a, b) == X) { la = a; lb = b; return; }
 }
 
-typedef int (*jk_launcher_t)(const JKArgs &, cudaStream_t, int, int, const JKArgs *, const long long *, int,
+typedef int (*jk_launcher_t)(const JKArgs &, cudaStream_t, int, int, int, const JKArgs *, const long long *, int,
                              std::string &);
 
 static int dispatch_jk(b200jk_plan *P, int la, int lb, int lc, int ld, const JKArgs &a, int fp32, cudaStream_t s,
-                       const JKArgs *margs = nullptr, const long long *mchunk = nullptr, int nmol = 0)
+                       const JKArgs *margs = nullptr, const long long *mchunk = nullptr, int nmol = 0, int variant = 0)
 {
         struct Entry { int la, lb, lc, ld; jk_launcher_t fn; };
         static const Entry table[] = {
@@ -370,7 +373,7 @@ static int dispatch_jk(b200jk_plan *P, int la, int lb, int lc, int ld, const JKA
         for (const Entry &e : table) {
                 if (e.la == la && e.lb == lb && e.lc == lc && e.ld == ld) {
                         std::string err;
-                        if (e.fn(a, s, P->nsm, fp32, margs, mchunk, nmol, err)) return fail(B200JK_ECUDA, err);
+                        if (e.fn(a, s, P->nsm, fp32, variant, margs, mchunk, nmol, err)) return fail(B200JK_ECUDA, err);
                         return B200JK_OK;
                 }
         }
@@ -514,6 +517,8 @@ struct HostPair {
         int i, j;              // segments, l_i >= l_j
         int prim0, nprim;
         double q;
+        double qs = 0;         // prefix-search key (maximum of q over its band)
+        int band = 0;
 };
 
 int b200jk_plan_create(const int32_t *atm, int natm, const int32_t *bas, int nbas,
@@ -645,19 +650,20 @@ int b200jk_plan_create(const int32_t *atm, int natm, const int32_t *bas, int nba
                 for (int b = 0; b < B2_NBUCKET; b++) c.boff[b + 1] += c.boff[b];
                 std::vector<int4> sh(hv.size());
                 std::vector<int2> pr(hv.size());
-                std::vector<double> q(hv.size());
+                std::vector<double> q(hv.size()), qs(hv.size());
                 std::vector<double4> Av(hv.size()), ABv(hv.size());
                 for (size_t t = 0; t < hv.size(); t++) {
                         const Seg &A = segs[hv[t].i], &B = segs[hv[t].j];
                         sh[t] = make_int4(A.cart_off, B.cart_off, A.parent, B.parent);
                         pr[t] = make_int2(hv[t].prim0, hv[t].nprim);
                         q[t] = hv[t].q;
+                        qs[t] = hv[t].qs;
                         Av[t] = make_double4(A.R[0], A.R[1], A.R[2], hv[t].i == hv[t].j ? 1.0 : 0.0);
                         ABv[t] = make_double4(A.R[0] - B.R[0], A.R[1] - B.R[1], A.R[2] - B.R[2], 0.0);
                 }
                 int r;
                 if ((r = dev_upload(c.sh, sh)) || (r = dev_upload(c.pr, pr)) || (r = dev_upload(c.q, q)) ||
-                    (r = dev_upload(c.A, Av)) || (r = dev_upload(c.AB, ABv)))
+                    (r = dev_upload(c.qs, qs)) || (r = dev_upload(c.A, Av)) || (r = dev_upload(c.AB, ABv)))
                         return r;
                 return B200JK_OK;
         };
@@ -704,12 +710,33 @@ int b200jk_plan_create(const int32_t *atm, int natm, const int32_t *bas, int nba
                                                 [&](const HostPair &p) { return !(p.q * qmax > P->tol); }),
                                  hv.end());
                 }
-                // bucket-major, descending q inside a bucket
-                std::stable_sort(hv.begin(), hv.end(), [](const HostPair &a, const HostPair &b) {
+                // Order inside a bucket: bands of the bound (factor 2, largest
+                // first), inside a band by first then second segment.  The
+                // prefix screen searches the band maxima qs (a superset of the
+                // passing kets; the exact test is per quartet).  Consecutive
+                // kets then mostly share their first segment, which the
+                // register family uses to carry K[., c] sums across the kets
+                // of a lane.
+                const double qcls = std::accumulate(hv.begin(), hv.end(), 0.0,
+                                                    [](double m, const HostPair &p) { return std::max(m, p.q); });
+                for (auto &p : hv)
+                        p.band = (p.q > 0 && qcls > 0) ? std::min(2000, (int)std::floor(std::log2(qcls / p.q))) : 2000;
+                std::stable_sort(hv.begin(), hv.end(), [&](const HostPair &a, const HostPair &b) {
                         const int ba = prim_bucket(a.nprim), bb = prim_bucket(b.nprim);
                         if (ba != bb) return ba < bb;
-                        return a.q > b.q;
+                        if (a.band != b.band) return a.band < b.band;
+                        if (segs[a.i].cart_off != segs[b.i].cart_off) return segs[a.i].cart_off < segs[b.i].cart_off;
+                        return segs[a.j].cart_off < segs[b.j].cart_off;
                 });
+                for (size_t t = 0; t < hv.size();) {
+                        size_t e = t;
+                        double m = 0;
+                        while (e < hv.size() && prim_bucket(hv[e].nprim) == prim_bucket(hv[t].nprim) &&
+                               hv[e].band == hv[t].band)
+                                m = std::max(m, hv[e++].q);
+                        for (size_t u = t; u < e; u++) hv[u].qs = m;
+                        t = e;
+                }
                 P->shell_pairs += (int64_t)hv.size();
                 if ((rc = upload_class(X, hv))) return bail(rc);
         }
@@ -849,7 +876,8 @@ int b200jk_get_jk(b200jk_plan *P, const double *dms, int n_dm, int hermi, int wi
                         int la = bra.la, lb = bra.lb, lc = ket.la, ld = ket.lb;
                         const int same = qcs[t].X == qcs[t].Y;
                         // chunk size of the family the dispatcher will pick
-                        const int chunk = family_chunk(la, lb, lc, ld);
+                        const int variant = t < P->kvar.size() ? P->kvar[t] : 0;
+                        const int chunk = family_chunk(la, lb, lc, ld, variant);
                         const int nseg = bra.n * B2_NBUCKET;
                         if (P->profiling) CUDA_TRY(cudaEventRecord(P->cls_ev[2 * t], s));
                         // pass 0: float64 quartets (all of them unless mixed);
@@ -884,7 +912,7 @@ int b200jk_get_jk(b200jk_plan *P, const double *dms, int n_dm, int hermi, int wi
                                 a.tol = P->tol > 0 ? P->tol : -1.0;
                                 a.nbas = P->nbas; a.naoc = P->naoc; a.n_dm = n_dm; a.nk = nk;
                                 a.with_j = with_j; a.with_k = with_k; a.same = same;
-                                if ((rc = dispatch_jk(P, la, lb, lc, ld, a, pass, s))) return rc;
+                                if ((rc = dispatch_jk(P, la, lb, lc, ld, a, pass, s, nullptr, nullptr, 0, variant))) return rc;
                                 launches += 2;   // count + class kernel (the scan is a CUB library kernel)
                         }
                         if (P->profiling) CUDA_TRY(cudaEventRecord(P->cls_ev[2 * t + 1], s));
@@ -969,6 +997,55 @@ int b200jk_set_mixed_threshold(b200jk_plan *plan, double tau)
         if (!plan) return fail(B200JK_EINVAL, "plan is NULL");
         if (!(tau == tau)) return fail(B200JK_EINVAL, "tau is NaN");
         plan->fp32_tau = tau;
+        return B200JK_OK;
+}
+
+int b200jk_autotune(b200jk_plan *P, const double *dm, int dev_ptrs, void *stream)
+{
+        if (!P || !dm) return fail(B200JK_EINVAL, "NULL argument");
+        CUDA_TRY(cudaSetDevice(P->device));
+        int rc = ensure_workspace(P, 1);
+        if (rc) return rc;
+        auto qcs = quartet_classes();
+        const int nclass = (int)qcs.size();
+        std::vector<int> best(nclass, 0);
+        std::vector<double> best_ms(nclass, 1e300);
+        const int saved_prof = P->profiling;
+        P->profiling = 1;
+        // the builds write into the plan's own output buffers
+        double *oj = dev_ptrs ? P->outJ.p : nullptr, *ok = dev_ptrs ? P->outK.p : nullptr;
+        std::vector<double> hj, hk;
+        if (!dev_ptrs) {
+                hj.resize((size_t)P->nao * P->nao);
+                hk.resize((size_t)P->nao * P->nao);
+                oj = hj.data();
+                ok = hk.data();
+        }
+        P->kvar.assign(nclass, 0);
+        if ((rc = b200jk_get_jk(P, dm, 1, 1, 1, 1, oj, ok, dev_ptrs, B200JK_PREC_FP64, stream))) goto done;   // warm-up
+        for (int v = 0; v < 2; v++) {
+                P->kvar.assign(nclass, v);
+                if ((rc = b200jk_get_jk(P, dm, 1, 1, 1, 1, oj, ok, dev_ptrs, B200JK_PREC_FP64, stream))) goto done;
+                for (int t = 0; t < nclass; t++) {
+                        int la, lb, lc, ld;
+                        class_l(qcs[t].X, la, lb);
+                        class_l(qcs[t].Y, lc, ld);
+                        if (v == 1 && family_ket_run(la, lb, lc, ld) == 1) continue;   // no such variant
+                        if (P->cls[t].ms < best_ms[t]) { best_ms[t] = P->cls[t].ms; best[t] = v; }
+                }
+        }
+        P->kvar = best;
+done:
+        P->profiling = saved_prof;
+        if (rc) P->kvar.assign(nclass, 0);
+        return rc;
+}
+
+int b200jk_get_tuning(const b200jk_plan *P, int *variants, int max, int *n)
+{
+        if (!P || !n) return fail(B200JK_EINVAL, "NULL argument");
+        *n = (int)quartet_classes().size();
+        for (int t = 0; t < *n && t < max && variants; t++) variants[t] = t < (int)P->kvar.size() ? P->kvar[t] : 0;
         return B200JK_OK;
 }
 
@@ -1077,7 +1154,7 @@ static int upload_pairs(const b200jk_plan *P, PairClassDev &c, int X, const std:
         }
         int r;
         if ((r = dev_upload(c.sh, sh)) || (r = dev_upload(c.pr, pr)) || (r = dev_upload(c.q, q)) ||
-            (r = dev_upload(c.A, Av)) || (r = dev_upload(c.AB, ABv)))
+            (r = dev_upload(c.qs, q)) || (r = dev_upload(c.A, Av)) || (r = dev_upload(c.AB, ABv)))
                 return r;
         return B200JK_OK;
 }
@@ -1561,7 +1638,8 @@ extern "C" int b200jk_batch_get_jk(b200jk_batch *B, const double *const *dms, in
                 int la, lb, lc, ld;
                 class_l(qcs[t].X, la, lb);
                 class_l(qcs[t].Y, lc, ld);
-                const int chunk = family_chunk(la, lb, lc, ld);
+                const int variant = t < B->plans[0]->kvar.size() ? B->plans[0]->kvar[t] : 0;
+                const int chunk = family_chunk(la, lb, lc, ld, variant);
                 for (int pass = 0; pass < (mixed ? 2 : 1); pass++) {
                         const int nm = ncnt[2 * t + pass];
                         if (nm == 0) continue;
@@ -1577,7 +1655,8 @@ extern "C" int b200jk_batch_get_jk(b200jk_batch *B, const double *const *dms, in
                         batch_chunk_starts<<<grid_for(nm + 1, 128), 128, 0, s>>>(B->chunk_off.p, dseg, nm, B->mchunk.p);
                         CUDA_TRY(cudaGetLastError());
                         const JKArgs &a0 = B->h_args[at[2 * t + pass]];
-                        if ((rc = dispatch_jk(B->plans[0], la, lb, lc, ld, a0, pass, s, dargs, B->mchunk.p, nm))) return rc;
+                        if ((rc = dispatch_jk(B->plans[0], la, lb, lc, ld, a0, pass, s, dargs, B->mchunk.p, nm, variant)))
+                                return rc;
                         launches += 3;
                 }
         }

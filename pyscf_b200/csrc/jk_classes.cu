@@ -22,7 +22,7 @@ struct LaunchCfg {
 // R is the evaluation type: double for the FP64 pass, float for the FP32 pass
 // of mixed precision (accumulation stays in float64 either way).  MULTI: one
 // launch over a batch of molecules (margs, mchunk, nmol on the device).
-template <int LA, int LB, int LC, int LD, typename R, bool MULTI>
+template <int LA, int LB, int LC, int LD, typename R, bool MULTI, int KR>
 int launch_one(const JKArgs &a, const JKArgs *margs, const long long *mchunk, int nmol, cudaStream_t s, int nsm,
                std::string &err)
 {
@@ -38,11 +38,11 @@ int launch_one(const JKArgs &a, const JKArgs *margs, const long long *mchunk, in
                         if constexpr (thread) {
                                 cfg.block = 128;
                                 cfg.smem = stage_table<R>(K::NR) ? sizeof(R) * rys_slice_elems<R>(K::NR) : 0;
-                                cfg.status = cudaFuncSetAttribute(jk_thread_kernel<LA, LB, LC, LD, (NP > 0 ? NP : 1), R, MULTI>,
+                                cfg.status = cudaFuncSetAttribute(jk_thread_kernel<LA, LB, LC, LD, (NP > 0 ? NP : 1), R, MULTI, KR>,
                                                                   cudaFuncAttributeMaxDynamicSharedMemorySize, (int)cfg.smem);
                                 if (cfg.status == cudaSuccess)
                                         cfg.status = cudaOccupancyMaxActiveBlocksPerMultiprocessor(
-                                                &nb, jk_thread_kernel<LA, LB, LC, LD, (NP > 0 ? NP : 1), R, MULTI>, 128, cfg.smem);
+                                                &nb, jk_thread_kernel<LA, LB, LC, LD, (NP > 0 ? NP : 1), R, MULTI, KR>, 128, cfg.smem);
                         } else {
                                 const size_t per_warp = sizeof(double) * WarpSmem<LA, LB, LC, LD, R>::SIZE *
                                                         (32 / group_size<LA, LB, LC, LD>());
@@ -64,7 +64,7 @@ int launch_one(const JKArgs &a, const JKArgs *margs, const long long *mchunk, in
                 return 1;
         }
         if constexpr (thread) {
-                jk_thread_kernel<LA, LB, LC, LD, NP, R, MULTI><<<cfg.grid, cfg.block, cfg.smem, s>>>(a, margs, mchunk, nmol);
+                jk_thread_kernel<LA, LB, LC, LD, NP, R, MULTI, KR><<<cfg.grid, cfg.block, cfg.smem, s>>>(a, margs, mchunk, nmol);
         } else {
                 jk_warp_kernel<LA, LB, LC, LD, R, MULTI><<<cfg.grid, cfg.block, cfg.smem, s>>>(
                         a, 8 * (32 / group_size<LA, LB, LC, LD>()), margs, mchunk, nmol);
@@ -80,12 +80,20 @@ int launch_one(const JKArgs &a, const JKArgs *margs, const long long *mchunk, in
 } // namespace
 
 // B2_FN_NAME is launch_jk_<la><lb><lc><ld>, declared in jk_launch.h
-int B2_FN_NAME(const JKArgs &a, cudaStream_t s, int nsm, int fp32, const JKArgs *margs, const long long *mchunk,
-               int nmol, std::string &err)
+int B2_FN_NAME(const JKArgs &a, cudaStream_t s, int nsm, int fp32, int variant, const JKArgs *margs,
+               const long long *mchunk, int nmol, std::string &err)
 {
-#define B2_L(R, M) launch_one<B2_BRA_LA, B2_BRA_LB, B2_KET_LC, B2_KET_LD, R, M>(a, margs, mchunk, nmol, s, nsm, err)
-        if (nmol > 0) return fp32 ? B2_L(float, true) : B2_L(double, true);
-        return fp32 ? B2_L(float, false) : B2_L(double, false);
+        constexpr int NP = thread_parts<B2_BRA_LA, B2_BRA_LB, B2_KET_LC, B2_KET_LD>();
+        constexpr int KRUN = NP > 0 ? ket_run<B2_BRA_LA, B2_BRA_LB, B2_KET_LC, B2_KET_LD, NP>() : 1;
+#define B2_L(R, M, KR) launch_one<B2_BRA_LA, B2_BRA_LB, B2_KET_LC, B2_KET_LD, R, M, KR>(a, margs, mchunk, nmol, s, nsm, err)
+        if constexpr (KRUN > 1) {
+                if (variant == 1) {
+                        if (nmol > 0) return fp32 ? B2_L(float, true, KRUN) : B2_L(double, true, KRUN);
+                        return fp32 ? B2_L(float, false, KRUN) : B2_L(double, false, KRUN);
+                }
+        }
+        if (nmol > 0) return fp32 ? B2_L(float, true, 1) : B2_L(double, true, 1);
+        return fp32 ? B2_L(float, false, 1) : B2_L(double, false, 1);
 #undef B2_L
 }
 

@@ -42,7 +42,8 @@ __host__ __device__ inline int prim_bucket(int nprim_pairs)
 struct PairView {
         const int4 *sh;      // (cart AO of i, cart AO of j, parent shell i, parent shell j)
         const int2 *pr;      // (first primitive pair, number of primitive pairs)
-        const double *q;     // parent-shell Schwarz bound (descending inside a bucket)
+        const double *q;     // parent-shell Schwarz bound
+        const double *qs;    // prefix-search key: non-increasing inside a bucket, >= q
         const double4 *A;    // (A, 1 if i == j else 0)
         const double4 *AB;   // (A - B, 0)
         int n;
@@ -153,7 +154,7 @@ __device__ __forceinline__ void count_segment(const PairView &bra, const PairVie
                 int lo = lo0, hi = hi0;
                 while (lo < hi) {
                         int mid = (lo + hi) >> 1;
-                        if (ket.q[mid] > thr) lo = mid + 1;
+                        if (ket.qs[mid] > thr) lo = mid + 1;
                         else hi = mid;
                 }
                 cnt = lo - lo0;
@@ -170,7 +171,7 @@ __device__ __forceinline__ void count_segment(const PairView &bra, const PairVie
                         hi = lo0 + cnt;
                         while (lo < hi) {
                                 int mid = (lo + hi) >> 1;
-                                if (ket.q[mid] >= thr32) lo = mid + 1;
+                                if (ket.qs[mid] >= thr32) lo = mid + 1;
                                 else hi = mid;
                         }
                         n64 = lo - lo0;
@@ -240,12 +241,27 @@ template <typename R> __host__ __device__ constexpr bool stage_table(int nr)
 template <> __device__ __forceinline__ const double *table_of<double>(const JKArgs &a) { return a.table; }
 template <> __device__ __forceinline__ const float *table_of<float>(const JKArgs &a) { return a.table_f; }
 
+// Kets per lane of the register family (the autotuner picks 1 or ket_run<>
+// per class).  With M > 1 a lane evaluates M
+// consecutive kets of its bra pair; kets of one bound band are ordered by
+// first segment, so consecutive kets mostly share it, and the lane carries
+// its K[a,c] and K[b,c] sums in registers while the segment stays the same
+// (one atomic per run instead of one per quartet: the contraction is bound
+// by the number of L2 atomics).  Classes kept whole in registers (NP = 1)
+// whose carried sums are at most 24 doubles.
+template <int LA, int LB, int LC, int LD, int NP>
+__host__ __device__ constexpr int ket_run()
+{
+        using K = Class4<LA, LB, LC, LD>;
+        return (NP == 1 && K::NA * K::NC + K::NB * K::NC <= 24) ? 4 : 1;
+}
+
 // MULTI: one launch for a batch of molecules (b200jk_batch_get_jk).
 // margs[m] holds the arguments of molecule m (its pair tables, matrices and
 // slices of the batch's chunk arrays, whose chunk numbers are global) and
 // mchunk[m] its first chunk in the batch's chunk queue, mchunk[nmol] the end;
 // a0 carries the shared fields (tables, statistics).
-template <int LA, int LB, int LC, int LD, int NP, typename R, bool MULTI>
+template <int LA, int LB, int LC, int LD, int NP, typename R, bool MULTI, int KR>
 __global__ void __launch_bounds__(128) jk_thread_kernel(JKArgs a0, const JKArgs *__restrict__ margs,
                                                         const long long *__restrict__ mchunk, int nmol)
 {
@@ -277,7 +293,26 @@ __global__ void __launch_bounds__(128) jk_thread_kernel(JKArgs a0, const JKArgs 
                 const size_t n = (size_t)a.naoc, nn = n * n;
                 const int sgi = find_bra(a.chunk_off, nseg, chunk);
                 const int ij = sgi / B2_NBUCKET;
-                const int pos = (int)(chunk - a.chunk_off[sgi]) * 32 + lane;
+                constexpr int M = KR;
+                const bool carry = M > 1 && a.n_dm == 1 && a.nk == 1 && a.with_k;
+                double acc_a[K::NA * K::NC], acc_b[K::NB * K::NC];
+                int cur_c = -1;
+                const int4 sb0 = a.bra.sh[ij];
+                auto flush = [&]() {
+                        if (cur_c < 0) return;
+#pragma unroll
+                        for (int x = 0; x < K::NA; x++)
+#pragma unroll
+                                for (int c = 0; c < K::NC; c++)
+                                        atomicAdd(a.Kacc + (sb0.x + x) * n + cur_c + c, acc_a[x * K::NC + c]);
+#pragma unroll
+                        for (int b = 0; b < K::NB; b++)
+#pragma unroll
+                                for (int c = 0; c < K::NC; c++)
+                                        atomicAdd(a.Kacc + (sb0.y + b) * n + cur_c + c, acc_b[b * K::NC + c]);
+                };
+              for (int jk = 0; jk < M; jk++) {
+                const int pos = (int)(chunk - a.chunk_off[sgi]) * (32 * M) + lane * M + jk;
                 const int kl = a.ket.boff[sgi % B2_NBUCKET] + a.kst[sgi] + pos;
                 const int4 sb = a.bra.sh[ij];
                 const int2 pb = a.bra.pr[ij];
@@ -310,6 +345,14 @@ __global__ void __launch_bounds__(128) jk_thread_kernel(JKArgs a0, const JKArgs 
                         npq += (unsigned long long)pb.y * pk.y;
                 }
                 const int ia = sb.x, ib = sb.y, ic = sk.x, id = sk.y;
+                if (carry && active && ic != cur_c) {
+                        flush();
+                        cur_c = ic;
+#pragma unroll
+                        for (int t = 0; t < K::NA * K::NC; t++) acc_a[t] = 0.0;
+#pragma unroll
+                        for (int t = 0; t < K::NB * K::NC; t++) acc_b[t] = 0.0;
+                }
                 for_parts([&](auto part_tag) {
                         constexpr int PART = decltype(part_tag)::value;
                         constexpr int A0 = PART * NAP;
@@ -415,7 +458,8 @@ __global__ void __launch_bounds__(128) jk_thread_kernel(JKArgs a0, const JKArgs 
 #pragma unroll
                                                                         for (int d = 0; d < K::ND; d++)
                                                                                 v += (double)Gp[((x * K::NB + b) * K::NC + c) * K::ND + d] * x_[b * K::ND + d];
-                                                                atomicAdd(Kt + (ia + A0 + x) * n + ic + c, v);
+                                                                if (carry) acc_a[(A0 + x) * K::NC + c] += v;
+                                                                else atomicAdd(Kt + (ia + A0 + x) * n + ic + c, v);
                                                         }
                                                 }
                                                 // K[b,d] += G X[a,c]  (this part's a only)
@@ -455,13 +499,16 @@ __global__ void __launch_bounds__(128) jk_thread_kernel(JKArgs a0, const JKArgs 
 #pragma unroll
                                                                         for (int d = 0; d < K::ND; d++)
                                                                                 v += (double)Gp[((x * K::NB + b) * K::NC + c) * K::ND + d] * x_[x * K::ND + d];
-                                                                atomicAdd(Kt + (ib + b) * n + ic + c, v);
+                                                                if (carry) acc_b[b * K::NC + c] += v;
+                                                                else atomicAdd(Kt + (ib + b) * n + ic + c, v);
                                                         }
                                                 }
                                         }
                                 }
                         }
                 }, std::make_integer_sequence<int, NP>{});
+              }
+                if (carry) flush();
               };
                 if constexpr (MULTI) body(margs[find_bra(mchunk, nmol, chunk)]);
                 else body(a0);

@@ -29,123 +29,134 @@ inline int family_group(int la, int lb, int lc, int ld)
         const int ng = ncart(la) * ncart(lb) * ncart(lc) * ncart(ld);
         return ng <= 100 ? 8 : (ng <= 400 ? 16 : 32);
 }
-// quartets per chunk: 32 (one per lane) or 8 per group of the warp
-inline int family_chunk(int la, int lb, int lc, int ld)
+// kets per lane of variant 1 of the register family (host twin of ket_run<>);
+// 1 where the class has no such variant
+inline int family_ket_run(int la, int lb, int lc, int ld)
 {
-        return family_is_thread(la, lb, lc, ld) ? 32 : 8 * (32 / family_group(la, lb, lc, ld));
+        const int np = family_thread_parts(la, lb, lc, ld);
+        const int na = ncart(la), nb = ncart(lb), nc = ncart(lc);
+        return (np == 1 && na * nc + nb * nc <= 24) ? 4 : 1;
+}
+// quartets per chunk: 32 x kets per lane in the register family (variant 0:
+// one ket per lane, 1: family_ket_run), 8 per group of the warp otherwise
+inline int family_chunk(int la, int lb, int lc, int ld, int variant = 0)
+{
+        if (family_thread_parts(la, lb, lc, ld) > 0)
+                return 32 * (variant == 1 ? family_ket_run(la, lb, lc, ld) : 1);
+        return 8 * (32 / family_group(la, lb, lc, ld));
 }
 
 // one launcher per quartet class (la lb | lc ld), (lc, ld) <= (la, lb)
-int launch_jk_0000(const JKArgs &a, cudaStream_t s, int nsm, int fp32, const JKArgs *margs,
-                   const long long *mchunk, int nmol, std::string &err);
-int launch_jk_1000(const JKArgs &a, cudaStream_t s, int nsm, int fp32, const JKArgs *margs,
-                   const long long *mchunk, int nmol, std::string &err);
-int launch_jk_1010(const JKArgs &a, cudaStream_t s, int nsm, int fp32, const JKArgs *margs,
-                   const long long *mchunk, int nmol, std::string &err);
-int launch_jk_1100(const JKArgs &a, cudaStream_t s, int nsm, int fp32, const JKArgs *margs,
-                   const long long *mchunk, int nmol, std::string &err);
-int launch_jk_1110(const JKArgs &a, cudaStream_t s, int nsm, int fp32, const JKArgs *margs,
-                   const long long *mchunk, int nmol, std::string &err);
-int launch_jk_1111(const JKArgs &a, cudaStream_t s, int nsm, int fp32, const JKArgs *margs,
-                   const long long *mchunk, int nmol, std::string &err);
-int launch_jk_2000(const JKArgs &a, cudaStream_t s, int nsm, int fp32, const JKArgs *margs,
-                   const long long *mchunk, int nmol, std::string &err);
-int launch_jk_2010(const JKArgs &a, cudaStream_t s, int nsm, int fp32, const JKArgs *margs,
-                   const long long *mchunk, int nmol, std::string &err);
-int launch_jk_2011(const JKArgs &a, cudaStream_t s, int nsm, int fp32, const JKArgs *margs,
-                   const long long *mchunk, int nmol, std::string &err);
-int launch_jk_2020(const JKArgs &a, cudaStream_t s, int nsm, int fp32, const JKArgs *margs,
-                   const long long *mchunk, int nmol, std::string &err);
-int launch_jk_2100(const JKArgs &a, cudaStream_t s, int nsm, int fp32, const JKArgs *margs,
-                   const long long *mchunk, int nmol, std::string &err);
-int launch_jk_2110(const JKArgs &a, cudaStream_t s, int nsm, int fp32, const JKArgs *margs,
-                   const long long *mchunk, int nmol, std::string &err);
-int launch_jk_2111(const JKArgs &a, cudaStream_t s, int nsm, int fp32, const JKArgs *margs,
-                   const long long *mchunk, int nmol, std::string &err);
-int launch_jk_2120(const JKArgs &a, cudaStream_t s, int nsm, int fp32, const JKArgs *margs,
-                   const long long *mchunk, int nmol, std::string &err);
-int launch_jk_2121(const JKArgs &a, cudaStream_t s, int nsm, int fp32, const JKArgs *margs,
-                   const long long *mchunk, int nmol, std::string &err);
-int launch_jk_2200(const JKArgs &a, cudaStream_t s, int nsm, int fp32, const JKArgs *margs,
-                   const long long *mchunk, int nmol, std::string &err);
-int launch_jk_2210(const JKArgs &a, cudaStream_t s, int nsm, int fp32, const JKArgs *margs,
-                   const long long *mchunk, int nmol, std::string &err);
-int launch_jk_2211(const JKArgs &a, cudaStream_t s, int nsm, int fp32, const JKArgs *margs,
-                   const long long *mchunk, int nmol, std::string &err);
-int launch_jk_2220(const JKArgs &a, cudaStream_t s, int nsm, int fp32, const JKArgs *margs,
-                   const long long *mchunk, int nmol, std::string &err);
-int launch_jk_2221(const JKArgs &a, cudaStream_t s, int nsm, int fp32, const JKArgs *margs,
-                   const long long *mchunk, int nmol, std::string &err);
-int launch_jk_2222(const JKArgs &a, cudaStream_t s, int nsm, int fp32, const JKArgs *margs,
-                   const long long *mchunk, int nmol, std::string &err);
-int launch_jk_3000(const JKArgs &a, cudaStream_t s, int nsm, int fp32, const JKArgs *margs,
-                   const long long *mchunk, int nmol, std::string &err);
-int launch_jk_3010(const JKArgs &a, cudaStream_t s, int nsm, int fp32, const JKArgs *margs,
-                   const long long *mchunk, int nmol, std::string &err);
-int launch_jk_3011(const JKArgs &a, cudaStream_t s, int nsm, int fp32, const JKArgs *margs,
-                   const long long *mchunk, int nmol, std::string &err);
-int launch_jk_3020(const JKArgs &a, cudaStream_t s, int nsm, int fp32, const JKArgs *margs,
-                   const long long *mchunk, int nmol, std::string &err);
-int launch_jk_3021(const JKArgs &a, cudaStream_t s, int nsm, int fp32, const JKArgs *margs,
-                   const long long *mchunk, int nmol, std::string &err);
-int launch_jk_3022(const JKArgs &a, cudaStream_t s, int nsm, int fp32, const JKArgs *margs,
-                   const long long *mchunk, int nmol, std::string &err);
-int launch_jk_3030(const JKArgs &a, cudaStream_t s, int nsm, int fp32, const JKArgs *margs,
-                   const long long *mchunk, int nmol, std::string &err);
-int launch_jk_3100(const JKArgs &a, cudaStream_t s, int nsm, int fp32, const JKArgs *margs,
-                   const long long *mchunk, int nmol, std::string &err);
-int launch_jk_3110(const JKArgs &a, cudaStream_t s, int nsm, int fp32, const JKArgs *margs,
-                   const long long *mchunk, int nmol, std::string &err);
-int launch_jk_3111(const JKArgs &a, cudaStream_t s, int nsm, int fp32, const JKArgs *margs,
-                   const long long *mchunk, int nmol, std::string &err);
-int launch_jk_3120(const JKArgs &a, cudaStream_t s, int nsm, int fp32, const JKArgs *margs,
-                   const long long *mchunk, int nmol, std::string &err);
-int launch_jk_3121(const JKArgs &a, cudaStream_t s, int nsm, int fp32, const JKArgs *margs,
-                   const long long *mchunk, int nmol, std::string &err);
-int launch_jk_3122(const JKArgs &a, cudaStream_t s, int nsm, int fp32, const JKArgs *margs,
-                   const long long *mchunk, int nmol, std::string &err);
-int launch_jk_3130(const JKArgs &a, cudaStream_t s, int nsm, int fp32, const JKArgs *margs,
-                   const long long *mchunk, int nmol, std::string &err);
-int launch_jk_3131(const JKArgs &a, cudaStream_t s, int nsm, int fp32, const JKArgs *margs,
-                   const long long *mchunk, int nmol, std::string &err);
-int launch_jk_3200(const JKArgs &a, cudaStream_t s, int nsm, int fp32, const JKArgs *margs,
-                   const long long *mchunk, int nmol, std::string &err);
-int launch_jk_3210(const JKArgs &a, cudaStream_t s, int nsm, int fp32, const JKArgs *margs,
-                   const long long *mchunk, int nmol, std::string &err);
-int launch_jk_3211(const JKArgs &a, cudaStream_t s, int nsm, int fp32, const JKArgs *margs,
-                   const long long *mchunk, int nmol, std::string &err);
-int launch_jk_3220(const JKArgs &a, cudaStream_t s, int nsm, int fp32, const JKArgs *margs,
-                   const long long *mchunk, int nmol, std::string &err);
-int launch_jk_3221(const JKArgs &a, cudaStream_t s, int nsm, int fp32, const JKArgs *margs,
-                   const long long *mchunk, int nmol, std::string &err);
-int launch_jk_3222(const JKArgs &a, cudaStream_t s, int nsm, int fp32, const JKArgs *margs,
-                   const long long *mchunk, int nmol, std::string &err);
-int launch_jk_3230(const JKArgs &a, cudaStream_t s, int nsm, int fp32, const JKArgs *margs,
-                   const long long *mchunk, int nmol, std::string &err);
-int launch_jk_3231(const JKArgs &a, cudaStream_t s, int nsm, int fp32, const JKArgs *margs,
-                   const long long *mchunk, int nmol, std::string &err);
-int launch_jk_3232(const JKArgs &a, cudaStream_t s, int nsm, int fp32, const JKArgs *margs,
-                   const long long *mchunk, int nmol, std::string &err);
-int launch_jk_3300(const JKArgs &a, cudaStream_t s, int nsm, int fp32, const JKArgs *margs,
-                   const long long *mchunk, int nmol, std::string &err);
-int launch_jk_3310(const JKArgs &a, cudaStream_t s, int nsm, int fp32, const JKArgs *margs,
-                   const long long *mchunk, int nmol, std::string &err);
-int launch_jk_3311(const JKArgs &a, cudaStream_t s, int nsm, int fp32, const JKArgs *margs,
-                   const long long *mchunk, int nmol, std::string &err);
-int launch_jk_3320(const JKArgs &a, cudaStream_t s, int nsm, int fp32, const JKArgs *margs,
-                   const long long *mchunk, int nmol, std::string &err);
-int launch_jk_3321(const JKArgs &a, cudaStream_t s, int nsm, int fp32, const JKArgs *margs,
-                   const long long *mchunk, int nmol, std::string &err);
-int launch_jk_3322(const JKArgs &a, cudaStream_t s, int nsm, int fp32, const JKArgs *margs,
-                   const long long *mchunk, int nmol, std::string &err);
-int launch_jk_3330(const JKArgs &a, cudaStream_t s, int nsm, int fp32, const JKArgs *margs,
-                   const long long *mchunk, int nmol, std::string &err);
-int launch_jk_3331(const JKArgs &a, cudaStream_t s, int nsm, int fp32, const JKArgs *margs,
-                   const long long *mchunk, int nmol, std::string &err);
-int launch_jk_3332(const JKArgs &a, cudaStream_t s, int nsm, int fp32, const JKArgs *margs,
-                   const long long *mchunk, int nmol, std::string &err);
-int launch_jk_3333(const JKArgs &a, cudaStream_t s, int nsm, int fp32, const JKArgs *margs,
-                   const long long *mchunk, int nmol, std::string &err);
+int launch_jk_0000(const JKArgs &a, cudaStream_t s, int nsm, int fp32, int variant,
+                   const JKArgs *margs, const long long *mchunk, int nmol, std::string &err);
+int launch_jk_1000(const JKArgs &a, cudaStream_t s, int nsm, int fp32, int variant,
+                   const JKArgs *margs, const long long *mchunk, int nmol, std::string &err);
+int launch_jk_1010(const JKArgs &a, cudaStream_t s, int nsm, int fp32, int variant,
+                   const JKArgs *margs, const long long *mchunk, int nmol, std::string &err);
+int launch_jk_1100(const JKArgs &a, cudaStream_t s, int nsm, int fp32, int variant,
+                   const JKArgs *margs, const long long *mchunk, int nmol, std::string &err);
+int launch_jk_1110(const JKArgs &a, cudaStream_t s, int nsm, int fp32, int variant,
+                   const JKArgs *margs, const long long *mchunk, int nmol, std::string &err);
+int launch_jk_1111(const JKArgs &a, cudaStream_t s, int nsm, int fp32, int variant,
+                   const JKArgs *margs, const long long *mchunk, int nmol, std::string &err);
+int launch_jk_2000(const JKArgs &a, cudaStream_t s, int nsm, int fp32, int variant,
+                   const JKArgs *margs, const long long *mchunk, int nmol, std::string &err);
+int launch_jk_2010(const JKArgs &a, cudaStream_t s, int nsm, int fp32, int variant,
+                   const JKArgs *margs, const long long *mchunk, int nmol, std::string &err);
+int launch_jk_2011(const JKArgs &a, cudaStream_t s, int nsm, int fp32, int variant,
+                   const JKArgs *margs, const long long *mchunk, int nmol, std::string &err);
+int launch_jk_2020(const JKArgs &a, cudaStream_t s, int nsm, int fp32, int variant,
+                   const JKArgs *margs, const long long *mchunk, int nmol, std::string &err);
+int launch_jk_2100(const JKArgs &a, cudaStream_t s, int nsm, int fp32, int variant,
+                   const JKArgs *margs, const long long *mchunk, int nmol, std::string &err);
+int launch_jk_2110(const JKArgs &a, cudaStream_t s, int nsm, int fp32, int variant,
+                   const JKArgs *margs, const long long *mchunk, int nmol, std::string &err);
+int launch_jk_2111(const JKArgs &a, cudaStream_t s, int nsm, int fp32, int variant,
+                   const JKArgs *margs, const long long *mchunk, int nmol, std::string &err);
+int launch_jk_2120(const JKArgs &a, cudaStream_t s, int nsm, int fp32, int variant,
+                   const JKArgs *margs, const long long *mchunk, int nmol, std::string &err);
+int launch_jk_2121(const JKArgs &a, cudaStream_t s, int nsm, int fp32, int variant,
+                   const JKArgs *margs, const long long *mchunk, int nmol, std::string &err);
+int launch_jk_2200(const JKArgs &a, cudaStream_t s, int nsm, int fp32, int variant,
+                   const JKArgs *margs, const long long *mchunk, int nmol, std::string &err);
+int launch_jk_2210(const JKArgs &a, cudaStream_t s, int nsm, int fp32, int variant,
+                   const JKArgs *margs, const long long *mchunk, int nmol, std::string &err);
+int launch_jk_2211(const JKArgs &a, cudaStream_t s, int nsm, int fp32, int variant,
+                   const JKArgs *margs, const long long *mchunk, int nmol, std::string &err);
+int launch_jk_2220(const JKArgs &a, cudaStream_t s, int nsm, int fp32, int variant,
+                   const JKArgs *margs, const long long *mchunk, int nmol, std::string &err);
+int launch_jk_2221(const JKArgs &a, cudaStream_t s, int nsm, int fp32, int variant,
+                   const JKArgs *margs, const long long *mchunk, int nmol, std::string &err);
+int launch_jk_2222(const JKArgs &a, cudaStream_t s, int nsm, int fp32, int variant,
+                   const JKArgs *margs, const long long *mchunk, int nmol, std::string &err);
+int launch_jk_3000(const JKArgs &a, cudaStream_t s, int nsm, int fp32, int variant,
+                   const JKArgs *margs, const long long *mchunk, int nmol, std::string &err);
+int launch_jk_3010(const JKArgs &a, cudaStream_t s, int nsm, int fp32, int variant,
+                   const JKArgs *margs, const long long *mchunk, int nmol, std::string &err);
+int launch_jk_3011(const JKArgs &a, cudaStream_t s, int nsm, int fp32, int variant,
+                   const JKArgs *margs, const long long *mchunk, int nmol, std::string &err);
+int launch_jk_3020(const JKArgs &a, cudaStream_t s, int nsm, int fp32, int variant,
+                   const JKArgs *margs, const long long *mchunk, int nmol, std::string &err);
+int launch_jk_3021(const JKArgs &a, cudaStream_t s, int nsm, int fp32, int variant,
+                   const JKArgs *margs, const long long *mchunk, int nmol, std::string &err);
+int launch_jk_3022(const JKArgs &a, cudaStream_t s, int nsm, int fp32, int variant,
+                   const JKArgs *margs, const long long *mchunk, int nmol, std::string &err);
+int launch_jk_3030(const JKArgs &a, cudaStream_t s, int nsm, int fp32, int variant,
+                   const JKArgs *margs, const long long *mchunk, int nmol, std::string &err);
+int launch_jk_3100(const JKArgs &a, cudaStream_t s, int nsm, int fp32, int variant,
+                   const JKArgs *margs, const long long *mchunk, int nmol, std::string &err);
+int launch_jk_3110(const JKArgs &a, cudaStream_t s, int nsm, int fp32, int variant,
+                   const JKArgs *margs, const long long *mchunk, int nmol, std::string &err);
+int launch_jk_3111(const JKArgs &a, cudaStream_t s, int nsm, int fp32, int variant,
+                   const JKArgs *margs, const long long *mchunk, int nmol, std::string &err);
+int launch_jk_3120(const JKArgs &a, cudaStream_t s, int nsm, int fp32, int variant,
+                   const JKArgs *margs, const long long *mchunk, int nmol, std::string &err);
+int launch_jk_3121(const JKArgs &a, cudaStream_t s, int nsm, int fp32, int variant,
+                   const JKArgs *margs, const long long *mchunk, int nmol, std::string &err);
+int launch_jk_3122(const JKArgs &a, cudaStream_t s, int nsm, int fp32, int variant,
+                   const JKArgs *margs, const long long *mchunk, int nmol, std::string &err);
+int launch_jk_3130(const JKArgs &a, cudaStream_t s, int nsm, int fp32, int variant,
+                   const JKArgs *margs, const long long *mchunk, int nmol, std::string &err);
+int launch_jk_3131(const JKArgs &a, cudaStream_t s, int nsm, int fp32, int variant,
+                   const JKArgs *margs, const long long *mchunk, int nmol, std::string &err);
+int launch_jk_3200(const JKArgs &a, cudaStream_t s, int nsm, int fp32, int variant,
+                   const JKArgs *margs, const long long *mchunk, int nmol, std::string &err);
+int launch_jk_3210(const JKArgs &a, cudaStream_t s, int nsm, int fp32, int variant,
+                   const JKArgs *margs, const long long *mchunk, int nmol, std::string &err);
+int launch_jk_3211(const JKArgs &a, cudaStream_t s, int nsm, int fp32, int variant,
+                   const JKArgs *margs, const long long *mchunk, int nmol, std::string &err);
+int launch_jk_3220(const JKArgs &a, cudaStream_t s, int nsm, int fp32, int variant,
+                   const JKArgs *margs, const long long *mchunk, int nmol, std::string &err);
+int launch_jk_3221(const JKArgs &a, cudaStream_t s, int nsm, int fp32, int variant,
+                   const JKArgs *margs, const long long *mchunk, int nmol, std::string &err);
+int launch_jk_3222(const JKArgs &a, cudaStream_t s, int nsm, int fp32, int variant,
+                   const JKArgs *margs, const long long *mchunk, int nmol, std::string &err);
+int launch_jk_3230(const JKArgs &a, cudaStream_t s, int nsm, int fp32, int variant,
+                   const JKArgs *margs, const long long *mchunk, int nmol, std::string &err);
+int launch_jk_3231(const JKArgs &a, cudaStream_t s, int nsm, int fp32, int variant,
+                   const JKArgs *margs, const long long *mchunk, int nmol, std::string &err);
+int launch_jk_3232(const JKArgs &a, cudaStream_t s, int nsm, int fp32, int variant,
+                   const JKArgs *margs, const long long *mchunk, int nmol, std::string &err);
+int launch_jk_3300(const JKArgs &a, cudaStream_t s, int nsm, int fp32, int variant,
+                   const JKArgs *margs, const long long *mchunk, int nmol, std::string &err);
+int launch_jk_3310(const JKArgs &a, cudaStream_t s, int nsm, int fp32, int variant,
+                   const JKArgs *margs, const long long *mchunk, int nmol, std::string &err);
+int launch_jk_3311(const JKArgs &a, cudaStream_t s, int nsm, int fp32, int variant,
+                   const JKArgs *margs, const long long *mchunk, int nmol, std::string &err);
+int launch_jk_3320(const JKArgs &a, cudaStream_t s, int nsm, int fp32, int variant,
+                   const JKArgs *margs, const long long *mchunk, int nmol, std::string &err);
+int launch_jk_3321(const JKArgs &a, cudaStream_t s, int nsm, int fp32, int variant,
+                   const JKArgs *margs, const long long *mchunk, int nmol, std::string &err);
+int launch_jk_3322(const JKArgs &a, cudaStream_t s, int nsm, int fp32, int variant,
+                   const JKArgs *margs, const long long *mchunk, int nmol, std::string &err);
+int launch_jk_3330(const JKArgs &a, cudaStream_t s, int nsm, int fp32, int variant,
+                   const JKArgs *margs, const long long *mchunk, int nmol, std::string &err);
+int launch_jk_3331(const JKArgs &a, cudaStream_t s, int nsm, int fp32, int variant,
+                   const JKArgs *margs, const long long *mchunk, int nmol, std::string &err);
+int launch_jk_3332(const JKArgs &a, cudaStream_t s, int nsm, int fp32, int variant,
+                   const JKArgs *margs, const long long *mchunk, int nmol, std::string &err);
+int launch_jk_3333(const JKArgs &a, cudaStream_t s, int nsm, int fp32, int variant,
+                   const JKArgs *margs, const long long *mchunk, int nmol, std::string &err);
 
 int launch_qcond(int la, int lb, const QArgs &q, cudaStream_t s, std::string &err);
 

@@ -27,7 +27,7 @@ EXPORTS = (
     'b200jk_stats', 'b200jk_hostcheck_cart_quartet', 'b200jk_class_stats', 'b200jk_set_profiling',
     'b200jk_measure_fp64_peak', 'b200jk_get_jk_noalloc', 'b200jk_set_mixed_threshold',
     'b200jk_hostcheck_cart_quartet_fp32', 'b200jk_grad_jk', 'b200jk_grad_stats', 'b200jk_get_grad_q_cond',
-    'b200jk_set_shard', 'b200jk_grad_class_stats', 'b200jk_batch_create', 'b200jk_batch_destroy', 'b200jk_batch_get_jk', 'b200jk_batch_stats',
+    'b200jk_set_shard', 'b200jk_grad_class_stats', 'b200jk_autotune', 'b200jk_get_tuning', 'b200jk_batch_create', 'b200jk_batch_destroy', 'b200jk_batch_get_jk', 'b200jk_batch_stats',
 )
 
 
@@ -89,6 +89,8 @@ def load(path=LIB_PATH):
         lib.b200jk_get_grad_q_cond.argtypes = [vp, vp]
         lib.b200jk_set_shard.argtypes = [vp, ip, ip]
         lib.b200jk_grad_class_stats.argtypes = [vp, ctypes.POINTER(ClassStat), ip, ctypes.POINTER(ip)]
+        lib.b200jk_autotune.argtypes = [vp, vp, ip, vp]
+        lib.b200jk_get_tuning.argtypes = [vp, ctypes.POINTER(ip), ip, ctypes.POINTER(ip)]
         lib.b200jk_batch_create.argtypes = [vp, ip, ctypes.POINTER(vp)]
         lib.b200jk_batch_destroy.argtypes = [vp]
         lib.b200jk_batch_get_jk.argtypes = [vp, vp, ip, ip, ip, vp, vp, ip, vp]
@@ -166,6 +168,29 @@ class Plan:
 
     def set_profiling(self, on=True):
         check(load().b200jk_set_profiling(self._h, int(bool(on))))
+
+    def autotune(self, dm):
+        """Pick the faster launch variant per quartet class on one FP64 build
+        of `dm` (host array or CUDA tensor); returns the variants."""
+        try:
+            import torch
+            is_dev = isinstance(dm, torch.Tensor) and dm.is_cuda
+        except ImportError:
+            is_dev = False
+        if is_dev:
+            d = dm.contiguous()
+            stream = torch.cuda.current_stream(d.device).cuda_stream
+            check(load().b200jk_autotune(self._h, ctypes.c_void_p(d.data_ptr()), 1, ctypes.c_void_p(stream)))
+        else:
+            d = numpy.ascontiguousarray(dm, dtype=numpy.double)
+            check(load().b200jk_autotune(self._h, _ptr(d), 0, None))
+        return self.tuning()
+
+    def tuning(self):
+        n = ctypes.c_int(0)
+        buf = (ctypes.c_int * 64)()
+        check(load().b200jk_get_tuning(self._h, buf, 64, ctypes.byref(n)))
+        return list(buf[:n.value])
 
     def set_shard(self, index, count):
         """Evaluate only bra pairs ij = index (mod count): partial J/K for one of count GPUs."""

@@ -178,3 +178,15 @@ def test_sharded_plans_sum_to_full_build(b2):
     vk = parts[0][1] + parts[1][1]
     assert abs(vj - f['vj_ns']).max() < TOL_JK
     assert abs(vk - f['vk_ns']).max() < TOL_JK
+
+
+def test_autotune_keeps_results(b2):
+    """The autotuner only switches launch variants: J/K stay the reference's."""
+    f = load_fixture('h2o8_vdz')
+    p = plan_for(b2, f)
+    tun = p.autotune(f['dm_conv'])
+    assert len(tun) == 55 and set(tun) <= {0, 1}
+    for dm, rj, rk in [(f['dm_rand'], f['vj_rand'], f['vk_rand']), (f['dm_conv'], f['vj_conv'], f['vk_conv'])]:
+        vj, vk = p.get_jk(dm, hermi=1)
+        assert abs(vj - rj).max() < TOL_JK
+        assert abs(vk - rk).max() < TOL_JK
