@@ -144,6 +144,11 @@ int b200jk_set_profiling(b200jk_plan *plan, int on);
  * counterpart (PySCF has no kernel variants to tune). */
 int b200jk_autotune(b200jk_plan *plan, const double *dm, int dev_ptrs, void *stream);
 
+/* Chunk order of the class kernels: tiles of tile_b bra pairs walked
+ * ket-chunk-major, so warps running together share ket data (default 64);
+ * 0 = bra-major order.  Sharded plans always use bra-major order. */
+int b200jk_set_tile(b200jk_plan *plan, int tile_b);
+
 /* The chosen variant per quartet class (55 classes, bra class >= ket class). */
 int b200jk_get_tuning(const b200jk_plan *plan, int *variants, int max, int *n);
 

@@ -236,6 +236,8 @@ struct b200jk_plan {
         // launch variant per quartet class (register family: 0 = one ket per
         // lane, 1 = family_ket_run kets per lane), chosen by b200jk_autotune
         std::vector<int> kvar;
+        // bra pairs per tile of the tiled chunk order (0: bra-major order)
+        int tile_b = 64;
         // packed ket blocks for the J contraction: class X's blocks start at
         // pk_off[X] (entries, in ket-list order); pk_src maps entries to the
         // Cartesian matrix
@@ -888,11 +890,25 @@ int b200jk_get_jk(b200jk_plan *P, const double *dms, int n_dm, int hermi, int wi
                                         chunk, mixed ? P->fp32_tau : 0.0, pass, P->shard, P->nshard, P->nkl.p, P->kst.p,
                                         P->nchunk.p);
                                 CUDA_TRY(cudaGetLastError());
-                                CUDA_TRY(cudaMemsetAsync(P->nchunk.p + nseg, 0, sizeof(long long), s));
+                                // tiled chunk order for unsharded plans (with shards the
+                                // stride over bra pairs would leave tile slots idle)
+                                const int tiled = P->nshard == 1 && P->tile_b > 0;
+                                const int ntb = (bra.n + P->tile_b - 1) / std::max(1, P->tile_b);
+                                const int nscan = tiled ? B2_NBUCKET * ntb : nseg;
+                                if (tiled) {
+                                        tile_count_kernel<<<grid_for(nscan, 256), 256, 0, s>>>(P->nkl.p, bra.n, chunk, P->tile_b,
+                                                                                             ntb, P->nchunk.p);
+                                        CUDA_TRY(cudaGetLastError());
+                                }
+                                CUDA_TRY(cudaMemsetAsync(P->nchunk.p + nscan, 0, sizeof(long long), s));
                                 size_t tmp = P->cub_tmp.n;
                                 CUDA_TRY(cub::DeviceScan::ExclusiveSum(P->cub_tmp.p, tmp, P->nchunk.p, P->chunk_off.p,
-                                                                       nseg + 1, s));
+                                                                       nscan + 1, s));
                                 JKArgs a;
+                                a.tiled = tiled;
+                                a.tile_b = P->tile_b;
+                                a.ntile = nscan;
+                                a.ntb = ntb;
                                 a.bra = bra.view();
                                 a.ket = ket.view();
                                 a.PP = P->PP.p; a.PK = P->PK.p;
@@ -1039,6 +1055,14 @@ done:
         P->profiling = saved_prof;
         if (rc) P->kvar.assign(nclass, 0);
         return rc;
+}
+
+int b200jk_set_tile(b200jk_plan *P, int tile_b)
+{
+        if (!P) return fail(B200JK_EINVAL, "plan is NULL");
+        if (tile_b < 0 || tile_b > 4096) return fail(B200JK_EINVAL, "tile width must be in [0, 4096]");
+        P->tile_b = tile_b;
+        return B200JK_OK;
 }
 
 int b200jk_get_tuning(const b200jk_plan *P, int *variants, int max, int *n)

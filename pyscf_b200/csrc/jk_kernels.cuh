@@ -73,6 +73,12 @@ struct JKArgs {
         const double *Dpk = nullptr;
         double *Jpk = nullptr;
         long long pk_stride = 0;
+        // Tiled chunk order (optional): chunk_off then holds the offsets of
+        // ntile tiles; tile t covers the bra pairs [(t % ntb)*tile_b, +tile_b)
+        // of ket bucket t / ntb, walked ket-chunk-major (chunk k of all its
+        // bra pairs, then chunk k + 1), so concurrent warps share ket data and
+        // the K rows of few bra pairs.  0 = bra-major chunk order.
+        int tiled = 0, tile_b = 16, ntile = 0, ntb = 0;
         double tol;
         int nbas, naoc, n_dm, nk;
         int with_j, with_k, same;
@@ -138,6 +144,36 @@ __device__ __forceinline__ bool quartet_passes(const JKArgs &a, int4 sb, double 
 // (bucket, rank) order.  Sharded over nshard GPUs, rank `shard` takes the bra
 // pairs ij = shard (mod nshard): pairs are sorted by their bound inside a
 // bucket, so striding spreads the cost evenly.
+// Tiled chunk order: tile t gets tile_b x (the most chunks of its bra pairs)
+// chunk slots; slots past a bra pair's own chunks stay idle.
+static __global__ void tile_count_kernel(const int *__restrict__ nkl, int nbra, int chunk, int tile_b, int ntb,
+                                         long long *tile_cnt)
+{
+        const int t = blockIdx.x * blockDim.x + threadIdx.x;
+        if (t >= B2_NBUCKET * ntb) return;
+        const int b = t / ntb, t0 = (t % ntb) * tile_b;
+        int m = 0;
+        for (int ij = t0; ij < min(nbra, t0 + tile_b); ij++) m = max(m, (nkl[ij * B2_NBUCKET + b] + chunk - 1) / chunk);
+        tile_cnt[t] = (long long)m * tile_b;
+}
+
+// chunk -> (segment, chunk of the segment); false for an idle slot
+__device__ __forceinline__ bool map_chunk(const JKArgs &a, long long chunk, int chunk_len, int &sgi, int &kc)
+{
+        if (!a.tiled) {
+                sgi = find_bra(a.chunk_off, a.bra.n * B2_NBUCKET, chunk);
+                kc = (int)(chunk - a.chunk_off[sgi]);
+                return true;
+        }
+        const int t = find_bra(a.chunk_off, a.ntile, chunk);
+        const int l = (int)(chunk - a.chunk_off[t]);
+        kc = l / a.tile_b;
+        const int ij = (t % a.ntb) * a.tile_b + l % a.tile_b;
+        if (ij >= a.bra.n) return false;
+        sgi = ij * B2_NBUCKET + t / a.ntb;
+        return kc * chunk_len < a.nkl[sgi];
+}
+
 // one (bra pair, ket bucket) segment t of a class: its ket range and chunks
 __device__ __forceinline__ void count_segment(const PairView &bra, const PairView &ket, int same, double tol,
                                               double dm, int chunk, double tau32, int pass, int shard, int nshard,
@@ -283,7 +319,7 @@ __global__ void __launch_bounds__(128) jk_thread_kernel(JKArgs a0, const JKArgs 
                 __syncthreads();
                 tab = reinterpret_cast<const R *>(smem_dyn);
         }
-        const long long total = MULTI ? mchunk[nmol] : a0.chunk_off[a0.bra.n * B2_NBUCKET];
+        const long long total = MULTI ? mchunk[nmol] : a0.chunk_off[a0.tiled ? a0.ntile : a0.bra.n * B2_NBUCKET];
         const long long nwarps = ((long long)gridDim.x * blockDim.x) >> 5;
         unsigned long long nq = 0, npq = 0;
         for (long long chunk = ((long long)blockIdx.x * blockDim.x + threadIdx.x) >> 5; chunk < total;
@@ -291,9 +327,11 @@ __global__ void __launch_bounds__(128) jk_thread_kernel(JKArgs a0, const JKArgs 
               auto body = [&](const JKArgs &a) {
                 const int nseg = a.bra.n * B2_NBUCKET;
                 const size_t n = (size_t)a.naoc, nn = n * n;
-                const int sgi = find_bra(a.chunk_off, nseg, chunk);
-                const int ij = sgi / B2_NBUCKET;
                 constexpr int M = KR;
+                int sgi, kc;
+                if (!map_chunk(a, chunk, 32 * M, sgi, kc)) return;
+                (void)nseg;
+                const int ij = sgi / B2_NBUCKET;
                 const bool carry = M > 1 && a.n_dm == 1 && a.nk == 1 && a.with_k;
                 double acc_a[K::NA * K::NC], acc_b[K::NB * K::NC];
                 int cur_c = -1;
@@ -312,7 +350,7 @@ __global__ void __launch_bounds__(128) jk_thread_kernel(JKArgs a0, const JKArgs 
                                         atomicAdd(a.Kacc + (sb0.y + b) * n + cur_c + c, acc_b[b * K::NC + c]);
                 };
               for (int jk = 0; jk < M; jk++) {
-                const int pos = (int)(chunk - a.chunk_off[sgi]) * (32 * M) + lane * M + jk;
+                const int pos = kc * (32 * M) + lane * M + jk;
                 const int kl = a.ket.boff[sgi % B2_NBUCKET] + a.kst[sgi] + pos;
                 const int4 sb = a.bra.sh[ij];
                 const int2 pb = a.bra.pr[ij];
@@ -688,7 +726,7 @@ __global__ void __launch_bounds__(128) jk_warp_kernel(JKArgs a0, int chunk_q, co
         const unsigned gmask = GS == 32 ? 0xffffffffu : (((1u << GS) - 1u) << (grp * GS));
         const int wib = threadIdx.x >> 5;
         double *sm = smem_dyn + (size_t)(wib * NGRP + grp) * S::SIZE;
-        const long long total = MULTI ? mchunk[nmol] : a0.chunk_off[a0.bra.n * B2_NBUCKET];
+        const long long total = MULTI ? mchunk[nmol] : a0.chunk_off[a0.tiled ? a0.ntile : a0.bra.n * B2_NBUCKET];
         const long long nwarps = ((long long)gridDim.x * blockDim.x) >> 5;
         unsigned long long nq = 0, npq = 0;
         for (long long chunk = ((long long)blockIdx.x * blockDim.x + threadIdx.x) >> 5; chunk < total;
@@ -696,11 +734,13 @@ __global__ void __launch_bounds__(128) jk_warp_kernel(JKArgs a0, int chunk_q, co
               auto body = [&](const JKArgs &a) {
                 const int nseg = a.bra.n * B2_NBUCKET;
                 const size_t n = (size_t)a.naoc, nn = n * n;
-                const int sgi = find_bra(a.chunk_off, nseg, chunk);
+                int sgi, kc;
+                if (!map_chunk(a, chunk, chunk_q, sgi, kc)) return;
+                (void)nseg;
                 const int ij = sgi / B2_NBUCKET;
                 const int kb = a.ket.boff[sgi % B2_NBUCKET] + a.kst[sgi];
-                const int kl0 = kb + (int)(chunk - a.chunk_off[sgi]) * chunk_q;
-                const int kl1 = kb + min((int)(chunk - a.chunk_off[sgi]) * chunk_q + chunk_q, a.nkl[sgi]);
+                const int kl0 = kb + kc * chunk_q;
+                const int kl1 = kb + min(kc * chunk_q + chunk_q, a.nkl[sgi]);
                 const int4 sb = a.bra.sh[ij];
                 const int2 pb = a.bra.pr[ij];
                 const double qij = a.bra.q[ij];

@@ -27,7 +27,7 @@ EXPORTS = (
     'b200jk_stats', 'b200jk_hostcheck_cart_quartet', 'b200jk_class_stats', 'b200jk_set_profiling',
     'b200jk_measure_fp64_peak', 'b200jk_get_jk_noalloc', 'b200jk_set_mixed_threshold',
     'b200jk_hostcheck_cart_quartet_fp32', 'b200jk_grad_jk', 'b200jk_grad_stats', 'b200jk_get_grad_q_cond',
-    'b200jk_set_shard', 'b200jk_grad_class_stats', 'b200jk_autotune', 'b200jk_get_tuning', 'b200jk_batch_create', 'b200jk_batch_destroy', 'b200jk_batch_get_jk', 'b200jk_batch_stats',
+    'b200jk_set_shard', 'b200jk_grad_class_stats', 'b200jk_autotune', 'b200jk_get_tuning', 'b200jk_set_tile', 'b200jk_batch_create', 'b200jk_batch_destroy', 'b200jk_batch_get_jk', 'b200jk_batch_stats',
 )
 
 
@@ -91,6 +91,7 @@ def load(path=LIB_PATH):
         lib.b200jk_grad_class_stats.argtypes = [vp, ctypes.POINTER(ClassStat), ip, ctypes.POINTER(ip)]
         lib.b200jk_autotune.argtypes = [vp, vp, ip, vp]
         lib.b200jk_get_tuning.argtypes = [vp, ctypes.POINTER(ip), ip, ctypes.POINTER(ip)]
+        lib.b200jk_set_tile.argtypes = [vp, ip]
         lib.b200jk_batch_create.argtypes = [vp, ip, ctypes.POINTER(vp)]
         lib.b200jk_batch_destroy.argtypes = [vp]
         lib.b200jk_batch_get_jk.argtypes = [vp, vp, ip, ip, ip, vp, vp, ip, vp]
@@ -185,6 +186,10 @@ class Plan:
             d = numpy.ascontiguousarray(dm, dtype=numpy.double)
             check(load().b200jk_autotune(self._h, _ptr(d), 0, None))
         return self.tuning()
+
+    def set_tile(self, tile_b):
+        """Bra pairs per tile of the ket-chunk-major order (0: bra-major)."""
+        check(load().b200jk_set_tile(self._h, int(tile_b)))
 
     def tuning(self):
         n = ctypes.c_int(0)
