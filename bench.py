@@ -267,11 +267,29 @@ def batch_report(local, flush, stream, steps, tau):
         for p, d in zip(plans, dms):
             p.get_jk_device(d, hermi=1)
     ms_seq = timed(one_by_one, 1)
+    # the batched build captured once in a CUDA graph and replayed
+    graph_ms = None
+    try:
+        batch.get_jk_device(dms, hermi=1)
+        vj = [torch.empty_like(d) for d in dms]
+        vk = [torch.empty_like(d) for d in dms]
+        side = torch.cuda.Stream(dev)
+        side.wait_stream(torch.cuda.current_stream(dev))
+        with torch.cuda.stream(side):
+            batch.get_jk_device_async(dms, vj, vk, hermi=1)
+        torch.cuda.current_stream(dev).wait_stream(side)
+        g = torch.cuda.CUDAGraph()
+        with torch.cuda.graph(g):
+            batch.get_jk_device_async(dms, vj, vk, hermi=1)
+        graph_ms = timed(g.replay, steps)
+    except Exception as e:  # the graph number must not sink the batch line
+        graph_ms = 'error: %s' % str(e)[:120]
     return {'workload': '512 x (H2O)n, n ~ U{1..16} (seed 404), 3x3x2 lattice sites, cc-pVDZ',
             'molecules': len(plans), 'total_nao': int(f['nao'].sum()), 'quartets_per_build': q,
             'batched_fp64_ms': ms_b64, 'batched_fp64_quartets_per_s': q / (ms_b64 * 1e-3),
             'batched_mixed_ms': ms_b32, 'mixed_tau': tau, 'mixed_fp32_fraction': f32,
             'one_by_one_fp64_ms': ms_seq, 'batching_speedup': ms_seq / ms_b64,
+            'cuda_graph_replay_fp64_ms': graph_ms,
             'kernel_launches_per_batched_build': launches,
             'density': 'per molecule C C^T, C nao x 5n N(0,1)/sqrt(nao), seed 405'}
 

@@ -197,6 +197,17 @@ int b200jk_batch_destroy(b200jk_batch *batch);
 int b200jk_batch_get_jk(b200jk_batch *batch, const double *const *dms, int hermi, int with_j, int with_k,
                         double *const *vj, double *const *vk, int precision_mode, void *stream);
 
+/* The same launches as b200jk_batch_get_jk with nothing else: no
+ * allocation, no host synchronisation, no statistics read-back, so that the
+ * caller can capture them in a CUDA graph (stream capture of `stream`) and
+ * replay the whole batched build; the graph reads dms[m] and writes vj[m],
+ * vk[m] at the addresses given here.  Needs one b200jk_batch_get_jk call
+ * with the same arguments first (it sizes every buffer); one captured graph
+ * per batch at a time (they share the pinned argument staging).  No
+ * reference counterpart. */
+int b200jk_batch_get_jk_async(b200jk_batch *batch, const double *const *dms, int hermi, int with_j, int with_k,
+                              double *const *vj, double *const *vk, int precision_mode, void *stream);
+
 /* Counters of the last batched build: quartets (all molecules), of them in
  * float32, device time (ms), kernels launched by this library. */
 int b200jk_batch_stats(const b200jk_batch *batch, int64_t *quartets, int64_t *fp32_quartets, double *ms,

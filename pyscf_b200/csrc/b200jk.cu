@@ -1477,6 +1477,11 @@ struct b200jk_batch {
         JKArgs *h_args = nullptr;       // pinned staging of the per-class argument arrays
         int *h_segoff = nullptr;
         size_t h_cap_args = 0, h_cap_seg = 0;
+        // staging of the asynchronous entry (read by captured graphs at replay)
+        JKArgs *h_args_async = nullptr;
+        int *h_segoff_async = nullptr;
+        const double *tbl = nullptr;
+        const float *tbl_f = nullptr;
         int64_t quartets = 0, prim_quartets = 0, fp32_quartets = 0, launches = 0;
         double last_ms = 0;
         ~b200jk_batch()
@@ -1485,6 +1490,8 @@ struct b200jk_batch {
                 chunk_off.release(); mchunk.release(); cub_tmp.release(); stats.release();
                 if (h_args) cudaFreeHost(h_args);
                 if (h_segoff) cudaFreeHost(h_segoff);
+                if (h_args_async) cudaFreeHost(h_args_async);
+                if (h_segoff_async) cudaFreeHost(h_segoff_async);
                 if (ev0) cudaEventDestroy(ev0);
                 if (ev1) cudaEventDestroy(ev1);
                 if (stream) cudaStreamDestroy(stream);
@@ -1511,6 +1518,8 @@ extern "C" int b200jk_batch_create(b200jk_plan *const *plans, int nmol, b200jk_b
                 delete B;
                 return fail(B200JK_ECUDA, "stream/event creation failed");
         }
+        B->tbl = table_ptr();
+        B->tbl_f = table_f_ptr();
         *out = B;
         return B200JK_OK;
 }
@@ -1521,8 +1530,12 @@ extern "C" int b200jk_batch_destroy(b200jk_batch *B)
         return B200JK_OK;
 }
 
-extern "C" int b200jk_batch_get_jk(b200jk_batch *B, const double *const *dms, int hermi, int with_j, int with_k,
-                                   double *const *vj, double *const *vk, int precision_mode, void *stream)
+// async: no allocation (every buffer must exist from an earlier synchronous
+// call), no host synchronisation, no statistics read-back, its own pinned
+// staging of the argument arrays -- the launches alone, so that a caller can
+// capture them in a CUDA graph
+static int batch_build(b200jk_batch *B, const double *const *dms, int hermi, int with_j, int with_k,
+                       double *const *vj, double *const *vk, int precision_mode, void *stream, bool async)
 {
         if (!B) return fail(B200JK_EINVAL, "batch is NULL");
         if (!dms) return fail(B200JK_EINVAL, "dms is NULL");
@@ -1539,8 +1552,14 @@ extern "C" int b200jk_batch_get_jk(b200jk_batch *B, const double *const *dms, in
         cudaStream_t s = stream ? (cudaStream_t)stream : B->stream;
         const int nk = hermi == 1 ? 1 : 2;
         int rc;
-        for (int m = 0; m < nmol; m++)
-                if ((rc = ensure_workspace(B->plans[m], 1))) return rc;
+        for (int m = 0; m < nmol; m++) {
+                if (async) {
+                        if (B->plans[m]->ws_ndm < 1)
+                                return fail(B200JK_EINVAL, "b200jk_batch_get_jk_async needs one b200jk_batch_get_jk call first");
+                } else if ((rc = ensure_workspace(B->plans[m], 1))) {
+                        return rc;
+                }
+        }
         auto qcs = quartet_classes();
         const int nclass = (int)qcs.size();
         // argument arrays of every (class, pass): only molecules with work in the class
@@ -1565,28 +1584,40 @@ extern "C" int b200jk_batch_get_jk(b200jk_batch *B, const double *const *dms, in
                         tot_seg += cnt + 1;
                 }
         }
-        if (tot_args > B->h_cap_args) {
-                if (B->h_args) cudaFreeHost(B->h_args);
-                B->h_args = nullptr;
-                CUDA_TRY(cudaMallocHost(&B->h_args, sizeof(JKArgs) * tot_args));
-                B->h_cap_args = tot_args;
+        if (async) {
+                if (tot_args > B->h_cap_args || tot_seg > B->h_cap_seg || !B->h_args_async || B->args.n < tot_args)
+                        return fail(B200JK_EINVAL, "b200jk_batch_get_jk_async needs one b200jk_batch_get_jk call first");
+        } else {
+                if (tot_args > B->h_cap_args || !B->h_args_async) {
+                        if (B->h_args) cudaFreeHost(B->h_args);
+                        if (B->h_args_async) cudaFreeHost(B->h_args_async);
+                        B->h_args = B->h_args_async = nullptr;
+                        CUDA_TRY(cudaMallocHost(&B->h_args, sizeof(JKArgs) * tot_args));
+                        CUDA_TRY(cudaMallocHost(&B->h_args_async, sizeof(JKArgs) * tot_args));
+                        B->h_cap_args = tot_args;
+                }
+                if (tot_seg > B->h_cap_seg || !B->h_segoff_async) {
+                        if (B->h_segoff) cudaFreeHost(B->h_segoff);
+                        if (B->h_segoff_async) cudaFreeHost(B->h_segoff_async);
+                        B->h_segoff = B->h_segoff_async = nullptr;
+                        CUDA_TRY(cudaMallocHost(&B->h_segoff, sizeof(int) * tot_seg));
+                        CUDA_TRY(cudaMallocHost(&B->h_segoff_async, sizeof(int) * tot_seg));
+                        B->h_cap_seg = tot_seg;
+                }
+                if ((rc = dev_alloc(B->args, std::max<size_t>(1, tot_args))) ||
+                    (rc = dev_alloc(B->segoff, std::max<size_t>(1, tot_seg))) || (rc = dev_alloc(B->nkl, max_segs)) ||
+                    (rc = dev_alloc(B->kst, max_segs)) || (rc = dev_alloc(B->nchunk, max_segs + 1)) ||
+                    (rc = dev_alloc(B->chunk_off, max_segs + 1)) || (rc = dev_alloc(B->mchunk, nmol + 1)) ||
+                    (rc = dev_alloc(B->stats, 4 * 64)))
+                        return rc;
+                size_t cub_bytes = 0;
+                cub::DeviceScan::ExclusiveSum(nullptr, cub_bytes, B->nchunk.p, B->chunk_off.p, max_segs + 1);
+                if ((rc = dev_alloc(B->cub_tmp, cub_bytes + 16))) return rc;
         }
-        if (tot_seg > B->h_cap_seg) {
-                if (B->h_segoff) cudaFreeHost(B->h_segoff);
-                B->h_segoff = nullptr;
-                CUDA_TRY(cudaMallocHost(&B->h_segoff, sizeof(int) * tot_seg));
-                B->h_cap_seg = tot_seg;
-        }
-        if ((rc = dev_alloc(B->args, std::max<size_t>(1, tot_args))) || (rc = dev_alloc(B->segoff, std::max<size_t>(1, tot_seg))) ||
-            (rc = dev_alloc(B->nkl, max_segs)) || (rc = dev_alloc(B->kst, max_segs)) ||
-            (rc = dev_alloc(B->nchunk, max_segs + 1)) || (rc = dev_alloc(B->chunk_off, max_segs + 1)) ||
-            (rc = dev_alloc(B->mchunk, nmol + 1)) || (rc = dev_alloc(B->stats, 4 * 64)))
-                return rc;
-        size_t cub_bytes = 0;
-        cub::DeviceScan::ExclusiveSum(nullptr, cub_bytes, B->nchunk.p, B->chunk_off.p, max_segs + 1);
-        if ((rc = dev_alloc(B->cub_tmp, cub_bytes + 16))) return rc;
+        JKArgs *h_args = async ? B->h_args_async : B->h_args;
+        int *h_segoff = async ? B->h_segoff_async : B->h_segoff;
 
-        CUDA_TRY(cudaEventRecord(B->ev0, s));
+        if (!async) CUDA_TRY(cudaEventRecord(B->ev0, s));
         int64_t launches = 0;
         // per molecule: screening data, Cartesian densities, cleared accumulators
         for (int m = 0; m < nmol; m++) {
@@ -1615,13 +1646,13 @@ extern "C" int b200jk_batch_get_jk(b200jk_batch *B, const double *const *dms, in
                 launches += 3;
         }
         CUDA_TRY(cudaMemsetAsync(B->stats.p, 0, 4 * 64 * sizeof(unsigned long long), s));
-        const double *tbl = table_ptr();
-        const float *tbl_f = table_f_ptr();
+        const double *tbl = B->tbl;
+        const float *tbl_f = B->tbl_f;
         // argument arrays (pointers only depend on the workspaces): fill and upload once
         for (int t = 0; t < nclass; t++) {
                 for (int pass = 0; pass < 2; pass++) {
-                        JKArgs *ha = B->h_args + at[2 * t + pass];
-                        int *hs = B->h_segoff + sat[2 * t + pass];
+                        JKArgs *ha = h_args + at[2 * t + pass];
+                        int *hs = h_segoff + sat[2 * t + pass];
                         int k = 0, seg = 0;
                         for (int m = 0; m < nmol; m++) {
                                 b200jk_plan *P = B->plans[m];
@@ -1656,8 +1687,8 @@ extern "C" int b200jk_batch_get_jk(b200jk_batch *B, const double *const *dms, in
                         hs[k] = seg;
                 }
         }
-        CUDA_TRY(cudaMemcpyAsync(B->args.p, B->h_args, sizeof(JKArgs) * tot_args, cudaMemcpyHostToDevice, s));
-        CUDA_TRY(cudaMemcpyAsync(B->segoff.p, B->h_segoff, sizeof(int) * tot_seg, cudaMemcpyHostToDevice, s));
+        CUDA_TRY(cudaMemcpyAsync(B->args.p, h_args, sizeof(JKArgs) * tot_args, cudaMemcpyHostToDevice, s));
+        CUDA_TRY(cudaMemcpyAsync(B->segoff.p, h_segoff, sizeof(int) * tot_seg, cudaMemcpyHostToDevice, s));
         for (int t = 0; t < nclass; t++) {
                 int la, lb, lc, ld;
                 class_l(qcs[t].X, la, lb);
@@ -1669,7 +1700,7 @@ extern "C" int b200jk_batch_get_jk(b200jk_batch *B, const double *const *dms, in
                         if (nm == 0) continue;
                         const JKArgs *dargs = B->args.p + at[2 * t + pass];
                         const int *dseg = B->segoff.p + sat[2 * t + pass];
-                        const int segs = B->h_segoff[sat[2 * t + pass] + nm];
+                        const int segs = h_segoff[sat[2 * t + pass] + nm];
                         count_kernel_multi<<<grid_for(segs, 256), 256, 0, s>>>(dargs, dseg, nm, chunk, mixed ? tau : 0.0,
                                                                               pass, B->nkl.p, B->kst.p, B->nchunk.p);
                         CUDA_TRY(cudaGetLastError());
@@ -1678,7 +1709,7 @@ extern "C" int b200jk_batch_get_jk(b200jk_batch *B, const double *const *dms, in
                         CUDA_TRY(cub::DeviceScan::ExclusiveSum(B->cub_tmp.p, tmp, B->nchunk.p, B->chunk_off.p, segs + 1, s));
                         batch_chunk_starts<<<grid_for(nm + 1, 128), 128, 0, s>>>(B->chunk_off.p, dseg, nm, B->mchunk.p);
                         CUDA_TRY(cudaGetLastError());
-                        const JKArgs &a0 = B->h_args[at[2 * t + pass]];
+                        const JKArgs &a0 = h_args[at[2 * t + pass]];
                         if ((rc = dispatch_jk(B->plans[0], la, lb, lc, ld, a0, pass, s, dargs, B->mchunk.p, nm, variant)))
                                 return rc;
                         launches += 3;
@@ -1710,6 +1741,7 @@ extern "C" int b200jk_batch_get_jk(b200jk_batch *B, const double *const *dms, in
                         launches++;
                 }
         }
+        if (async) return B200JK_OK;
         CUDA_TRY(cudaEventRecord(B->ev1, s));
         unsigned long long hs[4 * 64];
         CUDA_TRY(cudaMemcpyAsync(hs, B->stats.p, sizeof(hs), cudaMemcpyDeviceToHost, s));
@@ -1725,6 +1757,19 @@ extern "C" int b200jk_batch_get_jk(b200jk_batch *B, const double *const *dms, in
         B->last_ms = ms;
         B->launches = launches;
         return B200JK_OK;
+}
+
+extern "C" int b200jk_batch_get_jk(b200jk_batch *B, const double *const *dms, int hermi, int with_j, int with_k,
+                                   double *const *vj, double *const *vk, int precision_mode, void *stream)
+{
+        return batch_build(B, dms, hermi, with_j, with_k, vj, vk, precision_mode, stream, false);
+}
+
+extern "C" int b200jk_batch_get_jk_async(b200jk_batch *B, const double *const *dms, int hermi, int with_j,
+                                         int with_k, double *const *vj, double *const *vk, int precision_mode,
+                                         void *stream)
+{
+        return batch_build(B, dms, hermi, with_j, with_k, vj, vk, precision_mode, stream, true);
 }
 
 extern "C" int b200jk_batch_stats(const b200jk_batch *B, int64_t *quartets, int64_t *fp32_quartets, double *ms,

@@ -27,7 +27,7 @@ EXPORTS = (
     'b200jk_stats', 'b200jk_hostcheck_cart_quartet', 'b200jk_class_stats', 'b200jk_set_profiling',
     'b200jk_measure_fp64_peak', 'b200jk_get_jk_noalloc', 'b200jk_set_mixed_threshold',
     'b200jk_hostcheck_cart_quartet_fp32', 'b200jk_grad_jk', 'b200jk_grad_stats', 'b200jk_get_grad_q_cond',
-    'b200jk_set_shard', 'b200jk_grad_class_stats', 'b200jk_autotune', 'b200jk_get_tuning', 'b200jk_set_tile', 'b200jk_batch_create', 'b200jk_batch_destroy', 'b200jk_batch_get_jk', 'b200jk_batch_stats',
+    'b200jk_set_shard', 'b200jk_grad_class_stats', 'b200jk_autotune', 'b200jk_get_tuning', 'b200jk_set_tile', 'b200jk_batch_get_jk_async', 'b200jk_batch_create', 'b200jk_batch_destroy', 'b200jk_batch_get_jk', 'b200jk_batch_stats',
 )
 
 
@@ -95,6 +95,7 @@ def load(path=LIB_PATH):
         lib.b200jk_batch_create.argtypes = [vp, ip, ctypes.POINTER(vp)]
         lib.b200jk_batch_destroy.argtypes = [vp]
         lib.b200jk_batch_get_jk.argtypes = [vp, vp, ip, ip, ip, vp, vp, ip, vp]
+        lib.b200jk_batch_get_jk_async.argtypes = [vp, vp, ip, ip, ip, vp, vp, ip, vp]
         lib.b200jk_batch_stats.argtypes = [vp, ctypes.POINTER(ctypes.c_int64), ctypes.POINTER(ctypes.c_int64),
                                            ctypes.POINTER(dp), ctypes.POINTER(ctypes.c_int64)]
         _lib = lib
@@ -341,6 +342,19 @@ class Batch:
         check(load().b200jk_batch_get_jk(self._h, pd, int(hermi), int(bool(with_j)), int(bool(with_k)),
                                          pj, pk, int(precision), ctypes.c_void_p(stream)))
         return vj, vk
+
+    def get_jk_device_async(self, dms, vj, vk, hermi=1, precision=PREC_FP64):
+        """The launches of one batched build into the caller's tensors, on the
+        current stream, with no allocation or synchronisation (capturable in a
+        torch.cuda.CUDAGraph after one get_jk_device call)."""
+        import torch
+        P = ctypes.c_void_p * len(dms)
+        pd = P(*[d.data_ptr() for d in dms])
+        pj = P(*[t.data_ptr() for t in vj])
+        pk = P(*[t.data_ptr() for t in vk])
+        stream = torch.cuda.current_stream(dms[0].device).cuda_stream
+        check(load().b200jk_batch_get_jk_async(self._h, pd, int(hermi), 1, 1, pj, pk, int(precision),
+                                               ctypes.c_void_p(stream)))
 
     def stats(self):
         q, q32, n = ctypes.c_int64(0), ctypes.c_int64(0), ctypes.c_int64(0)

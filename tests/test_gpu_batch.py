@@ -64,3 +64,32 @@ def test_batch_general_density_and_mixed(b2):
     for f, j, k in zip(fs, vj, vk):
         assert abs(j.cpu().numpy() - f['vj_ns']).max() < 2e-5 * abs(f['vj_ns']).max()
         assert abs(k.cpu().numpy() - f['vk_ns']).max() < 2e-5 * abs(f['vk_ns']).max()
+
+
+def test_batch_cuda_graph(b2):
+    """A batched build captured in a CUDA graph: replays give the reference
+    J/K, also after the densities are refilled in place."""
+    import torch
+    names = ['h2o_vdz', 'h2o8_vdz', 'h2o2_vtz']
+    fs, plans = _plans(b2, names)
+    batch = b2.Batch(plans)
+    dms = [torch.tensor(f['dm_rand'], device='cuda:0') for f in fs]
+    batch.get_jk_device(dms, hermi=1)          # sizes every buffer
+    vj = [torch.empty_like(d) for d in dms]
+    vk = [torch.empty_like(d) for d in dms]
+    side = torch.cuda.Stream()
+    side.wait_stream(torch.cuda.current_stream())
+    with torch.cuda.stream(side):
+        batch.get_jk_device_async(dms, vj, vk, hermi=1)
+    torch.cuda.current_stream().wait_stream(side)
+    g = torch.cuda.CUDAGraph()
+    with torch.cuda.graph(g):
+        batch.get_jk_device_async(dms, vj, vk, hermi=1)
+    for key in ('rand', 'conv'):
+        for f, d in zip(fs, dms):
+            d.copy_(torch.tensor(f['dm_' + key], device='cuda:0'))
+        g.replay()
+        torch.cuda.synchronize()
+        for f, j, k in zip(fs, vj, vk):
+            assert abs(j.cpu().numpy() - f['vj_' + key]).max() < TOL_JK
+            assert abs(k.cpu().numpy() - f['vk_' + key]).max() < TOL_JK
