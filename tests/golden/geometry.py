@@ -100,4 +100,6 @@ def workloads():
         'h2o64_vtz_sub4': (water_cluster((4, 4, 4), 0.3, 303)[:12], 'cc-pvtz'),
         'h2o64_vtz_sub8': (water_cluster((4, 4, 4), 0.3, 303)[:24], 'cc-pvtz'),
         'h2o64_vtz_sub16': (water_cluster((4, 4, 4), 0.3, 303)[:48], 'cc-pvtz'),
+        # half of it: matrices above the 126 MB L2, the case profiled under ncu
+        'h2o64_vtz_sub32': (water_cluster((4, 4, 4), 0.3, 303)[:96], 'cc-pvtz'),
     }
