@@ -1046,7 +1046,7 @@ int b200jk_autotune(b200jk_plan *P, const double *dm, int dev_ptrs, void *stream
                         int la, lb, lc, ld;
                         class_l(qcs[t].X, la, lb);
                         class_l(qcs[t].Y, lc, ld);
-                        if (v == 1 && family_ket_run(la, lb, lc, ld) == 1) continue;   // no such variant
+                        if (v == 1 && !family_has_variant(la, lb, lc, ld)) continue;   // no such variant
                         if (P->cls[t].ms < best_ms[t]) { best_ms[t] = P->cls[t].ms; best[t] = v; }
                 }
         }

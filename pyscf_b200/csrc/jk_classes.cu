@@ -22,10 +22,12 @@ struct LaunchCfg {
 // R is the evaluation type: double for the FP64 pass, float for the FP32 pass
 // of mixed precision (accumulation stays in float64 either way).  MULTI: one
 // launch over a batch of molecules (margs, mchunk, nmol on the device).
-template <int LA, int LB, int LC, int LD, typename R, bool MULTI, int KR>
+template <int LA, int LB, int LC, int LD, typename R, bool MULTI, int KR, int GSV = 0>
 int launch_one(const JKArgs &a, const JKArgs *margs, const long long *mchunk, int nmol, cudaStream_t s, int nsm,
                std::string &err)
 {
+        // GSV > 0: lanes per quartet of the shared-memory family (a variant)
+        constexpr int GSX = GSV > 0 ? GSV : group_size<LA, LB, LC, LD>();
         using K = Class4<LA, LB, LC, LD>;
         constexpr int NP = thread_parts<LA, LB, LC, LD>();
         constexpr bool thread = NP > 0;
@@ -45,14 +47,14 @@ int launch_one(const JKArgs &a, const JKArgs *margs, const long long *mchunk, in
                                                 &nb, jk_thread_kernel<LA, LB, LC, LD, (NP > 0 ? NP : 1), R, MULTI, KR>, 128, cfg.smem);
                         } else {
                                 const size_t per_warp = sizeof(double) * WarpSmem<LA, LB, LC, LD, R>::SIZE *
-                                                        (32 / group_size<LA, LB, LC, LD>());
+                                                        (32 / GSX);
                                 const int wpb = (int)std::min<size_t>(4, std::max<size_t>(1, (200 * 1024) / per_warp));
                                 cfg.block = 32 * wpb;
                                 cfg.smem = per_warp * wpb;
-                                cfg.status = cudaFuncSetAttribute(jk_warp_kernel<LA, LB, LC, LD, R, MULTI>,
+                                cfg.status = cudaFuncSetAttribute(jk_warp_kernel<LA, LB, LC, LD, R, MULTI, GSX>,
                                                                   cudaFuncAttributeMaxDynamicSharedMemorySize, (int)cfg.smem);
                                 if (cfg.status == cudaSuccess)
-                                        cfg.status = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, jk_warp_kernel<LA, LB, LC, LD, R, MULTI>,
+                                        cfg.status = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, jk_warp_kernel<LA, LB, LC, LD, R, MULTI, GSX>,
                                                                                                    cfg.block, cfg.smem);
                         }
                         cfg.grid = (nb > 0 ? nb : 1) * nsm;
@@ -66,8 +68,8 @@ int launch_one(const JKArgs &a, const JKArgs *margs, const long long *mchunk, in
         if constexpr (thread) {
                 jk_thread_kernel<LA, LB, LC, LD, NP, R, MULTI, KR><<<cfg.grid, cfg.block, cfg.smem, s>>>(a, margs, mchunk, nmol);
         } else {
-                jk_warp_kernel<LA, LB, LC, LD, R, MULTI><<<cfg.grid, cfg.block, cfg.smem, s>>>(
-                        a, 8 * (32 / group_size<LA, LB, LC, LD>()), margs, mchunk, nmol);
+                jk_warp_kernel<LA, LB, LC, LD, R, MULTI, GSX><<<cfg.grid, cfg.block, cfg.smem, s>>>(
+                        a, 8 * (32 / GSX), margs, mchunk, nmol);
         }
         cudaError_t e = cudaGetLastError();
         if (e != cudaSuccess) {
@@ -85,7 +87,20 @@ int B2_FN_NAME(const JKArgs &a, cudaStream_t s, int nsm, int fp32, int variant, 
 {
         constexpr int NP = thread_parts<B2_BRA_LA, B2_BRA_LB, B2_KET_LC, B2_KET_LD>();
         constexpr int KRUN = NP > 0 ? ket_run<B2_BRA_LA, B2_BRA_LB, B2_KET_LC, B2_KET_LD, NP>() : 1;
+        // the shared-memory family's variant 1: half as many lanes per quartet
+        // (only where one warp's groups still fit the 200 KB a block may use here)
+        constexpr int GSH0 = NP > 0 ? 0 : group_size<B2_BRA_LA, B2_BRA_LB, B2_KET_LC, B2_KET_LD>() / 2;
+        constexpr int GSH = (GSH0 >= 8 && sizeof(double) * WarpSmem<B2_BRA_LA, B2_BRA_LB, B2_KET_LC, B2_KET_LD>::SIZE *
+                                                  (32 / (GSH0 > 0 ? GSH0 : 1)) <= 200 * 1024) ? GSH0 : 0;
 #define B2_L(R, M, KR) launch_one<B2_BRA_LA, B2_BRA_LB, B2_KET_LC, B2_KET_LD, R, M, KR>(a, margs, mchunk, nmol, s, nsm, err)
+#define B2_LG(R, M) launch_one<B2_BRA_LA, B2_BRA_LB, B2_KET_LC, B2_KET_LD, R, M, 1, GSH>(a, margs, mchunk, nmol, s, nsm, err)
+        if constexpr (GSH >= 8) {
+                if (variant == 1) {
+                        if (nmol > 0) return fp32 ? B2_LG(float, true) : B2_LG(double, true);
+                        return fp32 ? B2_LG(float, false) : B2_LG(double, false);
+                }
+        }
+#undef B2_LG
         if constexpr (KRUN > 1) {
                 if (variant == 1) {
                         if (nmol > 0) return fp32 ? B2_L(float, true, KRUN) : B2_L(double, true, KRUN);

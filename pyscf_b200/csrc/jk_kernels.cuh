@@ -712,13 +712,14 @@ __host__ __device__ constexpr int group_size()
         return K::NG <= 100 ? 8 : (K::NG <= 400 ? 16 : 32);
 }
 
-template <int LA, int LB, int LC, int LD, typename R, bool MULTI>
+// GS_: lanes per quartet (0: group_size<>; the autotuner may pick half of it)
+template <int LA, int LB, int LC, int LD, typename R, bool MULTI, int GS_ = 0>
 __global__ void __launch_bounds__(128) jk_warp_kernel(JKArgs a0, int chunk_q, const JKArgs *__restrict__ margs,
                                                       const long long *__restrict__ mchunk, int nmol)
 {
         using K = Class4<LA, LB, LC, LD>;
         using S = WarpSmem<LA, LB, LC, LD, R>;
-        constexpr int GS = group_size<LA, LB, LC, LD>();
+        constexpr int GS = GS_ > 0 ? GS_ : group_size<LA, LB, LC, LD>();
         constexpr int NGRP = 32 / GS;
         extern __shared__ __align__(32) double smem_dyn[];
         const int lane = threadIdx.x & 31;

@@ -37,13 +37,38 @@ inline int family_ket_run(int la, int lb, int lc, int ld)
         const int na = ncart(la), nb = ncart(lb), nc = ncart(lc);
         return (np == 1 && na * nc + nb * nc <= 24) ? 4 : 1;
 }
+// whether a class has a launch variant 1 for the autotuner to try: more kets
+// per lane (register family) or half as many lanes per quartet (shared-memory
+// family with groups of 16 or 32 lanes)
+// doubles of one group's shared memory (host twin of WarpSmem<..., double>::SIZE)
+inline int family_group_smem(int la, int lb, int lc, int ld)
+{
+        const int na = ncart(la), nb = ncart(lb), nc = ncart(lc), nd = ncart(ld);
+        const int ng = na * nb * nc * nd, sa = (la + 1) * (lb + 1) * (lc + 1) * (ld + 1);
+        const int nr = (la + lb + lc + ld) / 2 + 1;
+        const int x = ng + 3 * nr * sa + na * nb + nc * nd + nb * nc + nb * nd + na * nc + na * nd;
+        return (x + 3) & ~3;
+}
+// half-width groups (variant 1 of the shared-memory family: 32 -> 16 or
+// 16 -> 8 lanes) where one warp's groups fit the 200 KB a block may use
+inline bool family_half_groups(int la, int lb, int lc, int ld)
+{
+        const int gs = family_group(la, lb, lc, ld);
+        return gs >= 16 && 8.0 * family_group_smem(la, lb, lc, ld) * (32 / (gs / 2)) <= 200 * 1024;
+}
+inline bool family_has_variant(int la, int lb, int lc, int ld)
+{
+        if (family_thread_parts(la, lb, lc, ld) > 0) return family_ket_run(la, lb, lc, ld) > 1;
+        return family_half_groups(la, lb, lc, ld);
+}
 // quartets per chunk: 32 x kets per lane in the register family (variant 0:
 // one ket per lane, 1: family_ket_run), 8 per group of the warp otherwise
 inline int family_chunk(int la, int lb, int lc, int ld, int variant = 0)
 {
         if (family_thread_parts(la, lb, lc, ld) > 0)
                 return 32 * (variant == 1 ? family_ket_run(la, lb, lc, ld) : 1);
-        return 8 * (32 / family_group(la, lb, lc, ld));
+        const int gs = family_group(la, lb, lc, ld);
+        return 8 * (32 / (variant == 1 && family_half_groups(la, lb, lc, ld) ? gs / 2 : gs));   // 8 quartets per group
 }
 
 // one launcher per quartet class (la lb | lc ld), (lc, ld) <= (la, lb)
