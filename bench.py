@@ -336,8 +336,10 @@ def run_gpu(args):
             b2dist.reduce_jk(vj, vk)
         return vj, vk
 
-    # the per-class launch variants (kets per lane of the register family)
-    # are tuned once per plan on the workload's density, like the planning
+    # the per-class launch variants (kets per lane of the register family,
+    # lanes per quartet of the shared-memory family; float64 quartets and the
+    # float32 pass of mixed builds) are tuned once per plan on the workload's
+    # density, like the planning
     tuning = plan.autotune(d)
     for _ in range(args.warmup):
         build64()
@@ -492,7 +494,8 @@ def run_gpu(args):
                        'parallelism': ('bra-pair shards + NCCL all-reduce of [J;K], %d GPUs' % world) if world > 1
                        else 'single',
                        'l2': 'flushed (256 MB write) before every timed build',
-                       'autotuned_classes': int(sum(tuning))},
+                       'autotuned_classes': int(sum(tuning)),
+                       'autotuned_classes_fp32_pass': int(sum(plan.tuning(lib.PREC_MIXED)))},
             's_per_build': t_total / args.steps,
             'quartets_per_build': q_per_build, 'prim_quartets_per_build': _sum_over_ranks(tot['prim_quartets'], dist, dev) / args.steps,
             'fp64_tflops_build': build_flops / (t_total / args.steps) / 1e12 if world == 1 else None,
@@ -542,9 +545,16 @@ def run_one_build(args):
     from pyscf_b200 import lib
     f = load_workload(args.config)
     plan = lib.Plan(f['atm'], f['bas'], f['env'], direct_scf_tol=1e-13)
+    if args.autotune:
+        plan.autotune(f['dm'])
+    if args.variants is not None:
+        # the FP64 variants of an earlier tuning, replayed without timing
+        on = {int(x) for x in args.variants.split(',') if x}
+        plan.set_tuning([int(t in on) for t in range(55)])
     plan.get_jk(f['dm'], hermi=1)
     st = plan.stats()
-    print(json.dumps({'workload': args.config, 'ms': st['last_build_ms'], 'quartets': st['quartets']}))
+    print(json.dumps({'workload': args.config, 'ms': st['last_build_ms'], 'quartets': st['quartets'],
+                      'variants': ','.join(str(t) for t, v in enumerate(plan.tuning()) if v)}))
 
 
 class _Mol:
@@ -564,6 +574,9 @@ def main():
     ap.add_argument('--tau', type=float, default=1e-6, help='float32 threshold of the mixed-precision line')
     ap.add_argument('--one-build', action='store_true',
                     help='plan + one FP64 J/K build of the workload, nothing else (the case profiled under ncu)')
+    ap.add_argument('--autotune', action='store_true', help='--one-build: run the autotuner first')
+    ap.add_argument('--variants', default=None,
+                    help='--one-build: comma-separated quartet classes that use launch variant 1 (as printed)')
     args = ap.parse_args()
     if args.impl == 'reference':
         run_reference(args)

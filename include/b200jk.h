@@ -137,11 +137,13 @@ int b200jk_class_stats(const b200jk_plan *plan, b200jk_class_stat_t *out, int ma
 int b200jk_set_profiling(b200jk_plan *plan, int on);
 
 /* Autotuner: for every quartet class with more than one launch variant (the
- * register family with 1 or 4 kets per lane), time each variant on one FP64
- * J/K build of the density dm (nao x nao, symmetric; host array, or device
- * array with dev_ptrs = 1) and keep the faster for later builds of this plan
- * (and of batches whose first plan it is).  Three builds.  No reference
- * counterpart (PySCF has no kernel variants to tune). */
+ * register family with one or several kets per lane; the shared-memory
+ * family with full- or half-width lane groups per quartet), time each variant
+ * on FP64 J/K builds of the density dm (nao x nao, symmetric; host array, or
+ * device array with dev_ptrs = 1), then the float32 pass's variants on mixed
+ * builds at the plan's threshold, and keep the faster for later builds of
+ * this plan (and of batches whose first plan it is).  Five builds.  No
+ * reference counterpart (PySCF has no kernel variants to tune). */
 int b200jk_autotune(b200jk_plan *plan, const double *dm, int dev_ptrs, void *stream);
 
 /* Chunk order of the class kernels: tiles of tile_b bra pairs walked
@@ -149,8 +151,14 @@ int b200jk_autotune(b200jk_plan *plan, const double *dm, int dev_ptrs, void *str
  * 0 = bra-major order.  Sharded plans always use bra-major order. */
 int b200jk_set_tile(b200jk_plan *plan, int tile_b);
 
-/* The chosen variant per quartet class (55 classes, bra class >= ket class). */
-int b200jk_get_tuning(const b200jk_plan *plan, int *variants, int max, int *n);
+/* The chosen variant per quartet class (55 classes, bra class >= ket class)
+ * for float64 quartets (precision B200JK_PREC_FP64) or for the float32 pass
+ * of mixed builds (B200JK_PREC_MIXED). */
+int b200jk_get_tuning(const b200jk_plan *plan, int precision, int *variants, int max, int *n);
+
+/* Set the variants directly (n = 55; 0 everywhere, 1 only where the class has
+ * a second variant, else B200JK_EINVAL): replays a tuning without timing. */
+int b200jk_set_tuning(b200jk_plan *plan, int precision, const int *variants, int n);
 
 /* Nuclear-gradient J/K: the drop-in for pyscf.grad.rhf.get_jk(mol, dm)
  * (pyscf/grad/rhf.py:149-178, i.e. _vhf.direct_mapdm('int2e_ip1', 's2kl',

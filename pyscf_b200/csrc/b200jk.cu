@@ -234,8 +234,11 @@ struct b200jk_plan {
         // multi-GPU: this plan evaluates the bra pairs ij = shard (mod nshard)
         int shard = 0, nshard = 1;
         // launch variant per quartet class (register family: 0 = one ket per
-        // lane, 1 = family_ket_run kets per lane), chosen by b200jk_autotune
-        std::vector<int> kvar;
+        // lane, 1 = family_ket_run kets per lane; shared-memory family: 0 =
+        // family_group lanes per quartet, 1 = half as many), chosen by
+        // b200jk_autotune: kvar for float64 quartets, kvar32 for the float32
+        // pass of mixed builds
+        std::vector<int> kvar, kvar32;
         // bra pairs per tile of the tiled chunk order (0: bra-major order)
         int tile_b = 64;
         // packed ket blocks for the J contraction: class X's blocks start at
@@ -310,6 +313,13 @@ static void class_l(int X, int &la, int &lb)
 
 typedef int (*jk_launcher_t)(const JKArgs &, cudaStream_t, int, int, int, const JKArgs *, const long long *, int,
                              std::string &);
+
+// the launch variant of class t in precision pass `pass` (1: float32 quartets)
+static int class_variant(const b200jk_plan *P, size_t t, int pass)
+{
+        const std::vector<int> &v = pass == 1 ? P->kvar32 : P->kvar;
+        return t < v.size() ? v[t] : 0;
+}
 
 static int dispatch_jk(b200jk_plan *P, int la, int lb, int lc, int ld, const JKArgs &a, int fp32, cudaStream_t s,
                        const JKArgs *margs = nullptr, const long long *mchunk = nullptr, int nmol = 0, int variant = 0)
@@ -877,14 +887,14 @@ int b200jk_get_jk(b200jk_plan *P, const double *dms, int n_dm, int hermi, int wi
                         if (bra.n == 0 || ket.n == 0) continue;
                         int la = bra.la, lb = bra.lb, lc = ket.la, ld = ket.lb;
                         const int same = qcs[t].X == qcs[t].Y;
-                        // chunk size of the family the dispatcher will pick
-                        const int variant = t < P->kvar.size() ? P->kvar[t] : 0;
-                        const int chunk = family_chunk(la, lb, lc, ld, variant);
                         const int nseg = bra.n * B2_NBUCKET;
                         if (P->profiling) CUDA_TRY(cudaEventRecord(P->cls_ev[2 * t], s));
                         // pass 0: float64 quartets (all of them unless mixed);
                         // pass 1: the float32 quartets of mixed precision
                         for (int pass = 0; pass < (mixed ? 2 : 1); pass++) {
+                                // chunk size of the family the dispatcher will pick
+                                const int variant = class_variant(P, t, pass);
+                                const int chunk = family_chunk(la, lb, lc, ld, variant);
                                 count_kernel<<<grid_for(nseg, 256), 256, 0, s>>>(
                                         bra.view(), ket.view(), same, P->tol > 0 ? P->tol : 0.0, (const double *)P->dmax.p,
                                         chunk, mixed ? P->fp32_tau : 0.0, pass, P->shard, P->nshard, P->nkl.p, P->kst.p,
@@ -1038,22 +1048,36 @@ int b200jk_autotune(b200jk_plan *P, const double *dm, int dev_ptrs, void *stream
                 ok = hk.data();
         }
         P->kvar.assign(nclass, 0);
+        P->kvar32.assign(nclass, 0);
         if ((rc = b200jk_get_jk(P, dm, 1, 1, 1, 1, oj, ok, dev_ptrs, B200JK_PREC_FP64, stream))) goto done;   // warm-up
-        for (int v = 0; v < 2; v++) {
-                P->kvar.assign(nclass, v);
-                if ((rc = b200jk_get_jk(P, dm, 1, 1, 1, 1, oj, ok, dev_ptrs, B200JK_PREC_FP64, stream))) goto done;
-                for (int t = 0; t < nclass; t++) {
-                        int la, lb, lc, ld;
-                        class_l(qcs[t].X, la, lb);
-                        class_l(qcs[t].Y, lc, ld);
-                        if (v == 1 && !family_has_variant(la, lb, lc, ld)) continue;   // no such variant
-                        if (P->cls[t].ms < best_ms[t]) { best_ms[t] = P->cls[t].ms; best[t] = v; }
+        // float64 variants on FP64 builds, then the float32 pass's variants on
+        // mixed builds (class times there include the float64 pass, whose
+        // variant is already fixed, so the comparison is the float32 pass's)
+        for (int prec = 0; prec < 2; prec++) {
+                std::vector<int> &kv = prec ? P->kvar32 : P->kvar;
+                std::fill(best_ms.begin(), best_ms.end(), 1e300);
+                std::fill(best.begin(), best.end(), 0);
+                for (int v = 0; v < 2; v++) {
+                        kv.assign(nclass, v);
+                        if ((rc = b200jk_get_jk(P, dm, 1, 1, 1, 1, oj, ok, dev_ptrs,
+                                                prec ? B200JK_PREC_MIXED : B200JK_PREC_FP64, stream)))
+                                goto done;
+                        for (int t = 0; t < nclass; t++) {
+                                int la, lb, lc, ld;
+                                class_l(qcs[t].X, la, lb);
+                                class_l(qcs[t].Y, lc, ld);
+                                if (v == 1 && !family_has_variant(la, lb, lc, ld)) continue;   // no such variant
+                                if (P->cls[t].ms < best_ms[t]) { best_ms[t] = P->cls[t].ms; best[t] = v; }
+                        }
                 }
+                kv = best;
         }
-        P->kvar = best;
 done:
         P->profiling = saved_prof;
-        if (rc) P->kvar.assign(nclass, 0);
+        if (rc) {
+                P->kvar.assign(nclass, 0);
+                P->kvar32.assign(nclass, 0);
+        }
         return rc;
 }
 
@@ -1065,11 +1089,32 @@ int b200jk_set_tile(b200jk_plan *P, int tile_b)
         return B200JK_OK;
 }
 
-int b200jk_get_tuning(const b200jk_plan *P, int *variants, int max, int *n)
+int b200jk_get_tuning(const b200jk_plan *P, int precision, int *variants, int max, int *n)
 {
         if (!P || !n) return fail(B200JK_EINVAL, "NULL argument");
+        if (precision != B200JK_PREC_FP64 && precision != B200JK_PREC_MIXED)
+                return fail(B200JK_EINVAL, "precision must be B200JK_PREC_FP64 or B200JK_PREC_MIXED");
         *n = (int)quartet_classes().size();
-        for (int t = 0; t < *n && t < max && variants; t++) variants[t] = t < (int)P->kvar.size() ? P->kvar[t] : 0;
+        const int pass = precision == B200JK_PREC_MIXED ? 1 : 0;
+        for (int t = 0; t < *n && t < max && variants; t++) variants[t] = class_variant(P, t, pass);
+        return B200JK_OK;
+}
+
+int b200jk_set_tuning(b200jk_plan *P, int precision, const int *variants, int n)
+{
+        if (!P || !variants) return fail(B200JK_EINVAL, "NULL argument");
+        if (precision != B200JK_PREC_FP64 && precision != B200JK_PREC_MIXED)
+                return fail(B200JK_EINVAL, "precision must be B200JK_PREC_FP64 or B200JK_PREC_MIXED");
+        auto qcs = quartet_classes();
+        if (n != (int)qcs.size()) return fail(B200JK_EINVAL, "one variant per quartet class (55) is required");
+        for (int t = 0; t < n; t++) {
+                int la, lb, lc, ld;
+                class_l(qcs[t].X, la, lb);
+                class_l(qcs[t].Y, lc, ld);
+                if (variants[t] != 0 && !(variants[t] == 1 && family_has_variant(la, lb, lc, ld)))
+                        return fail(B200JK_EINVAL, "variant not available for this quartet class");
+        }
+        (precision == B200JK_PREC_MIXED ? P->kvar32 : P->kvar).assign(variants, variants + n);
         return B200JK_OK;
 }
 
@@ -1693,11 +1738,11 @@ static int batch_build(b200jk_batch *B, const double *const *dms, int hermi, int
                 int la, lb, lc, ld;
                 class_l(qcs[t].X, la, lb);
                 class_l(qcs[t].Y, lc, ld);
-                const int variant = t < B->plans[0]->kvar.size() ? B->plans[0]->kvar[t] : 0;
-                const int chunk = family_chunk(la, lb, lc, ld, variant);
                 for (int pass = 0; pass < (mixed ? 2 : 1); pass++) {
                         const int nm = ncnt[2 * t + pass];
                         if (nm == 0) continue;
+                        const int variant = class_variant(B->plans[0], t, pass);
+                        const int chunk = family_chunk(la, lb, lc, ld, variant);
                         const JKArgs *dargs = B->args.p + at[2 * t + pass];
                         const int *dseg = B->segoff.p + sat[2 * t + pass];
                         const int segs = h_segoff[sat[2 * t + pass] + nm];

@@ -27,7 +27,7 @@ EXPORTS = (
     'b200jk_stats', 'b200jk_hostcheck_cart_quartet', 'b200jk_class_stats', 'b200jk_set_profiling',
     'b200jk_measure_fp64_peak', 'b200jk_get_jk_noalloc', 'b200jk_set_mixed_threshold',
     'b200jk_hostcheck_cart_quartet_fp32', 'b200jk_grad_jk', 'b200jk_grad_stats', 'b200jk_get_grad_q_cond',
-    'b200jk_set_shard', 'b200jk_grad_class_stats', 'b200jk_autotune', 'b200jk_get_tuning', 'b200jk_set_tile', 'b200jk_batch_get_jk_async', 'b200jk_batch_create', 'b200jk_batch_destroy', 'b200jk_batch_get_jk', 'b200jk_batch_stats',
+    'b200jk_set_shard', 'b200jk_grad_class_stats', 'b200jk_autotune', 'b200jk_get_tuning', 'b200jk_set_tuning', 'b200jk_set_tile', 'b200jk_batch_get_jk_async', 'b200jk_batch_create', 'b200jk_batch_destroy', 'b200jk_batch_get_jk', 'b200jk_batch_stats',
 )
 
 
@@ -90,7 +90,8 @@ def load(path=LIB_PATH):
         lib.b200jk_set_shard.argtypes = [vp, ip, ip]
         lib.b200jk_grad_class_stats.argtypes = [vp, ctypes.POINTER(ClassStat), ip, ctypes.POINTER(ip)]
         lib.b200jk_autotune.argtypes = [vp, vp, ip, vp]
-        lib.b200jk_get_tuning.argtypes = [vp, ctypes.POINTER(ip), ip, ctypes.POINTER(ip)]
+        lib.b200jk_get_tuning.argtypes = [vp, ip, ctypes.POINTER(ip), ip, ctypes.POINTER(ip)]
+        lib.b200jk_set_tuning.argtypes = [vp, ip, ctypes.POINTER(ip), ip]
         lib.b200jk_set_tile.argtypes = [vp, ip]
         lib.b200jk_batch_create.argtypes = [vp, ip, ctypes.POINTER(vp)]
         lib.b200jk_batch_destroy.argtypes = [vp]
@@ -172,8 +173,9 @@ class Plan:
         check(load().b200jk_set_profiling(self._h, int(bool(on))))
 
     def autotune(self, dm):
-        """Pick the faster launch variant per quartet class on one FP64 build
-        of `dm` (host array or CUDA tensor); returns the variants."""
+        """Pick the faster launch variant per quartet class on FP64 builds of
+        `dm` (host array or CUDA tensor), then for the float32 pass on mixed
+        builds; returns the FP64 variants."""
         try:
             import torch
             is_dev = isinstance(dm, torch.Tensor) and dm.is_cuda
@@ -192,11 +194,17 @@ class Plan:
         """Bra pairs per tile of the ket-chunk-major order (0: bra-major)."""
         check(load().b200jk_set_tile(self._h, int(tile_b)))
 
-    def tuning(self):
+    def tuning(self, precision=PREC_FP64):
+        """Variant per quartet class for float64 quartets, or with
+        PREC_MIXED for the float32 pass of mixed builds."""
         n = ctypes.c_int(0)
         buf = (ctypes.c_int * 64)()
-        check(load().b200jk_get_tuning(self._h, buf, 64, ctypes.byref(n)))
+        check(load().b200jk_get_tuning(self._h, int(precision), buf, 64, ctypes.byref(n)))
         return list(buf[:n.value])
+
+    def set_tuning(self, variants, precision=PREC_FP64):
+        v = (ctypes.c_int * len(variants))(*[int(x) for x in variants])
+        check(load().b200jk_set_tuning(self._h, int(precision), v, len(variants)))
 
     def set_shard(self, index, count):
         """Evaluate only bra pairs ij = index (mod count): partial J/K for one of count GPUs."""

@@ -185,8 +185,45 @@ def test_autotune_keeps_results(b2):
     f = load_fixture('h2o8_vdz')
     p = plan_for(b2, f)
     tun = p.autotune(f['dm_conv'])
-    assert len(tun) == 55 and set(tun) <= {0, 1}
+    tun32 = p.tuning(b2.PREC_MIXED)
+    assert len(tun) == len(tun32) == 55 and set(tun) | set(tun32) <= {0, 1}
     for dm, rj, rk in [(f['dm_rand'], f['vj_rand'], f['vk_rand']), (f['dm_conv'], f['vj_conv'], f['vk_conv'])]:
         vj, vk = p.get_jk(dm, hermi=1)
         assert abs(vj - rj).max() < TOL_JK
         assert abs(vk - rk).max() < TOL_JK
+    vj, vk = p.get_jk(f['dm_conv'], hermi=1, precision=b2.PREC_MIXED)
+    assert abs(vj - f['vj_conv']).max() < 1e-8
+    assert abs(vk - f['vk_conv']).max() < 1e-8
+
+
+def test_set_tuning_every_variant(b2):
+    """Every class that has a second variant, forced to it in both
+    precisions, reproduces the reference J/K; a variant a class lacks is
+    refused."""
+    f = load_fixture('h2o2_vtz')
+    p = plan_for(b2, f)
+    p.autotune(f['dm_rand'])
+    have = [0] * 55
+    for t in range(55):
+        one = [0] * 55
+        one[t] = 1
+        try:
+            p.set_tuning(one)
+            have[t] = 1
+        except RuntimeError:
+            pass
+    assert sum(have) > 0
+    with pytest.raises(RuntimeError):
+        p.set_tuning([1] * 55)
+    with pytest.raises(RuntimeError):
+        p.set_tuning([0] * 54)
+    p.set_tuning(have)
+    p.set_tuning(have, b2.PREC_MIXED)
+    assert p.tuning() == have and p.tuning(b2.PREC_MIXED) == have
+    vj, vk = p.get_jk(f['dm_rand'], hermi=1)
+    assert abs(vj - f['vj_rand']).max() < TOL_JK
+    assert abs(vk - f['vk_rand']).max() < TOL_JK
+    p.set_mixed_threshold(1e30)
+    vj, vk = p.get_jk(f['dm_rand'], hermi=1, precision=b2.PREC_MIXED)
+    assert abs(vj - f['vj_rand']).max() < 2e-5 * abs(f['vj_rand']).max()
+    assert abs(vk - f['vk_rand']).max() < 2e-5 * abs(f['vk_rand']).max()
