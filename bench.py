@@ -294,6 +294,43 @@ def batch_report(local, flush, stream, steps, tau):
             'density': 'per molecule C C^T, C nao x 5n N(0,1)/sqrt(nao), seed 405'}
 
 
+def _fp(a):
+    """PySCF's lib.fp fingerprint (pyscf/lib/misc.py:1259-1263), on the GPU."""
+    import torch
+    a = a.reshape(-1)
+    w = torch.cos(torch.arange(a.numel(), device=a.device, dtype=torch.float64))
+    return float(torch.dot(w, a))
+
+
+def vs_oracle(workload, d, vj64, vk64, plan, tau):
+    """FP64 and mixed J/K against the reference drivers' J/K of the same
+    density (sampled rows, E2, fingerprints); None without the fixture."""
+    import torch
+    from pyscf_b200 import lib
+    path = os.path.join(GOLDEN, 'jk_%s.npz' % workload)
+    if not os.path.exists(path):
+        return {'error': 'no reference fixture %s' % os.path.basename(path)}
+    g = dict(numpy.load(path))
+    rows = torch.tensor(g['rows'], device=d.device, dtype=torch.long)
+    rj = torch.tensor(g['vj_rows'], device=d.device)
+    rk = torch.tensor(g['vk_rows'], device=d.device)
+    e2_ref = float(g['e2'])
+
+    def cmp(vj, vk):
+        e2 = float(0.5 * torch.sum(d * vj) - 0.25 * torch.sum(d * vk))
+        return {'max_dJ_rows': float((vj[rows] - rj).abs().max()), 'max_dK_rows': float((vk[rows] - rk).abs().max()),
+                'dE2_Eh': e2 - e2_ref, 'dfp_J': _fp(vj) - float(g['fp_j']), 'dfp_K': _fp(vk) - float(g['fp_k'])}
+    out = {'reference': 'PySCF CVHFnr_direct_drv (reference sources, oracle integral library), %d sampled rows '
+                        'of %d shells, E2 = %.10f' % (len(g['rows']), len(g['shells']), e2_ref),
+           'fp64': cmp(vj64, vk64)}
+    plan.set_mixed_threshold(tau)
+    vj, vk = plan.get_jk_device(d, hermi=1, precision=lib.PREC_MIXED)
+    plan.set_mixed_threshold(0.0)
+    out['mixed'] = cmp(vj, vk)
+    out['mixed']['tau'] = tau
+    return out
+
+
 def scf_report(local, tau):
     """Per-iteration errors of a mixed-precision RHF on C20H42/cc-pVDZ."""
     from pyscf_b200 import lib, rhf
@@ -407,6 +444,11 @@ def run_gpu(args):
                 'speedup_vs_fp64': ms64 / ms32, 'fp32_quartet_fraction': s32['fp32_quartets'] / max(1, s32['quartets']),
                 'max_dJ': dj, 'max_dK': dk, 'dE_Eh': de}
     mixed = [mixed_report(d, 'D', args.steps)]
+    # FP64 and mixed J/K of the workload density against the reference's
+    # driver (tests/golden/jk_<workload>.npz, written by
+    # tests/golden/make_h2o64_golden.py): sampled rows element-wise, the
+    # two-electron energy E2 = 1/2 tr(D J) - 1/4 tr(D K) and the fingerprints
+    oracle_cmp = vs_oracle(args.config, d, vj64, vk64, plan, args.tau) if world == 1 else None
     rng = numpy.random.default_rng(305)
     c2 = rng.standard_normal((nao, 64)) / numpy.sqrt(nao)
     dd = torch.tensor(1e-4 * (c2 @ c2.T), device=dev)
@@ -504,7 +546,6 @@ def run_gpu(args):
                          'achieved': achieved, 'peak': fp64_peak, 'unit': 'TFLOP/s', 'frac': achieved / fp64_peak,
                          'peak_source': 'measured FP64 FMA loop on this GPU (b200jk_measure_fp64_peak)',
                          'share': dom_ms * 1e-3 / (sum(times) / args.steps), 'traffic': traffic},
-            'mixed': mixed,
             'grad': grad_line,
             'batch': batch_line,
             'scf': scf_line,
@@ -518,7 +559,7 @@ def run_gpu(args):
                          'share': c['ms'] * 1e-3 / (sum(times) / args.steps),
                          'quartets_per_build': c['quartets'],
                          'tflops': flops.class_flops(c) / (c['ms'] * 1e-3) / 1e12 if c['ms'] > 0 else None}
-                        for c in sorted(cls, key=lambda c: -c['ms'])[:12]],
+                        for c in sorted(cls, key=lambda c: -c['ms'])[:8]],
             'gpu_launches': int(tot['kernel_launches']),
             'clocks': clocks,
         }
@@ -535,6 +576,19 @@ def run_gpu(args):
             except Exception as e:  # the baseline must not sink the GPU measurement
                 cb = {'value': None, 'error': str(e)[:200]}
         line['cpu_baseline'] = cb
+        # last, so that a truncated log still shows them: the mixed-precision
+        # builds (speed-up over FP64, float32 fraction, errors) and both
+        # precisions against the reference drivers' J/K
+        line['vs_oracle'] = oracle_cmp
+        line['mixed'] = mixed
+        m0 = mixed[0]
+        line['mixed_summary'] = {'speedup_vs_fp64': m0['speedup_vs_fp64'], 'ms_per_build': m0['ms_per_build'],
+                                 'fp64_ms_per_build': m0['fp64_ms_per_build'],
+                                 'fp32_quartet_fraction': m0['fp32_quartet_fraction'], 'tau': m0['tau'],
+                                 'dE2_vs_oracle_Eh': (oracle_cmp or {}).get('mixed', {}).get('dE2_Eh'),
+                                 'max_dJ_vs_oracle': (oracle_cmp or {}).get('mixed', {}).get('max_dJ_rows'),
+                                 'max_dK_vs_oracle': (oracle_cmp or {}).get('mixed', {}).get('max_dK_rows'),
+                                 'dD_speedup_vs_fp64': mixed[1]['speedup_vs_fp64'] if len(mixed) > 1 else None}
         print(json.dumps(line))
     if dist is not None:
         dist.barrier()

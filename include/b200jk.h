@@ -52,6 +52,10 @@ extern "C" {
                                     float32, all contraction and accumulation in
                                     float64; tau set by b200jk_set_mixed_threshold */
 
+#define B200JK_SCREEN_NRS8   0   /* CVHFnrs8_prescreen (J and K terms) */
+#define B200JK_SCREEN_VJ     1   /* CVHFnrs8_vj_prescreen (J terms only) */
+#define B200JK_SCREEN_VK     2   /* CVHFnrs8_vk_prescreen (K terms only) */
+
 typedef struct b200jk_plan b200jk_plan;
 typedef struct b200jk_batch b200jk_batch;
 
@@ -89,12 +93,26 @@ int b200jk_device_count(int *count);
 
 /* Build a plan for one molecule/basis: shell pairs, primitive pairs and the
  * Schwarz conditioner q_cond on GPU `device`.  direct_scf_tol <= 0 disables
- * screening (the reference's vhfopt=None). */
+ * screening (the reference's vhfopt=None).  The molecule arrays are checked
+ * on the host before any device work: atom indices and env pointers out of
+ * range give B200JK_EINVAL, l > 3 and env[PTR_RANGE_OMEGA] != 0 give
+ * B200JK_EUNSUPPORTED, without touching a GPU. */
 int b200jk_plan_create(const int32_t *atm, int natm, const int32_t *bas, int nbas,
                        const double *env, int env_len, int cart, double direct_scf_tol,
                        int device, b200jk_plan **out);
 
 int b200jk_plan_destroy(b200jk_plan *plan);
+
+/* Move the plan to a new geometry: env is the molecule's env array with new
+ * coordinates (same atoms and basis as at creation).  The shell pairs,
+ * primitive pairs and q_cond are planned again; workspaces, stream, tuning,
+ * shard, screen and mixed threshold are kept, so a geometry scan or an
+ * autograd forward pass reuses the plan instead of creating one per point.
+ * Graphs captured from batched builds of the plan become invalid (the next
+ * b200jk_batch_get_jk_async refuses until b200jk_batch_get_jk ran).  The
+ * reference rebuilds its _VHFOpt per geometry (SCF.init_direct_scf,
+ * pyscf/scf/hf.py:2045-2054, after mol.set_geom_). */
+int b200jk_plan_update_coords(b200jk_plan *plan, const double *env, int env_len);
 
 /* nao in the output basis, nbas. */
 int b200jk_plan_dims(const b200jk_plan *plan, int *nao, int *nbas);
@@ -105,8 +123,12 @@ int b200jk_get_q_cond(const b200jk_plan *plan, double *q_cond);
 /* J/K for n_dm densities.  dms, vj, vk are (n_dm, nao, nao) C-ordered;
  * vj / vk may be NULL when with_j / with_k is 0.  Outputs are overwritten.
  * hermi: 1 symmetric densities, 0 general, 2 antisymmetric (as PySCF).
- * dev_ptrs: 0 host arrays, 1 device arrays on the plan's GPU.
- * stream: a cudaStream_t or NULL. */
+ * dev_ptrs: 0 host arrays, 1 device arrays on the plan's GPU (other memory is
+ * rejected with B200JK_EINVAL).  stream: a cudaStream_t or NULL.
+ * Non-finite density entries are not rejected (nor are they by the
+ * reference): the screening bound ignores them and they propagate into the
+ * J/K elements of every quartet that contracts with them; the plan stays
+ * usable for the next build. */
 int b200jk_get_jk(b200jk_plan *plan, const double *dms, int n_dm, int hermi,
                   int with_j, int with_k, double *vj, double *vk,
                   int dev_ptrs, int precision_mode, void *stream);
@@ -114,16 +136,19 @@ int b200jk_get_jk(b200jk_plan *plan, const double *dms, int n_dm, int hermi,
 /* J/K like b200jk_get_jk, for callers that cannot let the library allocate
  * device memory (code running under a framework's caching allocator or a
  * fixed memory budget, where a cudaMalloc can fail or stall the device).  It
- * has no counterpart in the reference.  dms, vj, vk are device arrays on the
- * plan's GPU; nothing is allocated: all intermediates live in one fixed
- * 32 MiB scratch array that every GPU loading the library holds until exit,
- * which bounds the size (roughly nao_cart <= 600 for one density); larger
- * inputs are rejected with B200JK_EINVAL and a message.  The first call on a
- * device resolves the scratch array's device address; make that first call
- * before any stream capture.  All calls share the one array: calls that
- * overlap on the GPU (other streams, other threads) race and must be
- * serialised by the caller.  The plan itself is created (and allocated) by
- * b200jk_plan_create beforehand. */
+ * has no counterpart in the reference.  dms, vj, vk must be device arrays on
+ * the plan's GPU (anything else is rejected with B200JK_EINVAL); nothing is
+ * allocated: all intermediates live in one fixed 32 MiB scratch array that
+ * every GPU loading the library holds until exit, which bounds the size
+ * (roughly nao_cart <= 600 for one density); larger inputs are rejected with
+ * B200JK_EINVAL and a message giving the bytes needed.  The first call on a
+ * device also resolves the scratch array's device address (a one-time
+ * set-up); make that first call before any stream capture begins.  The call
+ * returns after `stream` has finished the build.  All calls share the one
+ * array: calls that overlap on the GPU (other streams, other threads) race
+ * and must be serialised by the caller.  A sharded plan (b200jk_set_shard)
+ * gives its partial J/K, as b200jk_get_jk does.  The plan itself is created
+ * (and allocated) by b200jk_plan_create beforehand. */
 int b200jk_get_jk_noalloc(b200jk_plan *plan, const double *dms, int n_dm, int hermi,
                           int with_j, int with_k, double *vj, double *vk, void *stream);
 
@@ -176,6 +201,19 @@ int b200jk_set_tuning(b200jk_plan *plan, int precision, const int *variants, int
 int b200jk_grad_jk(b200jk_plan *plan, const double *dms, int n_dm, int with_j, int with_k,
                    double *vj, double *vk, int dev_ptrs, double direct_scf_tol, void *stream);
 
+/* The two-electron part of the RHF nuclear gradient, contracted on the GPU
+ * without forming vj/vk: for one symmetric density dm (nao x nao, C order)
+ *     de[A][x] = 2 sum_{i in A} sum_j (vj - vk/2)[x][i][j] dm[i][j]
+ * with vj, vk those of b200jk_grad_jk, i.e. the term grad_elec adds from
+ * get_veff (pyscf/grad/rhf.py:62-68, get_veff :180-183 -> get_jk :149-178).
+ * Each quartet contributes sum_abcd (d_x ab|cd) W_abcd with
+ * W = 2 D_ab (D_cd + D_dc) - D_ac D_bd - D_ad D_bc, summed over the warp that
+ * owns the bra pair before one atomic per atom and direction: no
+ * (3, nao, nao) arrays are materialised.  de is (natm, 3), overwritten; host
+ * or device memory as dev_ptrs; the screen is b200jk_grad_jk's. */
+int b200jk_grad_contract(b200jk_plan *plan, const double *dm, double *de, int dev_ptrs,
+                         double direct_scf_tol, void *stream);
+
 /* Counters of the last gradient build: shell quartets (bra sides), primitive
  * quartets, device time (ms), kernels launched by this library. */
 int b200jk_grad_stats(const b200jk_plan *plan, int64_t *quartets, int64_t *prim_quartets, double *ms,
@@ -211,8 +249,12 @@ int b200jk_batch_get_jk(b200jk_batch *batch, const double *const *dms, int hermi
  * replay the whole batched build; the graph reads dms[m] and writes vj[m],
  * vk[m] at the addresses given here.  Needs one b200jk_batch_get_jk call
  * with the same arguments first (it sizes every buffer); one captured graph
- * per batch at a time (they share the pinned argument staging).  No
- * reference counterpart. */
+ * per batch at a time (they share the pinned argument staging).  A captured
+ * graph holds the addresses of the plans' workspaces: a later build on one
+ * of the plans that grows its workspace (b200jk_get_jk with more densities)
+ * or destroying a plan invalidates it.  This call detects the first case and
+ * returns B200JK_EINVAL until b200jk_batch_get_jk has run again; the caller
+ * must not replay graphs captured before.  No reference counterpart. */
 int b200jk_batch_get_jk_async(b200jk_batch *batch, const double *const *dms, int hermi, int with_j, int with_k,
                               double *const *vj, double *const *vk, int precision_mode, void *stream);
 
@@ -229,6 +271,16 @@ int b200jk_batch_stats(const b200jk_batch *batch, int64_t *quartets, int64_t *fp
  * (pyscf/lib/vhf/nr_direct.c:355-476) across GPUs. */
 int b200jk_set_shard(b200jk_plan *plan, int index, int count);
 
+/* Density part of the per-quartet screen for the plan's later builds:
+ * B200JK_SCREEN_NRS8 (default) keeps a quartet when
+ * max(4 D_ji, 4 D_lk, D_jk, D_jl, D_ik, D_il) q_ij q_kl > tol, _VJ uses the
+ * two J terms only, _VK the four K terms only.  The reference sets these on
+ * its _VHFOpt (CVHFnrs8_prescreen / CVHFnrs8_vj_prescreen /
+ * CVHFnrs8_vk_prescreen, pyscf/lib/vhf/optimizer.c:90-167); SCF.get_jk
+ * switches to the J or K screen when only one of J, K is built
+ * (pyscf/scf/hf.py:2069-2077). */
+int b200jk_set_prescreen(b200jk_plan *plan, int screen);
+
 /* Threshold tau of B200JK_PREC_MIXED (default 1e-6): a shell quartet whose
  * Schwarz bound times the largest density element, q_ij q_kl max|D|, is below
  * tau is evaluated in float32.  The bound uses the density passed to each
@@ -241,6 +293,11 @@ int b200jk_set_mixed_threshold(b200jk_plan *plan, double tau);
  * register-resident FMA loop over all SMs: the denominator of the FP64
  * roofline fraction. */
 int b200jk_measure_fp64_peak(int device, double *tflops);
+
+/* Test hook, no reference counterpart: the nth device allocation made by
+ * the library from now on fails as an out-of-memory condition would (the
+ * call returns B200JK_ENOMEM and frees what it had taken); 0 turns it off. */
+int b200jk_debug_fail_alloc(int nth);
 
 /* Host replay of the device integral code for one shell quartet (no GPU is
  * used): the Cartesian block (ab|cd) of shells shls[0..3] of the given

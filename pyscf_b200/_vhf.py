@@ -62,7 +62,7 @@ class VHFOpt:
                  direct_scf_tol=1e-13, device=0):
         if intor not in ('int2e', 'int2e_sph', 'int2e_cart'):
             raise NotImplementedError('VHFOpt supports the int2e Coulomb kernel only, not %s' % intor)
-        if prescreen not in ('CVHFnrs8_prescreen', 'CVHFnoscreen', None):
+        if prescreen not in _SCREENS and prescreen not in ('CVHFnoscreen', None):
             raise NotImplementedError('prescreen %s is not implemented' % prescreen)
         _check_env(mol._env)
         self.mol = mol
@@ -70,7 +70,7 @@ class VHFOpt:
         self._prescreen = prescreen
         self._qcondname = qcondname
         self._dmcondname = dmcondname
-        tol = direct_scf_tol if prescreen == 'CVHFnrs8_prescreen' else 0.0
+        tol = direct_scf_tol if prescreen in _SCREENS else 0.0
         self.plan = lib.Plan(mol._atm, mol._bas, mol._env, cart=getattr(mol, 'cart', False),
                              direct_scf_tol=tol, device=device)
         self._direct_scf_tol = direct_scf_tol
@@ -78,6 +78,25 @@ class VHFOpt:
     @property
     def direct_scf_tol(self):
         return self._direct_scf_tol
+
+    @property
+    def prescreen(self):
+        """Name of the per-quartet screen (the reference's _VHFOpt.prescreen,
+        pyscf/scf/_vhf.py:219-226).  SCF.get_jk swaps in the J-only or K-only
+        screen with lib.temporary_env when only one of J, K is built
+        (pyscf/scf/hf.py:2069-2077); each build uses the current value."""
+        return self._prescreen
+
+    @prescreen.setter
+    def prescreen(self, v):
+        if v not in _SCREENS:
+            if self._prescreen in (None, 'CVHFnoscreen') and v in (None, 'CVHFnoscreen'):
+                self._prescreen = v
+                return
+            raise NotImplementedError('prescreen %s is not implemented' % v)
+        if self._prescreen in (None, 'CVHFnoscreen'):
+            raise NotImplementedError('an unscreened VHFOpt cannot switch to %s' % v)
+        self._prescreen = v
 
     @property
     def q_cond(self):
@@ -90,14 +109,22 @@ class VHFOpt:
                 and self.plan.cart == bool(cart))
 
 
+# the reference's per-quartet screens and the engine's modes for them
+_SCREENS = {'CVHFnrs8_prescreen': lib.SCREEN_NRS8, 'CVHFnrs8_vj_prescreen': lib.SCREEN_VJ,
+            'CVHFnrs8_vk_prescreen': lib.SCREEN_VK}
+
+
 def _resolve_plan(vhfopt, atm, bas, env, cart):
     if isinstance(vhfopt, VHFOpt) and vhfopt.matches(atm, bas, env, cart):
+        vhfopt.plan.set_prescreen(_SCREENS.get(vhfopt.prescreen, lib.SCREEN_NRS8))
         return vhfopt.plan
     if vhfopt is None:
         # the reference runs CVHFnr_direct_drv without any screening here
         return cached_plan(atm, bas, env, cart, 0.0)
     tol = getattr(vhfopt, 'direct_scf_tol', 1e-13)
-    return cached_plan(atm, bas, env, cart, tol)
+    plan = cached_plan(atm, bas, env, cart, tol)
+    plan.set_prescreen(_SCREENS.get(getattr(vhfopt, 'prescreen', None), lib.SCREEN_NRS8))
+    return plan
 
 
 def direct(dms, atm, bas, env, vhfopt=None, hermi=0, cart=False,

@@ -50,6 +50,29 @@ def up_to_date(target=LIB):
     return all(os.path.getmtime(f) <= t for f in _deps())
 
 
+# headers each translation unit includes (directly or through another header)
+_RYS = ['rys_math.cuh', 'rys_table.inc', 'rys_table_f.inc']
+_JK = _RYS + ['jk_kernels.cuh', 'jk_launch.h']
+_GRAD = _JK + ['grad_kernels.cuh', 'grad_launch.h']
+UNIT_DEPS = {
+    'b200jk.cu': _GRAD + ['../../include/b200jk.h'],
+    'jk_qcond.cu': _JK,
+    'jk_classes.cu': _JK,
+    'grad_classes.cu': _GRAD,
+    'hostcheck.cpp': _RYS + ['../../include/b200jk.h'],
+}
+
+
+def _stale(obj, src, flags_file):
+    """Whether obj must be rebuilt: missing, older than its source, one of
+    its headers or this script, or built with other flags."""
+    if not os.path.exists(obj) or not os.path.exists(flags_file):
+        return True
+    t = os.path.getmtime(obj)
+    deps = [os.path.join(CSRC, src)] + [os.path.join(CSRC, h) for h in UNIT_DEPS[src]] + [os.path.abspath(__file__)]
+    return any(os.path.getmtime(d) > t for d in deps)
+
+
 def _units():
     nvcc = nvcc_path()
     common = [nvcc, *ARCH, '-O3', '-lineinfo', '-std=c++17', '-Xcompiler', '-fPIC',
@@ -75,6 +98,13 @@ def _units():
     return units
 
 
+def _source_of(cmd):
+    for a in cmd:
+        if a.startswith(CSRC + os.sep):
+            return os.path.basename(a)
+    raise ValueError(cmd)
+
+
 def build(force=False, verbose=False, extra=(), jobs=None):
     if not force and up_to_date():
         return LIB
@@ -82,14 +112,25 @@ def build(force=False, verbose=False, extra=(), jobs=None):
     units = _units()
     if extra:
         units = [(cmd[:-3] + list(extra) + cmd[-3:] if cmd[0] != 'g++' else cmd, o) for cmd, o in units]
+    # rebuild only the units whose sources, headers or flags changed
+    todo = []
+    for cmd, o in units:
+        flags_file = o + '.cmd'
+        line = ' '.join(cmd)
+        same_flags = os.path.exists(flags_file) and open(flags_file).read() == line
+        if force or not same_flags or _stale(o, _source_of(cmd), flags_file):
+            todo.append((cmd, o))
 
     def run(u):
         cmd, o = u
         r = subprocess.run(cmd, capture_output=True, text=True)
+        if r.returncode == 0:
+            with open(o + '.cmd', 'w') as fh:
+                fh.write(' '.join(cmd))
         return cmd, r
 
     with ThreadPoolExecutor(jobs or min(12, os.cpu_count() or 4)) as ex:
-        results = list(ex.map(run, units))
+        results = list(ex.map(run, todo))
     msgs = []
     for cmd, r in results:
         if r.returncode != 0:

@@ -22,6 +22,7 @@
 #include <algorithm>
 #include <numeric>
 #include <mutex>
+#include <atomic>
 
 #define RYS_TABLE_QUALIFIER static const
 #include "rys_math.cuh"
@@ -49,6 +50,39 @@ static int fail(int code, const std::string &msg)
                         return fail(B200JK_ECUDA, std::string(#expr) + ": " +          \
                                                       cudaGetErrorString(_e));         \
         } while (0)
+
+// A pointer the caller declares to be device memory must be memory the
+// kernels of `device` can address: device (or managed) memory of that GPU.
+// Host memory handed to a kernel would fault the GPU instead of returning an
+// error, so it is rejected here.
+static int check_dev_ptr(const void *p, int device, const char *what)
+{
+        if (!p) return B200JK_OK;
+        cudaPointerAttributes at;
+        const cudaError_t e = cudaPointerGetAttributes(&at, p);
+        if (e != cudaSuccess) {
+                cudaGetLastError();
+                return fail(B200JK_EINVAL, std::string(what) + " is not a CUDA pointer");
+        }
+        if (at.type != cudaMemoryTypeDevice && at.type != cudaMemoryTypeManaged)
+                return fail(B200JK_EINVAL, std::string(what) + " is not device memory (pass dev_ptrs = 0 for host arrays)");
+        if (at.type == cudaMemoryTypeDevice && at.device != device)
+                return fail(B200JK_EINVAL, std::string(what) + " lives on cuda:" + std::to_string(at.device) +
+                                                   ", the plan on cuda:" + std::to_string(device));
+        return B200JK_OK;
+}
+
+// Test hook: when positive, the n-th device allocation from now on fails as
+// an out-of-memory condition would (b200jk_debug_fail_alloc).  0 = off.
+static std::atomic<long long> g_fail_alloc_countdown{0};
+static bool alloc_should_fail()
+{
+        long long v = g_fail_alloc_countdown.load();
+        while (v > 0) {
+                if (g_fail_alloc_countdown.compare_exchange_weak(v, v - 1)) return v == 1;
+        }
+        return false;
+}
 
 // slot layout of PySCF's _atm/_bas/_env (pyscf/gto/mole.py:58-88)
 enum { CHARGE_OF = 0, PTR_COORD = 1, ATM_SLOTS = 6 };
@@ -145,7 +179,7 @@ static int dev_upload(DevArr<T> &d, const std::vector<T> &h)
         d.release();
         d.n = h.size();
         if (d.n == 0) return B200JK_OK;
-        if (cudaMalloc(&d.p, sizeof(T) * d.n) != cudaSuccess) {
+        if (alloc_should_fail() || cudaMalloc(&d.p, sizeof(T) * d.n) != cudaSuccess) {
                 d.p = nullptr;
                 return fail(B200JK_ENOMEM, "cudaMalloc failed for a plan table");
         }
@@ -159,7 +193,7 @@ static int dev_alloc(DevArr<T> &d, size_t n)
         if (d.n >= n && d.p) return B200JK_OK;
         d.release();
         if (n == 0) return B200JK_OK;
-        if (cudaMalloc(&d.p, sizeof(T) * n) != cudaSuccess) {
+        if (alloc_should_fail() || cudaMalloc(&d.p, sizeof(T) * n) != cudaSuccess) {
                 d.p = nullptr;
                 return fail(B200JK_ENOMEM, "cudaMalloc failed for a workspace buffer");
         }
@@ -205,7 +239,8 @@ struct GradPlan {
         DevArr<int2> goff;
         std::vector<size_t> goff_at;   // [X * NPAIRCLASS + Y], then NPAIRCLASS^2 + X for q0
         std::vector<double> h_q0;
-        DevArr<double> D, Dc, Ds, V, out, dmc, fac;
+        DevArr<double> D, Dc, Ds, V, out, dmc, fac, de;
+        DevArr<int> shell_atom;
         DevArr<unsigned long long> dmax, stats;
         DevArr<int> nkl, kst;
         DevArr<long long> nchunk, chunk_off;
@@ -221,6 +256,7 @@ struct GradPlan {
                 for (auto &c : bra) c.release();
                 for (auto &c : ket) c.release();
                 q0.release(); goff.release(); D.release(); Dc.release(); Ds.release(); V.release(); out.release();
+                de.release(); shell_atom.release();
                 dmc.release(); fac.release(); dmax.release(); stats.release(); nkl.release(); kst.release();
                 nchunk.release(); chunk_off.release(); cub_tmp.release();
         }
@@ -241,6 +277,8 @@ struct b200jk_plan {
         std::vector<int> kvar, kvar32;
         // bra pairs per tile of the tiled chunk order (0: bra-major order)
         int tile_b = 64;
+        // density part of the quartet screen (B200JK_SCREEN_*)
+        int screen = B200JK_SCREEN_NRS8;
         // packed ket blocks for the J contraction: class X's blocks start at
         // pk_off[X] (entries, in ket-list order); pk_src maps entries to the
         // Cartesian matrix
@@ -249,6 +287,8 @@ struct b200jk_plan {
         DevArr<long long> pk_src;
         DevArr<double> Dpk, Jpk;
         std::vector<int> ao_loc;
+        std::vector<int> shell_atom;   // atom of every PySCF shell (bas[:, ATOM_OF])
+        std::vector<int32_t> h_atm, h_bas;   // the molecule's atm / bas (for b200jk_plan_update_coords)
         std::vector<double> h_qcond;
         PairClassDev pc[NPAIRCLASS];
         DevArr<double4> PP;
@@ -262,8 +302,9 @@ struct b200jk_plan {
         std::vector<size_t> goff_at;   // per quartet class
         DevArr<int4> seg_info;
         DevArr<int> out_seg, out_comp, cart_seg, cart_comp, ao_loc_d;
-        // workspace
+        // workspace; ws_gen counts the times its buffers moved
         int ws_ndm = 0;
+        long long ws_gen = 0;
         DevArr<double> D, Dc, Ds, Jacc, Kacc, outJ, outK;
         DevArr<unsigned long long> dmax, stats;
         DevArr<int> nkl, kst;
@@ -493,11 +534,13 @@ static int build_segments(b200jk_plan *P, const int32_t *atm, int natm, const in
                           const double *env, int env_len, std::vector<Seg> &segs)
 {
         P->ao_loc.assign(nbas + 1, 0);
+        P->shell_atom.assign(nbas, 0);
         int cart_off = 0;
         for (int I = 0; I < nbas; I++) {
                 const int32_t *b = bas + (size_t)I * BAS_SLOTS;
                 const int ia = b[ATOM_OF], l = b[ANG_OF], np = b[NPRIM_OF], nc = b[NCTR_OF];
                 if (ia < 0 || ia >= natm) return fail(B200JK_EINVAL, "bas: atom index out of range");
+                P->shell_atom[I] = ia;
                 if (l < 0) return fail(B200JK_EINVAL, "bas: negative angular momentum");
                 if (l > LMAX) return fail(B200JK_EUNSUPPORTED, "angular momentum above f (l > 3) is not implemented");
                 if (np <= 0 || nc <= 0) return fail(B200JK_EINVAL, "bas: empty shell");
@@ -543,14 +586,6 @@ int b200jk_plan_create(const int32_t *atm, int natm, const int32_t *bas, int nba
                 return fail(B200JK_EINVAL, "empty or NULL molecule arrays");
         if (env[PTR_RANGE_OMEGA] != 0.0)
                 return fail(B200JK_EUNSUPPORTED, "range-separated Coulomb (env[PTR_RANGE_OMEGA] != 0) is not implemented");
-        int ndev = 0;
-        if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0)
-                return fail(B200JK_ECUDA, "no CUDA device is available");
-        if (device < 0 || device >= ndev) return fail(B200JK_EINVAL, "device index out of range");
-        CUDA_TRY(cudaSetDevice(device));
-        int rc = ensure_tables(device);
-        if (rc) return rc;
-
         b200jk_plan *P = new b200jk_plan();
         P->device = device;
         P->cart = cart ? 1 : 0;
@@ -558,16 +593,26 @@ int b200jk_plan_create(const int32_t *atm, int natm, const int32_t *bas, int nba
         P->nbas = nbas;
         P->tol = direct_scf_tol > 0 ? direct_scf_tol : 0.0;
         auto bail = [&](int code) { delete P; return code; };
+        // the molecule arrays are checked on the host before any device work:
+        // indices, pointers into env, l <= 3 (the plan object holds no device
+        // memory yet, so bailing out here touches no GPU)
+        std::vector<Seg> segs;
+        int rc = build_segments(P, atm, natm, bas, nbas, env, env_len, segs);
+        if (rc) return bail(rc);
+        int ndev = 0;
+        if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) {
+                cudaGetLastError();
+                return bail(fail(B200JK_ECUDA, "no CUDA device is available"));
+        }
+        if (device < 0 || device >= ndev) return bail(fail(B200JK_EINVAL, "device index out of range"));
+        if (cudaSetDevice(device) != cudaSuccess) return bail(fail(B200JK_ECUDA, "cudaSetDevice failed"));
+        if ((rc = ensure_tables(device))) return bail(rc);
         cudaDeviceProp prop;
         if (cudaGetDeviceProperties(&prop, device) != cudaSuccess) return bail(fail(B200JK_ECUDA, "cudaGetDeviceProperties failed"));
         P->nsm = prop.multiProcessorCount;
         if (cudaStreamCreateWithFlags(&P->stream, cudaStreamNonBlocking) != cudaSuccess ||
             cudaEventCreate(&P->ev0) != cudaSuccess || cudaEventCreate(&P->ev1) != cudaSuccess)
                 return bail(fail(B200JK_ECUDA, "stream/event creation failed"));
-
-        std::vector<Seg> segs;
-        rc = build_segments(P, atm, natm, bas, nbas, env, env_len, segs);
-        if (rc) return bail(rc);
 
         // segment info and basis maps
         std::vector<int4> seg_info(segs.size());
@@ -772,7 +817,46 @@ int b200jk_plan_create(const int32_t *atm, int natm, const int32_t *bas, int nba
         memset(&P->st, 0, sizeof(P->st));
         P->st.nao = P->nao; P->st.nao_cart = P->naoc; P->st.nbas = nbas; P->st.nseg = P->nseg;
         P->st.shell_pairs = P->shell_pairs; P->st.prim_pairs = P->prim_pairs;
+        P->h_atm.assign(atm, atm + (size_t)natm * ATM_SLOTS);
+        P->h_bas.assign(bas, bas + (size_t)nbas * BAS_SLOTS);
         *out = P;
+        return B200JK_OK;
+}
+
+int b200jk_plan_update_coords(b200jk_plan *P, const double *env, int env_len)
+{
+        if (!P) return fail(B200JK_EINVAL, "plan is NULL");
+        // the geometry-dependent tables are planned afresh for the new env
+        // (same atoms and basis), then moved into this plan; its workspaces,
+        // stream, tuning, shard, screen and threshold stay
+        b200jk_plan *T = nullptr;
+        int rc = b200jk_plan_create(P->h_atm.data(), P->natm, P->h_bas.data(), P->nbas, env, env_len, P->cart,
+                                    P->tol > 0 ? P->tol : 0.0, P->device, &T);
+        if (rc) return rc;
+        if (T->nao != P->nao || T->naoc != P->naoc || T->nseg != P->nseg) {
+                b200jk_plan_destroy(T);
+                return fail(B200JK_EINVAL, "the new env changes the basis dimensions");
+        }
+        std::swap(P->PP, T->PP);
+        std::swap(P->PK, T->PK);
+        std::swap(P->PE, T->PE);
+        std::swap(P->segl, T->segl);
+        for (int X = 0; X < NPAIRCLASS; X++) {
+                std::swap(P->pc[X], T->pc[X]);
+                std::swap(P->all_pairs[X], T->all_pairs[X]);
+        }
+        std::swap(P->qcond, T->qcond);
+        std::swap(P->h_qcond, T->h_qcond);
+        std::swap(P->pk_off, T->pk_off);
+        std::swap(P->pk_total, T->pk_total);
+        std::swap(P->pk_src, T->pk_src);
+        std::swap(P->grad, T->grad);   // derivative bounds belong to the old geometry
+        P->shell_pairs = T->shell_pairs;
+        P->prim_pairs = T->prim_pairs;
+        P->st = T->st;
+        // captured batched builds hold the old tables' addresses
+        P->ws_gen++;
+        b200jk_plan_destroy(T);
         return B200JK_OK;
 }
 
@@ -783,9 +867,18 @@ int b200jk_get_q_cond(const b200jk_plan *plan, double *q_cond)
         return B200JK_OK;
 }
 
+// the addresses of a plan's build workspace: a change means that work
+// recorded with the old addresses (a captured batched build) is stale
+static std::vector<const void *> workspace_key(const b200jk_plan *P)
+{
+        return {P->D.p, P->Dc.p, P->Ds.p, P->Jacc.p, P->Kacc.p, P->outJ.p, P->outK.p, P->dm_cond.p, P->dmax.p,
+                P->stats.p, P->Dpk.p, P->Jpk.p, P->nkl.p, P->kst.p, P->nchunk.p, P->chunk_off.p, P->cub_tmp.p};
+}
+
 static int ensure_workspace(b200jk_plan *P, int n_dm)
 {
         const size_t nn = (size_t)P->nao * P->nao, nc = (size_t)P->naoc * P->naoc;
+        const std::vector<const void *> key0 = workspace_key(P);
         int rc;
         if ((rc = dev_alloc(P->D, nn * n_dm)) || (rc = dev_alloc(P->Dc, nc * n_dm * 2)) ||
             (rc = dev_alloc(P->Ds, nc * n_dm)) || (rc = dev_alloc(P->Jacc, nc * n_dm)) ||
@@ -804,6 +897,7 @@ static int ensure_workspace(b200jk_plan *P, int n_dm)
         cub::DeviceScan::ExclusiveSum(nullptr, tmp, P->nchunk.p, P->chunk_off.p, maxn + 1);
         if ((rc = dev_alloc(P->cub_tmp, tmp + 16))) return rc;
         P->ws_ndm = std::max(P->ws_ndm, n_dm);
+        if (workspace_key(P) != key0) P->ws_gen++;
         return B200JK_OK;
 }
 
@@ -821,8 +915,11 @@ int b200jk_get_jk(b200jk_plan *P, const double *dms, int n_dm, int hermi, int wi
                 return fail(B200JK_EUNSUPPORTED, "precision_mode must be 0 (FP64) or 1 (mixed FP32/FP64)");
         const int mixed = precision_mode == B200JK_PREC_MIXED && P->fp32_tau > 0;
         CUDA_TRY(cudaSetDevice(P->device));
-        int rc = ensure_workspace(P, n_dm);
-        if (rc) return rc;
+        int rc;
+        if (dev_ptrs && ((rc = check_dev_ptr(dms, P->device, "dms")) || (with_j && (rc = check_dev_ptr(vj, P->device, "vj"))) ||
+                         (with_k && (rc = check_dev_ptr(vk, P->device, "vk")))))
+                return rc;
+        if ((rc = ensure_workspace(P, n_dm))) return rc;
         cudaStream_t s = stream ? (cudaStream_t)stream : P->stream;
         const size_t nn = (size_t)P->nao * P->nao, nc = (size_t)P->naoc * P->naoc;
         const int nk = hermi == 1 ? 1 : 2;
@@ -938,6 +1035,7 @@ int b200jk_get_jk(b200jk_plan *P, const double *dms, int n_dm, int hermi, int wi
                                 a.tol = P->tol > 0 ? P->tol : -1.0;
                                 a.nbas = P->nbas; a.naoc = P->naoc; a.n_dm = n_dm; a.nk = nk;
                                 a.with_j = with_j; a.with_k = with_k; a.same = same;
+                                a.screen = P->screen;
                                 if ((rc = dispatch_jk(P, la, lb, lc, ld, a, pass, s, nullptr, nullptr, 0, variant))) return rc;
                                 launches += 2;   // count + class kernel (the scan is a CUB library kernel)
                         }
@@ -1015,6 +1113,15 @@ int b200jk_set_shard(b200jk_plan *plan, int index, int count)
         if (count < 1 || index < 0 || index >= count) return fail(B200JK_EINVAL, "shard index must be in [0, count)");
         plan->shard = index;
         plan->nshard = count;
+        return B200JK_OK;
+}
+
+int b200jk_set_prescreen(b200jk_plan *plan, int screen)
+{
+        if (!plan) return fail(B200JK_EINVAL, "plan is NULL");
+        if (screen != B200JK_SCREEN_NRS8 && screen != B200JK_SCREEN_VJ && screen != B200JK_SCREEN_VK)
+                return fail(B200JK_EINVAL, "screen must be B200JK_SCREEN_NRS8, _VJ or _VK");
+        plan->screen = screen;
         return B200JK_OK;
 }
 
@@ -1159,6 +1266,13 @@ int b200jk_measure_fp64_peak(int device, double *tflops)
         sink.release();
         const double flops = 5.0 * grid * block * (double)iters * 8 * 2;
         *tflops = flops / (ms * 1e-3) / 1e12;
+        return B200JK_OK;
+}
+
+int b200jk_debug_fail_alloc(int nth)
+{
+        if (nth < 0) return fail(B200JK_EINVAL, "nth must be >= 0");
+        g_fail_alloc_countdown.store(nth);
         return B200JK_OK;
 }
 
@@ -1322,24 +1436,37 @@ static int ensure_grad(b200jk_plan *P, double tol)
         return B200JK_OK;
 }
 
-extern "C" int b200jk_grad_jk(b200jk_plan *P, const double *dms, int n_dm, int with_j, int with_k, double *vj,
-                              double *vk, int dev_ptrs, double direct_scf_tol, void *stream)
+// The gradient build: vj/vk (de == nullptr) or, for one symmetric density,
+// the fused force contraction into de[natm][3] (host or device, as dev_ptrs).
+static int grad_build(b200jk_plan *P, const double *dms, int n_dm, int with_j, int with_k, double *vj, double *vk,
+                      double *de, int dev_ptrs, double direct_scf_tol, void *stream)
 {
         if (!P) return fail(B200JK_EINVAL, "plan is NULL");
         if (!dms || n_dm <= 0) return fail(B200JK_EINVAL, "no density matrices");
-        if (with_j && !vj) return fail(B200JK_EINVAL, "vj is NULL while with_j is set");
-        if (with_k && !vk) return fail(B200JK_EINVAL, "vk is NULL while with_k is set");
+        if (!de && with_j && !vj) return fail(B200JK_EINVAL, "vj is NULL while with_j is set");
+        if (!de && with_k && !vk) return fail(B200JK_EINVAL, "vk is NULL while with_k is set");
         if (!(direct_scf_tol == direct_scf_tol)) return fail(B200JK_EINVAL, "direct_scf_tol is NaN");
+        const bool fused = de != nullptr;
+        if (fused) {
+                n_dm = 1;
+                with_j = with_k = 1;
+                vj = vk = nullptr;
+        }
         CUDA_TRY(cudaSetDevice(P->device));
+        int rc;
+        if (dev_ptrs && ((rc = check_dev_ptr(dms, P->device, "dms")) || (with_j && (rc = check_dev_ptr(vj, P->device, "vj"))) ||
+                         (with_k && (rc = check_dev_ptr(vk, P->device, "vk"))) || (rc = check_dev_ptr(de, P->device, "de"))))
+                return rc;
         const double tol = direct_scf_tol > 0 ? direct_scf_tol : 0.0;
-        int rc = ensure_grad(P, tol);
-        if (rc) return rc;
+        if ((rc = ensure_grad(P, tol))) return rc;
         GradPlan &g = P->grad;
         const size_t nn = (size_t)P->nao * P->nao, nc = (size_t)P->naoc * P->naoc;
         int maxn = 1;
         for (auto &c : g.bra) maxn = std::max(maxn, c.n * B2_NBUCKET);
+        if (fused && ((rc = dev_alloc(g.de, (size_t)3 * P->natm)) || (!g.shell_atom.p && (rc = dev_upload(g.shell_atom, P->shell_atom)))))
+                return rc;
         if ((rc = dev_alloc(g.D, nn * n_dm)) || (rc = dev_alloc(g.Dc, nc * n_dm)) || (rc = dev_alloc(g.Ds, nc * n_dm)) ||
-            (rc = dev_alloc(g.V, 6 * nc * n_dm)) || (rc = dev_alloc(g.out, dev_ptrs ? 1 : 6 * nn * n_dm)) ||
+            (rc = dev_alloc(g.V, fused ? 1 : 6 * nc * n_dm)) || (rc = dev_alloc(g.out, dev_ptrs || fused ? 1 : 6 * nn * n_dm)) ||
             (rc = dev_alloc(g.dmc, (size_t)P->nbas * P->nbas)) || (rc = dev_alloc(g.fac, 1)) ||
             (rc = dev_alloc(g.dmax, 1)) || (rc = dev_alloc(g.stats, 2 * NPAIRCLASS * NPAIRCLASS)) || (rc = dev_alloc(g.nkl, maxn)) ||
             (rc = dev_alloc(g.kst, maxn)) || (rc = dev_alloc(g.nchunk, maxn + 1)) || (rc = dev_alloc(g.chunk_off, maxn + 1)))
@@ -1379,8 +1506,9 @@ extern "C" int b200jk_grad_jk(b200jk_plan *P, const double *dms, int n_dm, int w
                 CUDA_TRY(cudaGetLastError());
                 launches += 2;
         }
-        CUDA_TRY(cudaMemsetAsync(g.V.p, 0, sizeof(double) * 6 * nc * n_dm, s));
-        double *Vj = g.V.p, *Vk = g.V.p + 3 * nc * n_dm;
+        if (fused) CUDA_TRY(cudaMemsetAsync(g.de.p, 0, sizeof(double) * 3 * P->natm, s));
+        else CUDA_TRY(cudaMemsetAsync(g.V.p, 0, sizeof(double) * 6 * nc * n_dm, s));
+        double *Vj = fused ? nullptr : g.V.p, *Vk = fused ? nullptr : g.V.p + 3 * nc * n_dm;
         for (int X = 0; X < NPAIRCLASS; X++) {
                 const PairClassDev &bra = g.bra[X];
                 if (bra.n == 0) continue;
@@ -1414,6 +1542,8 @@ extern "C" int b200jk_grad_jk(b200jk_plan *P, const double *dms, int n_dm, int w
                         a.tol = tol > 0 ? tol : -1.0;
                         a.nbas = P->nbas; a.naoc = P->naoc; a.n_dm = n_dm;
                         a.with_j = with_j; a.with_k = with_k;
+                        a.de = fused ? g.de.p : nullptr;
+                        a.shell_atom = fused ? g.shell_atom.p : nullptr;
                         std::string err;
                         if (P->profiling) CUDA_TRY(cudaEventRecord(g.cls_ev[2 * (X * NPAIRCLASS + Y)], s));
                         if (g_grad_launch[X](ket.la, ket.lb, a, s, P->nsm, err)) return fail(B200JK_ECUDA, err);
@@ -1427,6 +1557,11 @@ extern "C" int b200jk_grad_jk(b200jk_plan *P, const double *dms, int n_dm, int w
         // hold the negated contraction grad.rhf.get_jk returns
         double *oj = dev_ptrs ? vj : g.out.p, *ok = dev_ptrs ? vk : g.out.p + 3 * nn * n_dm;
         const long long nout = (long long)3 * n_dm * nn;
+        if (fused) {
+                // the forces are complete: no accumulators to transform
+                if (dev_ptrs) CUDA_TRY(cudaMemcpyAsync(de, g.de.p, sizeof(double) * 3 * P->natm, cudaMemcpyDeviceToDevice, s));
+                with_j = with_k = 0;
+        }
         if (with_j) {
                 grad_cart_to_out_kernel<<<grid_for(nout, 256), 256, 0, s>>>(Vj, 3 * n_dm, P->nao, P->naoc, P->out_seg.p,
                                                                           P->out_comp.p, P->seg_info.p, P->c2s.p, 1.0, oj);
@@ -1443,6 +1578,7 @@ extern "C" int b200jk_grad_jk(b200jk_plan *P, const double *dms, int n_dm, int w
         if (!dev_ptrs) {
                 if (with_j) CUDA_TRY(cudaMemcpyAsync(vj, oj, sizeof(double) * nout, cudaMemcpyDeviceToHost, s));
                 if (with_k) CUDA_TRY(cudaMemcpyAsync(vk, ok, sizeof(double) * nout, cudaMemcpyDeviceToHost, s));
+                if (fused) CUDA_TRY(cudaMemcpyAsync(de, g.de.p, sizeof(double) * 3 * P->natm, cudaMemcpyDeviceToHost, s));
         }
         std::vector<unsigned long long> hs(2 * NPAIRCLASS * NPAIRCLASS);
         CUDA_TRY(cudaMemcpyAsync(hs.data(), g.stats.p, sizeof(unsigned long long) * hs.size(), cudaMemcpyDeviceToHost, s));
@@ -1472,6 +1608,19 @@ extern "C" int b200jk_grad_jk(b200jk_plan *P, const double *dms, int n_dm, int w
         g.last_ms = ms;
         g.launches = launches;
         return B200JK_OK;
+}
+
+extern "C" int b200jk_grad_jk(b200jk_plan *P, const double *dms, int n_dm, int with_j, int with_k, double *vj,
+                              double *vk, int dev_ptrs, double direct_scf_tol, void *stream)
+{
+        return grad_build(P, dms, n_dm, with_j, with_k, vj, vk, nullptr, dev_ptrs, direct_scf_tol, stream);
+}
+
+extern "C" int b200jk_grad_contract(b200jk_plan *P, const double *dm, double *de, int dev_ptrs,
+                                    double direct_scf_tol, void *stream)
+{
+        if (!de) return fail(B200JK_EINVAL, "de is NULL");
+        return grad_build(P, dm, 1, 1, 1, nullptr, nullptr, de, dev_ptrs, direct_scf_tol, stream);
 }
 
 extern "C" int b200jk_grad_stats(const b200jk_plan *P, int64_t *quartets, int64_t *prim_quartets, double *ms,
@@ -1525,6 +1674,11 @@ struct b200jk_batch {
         // staging of the asynchronous entry (read by captured graphs at replay)
         JKArgs *h_args_async = nullptr;
         int *h_segoff_async = nullptr;
+        // workspace generation of every plan when the last synchronous build
+        // sized the buffers; the asynchronous entry refuses to run when a
+        // plan's workspace has moved since (its captured graphs would use the
+        // freed buffers)
+        std::vector<long long> ws_gen;
         const double *tbl = nullptr;
         const float *tbl_f = nullptr;
         int64_t quartets = 0, prim_quartets = 0, fp32_quartets = 0, launches = 0;
@@ -1599,11 +1753,22 @@ static int batch_build(b200jk_batch *B, const double *const *dms, int hermi, int
         int rc;
         for (int m = 0; m < nmol; m++) {
                 if (async) {
-                        if (B->plans[m]->ws_ndm < 1)
+                        if (B->plans[m]->ws_ndm < 1 || B->ws_gen.size() != (size_t)nmol)
                                 return fail(B200JK_EINVAL, "b200jk_batch_get_jk_async needs one b200jk_batch_get_jk call first");
-                } else if ((rc = ensure_workspace(B->plans[m], 1))) {
-                        return rc;
+                        if (B->plans[m]->ws_gen != B->ws_gen[m])
+                                return fail(B200JK_EINVAL, "a plan's workspace moved since the last b200jk_batch_get_jk "
+                                                           "(a larger build on it); call b200jk_batch_get_jk again");
+                } else {
+                        if ((rc = check_dev_ptr(dms[m], B->device, "dms[m]")) ||
+                            (with_j && (rc = check_dev_ptr(vj[m], B->device, "vj[m]"))) ||
+                            (with_k && (rc = check_dev_ptr(vk[m], B->device, "vk[m]"))))
+                                return rc;
+                        if ((rc = ensure_workspace(B->plans[m], 1))) return rc;
                 }
+        }
+        if (!async) {
+                B->ws_gen.resize(nmol);
+                for (int m = 0; m < nmol; m++) B->ws_gen[m] = B->plans[m]->ws_gen;
         }
         auto qcs = quartet_classes();
         const int nclass = (int)qcs.size();
@@ -1724,6 +1889,7 @@ static int batch_build(b200jk_batch *B, const double *const *dms, int hermi, int
                                 a.tol = P->tol > 0 ? P->tol : -1.0;
                                 a.nbas = P->nbas; a.naoc = P->naoc; a.n_dm = 1; a.nk = nk;
                                 a.with_j = with_j; a.with_k = with_k; a.same = qcs[t].X == qcs[t].Y;
+                                a.screen = P->screen;
                                 ha[k] = a;
                                 hs[k] = seg;
                                 k++;
@@ -1845,11 +2011,11 @@ extern "C" int b200jk_batch_stats(const b200jk_batch *B, int64_t *quartets, int6
 #define B200JK_NOALLOC_SCRATCH_BYTES (32ull << 20)
 static __device__ __align__(256) unsigned char g_noalloc_scratch[B200JK_NOALLOC_SCRATCH_BYTES];
 
-// Device address of g_noalloc_scratch on each device, resolved once per
-// device (with that device current) by the first no-alloc call on it.
-static std::once_flag g_noalloc_once[64];
+// Device address of g_noalloc_scratch on each device, resolved by the first
+// no-alloc call on that device that succeeds in doing so (with that device
+// current).  A failed attempt is not remembered: the next call tries again.
+static std::mutex g_noalloc_mu;
 static unsigned char *g_noalloc_ptr[64];
-static cudaError_t g_noalloc_err[64];
 
 static size_t noalloc_align(size_t x) { return (x + 255) & ~(size_t)255; }
 
@@ -1864,14 +2030,25 @@ extern "C" int b200jk_get_jk_noalloc(b200jk_plan *P, const double *dms, int n_dm
         const int dev = P->device;
         if (dev < 0 || dev >= 64) return fail(B200JK_EINVAL, "device index out of range");
         CUDA_TRY(cudaSetDevice(dev));
-        std::call_once(g_noalloc_once[dev], [dev]() {
-                void *p = nullptr;
-                g_noalloc_err[dev] = cudaGetSymbolAddress(&p, g_noalloc_scratch);
-                g_noalloc_ptr[dev] = (unsigned char *)p;
-        });
-        if (g_noalloc_err[dev] != cudaSuccess || !g_noalloc_ptr[dev])
-                return fail(B200JK_ECUDA, std::string("cudaGetSymbolAddress(g_noalloc_scratch): ") +
-                                                  cudaGetErrorString(g_noalloc_err[dev]));
+        // the kernels read and write these arrays directly: host memory would
+        // fault the GPU, so anything but device memory of the plan's GPU is an error
+        int rc;
+        if ((rc = check_dev_ptr(dms, dev, "dms")) || (with_j && (rc = check_dev_ptr(vj, dev, "vj"))) ||
+            (with_k && (rc = check_dev_ptr(vk, dev, "vk"))))
+                return rc;
+        unsigned char *base = nullptr;
+        {
+                std::lock_guard<std::mutex> lk(g_noalloc_mu);
+                if (!g_noalloc_ptr[dev]) {
+                        void *p = nullptr;
+                        const cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
+                        if (e != cudaSuccess || !p)
+                                return fail(B200JK_ECUDA, std::string("cudaGetSymbolAddress(g_noalloc_scratch): ") +
+                                                                  cudaGetErrorString(e));
+                        g_noalloc_ptr[dev] = (unsigned char *)p;
+                }
+                base = g_noalloc_ptr[dev];
+        }
 
         // carve the scratch array; reject sizes beyond it before any work
         const size_t nn = (size_t)P->nao * P->nao, nc = (size_t)P->naoc * P->naoc;
@@ -1902,7 +2079,6 @@ extern "C" int b200jk_get_jk_noalloc(b200jk_plan *P, const double *dms, int n_dm
                          off, P->naoc, n_dm, hermi, (unsigned long long)B200JK_NOALLOC_SCRATCH_BYTES);
                 return fail(B200JK_EINVAL, msg);
         }
-        unsigned char *base = g_noalloc_ptr[dev];
         double *Dc = (double *)(base + o_Dc), *Ds = (double *)(base + o_Ds);
         double *Jacc = (double *)(base + o_J), *Kacc = (double *)(base + o_K);
         double *dmc = (double *)(base + o_dmc);
@@ -1942,7 +2118,7 @@ extern "C" int b200jk_get_jk_noalloc(b200jk_plan *P, const double *dms, int n_dm
                 const int nseg = bra.n * B2_NBUCKET;
                 count_kernel<<<grid_for(nseg, 256), 256, 0, s>>>(bra.view(), ket.view(), same, P->tol > 0 ? P->tol : 0.0,
                                                                 (const double *)dmax, family_chunk(la, lb, lc, ld),
-                                                                0.0, 0, 0, 1, nkl, kst, nchunk);
+                                                                0.0, 0, P->shard, P->nshard, nkl, kst, nchunk);
                 CUDA_TRY(cudaGetLastError());
                 CUDA_TRY(cudaMemsetAsync(nchunk + nseg, 0, sizeof(long long), s));
                 size_t tmp = cub_bytes;
@@ -1963,8 +2139,8 @@ extern "C" int b200jk_get_jk_noalloc(b200jk_plan *P, const double *dms, int n_dm
                 a.tol = P->tol > 0 ? P->tol : -1.0;
                 a.nbas = P->nbas; a.naoc = P->naoc; a.n_dm = n_dm; a.nk = nk;
                 a.with_j = with_j; a.with_k = with_k; a.same = same;
-                int rc = dispatch_jk(P, la, lb, lc, ld, a, 0, s);
-                if (rc) return rc;
+                a.screen = P->screen;
+                if ((rc = dispatch_jk(P, la, lb, lc, ld, a, 0, s))) return rc;
         }
         for (int d = 0; d < n_dm; d++) {
                 if (with_j) {

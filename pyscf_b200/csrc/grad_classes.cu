@@ -26,8 +26,8 @@ struct GradCfg {
 // largest dynamic shared memory a block may request on sm_100
 constexpr size_t SMEM_MAX = 227 * 1024;
 
-template <int LA, int LB, int LC, int LD>
-int launch_grad_one(const GradArgs &a, cudaStream_t s, int nsm, std::string &err)
+template <int LA, int LB, int LC, int LD, bool FUSED>
+int launch_grad_impl(const GradArgs &a, cudaStream_t s, int nsm, std::string &err)
 {
         using S = GradSmem<LA, LB, LC, LD, 0>;
         constexpr int GS = grad_group_size<LA, LB, LC, LD>();
@@ -40,7 +40,7 @@ int launch_grad_one(const GradArgs &a, cudaStream_t s, int nsm, std::string &err
                                 int nb = 0;
                                 cfg.block = 128;
                                 cfg.status = cudaOccupancyMaxActiveBlocksPerMultiprocessor(
-                                        &nb, grad_thread_kernel<LA, LB, LC, LD>, 128, 0);
+                                        &nb, grad_thread_kernel<LA, LB, LC, LD, FUSED>, 128, 0);
                                 cfg.grid = (nb > 0 ? nb : 1) * nsm;
                                 cfg.ready = true;
                         }
@@ -49,7 +49,7 @@ int launch_grad_one(const GradArgs &a, cudaStream_t s, int nsm, std::string &err
                         err = std::string("gradient kernel configuration: ") + cudaGetErrorString(cfg.status);
                         return 1;
                 }
-                grad_thread_kernel<LA, LB, LC, LD><<<cfg.grid, cfg.block, 0, s>>>(a);
+                grad_thread_kernel<LA, LB, LC, LD, FUSED><<<cfg.grid, cfg.block, 0, s>>>(a);
                 cudaError_t e = cudaGetLastError();
                 if (e != cudaSuccess) {
                         err = std::string("gradient kernel launch: ") + cudaGetErrorString(e);
@@ -67,12 +67,12 @@ int launch_grad_one(const GradArgs &a, cudaStream_t s, int nsm, std::string &err
                                 const int wpb = (int)std::min<size_t>(4, std::max<size_t>(1, (200 * 1024) / per_warp));
                                 cfg.block = 32 * wpb;
                                 cfg.smem = per_warp * wpb;
-                                cfg.status = cudaFuncSetAttribute(grad_jk_kernel<LA, LB, LC, LD>,
+                                cfg.status = cudaFuncSetAttribute(grad_jk_kernel<LA, LB, LC, LD, FUSED>,
                                                                   cudaFuncAttributeMaxDynamicSharedMemorySize, (int)cfg.smem);
                                 int nb = 0;
                                 if (cfg.status == cudaSuccess)
                                         cfg.status = cudaOccupancyMaxActiveBlocksPerMultiprocessor(
-                                                &nb, grad_jk_kernel<LA, LB, LC, LD>, cfg.block, cfg.smem);
+                                                &nb, grad_jk_kernel<LA, LB, LC, LD, FUSED>, cfg.block, cfg.smem);
                                 cfg.grid = (nb > 0 ? nb : 1) * nsm;
                         }
                         cfg.ready = true;
@@ -82,13 +82,21 @@ int launch_grad_one(const GradArgs &a, cudaStream_t s, int nsm, std::string &err
                 err = std::string("gradient kernel configuration: ") + cudaGetErrorString(cfg.status);
                 return 1;
         }
-        grad_jk_kernel<LA, LB, LC, LD><<<cfg.grid, cfg.block, cfg.smem, s>>>(a, 8 * (32 / GS));
+        grad_jk_kernel<LA, LB, LC, LD, FUSED><<<cfg.grid, cfg.block, cfg.smem, s>>>(a, 8 * (32 / GS));
         cudaError_t e = cudaGetLastError();
         if (e != cudaSuccess) {
                 err = std::string("gradient kernel launch: ") + cudaGetErrorString(e);
                 return 1;
         }
         return 0;
+}
+
+// the vj/vk build, or the fused force contraction when a.de is set
+template <int LA, int LB, int LC, int LD>
+int launch_grad_one(const GradArgs &a, cudaStream_t s, int nsm, std::string &err)
+{
+        if (a.de) return launch_grad_impl<LA, LB, LC, LD, true>(a, s, nsm, err);
+        return launch_grad_impl<LA, LB, LC, LD, false>(a, s, nsm, err);
 }
 
 template <int LA, int LB>

@@ -137,7 +137,40 @@ struct GradArgs {
         unsigned long long *stats;   // [0] quartets (sides), [1] primitive quartets
         double tol;
         int nbas, naoc, n_dm, with_j, with_k;
+        // fused force contraction (b200jk_grad_contract): de[atom][x] of the
+        // parent shells' atoms (shell_atom[parent shell]); one symmetric density
+        double *de = nullptr;
+        const int *shell_atom = nullptr;
 };
+
+// Weight of one Cartesian element (ab|cd) in the two-electron force of a
+// symmetric density D (Cartesian, Ds = D + D^T): grad_elec adds
+// 2 sum_{i in A} sum_j (vj - vk/2)_x[i,j] D[i,j] (pyscf/grad/rhf.py:62-68), which
+// per quartet side is sum_abcd (d_x ab|cd) W[abcd] with
+//     W = 2 D_ab Ds_cd - D_bc D_ad - D_bd D_ac
+// for the derivative on a and, D being symmetric, the same W for b.
+__device__ __forceinline__ double grad_force_weight(double dab, double dcd, double xbc, double xad, double xbd,
+                                                    double xac)
+{
+        return 2.0 * dab * dcd - xbc * xad - xbd * xac;
+}
+
+// the per-lane side sums s[0..2] (derivative on a) and s[3..5] (on b) of a
+// warp that worked on one bra pair: summed over the warp, one atomic per
+// atom and direction
+__device__ __forceinline__ void grad_force_flush(const GradArgs &a, int4 sb, double s[6], int lane)
+{
+#pragma unroll
+        for (int q = 0; q < 6; q++) s[q] = warp_sum(s[q]);
+        if (lane == 0) {
+                const int atA = __ldg(a.shell_atom + sb.z), atB = __ldg(a.shell_atom + sb.w);
+#pragma unroll
+                for (int x = 0; x < 3; x++) {
+                        if (s[x] != 0.0) atomicAdd(a.de + 3 * atA + x, s[x]);
+                        if (s[3 + x] != 0.0) atomicAdd(a.de + 3 * atB + x, s[3 + x]);
+                }
+        }
+}
 
 // CVHFgrad_jk_prescreen for bra shells (i, j) (derivative on i) and ket
 // shells k >= l
@@ -246,7 +279,9 @@ __host__ __device__ constexpr int grad_group_size()
 
 // The gradient J/K kernel of class (LA LB | LC LD): groups of GS lanes walk
 // chunks of chunk_q quartets of one bra pair.
-template <int LA, int LB, int LC, int LD>
+// FUSED: the force contraction with one symmetric density instead of the
+// vj/vk accumulators (b200jk_grad_contract).
+template <int LA, int LB, int LC, int LD, bool FUSED = false>
 __global__ void __launch_bounds__(128) grad_jk_kernel(GradArgs a, int chunk_q)
 {
         using K = Class4<LA, LB, LC, LD>;
@@ -280,6 +315,7 @@ __global__ void __launch_bounds__(128) grad_jk_kernel(GradArgs a, int chunk_q)
                 const double AB[3] = {ABb.x, ABb.y, ABb.z};
                 const int ia = sb.x, ib = sb.y;
                 const bool bra_one_segment = Ab.w != 0.0;
+                double fs[6] = {0.0, 0.0, 0.0, 0.0, 0.0, 0.0};
                 for (int kl = kl0 + grp; kl < kl1; kl += NGRP) {
                         const int4 sk = a.ket.sh[kl];
                         const int kk = max(sk.z, sk.w), ll = min(sk.z, sk.w);
@@ -304,6 +340,32 @@ __global__ void __launch_bounds__(128) grad_jk_kernel(GradArgs a, int chunk_q)
                                 if (!needA && !needB) continue;
                                 grad_eval_pass<LA, LB, LC, LD, 0, GS>(sm, a, pb, pk, Ab, AB, C, CD, fac, c0, gl, gmask);
                                 const double *G = sm + S::G;
+                                if constexpr (FUSED) {
+                                        const double *X = a.Dc;
+                                        double *dsab = sm + S::DSAB, *dscd = sm + S::DSCD;
+                                        double *xbc = sm + S::XBC, *xbd = sm + S::XBD;
+                                        double *xac = sm + S::XAC, *xad = sm + S::XAD;
+                                        for (int t = gl; t < K::NAB; t += GS) dsab[t] = __ldg(X + (ia + t / K::NB) * n + ib + t % K::NB);
+                                        for (int t = gl; t < K::NCD; t += GS) dscd[t] = __ldg(a.Ds + (ic + t / K::ND) * n + id + t % K::ND);
+                                        for (int t = gl; t < K::NB * K::NC; t += GS) xbc[t] = __ldg(X + (ib + t / K::NC) * n + ic + t % K::NC);
+                                        for (int t = gl; t < K::NB * K::ND; t += GS) xbd[t] = __ldg(X + (ib + t / K::ND) * n + id + t % K::ND);
+                                        for (int t = gl; t < K::NA * K::NC; t += GS) xac[t] = __ldg(X + (ia + t / K::NC) * n + ic + t % K::NC);
+                                        for (int t = gl; t < K::NA * K::ND; t += GS) xad[t] = __ldg(X + (ia + t / K::ND) * n + id + t % K::ND);
+                                        __syncwarp(gmask);
+                                        for (int t = gl; t < NG; t += GS) {
+                                                const int d = t % K::ND, c = (t / K::ND) % K::NC;
+                                                const int b = (t / K::NCD) % K::NB, xa = t / (K::NCD * K::NB);
+                                                const double w = grad_force_weight(dsab[xa * K::NB + b], dscd[c * K::ND + d],
+                                                                                   xbc[b * K::NC + c], xad[xa * K::ND + d],
+                                                                                   xbd[b * K::ND + d], xac[xa * K::NC + c]);
+#pragma unroll
+                                                for (int q = 0; q < 6; q++)
+                                                        if (q >= c0 && q < c0 + GC::NCP && (q < 3 ? sideA : sideB))
+                                                                fs[q] += G[(q - c0) * NG + t] * w;
+                                        }
+                                        __syncwarp(gmask);
+                                        continue;
+                                }
                                 for (int s = 0; s < a.n_dm; s++) {
                                         const double *Ds = a.Ds + s * nn;
                                         const double *X = a.Dc + s * nn;
@@ -378,6 +440,7 @@ __global__ void __launch_bounds__(128) grad_jk_kernel(GradArgs a, int chunk_q)
                                 }
                         }
                 }
+                if constexpr (FUSED) grad_force_flush(a, sb, fs, lane);
         }
         if (a.stats && gl == 0 && nq) {
                 atomicAdd(a.stats + 0, nq);
@@ -435,7 +498,7 @@ __device__ __forceinline__ void grad_assemble(double *G, const double *Ex, const
         (grad_assemble_one<LA, LB, LC, LD, Ts>(G, Ex, Ey, Ez, ta, tb), ...);
 }
 
-template <int LA, int LB, int LC, int LD>
+template <int LA, int LB, int LC, int LD, bool FUSED = false>
 __global__ void __launch_bounds__(128) grad_thread_kernel(GradArgs a)
 {
         using K = Class4<LA, LB, LC, LD>;
@@ -511,6 +574,39 @@ __global__ void __launch_bounds__(128) grad_thread_kernel(GradArgs a)
                         }
                 }
                 const int ia = sb.x, ib = sb.y, ic = sk.x, id = sk.y;
+                if constexpr (FUSED) {
+                        double fs[6] = {0.0, 0.0, 0.0, 0.0, 0.0, 0.0};
+                        if (active) {
+                                const double *X = a.Dc;
+                                double dab[K::NAB], dcd[K::NCD], xbc[K::NB * K::NC], xbd[K::NB * K::ND];
+                                double xac[K::NA * K::NC], xad[K::NA * K::ND];
+#pragma unroll
+                                for (int t = 0; t < K::NAB; t++) dab[t] = __ldg(X + (ia + t / K::NB) * n + ib + t % K::NB);
+#pragma unroll
+                                for (int t = 0; t < K::NCD; t++) dcd[t] = __ldg(a.Ds + (ic + t / K::ND) * n + id + t % K::ND);
+#pragma unroll
+                                for (int t = 0; t < K::NB * K::NC; t++) xbc[t] = __ldg(X + (ib + t / K::NC) * n + ic + t % K::NC);
+#pragma unroll
+                                for (int t = 0; t < K::NB * K::ND; t++) xbd[t] = __ldg(X + (ib + t / K::ND) * n + id + t % K::ND);
+#pragma unroll
+                                for (int t = 0; t < K::NA * K::NC; t++) xac[t] = __ldg(X + (ia + t / K::NC) * n + ic + t % K::NC);
+#pragma unroll
+                                for (int t = 0; t < K::NA * K::ND; t++) xad[t] = __ldg(X + (ia + t / K::ND) * n + id + t % K::ND);
+#pragma unroll
+                                for (int t = 0; t < NG; t++) {
+                                        const int d = t % K::ND, c = (t / K::ND) % K::NC;
+                                        const int b = (t / K::NCD) % K::NB, xa = t / (K::NCD * K::NB);
+                                        const double w = grad_force_weight(dab[xa * K::NB + b], dcd[c * K::ND + d], xbc[b * K::NC + c],
+                                                                           xad[xa * K::ND + d], xbd[b * K::ND + d], xac[xa * K::NC + c]);
+#pragma unroll
+                                        for (int q = 0; q < 6; q++) fs[q] += G[q * NG + t] * w;
+                                }
+                                if (!sideA) fs[0] = fs[1] = fs[2] = 0.0;
+                                if (!sideB) fs[3] = fs[4] = fs[5] = 0.0;
+                        }
+                        grad_force_flush(a, sb, fs, lane);
+                        continue;
+                }
                 for (int s = 0; s < a.n_dm; s++) {
                         const double *Ds = a.Ds + s * nn;
                         const double *X = a.Dc + s * nn;

@@ -82,6 +82,9 @@ struct JKArgs {
         double tol;
         int nbas, naoc, n_dm, nk;
         int with_j, with_k, same;
+        // density part of the quartet screen: 0 the s8 screen (J and K),
+        // 1 its J terms only, 2 its K terms only (B200JK_SCREEN_*)
+        int screen = 0;
 };
 
 // Packed ket blocks: src[e] is the Cartesian matrix offset of packed entry e
@@ -118,6 +121,14 @@ __device__ __forceinline__ int find_bra(const long long *off, int n, long long c
         return lo;
 }
 
+// The reference's per-quartet screens (pyscf/lib/vhf/optimizer.c):
+//   s8 (CVHFnrs8_prescreen, :90-117)  q_ij q_kl > tol and
+//        max(4 D_ji, 4 D_lk, D_jk, D_jl, D_ik, D_il) q_ij q_kl > tol
+//   J  (CVHFnrs8_vj_prescreen, :119-141)  the 4 D_ji, 4 D_lk terms only
+//   K  (CVHFnrs8_vk_prescreen, :143-167)  the D_jk, D_jl, D_ik, D_il terms only
+// (SCF.get_jk picks J or K when only one is built, pyscf/scf/hf.py:2069-2077).
+// The OR of the reference's comparisons equals one comparison of the
+// maximum: rounding of d * qq is monotone in d and 4 d is exact.
 __device__ __forceinline__ bool quartet_passes(const JKArgs &a, int4 sb, double qij, int4 sk, double qkl)
 {
         const double qq = qij * qkl;
@@ -125,9 +136,12 @@ __device__ __forceinline__ bool quartet_passes(const JKArgs &a, int4 sb, double 
         const size_t n = (size_t)a.nbas;
         const double *dc = a.dm_cond;
         const int pi = sb.z, pj = sb.w, pk = sk.z, pl = sk.w;
-        double d = 4.0 * fmax(__ldg(dc + pj * n + pi), __ldg(dc + pl * n + pk));
-        d = fmax(d, fmax(__ldg(dc + pj * n + pk), __ldg(dc + pj * n + pl)));
-        d = fmax(d, fmax(__ldg(dc + pi * n + pk), __ldg(dc + pi * n + pl)));
+        double d = 0.0;
+        if (a.screen != 2) d = 4.0 * fmax(__ldg(dc + pj * n + pi), __ldg(dc + pl * n + pk));
+        if (a.screen != 1) {
+                d = fmax(d, fmax(__ldg(dc + pj * n + pk), __ldg(dc + pj * n + pl)));
+                d = fmax(d, fmax(__ldg(dc + pi * n + pk), __ldg(dc + pi * n + pl)));
+        }
         return d * qq > a.tol;
 }
 

@@ -7,14 +7,18 @@ reference's threshold 1e-14, returned negated, shape (3, nao, nao) per
 density.  ``patch_pyscf_grad()`` rebinds it in an unmodified PySCF, where
 ``GradientsBase.get_jk`` looks it up through the module (pyscf/grad/rhf.py:321).
 
-``grad_2e(plan, dm, aoslice)`` contracts the result into the two-electron part
-of the RHF gradient, the term grad_elec adds (pyscf/grad/rhf.py:67-69):
-    de[A] = 2 sum_x sum_{i in A} sum_j (vj - vk/2)[x, i, j] D[i, j].
+``grad_2e(vj, vk, dm, aoslice)`` contracts that result into the two-electron
+part of the RHF gradient, the term grad_elec adds (pyscf/grad/rhf.py:62-68):
+    de[A] = 2 sum_x sum_{i in A} sum_j (vj - vk/2)[x, i, j] D[i, j];
+``grad_2e_fused(plan, dm)`` gets the same (natm, 3) array from the GPU without
+forming vj/vk (b200jk_grad_contract: the quartets are contracted with
+D (x) D inside the derivative kernels).
 
 ``TwoElectronEnergy`` is a torch.autograd.Function of the nuclear coordinates
 (and the density): forward builds J/K on the GPU for the geometry and returns
-E2 = 1/2 tr(D J) - 1/4 tr(D K); backward runs the int2e_ip1 kernel and
-returns dE2/dR (at fixed AO density) and dE2/dD = J - K/2.
+E2 = 1/2 tr(D J) - 1/4 tr(D K); backward runs the fused int2e_ip1 kernels and
+returns dE2/dR (at fixed AO density) and dE2/dD = J - K/2.  One plan per
+molecule is kept and moved to each new geometry (b200jk_plan_update_coords).
 """
 import numpy
 
@@ -67,6 +71,29 @@ def grad_2e(vj, vk, dm, aoslice):
     return numpy.array([2.0 * numpy.einsum('xij,ij->x', vhf[:, p0:p1], dm[p0:p1]) for p0, p1 in aoslice])
 
 
+def grad_2e_fused(plan, dm, direct_scf_tol=GRAD_SCREEN_TOL):
+    """The same (natm, 3) two-electron gradient of a symmetric density, with
+    the contraction fused into the derivative kernels (no vj/vk formed)."""
+    return plan.grad_contract(dm, direct_scf_tol=direct_scf_tol)
+
+
+# one plan per molecule for TwoElectronEnergy, moved between geometries
+_ad_plans = {}
+
+
+def _ad_plan(atm, bas, env, cart, device):
+    key = (numpy.asarray(atm).tobytes(), numpy.asarray(bas).tobytes(), bool(cart), int(device))
+    p = _ad_plans.get(key)
+    if p is None:
+        if len(_ad_plans) >= 4:
+            _ad_plans.pop(next(iter(_ad_plans))).close()
+        p = lib.Plan(atm, bas, env, cart=bool(cart), direct_scf_tol=1e-13, device=device)
+        _ad_plans[key] = p
+    elif not numpy.array_equal(p.env, env):
+        p.update_coords(env)
+    return p
+
+
 _saved = {}
 
 
@@ -108,8 +135,7 @@ def _torch_function():
         def forward(ctx, coords, dm, atm, bas, env, cart=False):
             c = coords.detach().cpu().numpy().astype(numpy.double)
             env2 = _env_with_coords(atm, env, c)
-            plan = lib.Plan(atm, bas, env2, cart=bool(cart), direct_scf_tol=1e-13,
-                            device=dm.device.index if dm.is_cuda else 0)
+            plan = _ad_plan(atm, bas, env2, cart, dm.device.index if dm.is_cuda else 0)
             d = dm.detach()
             if d.is_cuda:
                 vj, vk = plan.get_jk_device(d.contiguous(), hermi=1)
@@ -119,7 +145,7 @@ def _torch_function():
             veff = vj - 0.5 * vk
             e2 = 0.5 * torch.sum(d * veff)
             ctx.plan = plan
-            ctx.aoslice = aoslice_by_atom(atm, bas, cart)
+            ctx.env = env2
             ctx.save_for_backward(d, veff)
             return e2.to(coords.dtype).to(coords.device)
 
@@ -128,16 +154,14 @@ def _torch_function():
             d, veff = ctx.saved_tensors
             g_coords = g_dm = None
             if ctx.needs_input_grad[0]:
+                # the shared plan may have moved to another geometry since
+                # this forward pass (another forward ran in between)
+                if not numpy.array_equal(ctx.plan.env, ctx.env):
+                    ctx.plan.update_coords(ctx.env)
                 if d.is_cuda:
-                    gj, gk = ctx.plan.grad_jk_device(d.contiguous(), direct_scf_tol=GRAD_SCREEN_TOL)
-                    vhf = gj - 0.5 * gk
-                    rows = []
-                    for p0, p1 in ctx.aoslice:
-                        rows.append(2.0 * torch.einsum('xij,ij->x', vhf[:, p0:p1], d[p0:p1]))
-                    g = torch.stack(rows)
+                    g = grad_2e_fused(ctx.plan, d.contiguous())
                 else:
-                    gj, gk = ctx.plan.grad_jk(d.numpy(), direct_scf_tol=GRAD_SCREEN_TOL)
-                    g = torch.from_numpy(grad_2e(gj, gk, d.numpy(), ctx.aoslice))
+                    g = torch.from_numpy(grad_2e_fused(ctx.plan, d.numpy()))
                 g_coords = (grad_out.to(g.device) * g).to(grad_out.device)
             if ctx.needs_input_grad[1]:
                 g_dm = grad_out.to(veff.device) * veff

@@ -19,6 +19,9 @@ B200JK_ECUDA = 3
 B200JK_ENOMEM = 4
 PREC_FP64 = 0
 PREC_MIXED = 1
+SCREEN_NRS8 = 0
+SCREEN_VJ = 1
+SCREEN_VK = 2
 
 # every entry point of include/b200jk.h
 EXPORTS = (
@@ -27,7 +30,7 @@ EXPORTS = (
     'b200jk_stats', 'b200jk_hostcheck_cart_quartet', 'b200jk_class_stats', 'b200jk_set_profiling',
     'b200jk_measure_fp64_peak', 'b200jk_get_jk_noalloc', 'b200jk_set_mixed_threshold',
     'b200jk_hostcheck_cart_quartet_fp32', 'b200jk_grad_jk', 'b200jk_grad_stats', 'b200jk_get_grad_q_cond',
-    'b200jk_set_shard', 'b200jk_grad_class_stats', 'b200jk_autotune', 'b200jk_get_tuning', 'b200jk_set_tuning', 'b200jk_set_tile', 'b200jk_batch_get_jk_async', 'b200jk_batch_create', 'b200jk_batch_destroy', 'b200jk_batch_get_jk', 'b200jk_batch_stats',
+    'b200jk_set_shard', 'b200jk_grad_class_stats', 'b200jk_autotune', 'b200jk_get_tuning', 'b200jk_set_tuning', 'b200jk_set_tile', 'b200jk_batch_get_jk_async', 'b200jk_batch_create', 'b200jk_batch_destroy', 'b200jk_batch_get_jk', 'b200jk_batch_stats', 'b200jk_debug_fail_alloc', 'b200jk_set_prescreen', 'b200jk_grad_contract', 'b200jk_plan_update_coords',
 )
 
 
@@ -83,6 +86,10 @@ def load(path=LIB_PATH):
         lib.b200jk_measure_fp64_peak.argtypes = [ip, ctypes.POINTER(dp)]
         lib.b200jk_get_jk_noalloc.argtypes = [vp, vp, ip, ip, ip, ip, vp, vp, vp]
         lib.b200jk_set_mixed_threshold.argtypes = [vp, dp]
+        lib.b200jk_set_prescreen.argtypes = [vp, ip]
+        lib.b200jk_grad_contract.argtypes = [vp, vp, vp, ip, dp, vp]
+        lib.b200jk_plan_update_coords.argtypes = [vp, vp, ip]
+        lib.b200jk_debug_fail_alloc.argtypes = [ip]
         lib.b200jk_grad_jk.argtypes = [vp, vp, ip, ip, ip, vp, vp, ip, dp, vp]
         lib.b200jk_grad_stats.argtypes = [vp, ctypes.POINTER(ctypes.c_int64), ctypes.POINTER(ctypes.c_int64),
                                           ctypes.POINTER(dp), ctypes.POINTER(ctypes.c_int64)]
@@ -141,6 +148,15 @@ class Plan:
         check(lib.b200jk_plan_dims(h, ctypes.byref(nao), ctypes.byref(nbas)))
         self.nao, self.nbas = nao.value, nbas.value
 
+    def update_coords(self, env):
+        """Re-plan for a new geometry (env with new coordinates, same atoms
+        and basis), keeping workspaces and tuning."""
+        env = numpy.array(env, dtype=numpy.double, order='C', copy=True)
+        if env.shape != self.env.shape:
+            raise ValueError('env of a different molecule')
+        check(load().b200jk_plan_update_coords(self._h, _ptr(env), env.size))
+        self.env = env
+
     def close(self):
         if getattr(self, '_h', None):
             load().b200jk_plan_destroy(self._h)
@@ -189,6 +205,12 @@ class Plan:
             d = numpy.ascontiguousarray(dm, dtype=numpy.double)
             check(load().b200jk_autotune(self._h, _ptr(d), 0, None))
         return self.tuning()
+
+    def set_prescreen(self, screen=SCREEN_NRS8):
+        """Density part of the quartet screen of later builds: SCREEN_NRS8
+        (CVHFnrs8_prescreen), SCREEN_VJ (CVHFnrs8_vj_prescreen) or SCREEN_VK
+        (CVHFnrs8_vk_prescreen)."""
+        check(load().b200jk_set_prescreen(self._h, int(screen)))
 
     def set_tile(self, tile_b):
         """Bra pairs per tile of the ket-chunk-major order (0: bra-major)."""
@@ -293,6 +315,32 @@ class Plan:
                                     float(direct_scf_tol), ctypes.c_void_p(stream)))
         shape = tuple(dms.shape[:-2]) + (3, nao, nao)
         return (vj.reshape(shape) if with_j else None), (vk.reshape(shape) if with_k else None)
+
+    def grad_contract(self, dm, direct_scf_tol=1e-14):
+        """Two-electron part of the RHF nuclear gradient, (natm, 3), for one
+        symmetric density (host array or float64 CUDA tensor), contracted on
+        the GPU without forming vj/vk (b200jk_grad_contract)."""
+        natm = self.atm.shape[0]
+        try:
+            import torch
+            is_dev = isinstance(dm, torch.Tensor) and dm.is_cuda
+        except ImportError:
+            is_dev = False
+        if is_dev:
+            d = dm.contiguous()
+            if tuple(d.shape) != (self.nao, self.nao) or d.dtype != torch.float64:
+                raise ValueError('dm must be a float64 (nao, nao) tensor')
+            de = torch.empty((natm, 3), dtype=torch.float64, device=d.device)
+            stream = torch.cuda.current_stream(d.device).cuda_stream
+            check(load().b200jk_grad_contract(self._h, ctypes.c_void_p(d.data_ptr()), ctypes.c_void_p(de.data_ptr()),
+                                              1, float(direct_scf_tol), ctypes.c_void_p(stream)))
+            return de
+        d = numpy.ascontiguousarray(dm, dtype=numpy.double)
+        if d.shape != (self.nao, self.nao):
+            raise ValueError('density shape %s does not match nao=%d' % (d.shape, self.nao))
+        de = numpy.empty((natm, 3))
+        check(load().b200jk_grad_contract(self._h, _ptr(d), _ptr(de), 0, float(direct_scf_tol), None))
+        return de
 
     def grad_stats(self):
         q, pq, n = ctypes.c_int64(0), ctypes.c_int64(0), ctypes.c_int64(0)

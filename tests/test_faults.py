@@ -1,0 +1,113 @@
+"""Host-side fault handling of the C ABI (no GPU needed).
+
+The reference reports these conditions by assert/exit in C
+(pyscf/lib/vhf/optimizer.c:396-400, pyscf/lib/vhf/nr_direct_dot.c:24-25) or by
+RuntimeError in Python (pyscf/scf/_vhf.py:594-597); the engine returns a
+status code and a message instead, and checks the molecule arrays on the host
+before it touches a GPU, so every case here runs on a CPU-only machine.
+The device-side counterparts (an allocation failure forced by the test hook,
+host memory passed as device memory, NaN densities) are in
+tests/test_gpu_faults.py.
+"""
+import ctypes
+
+import numpy
+import pytest
+
+from conftest import load_fixture
+
+
+def _create(atm, bas, env, tol=1e-13):
+    from pyscf_b200 import lib
+    l = lib.load()
+    h = ctypes.c_void_p()
+    atm = numpy.ascontiguousarray(atm, dtype=numpy.int32)
+    bas = numpy.ascontiguousarray(bas, dtype=numpy.int32)
+    env = numpy.ascontiguousarray(env, dtype=numpy.double)
+    rc = l.b200jk_plan_create(atm.ctypes.data_as(ctypes.c_void_p), atm.shape[0],
+                              bas.ctypes.data_as(ctypes.c_void_p), bas.shape[0],
+                              env.ctypes.data_as(ctypes.c_void_p), env.size, 0, tol, 0, ctypes.byref(h))
+    msg = l.b200jk_last_error().decode()
+    if rc == lib.B200JK_OK:
+        l.b200jk_plan_destroy(h)
+    return rc, msg
+
+
+@pytest.fixture(scope='module')
+def h2o():
+    return load_fixture('h2o_631g')
+
+
+def test_g_shell_is_unsupported(h2o):
+    from pyscf_b200 import lib
+    bas = h2o['bas'].copy()
+    bas[0, 1] = 4            # l = 4 (g): beyond the l <= 3 kernels
+    rc, msg = _create(h2o['atm'], bas, h2o['env'])
+    assert rc == lib.B200JK_EUNSUPPORTED
+    assert 'l > 3' in msg
+
+
+def test_range_separated_coulomb_is_unsupported(h2o):
+    from pyscf_b200 import lib
+    env = h2o['env'].copy()
+    env[8] = 0.3             # env[PTR_RANGE_OMEGA] (pyscf/gto/mole.py:76)
+    rc, msg = _create(h2o['atm'], h2o['bas'], env)
+    assert rc == lib.B200JK_EUNSUPPORTED
+    assert 'omega' in msg.lower() or 'range' in msg.lower()
+
+
+@pytest.mark.parametrize('slot, value, text', [
+    (0, 99, 'atom index'),          # ATOM_OF beyond natm
+    (0, -1, 'atom index'),
+    (1, -1, 'negative angular'),    # ANG_OF
+    (2, 0, 'empty shell'),          # NPRIM_OF
+    (3, 0, 'empty shell'),          # NCTR_OF
+    (5, 10 ** 6, 'outside env'),    # PTR_EXP
+    (6, -5, 'outside env'),         # PTR_COEFF
+])
+def test_bad_bas_rows_rejected(h2o, slot, value, text):
+    from pyscf_b200 import lib
+    bas = h2o['bas'].copy()
+    bas[1, slot] = value
+    rc, msg = _create(h2o['atm'], bas, h2o['env'])
+    assert rc == lib.B200JK_EINVAL, msg
+    assert text in msg
+
+
+def test_bad_coordinate_pointer_rejected(h2o):
+    from pyscf_b200 import lib
+    atm = h2o['atm'].copy()
+    atm[0, 1] = h2o['env'].size     # PTR_COORD past the end of env
+    rc, msg = _create(atm, h2o['bas'], h2o['env'])
+    assert rc == lib.B200JK_EINVAL
+    assert 'coordinate' in msg
+
+
+def test_valid_molecule_passes_the_host_checks(h2o):
+    """A valid molecule gets past the host checks: without a GPU the first
+    failure is the missing device, not the arrays."""
+    from pyscf_b200 import lib
+    rc, msg = _create(h2o['atm'], h2o['bas'], h2o['env'])
+    if lib.device_count() > 0:
+        assert rc == lib.B200JK_OK
+    else:
+        assert rc == lib.B200JK_ECUDA and 'device' in msg
+
+
+def test_alloc_hook_arguments():
+    from pyscf_b200 import lib
+    l = lib.load()
+    assert l.b200jk_debug_fail_alloc(-1) == lib.B200JK_EINVAL
+    assert l.b200jk_debug_fail_alloc(0) == lib.B200JK_OK
+
+
+def test_python_layer_rejects_omega_and_other_intors(h2o):
+    """_vhf.direct keeps the reference's Python-side errors: an intor other
+    than int2e and a range-separated molecule are refused before the engine
+    is reached (pyscf/scf/_vhf.py:405-464 accepts only what its drivers have)."""
+    from pyscf_b200 import _vhf
+    dm = numpy.eye(13)
+    env = h2o['env'].copy()
+    env[8] = 0.3
+    with pytest.raises((NotImplementedError, RuntimeError, ValueError)):
+        _vhf.direct(dm, h2o['atm'], h2o['bas'], env, vhfopt=None, hermi=1)
