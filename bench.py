@@ -331,6 +331,46 @@ def vs_oracle(workload, d, vj64, vk64, plan, tau):
     return out
 
 
+def batch_scf_report(local, steps):
+    """Whole SCF iterations of the 512-molecule workload as one CUDA graph:
+    batched J/K, Fock, DIIS and purified density of every molecule."""
+    import torch
+    from pyscf_b200 import lib, batch_scf
+    f = dict(numpy.load(os.path.join(GOLDEN, 'batch_h2o_vdz512.npz')))
+    plans, nelec, enuc = [], [], []
+    for m in range(len(f['nao'])):
+        a0, a1 = f['atm_off'][m], f['atm_off'][m + 1]
+        b0, b1 = f['bas_off'][m], f['bas_off'][m + 1]
+        e0, e1 = f['env_off'][m], f['env_off'][m + 1]
+        atm, env = f['atm'][a0:a1], f['env'][e0:e1]
+        plans.append(lib.Plan(atm, f['bas'][b0:b1], env, direct_scf_tol=1e-13, device=local))
+        nelec.append(10 * int(f['nwater'][m]))
+        z = atm[:, 0].astype(float)
+        xyz = numpy.array([env[q:q + 3] for q in atm[:, 1]])
+        r = numpy.linalg.norm(xyz[:, None] - xyz[None], axis=-1)
+        iu = numpy.triu_indices(len(z), 1)
+        enuc.append(float((z[:, None] * z[None] / numpy.where(r > 0, r, 1.0))[iu].sum()))
+    t0 = time.perf_counter()
+    scf = batch_scf.BatchRHF(plans, nelec, enuc)
+    scf.start()
+    scf.capture()
+    setup = time.perf_counter() - t0
+    stream = torch.cuda.current_stream(torch.device('cuda', local))
+    e0_ = torch.cuda.Event(enable_timing=True)
+    e1_ = torch.cuda.Event(enable_timing=True)
+    e0_.record(stream)
+    for _ in range(steps):
+        scf.graph.replay()
+    e1_.record(stream)
+    e1_.synchronize()
+    ms = e0_.elapsed_time(e1_) / steps
+    e, de = scf.run(0)
+    return {'workload': '512 x (H2O)n cc-pVDZ, one SCF iteration of all molecules per CUDA-graph replay '
+                        '(batched J/K, Fock, CDIIS, purified density)', 'molecules': len(plans),
+            'ms_per_iteration': ms, 'replays_timed': steps, 'setup_s': setup,
+            'max_dE_last_iteration': float(de.max()), 'max_idempotency_error': float(scf.idem_err.max())}
+
+
 def scf_report(local, tau):
     """Per-iteration errors of a mixed-precision RHF on C20H42/cc-pVDZ."""
     from pyscf_b200 import lib, rhf
@@ -504,6 +544,13 @@ def run_gpu(args):
         except Exception as e:  # the SCF line must not sink the J/K measurement
             scf_line = {'error': str(e)[:200]}
 
+    batch_scf_line = None
+    if world == 1:
+        try:
+            batch_scf_line = batch_scf_report(local, max(1, min(args.steps, 3)))
+        except Exception as e:  # the batched-SCF line must not sink the J/K measurement
+            batch_scf_line = {'error': str(e)[:200]}
+
     # end to end through the public API, host arrays in pinned memory
     dm_host = torch.from_numpy(f['dm']).pin_memory().numpy()
     out = torch.empty((2, nao, nao), dtype=torch.float64).pin_memory().numpy()
@@ -549,6 +596,7 @@ def run_gpu(args):
             'grad': grad_line,
             'batch': batch_line,
             'scf': scf_line,
+            'batch_scf': batch_scf_line,
             'e2e': {'value': q_per_build / t_e2e, 'unit': 'shell quartets/s',
                     's_per_build': t_e2e, 'h2d_bytes_per_step': int(nao * nao * 8),
                     'd2h_bytes_per_step': int(2 * nao * nao * 8),
@@ -602,13 +650,18 @@ def run_one_build(args):
     if args.autotune:
         plan.autotune(f['dm'])
     if args.variants is not None:
-        # the FP64 variants of an earlier tuning, replayed without timing
-        on = {int(x) for x in args.variants.split(',') if x}
-        plan.set_tuning([int(t in on) for t in range(55)])
+        # the FP64 variants of an earlier tuning, replayed without timing:
+        # class index, or class:variant
+        tun = [0] * 55
+        for x in args.variants.split(','):
+            if x:
+                t, _, v = x.partition(':')
+                tun[int(t)] = int(v) if v else 1
+        plan.set_tuning(tun)
     plan.get_jk(f['dm'], hermi=1)
     st = plan.stats()
     print(json.dumps({'workload': args.config, 'ms': st['last_build_ms'], 'quartets': st['quartets'],
-                      'variants': ','.join(str(t) for t, v in enumerate(plan.tuning()) if v)}))
+                      'variants': ','.join('%d:%d' % (t, v) for t, v in enumerate(plan.tuning()) if v)}))
 
 
 class _Mol:
@@ -630,7 +683,8 @@ def main():
                     help='plan + one FP64 J/K build of the workload, nothing else (the case profiled under ncu)')
     ap.add_argument('--autotune', action='store_true', help='--one-build: run the autotuner first')
     ap.add_argument('--variants', default=None,
-                    help='--one-build: comma-separated quartet classes that use launch variant 1 (as printed)')
+                    help='--one-build: comma-separated class:variant pairs (a bare class index means variant 1), '
+                         'as printed by --autotune')
     args = ap.parse_args()
     if args.impl == 'reference':
         run_reference(args)

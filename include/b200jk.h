@@ -117,6 +117,17 @@ int b200jk_plan_update_coords(b200jk_plan *plan, const double *env, int env_len)
 /* nao in the output basis, nbas. */
 int b200jk_plan_dims(const b200jk_plan *plan, int *nao, int *nbas);
 
+/* One-electron integrals of the plan's basis in the output AO basis,
+ * (nao, nao) C order, host or device memory as dev_ptrs (either may be NULL):
+ *   ovlp   the overlap matrix, int1e_ovlp (SCF.get_ovlp, pyscf/scf/hf.py:341)
+ *   hcore  kinetic energy + nuclear attraction of the point (or fractional)
+ *          nuclear charges of atm, int1e_kin + int1e_nuc (get_hcore,
+ *          pyscf/scf/hf.py:315-340, without ECP and finite-nucleus terms:
+ *          atoms with those give B200JK_EUNSUPPORTED).
+ * No Schwarz screening; primitive pairs as in the J/K build (exp(-ab/(a+b)
+ * |AB|^2) >= e^-60). */
+int b200jk_int1e(b200jk_plan *plan, double *ovlp, double *hcore, int dev_ptrs, void *stream);
+
 /* Copy q_cond (nbas x nbas, C order) to host memory. */
 int b200jk_get_q_cond(const b200jk_plan *plan, double *q_cond);
 
@@ -162,7 +173,7 @@ int b200jk_class_stats(const b200jk_plan *plan, b200jk_class_stat_t *out, int ma
 int b200jk_set_profiling(b200jk_plan *plan, int on);
 
 /* Autotuner: for every quartet class with more than one launch variant (the
- * register family with one or several kets per lane; the shared-memory
+ * register family with one or several kets per lane, or bra runs; the shared-memory
  * family with full- or half-width lane groups per quartet), time each variant
  * on FP64 J/K builds of the density dm (nao x nao, symmetric; host array, or
  * device array with dev_ptrs = 1), then the float32 pass's variants on mixed
@@ -181,8 +192,12 @@ int b200jk_set_tile(b200jk_plan *plan, int tile_b);
  * of mixed builds (B200JK_PREC_MIXED). */
 int b200jk_get_tuning(const b200jk_plan *plan, int precision, int *variants, int max, int *n);
 
-/* Set the variants directly (n = 55; 0 everywhere, 1 only where the class has
- * a second variant, else B200JK_EINVAL): replays a tuning without timing. */
+/* Set the variants directly (n = 55; 0 everywhere, 1 or 2 only where the
+ * class has that variant, 2 only for B200JK_PREC_FP64, else B200JK_EINVAL):
+ * replays a tuning without timing.  Variant 2 (register family, bra runs: a
+ * warp keeps its kets for 4 consecutive bra pairs and carries their K[a,*]
+ * and ket-side J sums in registers) applies to the float64 pass of unsharded
+ * builds of one symmetric density; other builds run such classes as 0. */
 int b200jk_set_tuning(b200jk_plan *plan, int precision, const int *variants, int n);
 
 /* Nuclear-gradient J/K: the drop-in for pyscf.grad.rhf.get_jk(mol, dm)
@@ -287,7 +302,28 @@ int b200jk_set_prescreen(b200jk_plan *plan, int screen);
  * build, so incremental (difference-density) builds move more quartets to
  * float32 as the SCF converges.  tau <= 0 makes mixed mode all-float64.
  * No reference counterpart: PySCF evaluates every quartet in float64. */
-int b200jk_set_mixed_threshold(b200jk_plan *plan, double tau);
+int b200jk_set_mixed_threshold(b200jk_plan *plan, double tau);   /* also clears per-class thresholds */
+
+/* Per-class float32 thresholds of B200JK_PREC_MIXED (n = 55, one per quartet
+ * class in the order of b200jk_class_stats; >= 0, 0 keeps the class in
+ * float64); tau NULL or n = 0 returns to the plan's single threshold, as
+ * b200jk_set_mixed_threshold does.  Batches use their first plan's. */
+int b200jk_set_class_thresholds(b200jk_plan *plan, const double *tau, int n);
+int b200jk_get_class_thresholds(const b200jk_plan *plan, double *tau, int max, int *n);
+
+/* Mixed-precision tuner: picks the float32 threshold of every quartet class
+ * for the density dm (nao x nao, symmetric; host, or device with dev_ptrs).
+ * Classes whose float32 kernels are not faster than their float64 ones (class
+ * CUDA events of an all-float64 and an all-float32 build) stay in float64;
+ * the others get the largest threshold of the ladder 1e-2 ... 1e-8 for which
+ * the two-electron energy E2 = 1/2 tr(D J) - 1/4 tr(D K) of the mixed build
+ * stays within `budget` (Eh) of the all-float64 build's.  The thresholds are
+ * kept for later builds (b200jk_get_class_thresholds).  result, if not NULL,
+ * receives {chosen threshold, dE2, max|dJ|, max|dK|} of the accepted build
+ * against the float64 one.  At most 9 builds.  No reference counterpart
+ * (PySCF evaluates every quartet in float64). */
+int b200jk_autotune_mixed(b200jk_plan *plan, const double *dm, int dev_ptrs, double budget, double *result,
+                          void *stream);
 
 /* Measured FP64 FMA throughput of device `device` (TFLOP/s), from a
  * register-resident FMA loop over all SMs: the denominator of the FP64

@@ -36,9 +36,20 @@ import sys
 import glob
 
 HERE = os.path.dirname(os.path.abspath(__file__))
-REF_ROOT = os.environ.get('PYSCF_REFERENCE_ROOT', '/root/reference')
-REF_LIB = os.path.join(REF_ROOT, 'pyscf', 'lib')
 OUT_REF = os.path.join(HERE, '_ref')
+
+
+def _recorded_root():
+    """The checkout an earlier build_ref() compiled from (recorded in the
+    git-ignored oracle/_ref), so later runs find it without the variable."""
+    p = os.path.join(OUT_REF, 'reference_root')
+    return open(p).read().strip() if os.path.exists(p) else ''
+
+
+# the reference checkout: PYSCF_REFERENCE_ROOT, else the one the last
+# build_ref() used; without either only the restatement (liboracle.so) builds
+REF_ROOT = os.environ.get('PYSCF_REFERENCE_ROOT') or _recorded_root()
+REF_LIB = os.path.join(REF_ROOT, 'pyscf', 'lib')
 OUT_LIBDIR = os.path.join(OUT_REF, 'pyext', 'pyscf', 'lib')
 CFLAGS = ['-O2', '-fPIC', '-fopenmp', '-std=gnu99', '-w']
 
@@ -115,6 +126,8 @@ def build_ref(force=False):
     if blas is None:
         raise RuntimeError('no BLAS exporting dgemm_ found')
     os.makedirs(OUT_LIBDIR, exist_ok=True)
+    with open(os.path.join(OUT_REF, 'reference_root'), 'w') as fh:
+        fh.write(os.path.abspath(REF_ROOT))
     objdir = os.path.join(OUT_REF, 'obj')
     os.makedirs(objdir, exist_ok=True)
     stamp = os.path.join(OUT_LIBDIR, 'libcvhf.so')

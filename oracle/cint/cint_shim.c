@@ -541,6 +541,13 @@ static int int2e_generic(double *out, const int *dims, const int *shls,
         double rrab = AB[0] * AB[0] + AB[1] * AB[1] + AB[2] * AB[2];
         double rrcd = CD[0] * CD[0] + CD[1] * CD[1] + CD[2] * CD[2];
         double cutoff = expcutoff_of(env);
+        /* range-separated Coulomb (libcint's env[PTR_RANGE_OMEGA], set by
+         * mol.with_range_coulomb): omega > 0 is erf(omega r)/r, omega < 0
+         * erfc(|omega| r)/r.  The Obara-Saika recurrence is a polynomial in
+         * the Rys variable t^2, so attenuating the operator only changes the
+         * auxiliary integrals: F_m(T) -> theta^(m+1/2) F_m(theta T) with
+         * theta = omega^2 / (omega^2 + rho) for erf, F_m - that for erfc. */
+        const double omega = env[PTR_RANGE_OMEGA];
 
         int nab_c = ncart(la + raise_a) * ncart(lb);
         int ncd_c = ncart(lc + raise_c) * ncart(ld);
@@ -590,6 +597,17 @@ static int int2e_generic(double *out, const int *dims, const int *shls,
                         double T = rho * (PQ[0] * PQ[0] + PQ[1] * PQ[1] + PQ[2] * PQ[2]);
                         double pref = 2 * pow(M_PI, 2.5) / (p * q * sqrt(p + q)) * Kab * Kcd;
                         oracle_boys(L, T, fm);
+                        if (omega != 0) {
+                                double gm[MMAX + 1];
+                                const double theta = omega * omega / (omega * omega + rho);
+                                oracle_boys(L, theta * T, gm);
+                                double tp = sqrt(theta);
+                                for (int m = 0; m <= L; m++) {
+                                        gm[m] *= tp;
+                                        tp *= theta;
+                                        fm[m] = omega > 0 ? gm[m] : fm[m] - gm[m];
+                                }
+                        }
                         for (int m = 0; m <= L; m++) fm[m] *= pref;
                         vrr2e(V, Ea, Fc, fm, PA, WP, QC, WQ, p, q);
                         /* accumulate contracted rows */

@@ -45,10 +45,78 @@ def cached_plan(atm, bas, env, cart=False, direct_scf_tol=0.0, device=0):
     return p
 
 
-def _check_env(env):
+PTR_RANGE_OMEGA = 8   # pyscf/gto/mole.py:76
+
+
+def _omega(env):
     env = numpy.asarray(env)
-    if env.size > 8 and env[8] != 0:
-        raise NotImplementedError('range-separated Coulomb (omega != 0) is not implemented in pyscf_b200')
+    return float(env[PTR_RANGE_OMEGA]) if env.size > PTR_RANGE_OMEGA else 0.0
+
+
+def _with_omega(env, omega):
+    env = numpy.array(env, dtype=numpy.double, copy=True)
+    env[PTR_RANGE_OMEGA] = omega
+    return env
+
+
+class ShortRangePlan:
+    """J/K of the short-range operator erfc(w r12)/r12 (env[PTR_RANGE_OMEGA]
+    = -w < 0, as mol.with_short_range_coulomb sets it): the full-range build
+    minus the long-range erf(w r12)/r12 build, erfc = 1 - erf, each on its own
+    device plan with its own Schwarz bounds.  The reference evaluates the
+    erfc integrals directly (libcint, through the same CVHFnr_direct_drv,
+    pyscf/scf/_vhf.py:611-627 without optimize_sr)."""
+
+    def __init__(self, atm, bas, env, cart=False, direct_scf_tol=1e-13, device=0):
+        w = -_omega(env)
+        self.full = cached_plan(atm, bas, _with_omega(env, 0.0), cart, direct_scf_tol, device)
+        self.lr = cached_plan(atm, bas, _with_omega(env, w), cart, direct_scf_tol, device)
+        self.nao, self.nbas = self.full.nao, self.full.nbas
+        self.device = self.full.device
+
+    def set_prescreen(self, screen=lib.SCREEN_NRS8):
+        self.full.set_prescreen(screen)
+        self.lr.set_prescreen(screen)
+
+    def get_jk(self, dms, hermi=1, with_j=True, with_k=True, out_j=None, out_k=None, precision=lib.PREC_FP64,
+               stream=None):
+        fj, fk = self.full.get_jk(dms, hermi, with_j, with_k, precision=precision)
+        lj, lk = self.lr.get_jk(dms, hermi, with_j, with_k, precision=precision)
+        vj = vk = None
+        if with_j:
+            vj = fj - lj
+            if out_j is not None:
+                out_j[...] = vj.reshape(out_j.shape)
+                vj = out_j
+        if with_k:
+            vk = fk - lk
+            if out_k is not None:
+                out_k[...] = vk.reshape(out_k.shape)
+                vk = out_k
+        return vj, vk
+
+    def get_jk_device(self, dms, hermi=1, with_j=True, with_k=True, precision=lib.PREC_FP64):
+        fj, fk = self.full.get_jk_device(dms, hermi, with_j, with_k, precision)
+        lj, lk = self.lr.get_jk_device(dms, hermi, with_j, with_k, precision)
+        return (fj - lj if with_j else None), (fk - lk if with_k else None)
+
+    def grad_jk(self, dms, with_j=True, with_k=True, direct_scf_tol=1e-14):
+        fj, fk = self.full.grad_jk(dms, with_j, with_k, direct_scf_tol)
+        lj, lk = self.lr.grad_jk(dms, with_j, with_k, direct_scf_tol)
+        return (fj - lj if with_j else None), (fk - lk if with_k else None)
+
+    def close(self):
+        pass
+
+
+def make_plan(atm, bas, env, cart=False, direct_scf_tol=1e-13, device=0, cached=True):
+    """The device plan of a molecule: long range (omega > 0) and full range
+    run in the kernels; short range (omega < 0) as full minus long range."""
+    if _omega(env) < 0:
+        return ShortRangePlan(atm, bas, env, cart, direct_scf_tol, device)
+    if cached:
+        return cached_plan(atm, bas, env, cart, direct_scf_tol, device)
+    return lib.Plan(atm, bas, env, cart=cart, direct_scf_tol=direct_scf_tol, device=device)
 
 
 class VHFOpt:
@@ -64,15 +132,18 @@ class VHFOpt:
             raise NotImplementedError('VHFOpt supports the int2e Coulomb kernel only, not %s' % intor)
         if prescreen not in _SCREENS and prescreen not in ('CVHFnoscreen', None):
             raise NotImplementedError('prescreen %s is not implemented' % prescreen)
-        _check_env(mol._env)
         self.mol = mol
         self._intor = intor
         self._prescreen = prescreen
         self._qcondname = qcondname
         self._dmcondname = dmcondname
         tol = direct_scf_tol if prescreen in _SCREENS else 0.0
-        self.plan = lib.Plan(mol._atm, mol._bas, mol._env, cart=getattr(mol, 'cart', False),
-                             direct_scf_tol=tol, device=device)
+        # the molecule's current operator: full, long range (omega > 0) or
+        # short range (omega < 0), as SCF.get_jk builds one _VHFOpt per omega
+        self.plan = make_plan(mol._atm, mol._bas, mol._env, getattr(mol, 'cart', False), tol, device,
+                              cached=False)
+        self._arrays = (numpy.array(mol._atm, dtype=numpy.int32), numpy.array(mol._bas, dtype=numpy.int32),
+                        numpy.array(mol._env, dtype=numpy.double), bool(getattr(mol, 'cart', False)))
         self._direct_scf_tol = direct_scf_tol
 
     @property
@@ -103,10 +174,10 @@ class VHFOpt:
         return self.plan.q_cond
 
     def matches(self, atm, bas, env, cart):
-        return (self.plan.atm.shape == numpy.shape(atm) and self.plan.bas.shape == numpy.shape(bas)
-                and numpy.array_equal(self.plan.atm, atm) and numpy.array_equal(self.plan.bas, bas)
-                and self.plan.env.shape == numpy.shape(env) and numpy.array_equal(self.plan.env, env)
-                and self.plan.cart == bool(cart))
+        a, b, e, c = self._arrays
+        return (a.shape == numpy.shape(atm) and b.shape == numpy.shape(bas) and numpy.array_equal(a, atm)
+                and numpy.array_equal(b, bas) and e.shape == numpy.shape(env) and numpy.array_equal(e, env)
+                and c == bool(cart))
 
 
 # the reference's per-quartet screens and the engine's modes for them
@@ -120,17 +191,18 @@ def _resolve_plan(vhfopt, atm, bas, env, cart):
         return vhfopt.plan
     if vhfopt is None:
         # the reference runs CVHFnr_direct_drv without any screening here
-        return cached_plan(atm, bas, env, cart, 0.0)
+        return make_plan(atm, bas, env, cart, 0.0)
     tol = getattr(vhfopt, 'direct_scf_tol', 1e-13)
-    plan = cached_plan(atm, bas, env, cart, tol)
+    plan = make_plan(atm, bas, env, cart, tol)
     plan.set_prescreen(_SCREENS.get(getattr(vhfopt, 'prescreen', None), lib.SCREEN_NRS8))
     return plan
 
 
 def direct(dms, atm, bas, env, vhfopt=None, hermi=0, cart=False,
            with_j=True, with_k=True, out=None, optimize_sr=False):
-    """J and K of one or several densities (pyscf/scf/_vhf.py:405-464)."""
-    _check_env(env)
+    """J and K of one or several densities (pyscf/scf/_vhf.py:405-464);
+    env[PTR_RANGE_OMEGA] selects the operator as in the reference (0 full,
+    > 0 erf(w r)/r, < 0 erfc(|w| r)/r)."""
     try:
         import torch
         is_torch = isinstance(dms, torch.Tensor)

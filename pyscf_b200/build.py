@@ -21,7 +21,7 @@ CSRC = os.path.join(HERE, 'csrc')
 OBJ = os.path.join(HERE, '_build')
 LIB = os.path.join(HERE, 'libb200jk.so')
 HEADERS = ['rys_math.cuh', 'jk_kernels.cuh', 'jk_launch.h', 'rys_table.inc', 'rys_table_f.inc',
-           'grad_kernels.cuh', 'grad_launch.h']
+           'grad_kernels.cuh', 'grad_launch.h', 'int1e_kernels.cuh']
 ARCH = ['-gencode', 'arch=compute_100a,code=sm_100a']
 PAIR_CLASSES = [(la, lb) for la in range(4) for lb in range(la + 1)]
 QUARTET_CLASSES = [(la, lb, lc, ld) for x, (la, lb) in enumerate(PAIR_CLASSES)
@@ -55,7 +55,7 @@ _RYS = ['rys_math.cuh', 'rys_table.inc', 'rys_table_f.inc']
 _JK = _RYS + ['jk_kernels.cuh', 'jk_launch.h']
 _GRAD = _JK + ['grad_kernels.cuh', 'grad_launch.h']
 UNIT_DEPS = {
-    'b200jk.cu': _GRAD + ['../../include/b200jk.h'],
+    'b200jk.cu': _GRAD + ['int1e_kernels.cuh', '../../include/b200jk.h'],
     'jk_qcond.cu': _JK,
     'jk_classes.cu': _JK,
     'grad_classes.cu': _GRAD,
@@ -73,6 +73,23 @@ def _stale(obj, src, flags_file):
     return any(os.path.getmtime(d) > t for d in deps)
 
 
+# quartet classes whose register-family kernels are compiled for 4 blocks per
+# SM (at most 128 registers a thread): the classes where that build was the
+# faster one on the FP64 build of (H2O)64/cc-pVTZ against the compiler's own
+# allocation (class CUDA events, both builds with launch variants 0 and 2; a
+# few spills buy 16 resident warps instead of 12 or fewer).  B2_THREAD_MINB=<n> in the environment overrides it
+# for every class.
+THREAD_MINB4 = {(1, 0, 0, 0), (1, 1, 0, 0), (2, 0, 0, 0), (2, 1, 0, 0), (3, 1, 0, 0), (3, 2, 0, 0),
+                (3, 3, 0, 0)}
+
+
+def _thread_minb(cls):
+    env = os.environ.get('B2_THREAD_MINB')
+    if env:
+        return int(env)
+    return 4 if cls in THREAD_MINB4 else 0
+
+
 def _units():
     nvcc = nvcc_path()
     common = [nvcc, *ARCH, '-O3', '-lineinfo', '-std=c++17', '-Xcompiler', '-fPIC',
@@ -87,6 +104,7 @@ def _units():
         o = os.path.join(OBJ, 'jk_%s.o' % tag)
         units.append((common + ['-DB2_BRA_LA=%d' % la, '-DB2_BRA_LB=%d' % lb, '-DB2_KET_LC=%d' % lc,
                                 '-DB2_KET_LD=%d' % ld, '-DB2_FN_NAME=launch_jk_%s' % tag,
+                                '-DB2_THREAD_MINB=%d' % _thread_minb((la, lb, lc, ld)),
                                 os.path.join(CSRC, 'jk_classes.cu'), '-o', o], o))
     for la, lb in PAIR_CLASSES:
         o = os.path.join(OBJ, 'grad_%d%d.o' % (la, lb))
@@ -106,8 +124,9 @@ def _source_of(cmd):
 
 
 def build(force=False, verbose=False, extra=(), jobs=None):
-    if not force and up_to_date():
-        return LIB
+    # every unit is checked against its own sources (an object compiled while
+    # its source was being edited is older than the edit even when the library
+    # was linked after it); the library is relinked when an object changed
     os.makedirs(OBJ, exist_ok=True)
     units = _units()
     if extra:
@@ -137,7 +156,10 @@ def build(force=False, verbose=False, extra=(), jobs=None):
             raise RuntimeError('compile failed: %s\n%s%s' % (' '.join(cmd), r.stdout, r.stderr))
         if verbose and (r.stdout or r.stderr):
             msgs.append(r.stdout + r.stderr)
-    link = [nvcc_path(), *ARCH, '--shared', '-Xcompiler', '-fPIC', '-o', LIB + '.tmp'] + [o for _, o in units]
+    objs = [o for _, o in units]
+    if not todo and os.path.exists(LIB) and all(os.path.getmtime(o) <= os.path.getmtime(LIB) for o in objs):
+        return LIB
+    link = [nvcc_path(), *ARCH, '--shared', '-Xcompiler', '-fPIC', '-o', LIB + '.tmp'] + objs
     r = subprocess.run(link, capture_output=True, text=True)
     if r.returncode != 0:
         raise RuntimeError('link failed:\n' + r.stdout + r.stderr)

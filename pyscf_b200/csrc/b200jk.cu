@@ -28,6 +28,7 @@
 #include "rys_math.cuh"
 #include "jk_launch.h"
 #include "grad_launch.h"
+#include "int1e_kernels.cuh"
 #include "../../include/b200jk.h"
 
 using namespace b200jk;
@@ -83,6 +84,8 @@ static bool alloc_should_fail()
         }
         return false;
 }
+
+static inline unsigned grid_for(long long n, int block) { return (unsigned)((n + block - 1) / block); }
 
 // slot layout of PySCF's _atm/_bas/_env (pyscf/gto/mole.py:58-88)
 enum { CHARGE_OF = 0, PTR_COORD = 1, ATM_SLOTS = 6 };
@@ -265,8 +268,11 @@ struct GradPlan {
 struct b200jk_plan {
         int device = 0, cart = 0, natm = 0, nbas = 0, nao = 0, naoc = 0, nseg = 0;
         double tol = 0;
-        // mixed precision: quartets with q_ij q_kl max|D| below fp32_tau run in float32
+        // mixed precision: quartets with q_ij q_kl max|D| below fp32_tau run in
+        // float32; tau_class (when set: one per quartet class, from
+        // b200jk_set_class_thresholds or b200jk_autotune_mixed) replaces it per class
         double fp32_tau = 1e-6;
+        std::vector<double> tau_class;
         // multi-GPU: this plan evaluates the bra pairs ij = shard (mod nshard)
         int shard = 0, nshard = 1;
         // launch variant per quartet class (register family: 0 = one ket per
@@ -279,6 +285,8 @@ struct b200jk_plan {
         int tile_b = 64;
         // density part of the quartet screen (B200JK_SCREEN_*)
         int screen = B200JK_SCREEN_NRS8;
+        // omega^2 of the long-range operator erf(omega r12)/r12 (0: Coulomb)
+        double omega2 = 0.0;
         // packed ket blocks for the J contraction: class X's blocks start at
         // pk_off[X] (entries, in ket-list order); pk_src maps entries to the
         // Cartesian matrix
@@ -289,6 +297,17 @@ struct b200jk_plan {
         std::vector<int> ao_loc;
         std::vector<int> shell_atom;   // atom of every PySCF shell (bas[:, ATOM_OF])
         std::vector<int32_t> h_atm, h_bas;   // the molecule's atm / bas (for b200jk_plan_update_coords)
+        // nuclei of the one-electron integrals: (x, y, z, Z); nuc_model_ok is
+        // false when an atom has a finite-nucleus model or an ECP core
+        std::vector<double4> h_atoms;
+        bool nuc_model_ok = true;
+        // one-electron integrals: pair list and buffers (built on first use)
+        DevArr<int4> i1_pair;
+        DevArr<long long> i1_off;
+        DevArr<double4> i1_seg, i1_atoms;
+        DevArr<int> i1_seg_cart;
+        DevArr<double> i1_S, i1_H, i1_zero, i1_out;
+        int i1_npair = -1;
         std::vector<double> h_qcond;
         PairClassDev pc[NPAIRCLASS];
         DevArr<double4> PP;
@@ -326,6 +345,8 @@ struct b200jk_plan {
                 goff_all.release(); seg_info.release(); out_seg.release(); out_comp.release();
                 cart_seg.release(); cart_comp.release(); ao_loc_d.release();
                 D.release(); Dc.release(); Ds.release(); Jacc.release(); Kacc.release(); outJ.release(); outK.release();
+                i1_pair.release(); i1_off.release(); i1_seg.release(); i1_atoms.release(); i1_seg_cart.release();
+                i1_S.release(); i1_H.release(); i1_zero.release(); i1_out.release();
                 dmax.release(); stats.release(); nkl.release(); kst.release(); nchunk.release(); chunk_off.release(); cub_tmp.release();
                 for (auto e : cls_ev) cudaEventDestroy(e);
                 if (ev0) cudaEventDestroy(ev0);
@@ -360,6 +381,13 @@ static int class_variant(const b200jk_plan *P, size_t t, int pass)
 {
         const std::vector<int> &v = pass == 1 ? P->kvar32 : P->kvar;
         return t < v.size() ? v[t] : 0;
+}
+
+// the float32 threshold of quartet class t in mixed builds
+static double class_tau(const b200jk_plan *P, size_t t)
+{
+        if (P->tau_class.size() > t) return P->tau_class[t];
+        return P->fp32_tau;
 }
 
 static int dispatch_jk(b200jk_plan *P, int la, int lb, int lc, int ld, const JKArgs &a, int fp32, cudaStream_t s,
@@ -584,10 +612,17 @@ int b200jk_plan_create(const int32_t *atm, int natm, const int32_t *bas, int nba
         *out = nullptr;
         if (!atm || !bas || !env || natm <= 0 || nbas <= 0 || env_len <= PTR_RANGE_OMEGA)
                 return fail(B200JK_EINVAL, "empty or NULL molecule arrays");
-        if (env[PTR_RANGE_OMEGA] != 0.0)
-                return fail(B200JK_EUNSUPPORTED, "range-separated Coulomb (env[PTR_RANGE_OMEGA] != 0) is not implemented");
+        // env[PTR_RANGE_OMEGA] > 0: the long-range operator erf(omega r12)/r12,
+        // as libcint evaluates it under mol.with_range_coulomb(omega); < 0
+        // (short range, erfc) is built by callers as full minus long range
+        const double omega = env[PTR_RANGE_OMEGA];
+        if (!(omega == omega)) return fail(B200JK_EINVAL, "env[PTR_RANGE_OMEGA] is NaN");
+        if (omega < 0.0)
+                return fail(B200JK_EUNSUPPORTED, "short-range Coulomb (env[PTR_RANGE_OMEGA] < 0) is not a plan of its own: "
+                                                 "subtract the long-range build (omega = |omega|) from the full one");
         b200jk_plan *P = new b200jk_plan();
         P->device = device;
+        P->omega2 = omega > 0 ? omega * omega : 0.0;
         P->cart = cart ? 1 : 0;
         P->natm = natm;
         P->nbas = nbas;
@@ -599,6 +634,21 @@ int b200jk_plan_create(const int32_t *atm, int natm, const int32_t *bas, int nba
         std::vector<Seg> segs;
         int rc = build_segments(P, atm, natm, bas, nbas, env, env_len, segs);
         if (rc) return bail(rc);
+        // nuclei (libcint's int1e_nuc reads the same slots, pyscf/gto/mole.py:58-94)
+        for (int ia = 0; ia < natm; ia++) {
+                const int32_t *ar = atm + (size_t)ia * ATM_SLOTS;
+                const int pc = ar[PTR_COORD], model = ar[2];   // NUC_MOD_OF
+                if (pc < 0 || pc + 3 > env_len) return bail(fail(B200JK_EINVAL, "atm: coordinate pointer outside env"));
+                double z = (double)ar[CHARGE_OF];
+                if (model == 3) {   // NUC_FRAC_CHARGE: the charge is env[atm[PTR_FRAC_CHARGE]]
+                        const int pz = ar[4];
+                        if (pz < 0 || pz >= env_len) return bail(fail(B200JK_EINVAL, "atm: fractional-charge pointer outside env"));
+                        z = env[pz];
+                } else if (model != 0 && model != 1) {
+                        P->nuc_model_ok = false;   // NUC_GAUSS or NUC_ECP
+                }
+                P->h_atoms.push_back(make_double4(env[pc], env[pc + 1], env[pc + 2], z));
+        }
         int ndev = 0;
         if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) {
                 cudaGetLastError();
@@ -733,6 +783,7 @@ int b200jk_plan_create(const int32_t *atm, int natm, const int32_t *bas, int nba
                 auto qcs = quartet_classes();
                 for (int X = 0; X < NPAIRCLASS; X++) {
                         QArgs qa;
+                        qa.omega2 = P->omega2;
                         qa.pairs = P->pc[X].view();
                         qa.PP = P->PP.p; qa.PK = P->PK.p;
                         qa.table = table_ptr();
@@ -851,12 +902,88 @@ int b200jk_plan_update_coords(b200jk_plan *P, const double *env, int env_len)
         std::swap(P->pk_total, T->pk_total);
         std::swap(P->pk_src, T->pk_src);
         std::swap(P->grad, T->grad);   // derivative bounds belong to the old geometry
+        std::swap(P->h_atoms, T->h_atoms);
+        P->nuc_model_ok = T->nuc_model_ok;
+        P->i1_npair = -1;              // the one-electron pair list is planned again on next use
         P->shell_pairs = T->shell_pairs;
         P->prim_pairs = T->prim_pairs;
         P->st = T->st;
         // captured batched builds hold the old tables' addresses
         P->ws_gen++;
         b200jk_plan_destroy(T);
+        return B200JK_OK;
+}
+
+int b200jk_int1e(b200jk_plan *P, double *ovlp, double *hcore, int dev_ptrs, void *stream)
+{
+        if (!P) return fail(B200JK_EINVAL, "plan is NULL");
+        if (!ovlp && !hcore) return fail(B200JK_EINVAL, "no output requested");
+        if (hcore && !P->nuc_model_ok)
+                return fail(B200JK_EUNSUPPORTED, "finite-nucleus models and ECP atoms are not implemented in the "
+                                                 "nuclear-attraction integrals");
+        CUDA_TRY(cudaSetDevice(P->device));
+        int rc;
+        if (dev_ptrs && ((ovlp && (rc = check_dev_ptr(ovlp, P->device, "ovlp"))) ||
+                         (hcore && (rc = check_dev_ptr(hcore, P->device, "hcore")))))
+                return rc;
+        const size_t nc = (size_t)P->naoc * P->naoc, nn = (size_t)P->nao * P->nao;
+        if (P->i1_npair < 0) {
+                // every segment pair with a primitive pair (no Schwarz screening here)
+                std::vector<int4> hp;
+                std::vector<long long> off(1, 0);
+                for (int X = 0; X < NPAIRCLASS; X++)
+                        for (const PairLite &q : P->all_pairs[X]) {
+                                hp.push_back(make_int4(q.i, q.j, q.prim0, q.nprim));
+                                off.push_back(off.back() + (long long)ncart(P->segl[q.i].l) * ncart(P->segl[q.j].l));
+                        }
+                std::vector<double4> hs(P->segl.size());
+                std::vector<int> hc(P->segl.size());
+                for (size_t t = 0; t < P->segl.size(); t++) {
+                        hs[t] = make_double4(P->segl[t].R[0], P->segl[t].R[1], P->segl[t].R[2], (double)P->segl[t].l);
+                        hc[t] = P->segl[t].cart_off;
+                }
+                if ((rc = dev_upload(P->i1_pair, hp)) || (rc = dev_upload(P->i1_off, off)) || (rc = dev_upload(P->i1_seg, hs)) ||
+                    (rc = dev_upload(P->i1_seg_cart, hc)) || (rc = dev_upload(P->i1_atoms, P->h_atoms)) ||
+                    (rc = dev_alloc(P->i1_S, nc)) || (rc = dev_alloc(P->i1_H, nc)) || (rc = dev_alloc(P->i1_zero, nc)) ||
+                    (rc = dev_alloc(P->i1_out, 2 * nn)))
+                        return rc;
+                CUDA_TRY(cudaMemset(P->i1_zero.p, 0, sizeof(double) * nc));
+                P->i1_npair = (int)hp.size();
+        }
+        cudaStream_t s = stream ? (cudaStream_t)stream : P->stream;
+        CUDA_TRY(cudaMemsetAsync(P->i1_S.p, 0, sizeof(double) * nc, s));
+        CUDA_TRY(cudaMemsetAsync(P->i1_H.p, 0, sizeof(double) * nc, s));
+        long long nelem = 0;
+        CUDA_TRY(cudaMemcpy(&nelem, P->i1_off.p + P->i1_npair, sizeof(long long), cudaMemcpyDeviceToHost));
+        if (nelem > 0) {
+                Int1eArgs a;
+                a.pair = P->i1_pair.p; a.elem_off = P->i1_off.p; a.npair = P->i1_npair;
+                a.seg = P->i1_seg.p; a.seg_cart = P->i1_seg_cart.p;
+                a.PP = P->PP.p; a.PK = P->PK.p; a.PE = P->PE.p;
+                a.atoms = P->i1_atoms.p; a.natm = (int)P->h_atoms.size(); a.naoc = P->naoc;
+                a.table = table_ptr();
+                a.S = P->i1_S.p; a.H = P->i1_H.p;
+                int1e_kernel<<<grid_for(nelem, 128), 128, 0, s>>>(a);
+                CUDA_TRY(cudaGetLastError());
+        }
+        double *os = dev_ptrs ? ovlp : P->i1_out.p, *oh = dev_ptrs ? hcore : P->i1_out.p + nn;
+        if (ovlp) {
+                cart_to_out_kernel<<<grid_for((long long)nn, 256), 256, 0, s>>>(P->i1_S.p, P->i1_zero.p, P->nao, P->naoc,
+                                                                               P->out_seg.p, P->out_comp.p, P->seg_info.p,
+                                                                               P->c2s.p, P->cart, 1, os);
+                CUDA_TRY(cudaGetLastError());
+        }
+        if (hcore) {
+                cart_to_out_kernel<<<grid_for((long long)nn, 256), 256, 0, s>>>(P->i1_H.p, P->i1_zero.p, P->nao, P->naoc,
+                                                                               P->out_seg.p, P->out_comp.p, P->seg_info.p,
+                                                                               P->c2s.p, P->cart, 1, oh);
+                CUDA_TRY(cudaGetLastError());
+        }
+        if (!dev_ptrs) {
+                if (ovlp) CUDA_TRY(cudaMemcpyAsync(ovlp, os, sizeof(double) * nn, cudaMemcpyDeviceToHost, s));
+                if (hcore) CUDA_TRY(cudaMemcpyAsync(hcore, oh, sizeof(double) * nn, cudaMemcpyDeviceToHost, s));
+        }
+        CUDA_TRY(cudaStreamSynchronize(s));
         return B200JK_OK;
 }
 
@@ -901,7 +1028,6 @@ static int ensure_workspace(b200jk_plan *P, int n_dm)
         return B200JK_OK;
 }
 
-static inline unsigned grid_for(long long n, int block) { return (unsigned)((n + block - 1) / block); }
 
 int b200jk_get_jk(b200jk_plan *P, const double *dms, int n_dm, int hermi, int with_j, int with_k,
                   double *vj, double *vk, int dev_ptrs, int precision_mode, void *stream)
@@ -913,7 +1039,7 @@ int b200jk_get_jk(b200jk_plan *P, const double *dms, int n_dm, int hermi, int wi
         if (with_k && !vk) return fail(B200JK_EINVAL, "vk is NULL while with_k is set");
         if (precision_mode != B200JK_PREC_FP64 && precision_mode != B200JK_PREC_MIXED)
                 return fail(B200JK_EUNSUPPORTED, "precision_mode must be 0 (FP64) or 1 (mixed FP32/FP64)");
-        const int mixed = precision_mode == B200JK_PREC_MIXED && P->fp32_tau > 0;
+        const int mixed = precision_mode == B200JK_PREC_MIXED;
         CUDA_TRY(cudaSetDevice(P->device));
         int rc;
         if (dev_ptrs && ((rc = check_dev_ptr(dms, P->device, "dms")) || (with_j && (rc = check_dev_ptr(vj, P->device, "vj"))) ||
@@ -988,23 +1114,31 @@ int b200jk_get_jk(b200jk_plan *P, const double *dms, int n_dm, int hermi, int wi
                         if (P->profiling) CUDA_TRY(cudaEventRecord(P->cls_ev[2 * t], s));
                         // pass 0: float64 quartets (all of them unless mixed);
                         // pass 1: the float32 quartets of mixed precision
-                        for (int pass = 0; pass < (mixed ? 2 : 1); pass++) {
-                                // chunk size of the family the dispatcher will pick
-                                const int variant = class_variant(P, t, pass);
-                                const int chunk = family_chunk(la, lb, lc, ld, variant);
-                                count_kernel<<<grid_for(nseg, 256), 256, 0, s>>>(
-                                        bra.view(), ket.view(), same, P->tol > 0 ? P->tol : 0.0, (const double *)P->dmax.p,
-                                        chunk, mixed ? P->fp32_tau : 0.0, pass, P->shard, P->nshard, P->nkl.p, P->kst.p,
-                                        P->nchunk.p);
-                                CUDA_TRY(cudaGetLastError());
+                        const double tau_c = mixed ? class_tau(P, t) : 0.0;
+                        for (int pass = 0; pass < (tau_c > 0 ? 2 : 1); pass++) {
                                 // tiled chunk order for unsharded plans (with shards the
                                 // stride over bra pairs would leave tile slots idle)
                                 const int tiled = P->nshard == 1 && P->tile_b > 0;
+                                // chunk size of the family the dispatcher will pick; bra
+                                // runs (variant 2) need the tiled float64 pass of one
+                                // symmetric density, else the class runs variant 0
+                                int variant = class_variant(P, t, pass);
+                                const int brun = family_bra_run(la, lb, lc, ld);
+                                if (variant == 2 && (pass == 1 || !tiled || n_dm != 1 || nk != 1 || brun <= 1 ||
+                                                     P->tile_b % brun != 0))
+                                        variant = 0;
+                                const int chunk = family_chunk(la, lb, lc, ld, variant);
+                                count_kernel<<<grid_for(nseg, 256), 256, 0, s>>>(
+                                        bra.view(), ket.view(), same, P->tol > 0 ? P->tol : 0.0, (const double *)P->dmax.p,
+                                        chunk, tau_c, pass, P->shard, P->nshard, P->nkl.p, P->kst.p,
+                                        P->nchunk.p);
+                                CUDA_TRY(cudaGetLastError());
                                 const int ntb = (bra.n + P->tile_b - 1) / std::max(1, P->tile_b);
                                 const int nscan = tiled ? B2_NBUCKET * ntb : nseg;
                                 if (tiled) {
+                                        const int nslot = variant == 2 ? P->tile_b / brun : P->tile_b;
                                         tile_count_kernel<<<grid_for(nscan, 256), 256, 0, s>>>(P->nkl.p, bra.n, chunk, P->tile_b,
-                                                                                             ntb, P->nchunk.p);
+                                                                                             ntb, nslot, P->nchunk.p);
                                         CUDA_TRY(cudaGetLastError());
                                 }
                                 CUDA_TRY(cudaMemsetAsync(P->nchunk.p + nscan, 0, sizeof(long long), s));
@@ -1036,6 +1170,7 @@ int b200jk_get_jk(b200jk_plan *P, const double *dms, int n_dm, int hermi, int wi
                                 a.nbas = P->nbas; a.naoc = P->naoc; a.n_dm = n_dm; a.nk = nk;
                                 a.with_j = with_j; a.with_k = with_k; a.same = same;
                                 a.screen = P->screen;
+                                a.omega2 = P->omega2;
                                 if ((rc = dispatch_jk(P, la, lb, lc, ld, a, pass, s, nullptr, nullptr, 0, variant))) return rc;
                                 launches += 2;   // count + class kernel (the scan is a CUB library kernel)
                         }
@@ -1125,12 +1260,170 @@ int b200jk_set_prescreen(b200jk_plan *plan, int screen)
         return B200JK_OK;
 }
 
+int b200jk_set_class_thresholds(b200jk_plan *plan, const double *tau, int n)
+{
+        if (!plan) return fail(B200JK_EINVAL, "plan is NULL");
+        const int nclass = (int)quartet_classes().size();
+        if (!tau || n == 0) {
+                plan->tau_class.clear();
+                return B200JK_OK;
+        }
+        if (n != nclass) return fail(B200JK_EINVAL, "one threshold per quartet class (55) is required");
+        for (int t = 0; t < n; t++)
+                if (!(tau[t] >= 0)) return fail(B200JK_EINVAL, "thresholds must be >= 0");
+        plan->tau_class.assign(tau, tau + n);
+        return B200JK_OK;
+}
+
+int b200jk_get_class_thresholds(const b200jk_plan *plan, double *tau, int max, int *n)
+{
+        if (!plan || !n) return fail(B200JK_EINVAL, "NULL argument");
+        const int nclass = (int)quartet_classes().size();
+        *n = nclass;
+        for (int t = 0; t < nclass && t < max && tau; t++) tau[t] = class_tau(plan, t);
+        return B200JK_OK;
+}
+
 int b200jk_set_mixed_threshold(b200jk_plan *plan, double tau)
 {
         if (!plan) return fail(B200JK_EINVAL, "plan is NULL");
         if (!(tau == tau)) return fail(B200JK_EINVAL, "tau is NaN");
         plan->fp32_tau = tau;
+        plan->tau_class.clear();
         return B200JK_OK;
+}
+
+// sums[0] += sum D*J, sums[1] += sum D*K; dmax_bits: max |A - B| over n as
+// bits of a non-negative double (for the mixed-precision tuner)
+static __global__ void e2_terms_kernel(const double *D, const double *J, const double *K, long long n, double *sums)
+{
+        double sj = 0.0, sk = 0.0;
+        for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x) {
+                sj += D[i] * J[i];
+                sk += D[i] * K[i];
+        }
+        sj = warp_sum(sj);
+        sk = warp_sum(sk);
+        if ((threadIdx.x & 31) == 0) {
+                atomicAdd(sums, sj);
+                atomicAdd(sums + 1, sk);
+        }
+}
+
+static __global__ void max_abs_diff_kernel(const double *A, const double *B, long long n, unsigned long long *bits)
+{
+        double m = 0.0;
+        for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x)
+                m = fmax(m, fabs(A[i] - B[i]));
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) m = fmax(m, __shfl_xor_sync(0xffffffffu, m, o));
+        if ((threadIdx.x & 31) == 0) atomicMax(bits, (unsigned long long)__double_as_longlong(m));
+}
+
+int b200jk_autotune_mixed(b200jk_plan *P, const double *dm, int dev_ptrs, double budget, double *result,
+                          void *stream)
+{
+        if (!P || !dm) return fail(B200JK_EINVAL, "NULL argument");
+        if (!(budget > 0)) return fail(B200JK_EINVAL, "the error budget must be > 0");
+        CUDA_TRY(cudaSetDevice(P->device));
+        int rc = ensure_workspace(P, 1);
+        if (rc) return rc;
+        cudaStream_t s = stream ? (cudaStream_t)stream : P->stream;
+        const int nclass = (int)quartet_classes().size();
+        const size_t nn = (size_t)P->nao * P->nao;
+        // reference J/K of the FP64 build, the density on the device, reduction slots
+        DevArr<double> ref, dd, sums;
+        DevArr<unsigned long long> bits;
+        auto cleanup = [&]() { ref.release(); dd.release(); sums.release(); bits.release(); };
+        if ((rc = dev_alloc(ref, 2 * nn)) || (rc = dev_alloc(dd, nn)) || (rc = dev_alloc(sums, 2)) ||
+            (rc = dev_alloc(bits, 2))) {
+                cleanup();
+                return rc;
+        }
+        const int saved_prof = P->profiling;
+        const std::vector<double> saved_tau = P->tau_class;
+        P->profiling = 1;
+        double *oj = P->outJ.p, *ok = P->outK.p;
+        if (cudaMemcpyAsync(dd.p, dm, sizeof(double) * nn, dev_ptrs ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice,
+                            s) != cudaSuccess) {
+                P->profiling = saved_prof;
+                cleanup();
+                return fail(B200JK_ECUDA, "copy of the density failed");
+        }
+        const unsigned grid = (unsigned)std::min<long long>(4 * P->nsm, (long long)(nn + 255) / 256);
+        std::vector<double> t64(nclass), t32(nclass), tau(nclass, 0.0);
+        double e64 = 0, chosen = 0, de = 0, dj = 0, dk = 0;
+        auto build = [&](int prec) -> int {
+                return b200jk_get_jk(P, dd.p, 1, 1, 1, 1, oj, ok, 1, prec, stream);
+        };
+        auto e2_and_diff = [&](double &e2, double &maxj, double &maxk) -> int {
+                CUDA_TRY(cudaMemsetAsync(sums.p, 0, 2 * sizeof(double), s));
+                CUDA_TRY(cudaMemsetAsync(bits.p, 0, 2 * sizeof(unsigned long long), s));
+                e2_terms_kernel<<<grid, 256, 0, s>>>(dd.p, oj, ok, (long long)nn, sums.p);
+                max_abs_diff_kernel<<<grid, 256, 0, s>>>(oj, ref.p, (long long)nn, bits.p);
+                max_abs_diff_kernel<<<grid, 256, 0, s>>>(ok, ref.p + nn, (long long)nn, bits.p + 1);
+                CUDA_TRY(cudaGetLastError());
+                double hs[2];
+                unsigned long long hb[2];
+                CUDA_TRY(cudaMemcpyAsync(hs, sums.p, sizeof(hs), cudaMemcpyDeviceToHost, s));
+                CUDA_TRY(cudaMemcpyAsync(hb, bits.p, sizeof(hb), cudaMemcpyDeviceToHost, s));
+                CUDA_TRY(cudaStreamSynchronize(s));
+                e2 = 0.5 * hs[0] - 0.25 * hs[1];
+                memcpy(&maxj, &hb[0], sizeof(double));
+                memcpy(&maxk, &hb[1], sizeof(double));
+                return B200JK_OK;
+        };
+        // 1. FP64 build: reference J/K and per-class times
+        if ((rc = build(B200JK_PREC_FP64))) goto done;
+        if (cudaMemcpyAsync(ref.p, oj, sizeof(double) * nn, cudaMemcpyDeviceToDevice, s) != cudaSuccess ||
+            cudaMemcpyAsync(ref.p + nn, ok, sizeof(double) * nn, cudaMemcpyDeviceToDevice, s) != cudaSuccess) {
+                rc = fail(B200JK_ECUDA, "copy of the FP64 J/K failed");
+                goto done;
+        }
+        for (int t = 0; t < nclass; t++) t64[t] = P->cls.size() > (size_t)t ? P->cls[t].ms : 0.0;
+        {
+                double a, b;
+                if ((rc = e2_and_diff(e64, a, b))) goto done;
+        }
+        // 2. every quartet in float32: per-class times of the float32 kernels
+        P->tau_class.assign(nclass, 1e300);
+        if ((rc = build(B200JK_PREC_MIXED))) goto done;
+        for (int t = 0; t < nclass; t++) t32[t] = P->cls.size() > (size_t)t ? P->cls[t].ms : 0.0;
+        // 3. the largest threshold of the ladder, applied to the classes whose
+        // float32 pass is faster, whose two-electron energy stays within budget
+        {
+                const double ladder[] = {1e-2, 1e-3, 1e-4, 1e-5, 1e-6, 1e-7, 1e-8};
+                bool ok_found = false;
+                for (double tv : ladder) {
+                        for (int t = 0; t < nclass; t++) tau[t] = (t32[t] > 0 && t32[t] < 0.97 * t64[t]) ? tv : 0.0;
+                        P->tau_class = tau;
+                        if ((rc = build(B200JK_PREC_MIXED))) goto done;
+                        double e2;
+                        if ((rc = e2_and_diff(e2, dj, dk))) goto done;
+                        de = e2 - e64;
+                        if (fabs(de) <= budget) {
+                                chosen = tv;
+                                ok_found = true;
+                                break;
+                        }
+                }
+                if (!ok_found) {
+                        std::fill(tau.begin(), tau.end(), 0.0);
+                        P->tau_class = tau;
+                        chosen = 0;
+                }
+        }
+        if (result) {
+                result[0] = chosen;
+                result[1] = de;
+                result[2] = dj;
+                result[3] = dk;
+        }
+done:
+        P->profiling = saved_prof;
+        if (rc) P->tau_class = saved_tau;
+        cleanup();
+        return rc;
 }
 
 int b200jk_autotune(b200jk_plan *P, const double *dm, int dev_ptrs, void *stream)
@@ -1164,7 +1457,8 @@ int b200jk_autotune(b200jk_plan *P, const double *dm, int dev_ptrs, void *stream
                 std::vector<int> &kv = prec ? P->kvar32 : P->kvar;
                 std::fill(best_ms.begin(), best_ms.end(), 1e300);
                 std::fill(best.begin(), best.end(), 0);
-                for (int v = 0; v < 2; v++) {
+                for (int v = 0; v < 3; v++) {
+                        if (v == 2 && prec == 1) break;   // bra runs: float64 pass only
                         kv.assign(nclass, v);
                         if ((rc = b200jk_get_jk(P, dm, 1, 1, 1, 1, oj, ok, dev_ptrs,
                                                 prec ? B200JK_PREC_MIXED : B200JK_PREC_FP64, stream)))
@@ -1173,7 +1467,7 @@ int b200jk_autotune(b200jk_plan *P, const double *dm, int dev_ptrs, void *stream
                                 int la, lb, lc, ld;
                                 class_l(qcs[t].X, la, lb);
                                 class_l(qcs[t].Y, lc, ld);
-                                if (v == 1 && !family_has_variant(la, lb, lc, ld)) continue;   // no such variant
+                                if (!family_has_variant_n(la, lb, lc, ld, v)) continue;   // no such variant
                                 if (P->cls[t].ms < best_ms[t]) { best_ms[t] = P->cls[t].ms; best[t] = v; }
                         }
                 }
@@ -1218,7 +1512,8 @@ int b200jk_set_tuning(b200jk_plan *P, int precision, const int *variants, int n)
                 int la, lb, lc, ld;
                 class_l(qcs[t].X, la, lb);
                 class_l(qcs[t].Y, lc, ld);
-                if (variants[t] != 0 && !(variants[t] == 1 && family_has_variant(la, lb, lc, ld)))
+                if (variants[t] < 0 || variants[t] > 2 || !family_has_variant_n(la, lb, lc, ld, variants[t]) ||
+                    (variants[t] == 2 && precision == B200JK_PREC_MIXED))
                         return fail(B200JK_EINVAL, "variant not available for this quartet class");
         }
         (precision == B200JK_PREC_MIXED ? P->kvar32 : P->kvar).assign(variants, variants + n);
@@ -1377,6 +1672,7 @@ static int ensure_grad(b200jk_plan *P, double tol)
                         PairClassDev tmp;
                         if ((rc = upload_pairs(P, tmp, X, hv, std::vector<double>(hv.size(), 0.0)))) return rc;
                         GradQArgs q;
+                        q.omega2 = P->omega2;
                         q.pairs = tmp.view();
                         q.PP = P->PP.p; q.PK = P->PK.p; q.PE = P->PE.p;
                         q.table = table_ptr();
@@ -1543,6 +1839,7 @@ static int grad_build(b200jk_plan *P, const double *dms, int n_dm, int with_j, i
                         a.nbas = P->nbas; a.naoc = P->naoc; a.n_dm = n_dm;
                         a.with_j = with_j; a.with_k = with_k;
                         a.de = fused ? g.de.p : nullptr;
+                        a.omega2 = P->omega2;
                         a.shell_atom = fused ? g.shell_atom.p : nullptr;
                         std::string err;
                         if (P->profiling) CUDA_TRY(cudaEventRecord(g.cls_ev[2 * (X * NPAIRCLASS + Y)], s));
@@ -1745,8 +2042,8 @@ static int batch_build(b200jk_batch *B, const double *const *dms, int hermi, int
         const int nmol = (int)B->plans.size();
         for (int m = 0; m < nmol; m++)
                 if (!dms[m] || (with_j && !vj[m]) || (with_k && !vk[m])) return fail(B200JK_EINVAL, "NULL device pointer in the batch");
-        const double tau = B->plans[0]->fp32_tau;
-        const int mixed = precision_mode == B200JK_PREC_MIXED && tau > 0;
+        // thresholds of the first plan (per class when it has them)
+        const int mixed = precision_mode == B200JK_PREC_MIXED;
         CUDA_TRY(cudaSetDevice(B->device));
         cudaStream_t s = stream ? (cudaStream_t)stream : B->stream;
         const int nk = hermi == 1 ? 1 : 2;
@@ -1890,6 +2187,7 @@ static int batch_build(b200jk_batch *B, const double *const *dms, int hermi, int
                                 a.nbas = P->nbas; a.naoc = P->naoc; a.n_dm = 1; a.nk = nk;
                                 a.with_j = with_j; a.with_k = with_k; a.same = qcs[t].X == qcs[t].Y;
                                 a.screen = P->screen;
+                                a.omega2 = P->omega2;
                                 ha[k] = a;
                                 hs[k] = seg;
                                 k++;
@@ -1904,7 +2202,8 @@ static int batch_build(b200jk_batch *B, const double *const *dms, int hermi, int
                 int la, lb, lc, ld;
                 class_l(qcs[t].X, la, lb);
                 class_l(qcs[t].Y, lc, ld);
-                for (int pass = 0; pass < (mixed ? 2 : 1); pass++) {
+                const double tau = mixed ? class_tau(B->plans[0], t) : 0.0;
+                for (int pass = 0; pass < (tau > 0 ? 2 : 1); pass++) {
                         const int nm = ncnt[2 * t + pass];
                         if (nm == 0) continue;
                         const int variant = class_variant(B->plans[0], t, pass);
@@ -1912,7 +2211,7 @@ static int batch_build(b200jk_batch *B, const double *const *dms, int hermi, int
                         const JKArgs *dargs = B->args.p + at[2 * t + pass];
                         const int *dseg = B->segoff.p + sat[2 * t + pass];
                         const int segs = h_segoff[sat[2 * t + pass] + nm];
-                        count_kernel_multi<<<grid_for(segs, 256), 256, 0, s>>>(dargs, dseg, nm, chunk, mixed ? tau : 0.0,
+                        count_kernel_multi<<<grid_for(segs, 256), 256, 0, s>>>(dargs, dseg, nm, chunk, tau,
                                                                               pass, B->nkl.p, B->kst.p, B->nchunk.p);
                         CUDA_TRY(cudaGetLastError());
                         CUDA_TRY(cudaMemsetAsync(B->nchunk.p + segs, 0, sizeof(long long), s));
@@ -2140,6 +2439,7 @@ extern "C" int b200jk_get_jk_noalloc(b200jk_plan *P, const double *dms, int n_dm
                 a.nbas = P->nbas; a.naoc = P->naoc; a.n_dm = n_dm; a.nk = nk;
                 a.with_j = with_j; a.with_k = with_k; a.same = same;
                 a.screen = P->screen;
+                                a.omega2 = P->omega2;
                 if ((rc = dispatch_jk(P, la, lb, lc, ld, a, 0, s))) return rc;
         }
         for (int d = 0; d < n_dm; d++) {

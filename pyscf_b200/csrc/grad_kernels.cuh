@@ -141,6 +141,8 @@ struct GradArgs {
         // parent shells' atoms (shell_atom[parent shell]); one symmetric density
         double *de = nullptr;
         const int *shell_atom = nullptr;
+        // omega^2 of the long-range operator erf(omega r12)/r12, 0 = Coulomb
+        double omega2 = 0.0;
 };
 
 // Weight of one Cartesian element (ab|cd) in the two-electron force of a
@@ -217,7 +219,7 @@ __device__ __forceinline__ void grad_eval_pass(double *sm, const GradArgs &a, in
                         for (int task = gl; task < 3 * NR; task += GS) {
                                 const int r = task / 3, dir = task - 3 * r;
                                 PrimQ<double> sq;
-                                prim_setup<double>(sq, P.w, KP.y, Pv, Q.w, KQ.y, Qv, A, C, Kab * KQ.x);
+                                prim_setup<double>(sq, P.w, KP.y, Pv, Q.w, KQ.y, Qv, A, C, Kab * KQ.x, a.omega2);
                                 double ur, wr;
                                 rys_root_one<NR, double>(sq.T, table, r, ur, wr);
                                 RysCoef<double> rc;
@@ -556,7 +558,7 @@ __global__ void __launch_bounds__(128) grad_thread_kernel(GradArgs a)
                                         const double2 KQ = a.PK[pk.x + kp];
                                         const double Qv[3] = {Q.x - Ab.x, Q.y - Ab.y, Q.z - Ab.z};
                                         PrimQ<double> sq;
-                                        prim_setup<double>(sq, P.w, KP.y, Pv, Q.w, KQ.y, Qv, A0, C, Kab * KQ.x);
+                                        prim_setup<double>(sq, P.w, KP.y, Pv, Q.w, KQ.y, Qv, A0, C, Kab * KQ.x, a.omega2);
                                         double u[NR], w[NR];
                                         rys_roots_slice<NR, double>(sq.T, table, u, w);
 #pragma unroll
@@ -713,6 +715,7 @@ __global__ void __launch_bounds__(128) grad_thread_kernel(GradArgs a)
 // transforms them to the output basis and folds sqrt(max |.|) into the
 // parent-shell entries q0[A,B] (derivative on A) and q0[B,A].
 struct GradQArgs {
+        double omega2;               // as GradArgs::omega2
         PairView pairs;
         const double4 *PP;
         const double2 *PK;
@@ -741,6 +744,7 @@ __global__ void __launch_bounds__(32) grad_q0_kernel(GradQArgs q)
         a.PE = q.PE;
         a.table = q.table;
         a.goff = q.goff;
+        a.omega2 = q.omega2;
         const int4 sh = q.pairs.sh[ij];
         const int2 pr = q.pairs.pr[ij];
         const double4 Av = q.pairs.A[ij];

@@ -79,6 +79,42 @@ int launch_one(const JKArgs &a, const JKArgs *margs, const long long *mchunk, in
         return 0;
 }
 
+// variant 2 of the register family: bra runs of BR pairs (float64 pass,
+// tiled chunk order, one symmetric density; the host checks these)
+template <int LA, int LB, int LC, int LD, int BR>
+int launch_run(const JKArgs &a, cudaStream_t s, int nsm, std::string &err)
+{
+        using K = Class4<LA, LB, LC, LD>;
+        static LaunchCfg cfg;
+        static std::mutex mu;
+        {
+                std::lock_guard<std::mutex> lk(mu);
+                if (!cfg.ready) {
+                        int nb = 0;
+                        cfg.block = 128;
+                        cfg.smem = stage_table<double>(K::NR) ? sizeof(double) * rys_slice_elems<double>(K::NR) : 0;
+                        cfg.status = cudaFuncSetAttribute(jk_thread_run_kernel<LA, LB, LC, LD, BR>,
+                                                          cudaFuncAttributeMaxDynamicSharedMemorySize, (int)cfg.smem);
+                        if (cfg.status == cudaSuccess)
+                                cfg.status = cudaOccupancyMaxActiveBlocksPerMultiprocessor(
+                                        &nb, jk_thread_run_kernel<LA, LB, LC, LD, BR>, 128, cfg.smem);
+                        cfg.grid = (nb > 0 ? nb : 1) * nsm;
+                        cfg.ready = true;
+                }
+        }
+        if (cfg.status != cudaSuccess) {
+                err = std::string("kernel configuration: ") + cudaGetErrorString(cfg.status);
+                return 1;
+        }
+        jk_thread_run_kernel<LA, LB, LC, LD, BR><<<cfg.grid, cfg.block, cfg.smem, s>>>(a);
+        cudaError_t e = cudaGetLastError();
+        if (e != cudaSuccess) {
+                err = std::string("kernel launch: ") + cudaGetErrorString(e);
+                return 1;
+        }
+        return 0;
+}
+
 } // namespace
 
 // B2_FN_NAME is launch_jk_<la><lb><lc><ld>, declared in jk_launch.h
@@ -92,6 +128,16 @@ int B2_FN_NAME(const JKArgs &a, cudaStream_t s, int nsm, int fp32, int variant, 
         constexpr int GSH0 = NP > 0 ? 0 : group_size<B2_BRA_LA, B2_BRA_LB, B2_KET_LC, B2_KET_LD>() / 2;
         constexpr int GSH = (GSH0 >= 8 && sizeof(double) * WarpSmem<B2_BRA_LA, B2_BRA_LB, B2_KET_LC, B2_KET_LD>::SIZE *
                                                   (32 / (GSH0 > 0 ? GSH0 : 1)) <= 200 * 1024) ? GSH0 : 0;
+        constexpr int BRUN = NP > 0 ? bra_run<B2_BRA_LA, B2_BRA_LB, B2_KET_LC, B2_KET_LD, NP>() : 1;
+        if constexpr (BRUN > 1) {
+                if (variant == 2) {
+                        if (nmol > 0 || fp32 || !a.tiled || a.n_dm != 1 || a.nk != 1) {
+                                err = "launch variant 2 (bra runs) needs the tiled float64 pass of one symmetric density";
+                                return 1;
+                        }
+                        return launch_run<B2_BRA_LA, B2_BRA_LB, B2_KET_LC, B2_KET_LD, BRUN>(a, s, nsm, err);
+                }
+        }
 #define B2_L(R, M, KR) launch_one<B2_BRA_LA, B2_BRA_LB, B2_KET_LC, B2_KET_LD, R, M, KR>(a, margs, mchunk, nmol, s, nsm, err)
 #define B2_LG(R, M) launch_one<B2_BRA_LA, B2_BRA_LB, B2_KET_LC, B2_KET_LD, R, M, 1, GSH>(a, margs, mchunk, nmol, s, nsm, err)
         if constexpr (GSH >= 8) {

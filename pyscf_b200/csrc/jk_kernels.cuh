@@ -85,6 +85,8 @@ struct JKArgs {
         // density part of the quartet screen: 0 the s8 screen (J and K),
         // 1 its J terms only, 2 its K terms only (B200JK_SCREEN_*)
         int screen = 0;
+        // omega^2 of the long-range operator erf(omega r12)/r12, 0 = Coulomb
+        double omega2 = 0.0;
 };
 
 // Packed ket blocks: src[e] is the Cartesian matrix offset of packed entry e
@@ -160,15 +162,17 @@ __device__ __forceinline__ bool quartet_passes(const JKArgs &a, int4 sb, double 
 // bucket, so striding spreads the cost evenly.
 // Tiled chunk order: tile t gets tile_b x (the most chunks of its bra pairs)
 // chunk slots; slots past a bra pair's own chunks stay idle.
+// nslot chunk slots per ket chunk of a tile: tile_b (one bra pair per slot)
+// or tile_b / BR (bra runs of the register family's variant 2)
 static __global__ void tile_count_kernel(const int *__restrict__ nkl, int nbra, int chunk, int tile_b, int ntb,
-                                         long long *tile_cnt)
+                                         int nslot, long long *tile_cnt)
 {
         const int t = blockIdx.x * blockDim.x + threadIdx.x;
         if (t >= B2_NBUCKET * ntb) return;
         const int b = t / ntb, t0 = (t % ntb) * tile_b;
         int m = 0;
         for (int ij = t0; ij < min(nbra, t0 + tile_b); ij++) m = max(m, (nkl[ij * B2_NBUCKET + b] + chunk - 1) / chunk);
-        tile_cnt[t] = (long long)m * tile_b;
+        tile_cnt[t] = (long long)m * nslot;
 }
 
 // chunk -> (segment, chunk of the segment); false for an idle slot
@@ -311,8 +315,20 @@ __host__ __device__ constexpr int ket_run()
 // slices of the batch's chunk arrays, whose chunk numbers are global) and
 // mchunk[m] its first chunk in the batch's chunk queue, mchunk[nmol] the end;
 // a0 carries the shared fields (tables, statistics).
+// Blocks per SM the register family's kernels are compiled for (a
+// translation-unit flag, set per class by the build from measured times):
+// 0 leaves register allocation to the compiler (an explicit 1 does not: it
+// lets the allocator use far more registers); 4 caps a thread at 128
+// registers, trading a few spills for 16 resident warps instead of 12 or 8 on
+// the latency-bound classes whose blocks need more.  Float64 kernels only:
+// the float32 ones need far fewer registers, and a cap above their natural
+// count would only let them grow.
+#ifndef B2_THREAD_MINB
+#define B2_THREAD_MINB 0
+#endif
+
 template <int LA, int LB, int LC, int LD, int NP, typename R, bool MULTI, int KR>
-__global__ void __launch_bounds__(128) jk_thread_kernel(JKArgs a0, const JKArgs *__restrict__ margs,
+__global__ void __launch_bounds__(128, (sizeof(R) == 8 ? B2_THREAD_MINB : 0)) jk_thread_kernel(JKArgs a0, const JKArgs *__restrict__ margs,
                                                         const long long *__restrict__ mchunk, int nmol)
 {
         using K = Class4<LA, LB, LC, LD>;
@@ -423,7 +439,7 @@ __global__ void __launch_bounds__(128) jk_thread_kernel(JKArgs a0, const JKArgs 
                                                 const R Qv[3] = {(R)(Q.x - Ab.x), (R)(Q.y - Ab.y), (R)(Q.z - Ab.z)};
                                                 PrimQ<R> sq;
                                                 prim_setup<R>(sq, (R)P.w, (R)KP.y, Pv, (R)Q.w, (R)KQ.y, Qv, A, C,
-                                                              Kab * (R)KQ.x);
+                                                              Kab * (R)KQ.x, (R)a.omega2);
                                                 add_prim_quartet_part<LA, LB, LC, LD, PART * NGP, NGP, R>(Gp, tab, sq, AB, CD);
                                         }
                                 }
@@ -577,6 +593,234 @@ __global__ void __launch_bounds__(128) jk_thread_kernel(JKArgs a0, const JKArgs 
         }
 }
 
+// Bra-run length of the register family's launch variant 2 (1: the class
+// has none): whole blocks in registers (NP = 1) and at most 32 carried
+// doubles per lane (K[a,c], K[a,d] and the ket's J block).
+template <int LA, int LB, int LC, int LD, int NP>
+__host__ __device__ constexpr int bra_run()
+{
+        using K = Class4<LA, LB, LC, LD>;
+        return (NP == 1 && K::NA * (K::NC + K::ND) + K::NCD <= 32) ? 4 : 1;
+}
+
+// Register family, bra runs (launch variant 2, float64 pass of unsharded
+// tiled builds with one symmetric density).  A warp takes one chunk of 32
+// kets (one per lane) and the BR consecutive bra pairs of one run of its
+// tile: kets of the chunk are the same positions of the ket bucket for every
+// bra pair of the run (kst = 0 in the float64 pass), so each lane keeps its
+// ket's J block and, while consecutive bra pairs share their first segment a
+// (pairs of a bound band are ordered by first segment), its K[a,c] and
+// K[a,d] sums in registers: one atomic per run instead of one per quartet for
+// those images.  K[b,c], K[b,d] still take one atomic per quartet and J[a,b]
+// one per bra pair and warp.
+template <int LA, int LB, int LC, int LD, int BR>
+__global__ void __launch_bounds__(128, B2_THREAD_MINB) jk_thread_run_kernel(JKArgs a)
+{
+        using K = Class4<LA, LB, LC, LD>;
+        constexpr int NG = K::NG;
+        const int lane = threadIdx.x & 31;
+        extern __shared__ __align__(32) double smem_dyn[];
+        const double *tab = a.table + RysLayout<double>::offset(K::NR);
+        if constexpr (stage_table<double>(K::NR)) {
+                constexpr int NS = rys_slice_elems<double>(K::NR);
+                const RysVec4<double> *src = reinterpret_cast<const RysVec4<double> *>(tab);
+                RysVec4<double> *dst = reinterpret_cast<RysVec4<double> *>(smem_dyn);
+                for (int t = threadIdx.x; t < NS / 4; t += blockDim.x) dst[t] = src[t];
+                __syncthreads();
+                tab = reinterpret_cast<const double *>(smem_dyn);
+        }
+        const size_t n = (size_t)a.naoc;
+        const int nrun = a.tile_b / BR;   // runs per tile
+        const long long total = a.chunk_off[a.ntile];
+        const long long nwarps = ((long long)gridDim.x * blockDim.x) >> 5;
+        unsigned long long nq = 0, npq = 0;
+        for (long long chunk = ((long long)blockIdx.x * blockDim.x + threadIdx.x) >> 5; chunk < total;
+             chunk += nwarps) {
+                const int t = find_bra(a.chunk_off, a.ntile, chunk);
+                const int l = (int)(chunk - a.chunk_off[t]);
+                const int kc = l / nrun, run = l % nrun;
+                const int bucket = t / a.ntb;
+                const int ij0 = (t % a.ntb) * a.tile_b + run * BR;
+                const int pos = kc * 32 + lane;
+                const int kl = a.ket.boff[bucket] + pos;
+                const bool ket_ok = kl < a.ket.boff[bucket + 1];
+                int4 sk = make_int4(0, 0, 0, 0);
+                int2 pk = make_int2(0, 0);
+                double4 Ak = make_double4(0, 0, 0, 0), CDk = make_double4(0, 0, 0, 0);
+                double qkl = 0.0;
+                if (ket_ok) {
+                        sk = a.ket.sh[kl];
+                        pk = a.ket.pr[kl];
+                        Ak = a.ket.A[kl];
+                        CDk = a.ket.AB[kl];
+                        qkl = a.ket.q[kl];
+                }
+                const int ic = sk.x, id = sk.y;
+                double accj[K::NCD], acc_c[K::NA * K::NC], acc_d[K::NA * K::ND];
+#pragma unroll
+                for (int u = 0; u < K::NCD; u++) accj[u] = 0.0;
+                bool anyj = false, anyk = false;
+                int cur_a = -1;
+                auto flush_k = [&]() {
+                        if (!anyk) return;
+#pragma unroll
+                        for (int x = 0; x < K::NA; x++) {
+#pragma unroll
+                                for (int c = 0; c < K::NC; c++) atomicAdd(a.Kacc + (cur_a + x) * n + ic + c, acc_c[x * K::NC + c]);
+#pragma unroll
+                                for (int d = 0; d < K::ND; d++) atomicAdd(a.Kacc + (cur_a + x) * n + id + d, acc_d[x * K::ND + d]);
+                        }
+                        anyk = false;
+                };
+                for (int r = 0; r < BR; r++) {
+                        const int ij = ij0 + r;
+                        if (ij >= a.bra.n) break;
+                        const int sgi = ij * B2_NBUCKET + bucket;
+                        const int nk = a.nkl[sgi];
+                        if (kc * 32 >= nk) continue;   // warp-uniform
+                        const int4 sb = a.bra.sh[ij];
+                        const int2 pb = a.bra.pr[ij];
+                        const double qij = a.bra.q[ij];
+                        const double4 Ab = a.bra.A[ij];
+                        const double4 ABb = a.bra.AB[ij];
+                        const bool active = pos < nk && quartet_passes(a, sb, qij, sk, qkl);
+                        if (sb.x != cur_a) {   // warp-uniform: the bra pair is the warp's
+                                flush_k();
+                                cur_a = sb.x;
+#pragma unroll
+                                for (int u = 0; u < K::NA * K::NC; u++) acc_c[u] = 0.0;
+#pragma unroll
+                                for (int u = 0; u < K::NA * K::ND; u++) acc_d[u] = 0.0;
+                        }
+                        double G[NG];
+#pragma unroll
+                        for (int u = 0; u < NG; u++) G[u] = 0.0;
+                        if (active) {
+                                double fac = 1.0;
+                                if (Ab.w != 0.0) fac *= 0.5;
+                                if (Ak.w != 0.0) fac *= 0.5;
+                                if (a.same && ij == kl) fac *= 0.5;
+                                const double A0[3] = {0.0, 0.0, 0.0}, AB[3] = {ABb.x, ABb.y, ABb.z};
+                                const double C[3] = {Ak.x - Ab.x, Ak.y - Ab.y, Ak.z - Ab.z};
+                                const double CD[3] = {CDk.x, CDk.y, CDk.z};
+                                for (int ip = 0; ip < pb.y; ip++) {
+                                        const double4 P = a.PP[pb.x + ip];
+                                        const double2 KP = a.PK[pb.x + ip];
+                                        const double Kab = KP.x * fac;
+                                        const double Pv[3] = {P.x - Ab.x, P.y - Ab.y, P.z - Ab.z};
+                                        for (int kp = 0; kp < pk.y; kp++) {
+                                                const double4 Q = a.PP[pk.x + kp];
+                                                const double2 KQ = a.PK[pk.x + kp];
+                                                const double Qv[3] = {Q.x - Ab.x, Q.y - Ab.y, Q.z - Ab.z};
+                                                PrimQ<double> sq;
+                                                prim_setup<double>(sq, P.w, KP.y, Pv, Q.w, KQ.y, Qv, A0, C, Kab * KQ.x, a.omega2);
+                                                add_prim_quartet_part<LA, LB, LC, LD, 0, NG, double>(G, tab, sq, AB, CD);
+                                        }
+                                }
+                                nq++;
+                                npq += (unsigned long long)pb.y * pk.y;
+                                anyk = a.with_k != 0;
+                        }
+                        const int ia = sb.x, ib = sb.y;
+                        // J: bra block summed over the warp, ket block carried
+                        if (a.with_j) {
+                                double dcd[K::NCD];
+#pragma unroll
+                                for (int u = 0; u < K::NCD; u++)
+                                        dcd[u] = !active ? 0.0
+                                                : (a.Dpk ? __ldg(a.Dpk + (long long)kl * K::NCD + u)
+                                                         : __ldg(a.Ds + (ic + u / K::ND) * n + id + u % K::ND));
+                                if (active) {
+                                        anyj = true;
+#pragma unroll
+                                        for (int x = 0; x < K::NA; x++)
+#pragma unroll
+                                                for (int y = 0; y < K::NB; y++) {
+                                                        const double dab = __ldg(a.Ds + (ia + x) * n + ib + y);
+#pragma unroll
+                                                        for (int u = 0; u < K::NCD; u++) accj[u] += G[(x * K::NB + y) * K::NCD + u] * dab;
+                                                }
+                                }
+#pragma unroll
+                                for (int tt = 0; tt < K::NAB; tt++) {
+                                        double v = 0.0;
+#pragma unroll
+                                        for (int u = 0; u < K::NCD; u++) v += G[tt * K::NCD + u] * dcd[u];
+                                        v = warp_sum(v);
+                                        if (lane == 0 && v != 0.0) atomicAdd(a.Jacc + (ia + tt / K::NB) * n + ib + tt % K::NB, v);
+                                }
+                        }
+                        if (a.with_k && active) {
+                                const double *X = a.Dk;
+                                double *Kt = a.Kacc;
+#pragma unroll
+                                for (int x = 0; x < K::NA; x++) {
+                                        // K[a,d] += G X[b,c], K[a,c] += G X[b,d]: carried
+#pragma unroll
+                                        for (int b = 0; b < K::NB; b++) {
+#pragma unroll
+                                                for (int c = 0; c < K::NC; c++) {
+                                                        const double xbc = __ldg(X + (ib + b) * n + ic + c);
+#pragma unroll
+                                                        for (int d = 0; d < K::ND; d++)
+                                                                acc_d[x * K::ND + d] += G[((x * K::NB + b) * K::NC + c) * K::ND + d] * xbc;
+                                                }
+#pragma unroll
+                                                for (int d = 0; d < K::ND; d++) {
+                                                        const double xbd = __ldg(X + (ib + b) * n + id + d);
+#pragma unroll
+                                                        for (int c = 0; c < K::NC; c++)
+                                                                acc_c[x * K::NC + c] += G[((x * K::NB + b) * K::NC + c) * K::ND + d] * xbd;
+                                                }
+                                        }
+                                }
+                                // K[b,d] += G X[a,c], K[b,c] += G X[a,d]: one atomic per element
+#pragma unroll
+                                for (int b = 0; b < K::NB; b++) {
+#pragma unroll
+                                        for (int d = 0; d < K::ND; d++) {
+                                                double v = 0.0;
+#pragma unroll
+                                                for (int x = 0; x < K::NA; x++)
+#pragma unroll
+                                                        for (int c = 0; c < K::NC; c++)
+                                                                v += G[((x * K::NB + b) * K::NC + c) * K::ND + d] * __ldg(X + (ia + x) * n + ic + c);
+                                                atomicAdd(Kt + (ib + b) * n + id + d, v);
+                                        }
+#pragma unroll
+                                        for (int c = 0; c < K::NC; c++) {
+                                                double v = 0.0;
+#pragma unroll
+                                                for (int x = 0; x < K::NA; x++)
+#pragma unroll
+                                                        for (int d = 0; d < K::ND; d++)
+                                                                v += G[((x * K::NB + b) * K::NC + c) * K::ND + d] * __ldg(X + (ia + x) * n + id + d);
+                                                atomicAdd(Kt + (ib + b) * n + ic + c, v);
+                                        }
+                                }
+                        }
+                }
+                if (a.with_k) flush_k();
+                if (a.with_j && anyj) {
+#pragma unroll
+                        for (int u = 0; u < K::NCD; u++) {
+                                if (a.Jpk) atomicAdd(a.Jpk + (long long)kl * K::NCD + u, accj[u]);
+                                else atomicAdd(a.Jacc + (ic + u / K::ND) * n + id + u % K::ND, accj[u]);
+                        }
+                }
+        }
+        if (a.stats) {
+                for (int o = 16; o > 0; o >>= 1) {
+                        nq += __shfl_xor_sync(0xffffffffu, nq, o);
+                        npq += __shfl_xor_sync(0xffffffffu, npq, o);
+                }
+                if (lane == 0 && nq) {
+                        atomicAdd(a.stats + 0, nq);
+                        atomicAdd(a.stats + 1, npq);
+                }
+        }
+}
+
 // Parts of the register family for a class: 0 = class goes to the shared-
 // memory family.  Budget: live integrals of a part plus the three 2D slices
 // of one root.
@@ -657,10 +901,48 @@ __device__ __forceinline__ void warp_slice_to_smem(R *h, R g00, const RysCoef<R>
 // then the Cartesian block is accumulated with components spread over it.
 // `gl` is the lane index inside the group, `gmask` the group's lane mask.
 // A, C, and the P, Q read here are relative to the origin O (the bra centre)
+// Components per lane of a group of GS lanes, and whether their packed
+// 2D-integral offsets are kept in registers (loaded once per kernel; the
+// assembly then reads only the three 2D values from shared memory per
+// component and root, instead of a fourth access for the offset).
+template <int LA, int LB, int LC, int LD, int GS>
+__host__ __device__ constexpr int group_nt()
+{
+        return (Class4<LA, LB, LC, LD>::NG + GS - 1) / GS;
+}
+// packed offsets kept in registers for at most this many components a lane
+#ifndef B2_GOFF_REGS
+#define B2_GOFF_REGS 8
+#endif
+
+// (float64 kernels only: the float32 ones are register-bound already)
+template <int LA, int LB, int LC, int LD, int GS, typename R>
+__host__ __device__ constexpr bool group_goff_in_regs()
+{
+        return sizeof(R) == 8 && group_nt<LA, LB, LC, LD, GS>() <= B2_GOFF_REGS;
+}
+template <int LA, int LB, int LC, int LD, int GS, typename R>
+__host__ __device__ constexpr int group_goff_regs()
+{
+        return group_goff_in_regs<LA, LB, LC, LD, GS, R>() ? group_nt<LA, LB, LC, LD, GS>() : 1;
+}
+template <int LA, int LB, int LC, int LD, int GS, typename R>
+__device__ __forceinline__ void group_load_goff(const int *goff, int gl, int *goff_r)
+{
+        constexpr int NT = group_nt<LA, LB, LC, LD, GS>();
+        if constexpr (group_goff_in_regs<LA, LB, LC, LD, GS, R>()) {
+#pragma unroll
+                for (int i = 0; i < NT; i++) {
+                        const int t = gl + i * GS;
+                        goff_r[i] = t < Class4<LA, LB, LC, LD>::NG ? __ldg(goff + t) : 0;
+                }
+        }
+}
+
 template <int LA, int LB, int LC, int LD, int GS, typename R>
 __device__ __forceinline__ void group_eval_block(double *sm, const JKArgs &a, int2 pb, int2 pk, const double4 O,
                                                  const R A[3], const R AB[3], const R C[3], const R CD[3],
-                                                 R fac, int gl, unsigned gmask)
+                                                 R fac, int gl, unsigned gmask, const int *goff_r)
 {
         using K = Class4<LA, LB, LC, LD>;
         using S = WarpSmem<LA, LB, LC, LD, R>;
@@ -685,7 +967,7 @@ __device__ __forceinline__ void group_eval_block(double *sm, const JKArgs &a, in
                         for (int task = gl; task < NTASK; task += GS) {
                                 const int r = PER_ROOT ? task : task / 3;
                                 PrimQ<R> sq;
-                                prim_setup<R>(sq, (R)P.w, (R)KP.y, Pv, (R)Q.w, (R)KQ.y, Qv, A, C, Kab * (R)KQ.x);
+                                prim_setup<R>(sq, (R)P.w, (R)KP.y, Pv, (R)Q.w, (R)KQ.y, Qv, A, C, Kab * (R)KQ.x, (R)a.omega2);
                                 R ur, wr;
                                 rys_root_one<K::NR, R>(sq.T, table, r, ur, wr);
                                 RysCoef<R> rc;
@@ -704,14 +986,31 @@ __device__ __forceinline__ void group_eval_block(double *sm, const JKArgs &a, in
                                 }
                         }
                         __syncwarp(gmask);
-                        for (int t = gl; t < K::NG; t += GS) {
-                                const int o = __ldg(a.goff + t);
-                                const int ox = o & 1023, oy = (o >> 10) & 1023, oz = o >> 20;
-                                R v = (R)0;
+                        constexpr int NT = group_nt<LA, LB, LC, LD, GS>();
+                        if constexpr (group_goff_in_regs<LA, LB, LC, LD, GS, R>()) {
 #pragma unroll
-                                for (int r = 0; r < K::NR; r++)
-                                        v += H[r * K::SA + ox] * H[(K::NR + r) * K::SA + oy] * H[(2 * K::NR + r) * K::SA + oz];
-                                G[t] += v;
+                                for (int i = 0; i < NT; i++) {
+                                        const int t = gl + i * GS;
+                                        if (K::NG % GS == 0 || t < K::NG) {
+                                                const int o = goff_r[i];
+                                                const int ox = o & 1023, oy = (o >> 10) & 1023, oz = o >> 20;
+                                                R v = (R)0;
+#pragma unroll
+                                                for (int r = 0; r < K::NR; r++)
+                                                        v += H[r * K::SA + ox] * H[(K::NR + r) * K::SA + oy] * H[(2 * K::NR + r) * K::SA + oz];
+                                                G[t] += v;
+                                        }
+                                }
+                        } else {
+                                for (int t = gl; t < K::NG; t += GS) {
+                                        const int o = __ldg(a.goff + t);
+                                        const int ox = o & 1023, oy = (o >> 10) & 1023, oz = o >> 20;
+                                        R v = (R)0;
+#pragma unroll
+                                        for (int r = 0; r < K::NR; r++)
+                                                v += H[r * K::SA + ox] * H[(K::NR + r) * K::SA + oy] * H[(2 * K::NR + r) * K::SA + oz];
+                                        G[t] += v;
+                                }
                         }
                 }
         }
@@ -726,9 +1025,29 @@ __host__ __device__ constexpr int group_size()
         return K::NG <= 100 ? 8 : (K::NG <= 400 ? 16 : 32);
 }
 
+// Blocks per SM the shared-memory family's float64 kernels are compiled for:
+// 4 (at most 128 registers a thread) where the groups' shared memory admits 4
+// blocks of the launch's size, so that registers do not lower the residency
+// the shared memory allows; 0 (compiler's choice) otherwise and for the
+// float32 kernels.  Must agree with the
+// launch configuration in jk_classes.cu (warps per block, bytes per warp).
+template <int LA, int LB, int LC, int LD, typename R, int GS_>
+__host__ __device__ constexpr int warp_min_blocks()
+{
+        constexpr int GS = GS_ > 0 ? GS_ : group_size<LA, LB, LC, LD>();
+        constexpr long per_warp = 8L * WarpSmem<LA, LB, LC, LD, R>::SIZE * (32 / GS);
+        constexpr long wpb0 = (200L * 1024) / per_warp;
+        constexpr long wpb = wpb0 < 1 ? 1 : (wpb0 > 4 ? 4 : wpb0);
+        constexpr long by_smem = (227L * 1024) / (per_warp * wpb);
+        // float32 kernels: the compiler's choice (0, not 1, which lets the
+        // allocator take far more registers)
+        if (sizeof(R) == 4) return 0;
+        return by_smem >= 4 ? 4 : 0;
+}
+
 // GS_: lanes per quartet (0: group_size<>; the autotuner may pick half of it)
 template <int LA, int LB, int LC, int LD, typename R, bool MULTI, int GS_ = 0>
-__global__ void __launch_bounds__(128) jk_warp_kernel(JKArgs a0, int chunk_q, const JKArgs *__restrict__ margs,
+__global__ void __launch_bounds__(128, (warp_min_blocks<LA, LB, LC, LD, R, GS_>())) jk_warp_kernel(JKArgs a0, int chunk_q, const JKArgs *__restrict__ margs,
                                                       const long long *__restrict__ mchunk, int nmol)
 {
         using K = Class4<LA, LB, LC, LD>;
@@ -744,6 +1063,13 @@ __global__ void __launch_bounds__(128) jk_warp_kernel(JKArgs a0, int chunk_q, co
         const long long total = MULTI ? mchunk[nmol] : a0.chunk_off[a0.tiled ? a0.ntile : a0.bra.n * B2_NBUCKET];
         const long long nwarps = ((long long)gridDim.x * blockDim.x) >> 5;
         unsigned long long nq = 0, npq = 0;
+        // offsets of this lane's components (the same for every molecule of a batch)
+        int goff_r[group_goff_regs<LA, LB, LC, LD, GS, R>()];
+        group_load_goff<LA, LB, LC, LD, GS, R>(a0.goff, gl, goff_r);
+        // bra-side J of one density: all kets of a chunk share its bra pair, so
+        // each lane sums its J[a,b] components over the chunk and the groups
+        // of the warp combine them before one atomic per element
+        constexpr int NJB = sizeof(R) == 8 ? (K::NAB + GS - 1) / GS : 1;
         for (long long chunk = ((long long)blockIdx.x * blockDim.x + threadIdx.x) >> 5; chunk < total;
              chunk += nwarps) {
               auto body = [&](const JKArgs &a) {
@@ -763,6 +1089,16 @@ __global__ void __launch_bounds__(128) jk_warp_kernel(JKArgs a0, int chunk_q, co
                 const double4 ABb = a.bra.AB[ij];
                 const R A[3] = {(R)0, (R)0, (R)0}, AB[3] = {(R)ABb.x, (R)ABb.y, (R)ABb.z};
                 const int ia = sb.x, ib = sb.y;
+                // (float64 kernels only: the float32 ones are register-bound)
+                const bool jab_sum = sizeof(R) == 8 && a.with_j && a.n_dm == 1;
+                double jab[sizeof(R) == 8 ? NJB : 1];
+#pragma unroll
+                for (int i = 0; i < NJB; i++) jab[i] = 0.0;
+                if (jab_sum) {
+                        // the chunk's bra block of Ds, staged once
+                        double *dsab = sm + S::DSAB;
+                        for (int t = gl; t < K::NAB; t += GS) dsab[t] = __ldg(a.Ds + (ia + t / K::NB) * n + ib + t % K::NB);
+                }
                 for (int kl = kl0 + grp; kl < kl1; kl += NGRP) {
                         const int4 sk = a.ket.sh[kl];
                         if (!quartet_passes(a, sb, qij, sk, a.ket.q[kl])) continue;
@@ -775,7 +1111,7 @@ __global__ void __launch_bounds__(128) jk_warp_kernel(JKArgs a0, int chunk_q, co
                         if (a.same && ij == kl) fac *= (R)0.5;
                         const R C[3] = {(R)(Ak.x - Ab.x), (R)(Ak.y - Ab.y), (R)(Ak.z - Ab.z)};
                         const R CD[3] = {(R)CDk.x, (R)CDk.y, (R)CDk.z};
-                        group_eval_block<LA, LB, LC, LD, GS, R>(sm, a, pb, pk, Ab, A, AB, C, CD, fac, gl, gmask);
+                        group_eval_block<LA, LB, LC, LD, GS, R>(sm, a, pb, pk, Ab, A, AB, C, CD, fac, gl, gmask, goff_r);
                         if (gl == 0) {
                                 nq++;
                                 npq += (unsigned long long)pb.y * pk.y;
@@ -787,7 +1123,8 @@ __global__ void __launch_bounds__(128) jk_warp_kernel(JKArgs a0, int chunk_q, co
                                         const double *Ds = a.Ds + s * nn;
                                         double *J = a.Jacc + s * nn;
                                         double *dsab = sm + S::DSAB, *dscd = sm + S::DSCD;
-                                        for (int t = gl; t < K::NAB; t += GS) dsab[t] = __ldg(Ds + (ia + t / K::NB) * n + ib + t % K::NB);
+                                        if (!jab_sum)
+                                                for (int t = gl; t < K::NAB; t += GS) dsab[t] = __ldg(Ds + (ia + t / K::NB) * n + ib + t % K::NB);
                                         for (int t = gl; t < K::NCD; t += GS)
                                                 dscd[t] = a.Dpk ? __ldg(a.Dpk + s * a.pk_stride + (long long)kl * K::NCD + t)
                                                                 : __ldg(Ds + (ic + t / K::ND) * n + id + t % K::ND);
@@ -798,10 +1135,22 @@ __global__ void __launch_bounds__(128) jk_warp_kernel(JKArgs a0, int chunk_q, co
                                                 if (a.Jpk) atomicAdd(a.Jpk + s * a.pk_stride + (long long)kl * K::NCD + t, v);
                                                 else atomicAdd(J + (ic + t / K::ND) * n + id + t % K::ND, v);
                                         }
-                                        for (int t = gl; t < K::NAB; t += GS) {
-                                                double v = 0.0;
-                                                for (int u = 0; u < K::NCD; u++) v += (double)G[t * K::NCD + u] * dscd[u];
-                                                atomicAdd(J + (ia + t / K::NB) * n + ib + t % K::NB, v);
+                                        if (jab_sum) {
+#pragma unroll
+                                                for (int i = 0; i < NJB; i++) {
+                                                        const int t = gl + i * GS;
+                                                        if (t < K::NAB) {
+                                                                double v = 0.0;
+                                                                for (int u = 0; u < K::NCD; u++) v += (double)G[t * K::NCD + u] * dscd[u];
+                                                                jab[i] += v;
+                                                        }
+                                                }
+                                        } else {
+                                                for (int t = gl; t < K::NAB; t += GS) {
+                                                        double v = 0.0;
+                                                        for (int u = 0; u < K::NCD; u++) v += (double)G[t * K::NCD + u] * dscd[u];
+                                                        atomicAdd(J + (ia + t / K::NB) * n + ib + t % K::NB, v);
+                                                }
                                         }
                                         __syncwarp(gmask);
                                 }
@@ -857,6 +1206,15 @@ __global__ void __launch_bounds__(128) jk_warp_kernel(JKArgs a0, int chunk_q, co
                                 }
                         }
                 }
+                if (jab_sum) {
+#pragma unroll
+                        for (int i = 0; i < NJB; i++) {
+                                double v = jab[i];
+                                for (int o = GS; o < 32; o <<= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+                                const int t = gl + i * GS;
+                                if (grp == 0 && t < K::NAB && v != 0.0) atomicAdd(a.Jacc + (ia + t / K::NB) * n + ib + t % K::NB, v);
+                        }
+                }
               };
                 if constexpr (MULTI) body(margs[find_bra(mchunk, nmol, chunk)]);
                 else body(a0);
@@ -872,6 +1230,7 @@ __global__ void __launch_bounds__(128) jk_warp_kernel(JKArgs a0, int chunk_q, co
 // the diagonal to the output basis and folds sqrt(max |(ab|ab)|) into the
 // parent-shell entry (CVHFnr_int2e_q_cond, pyscf/lib/vhf/optimizer.c:408-454).
 struct QArgs {
+        double omega2;               // as JKArgs::omega2
         PairView pairs;
         const double4 *PP;
         const double2 *PK;
@@ -897,12 +1256,15 @@ __global__ void __launch_bounds__(32) qcond_kernel(QArgs q)
         a.PK = q.PK;
         a.table = q.table;
         a.goff = q.goff;
+        a.omega2 = q.omega2;
         const int4 sh = q.pairs.sh[ij];
         const int2 pr = q.pairs.pr[ij];
         const double4 Av = q.pairs.A[ij];
         const double4 ABv = q.pairs.AB[ij];
         const double A[3] = {0.0, 0.0, 0.0}, AB[3] = {ABv.x, ABv.y, ABv.z};
-        group_eval_block<LA, LB, LA, LB, 32, double>(sm, a, pr, pr, Av, A, AB, A, AB, 1.0, lane, 0xffffffffu);
+        int goff_r[group_goff_regs<LA, LB, LA, LB, 32, double>()];
+        group_load_goff<LA, LB, LA, LB, 32, double>(q.goff, lane, goff_r);
+        group_eval_block<LA, LB, LA, LB, 32, double>(sm, a, pr, pr, Av, A, AB, A, AB, 1.0, lane, 0xffffffffu, goff_r);
         const double *G = sm + S::G;
         const int nsa = q.cart ? K::NA : 2 * LA + 1, nsb = q.cart ? K::NB : 2 * LB + 1;
         const double *ca = q.c2s + LA * 100, *cb = q.c2s + LB * 100;

@@ -61,12 +61,29 @@ inline bool family_has_variant(int la, int lb, int lc, int ld)
         if (family_thread_parts(la, lb, lc, ld) > 0) return family_ket_run(la, lb, lc, ld) > 1;
         return family_half_groups(la, lb, lc, ld);
 }
+// bra pairs per run of the register family's variant 2 (host twin of
+// bra_run<>); 1 where the class has no such variant
+inline int family_bra_run(int la, int lb, int lc, int ld)
+{
+        const int np = family_thread_parts(la, lb, lc, ld);
+        const int na = ncart(la), nc = ncart(lc), nd = ncart(ld);
+        return (np == 1 && na * (nc + nd) + nc * nd <= 32) ? 4 : 1;
+}
+// launch variants of a class: 0 always, 1 (more kets per lane or half-width
+// groups) and 2 (bra runs) where the class has them
+inline bool family_has_variant_n(int la, int lb, int lc, int ld, int v)
+{
+        if (v == 0) return true;
+        if (v == 1) return family_has_variant(la, lb, lc, ld);
+        if (v == 2) return family_bra_run(la, lb, lc, ld) > 1;
+        return false;
+}
 // quartets per chunk: 32 x kets per lane in the register family (variant 0:
 // one ket per lane, 1: family_ket_run), 8 per group of the warp otherwise
 inline int family_chunk(int la, int lb, int lc, int ld, int variant = 0)
 {
         if (family_thread_parts(la, lb, lc, ld) > 0)
-                return 32 * (variant == 1 ? family_ket_run(la, lb, lc, ld) : 1);
+                return 32 * (variant == 1 ? family_ket_run(la, lb, lc, ld) : 1);   // bra runs: 32 kets too
         const int gs = family_group(la, lb, lc, ld);
         return 8 * (32 / (variant == 1 && family_half_groups(la, lb, lc, ld) ? gs / 2 : gs));   // 8 quartets per group
 }

@@ -339,13 +339,19 @@ struct PrimQ {
         R ipq;          // 1/(p+q)
         R qf0, pf0;     // q/(p+q), p/(p+q)
         R i2p, i2q;     // 1/(2p), 1/(2q)
-        R T;            // rho |PQ|^2
-        R pref;         // 2 pi^{5/2} K_ab K_cd / (p q sqrt(p+q))
+        R T;            // rho |PQ|^2 (times theta for erf-attenuated Coulomb)
+        R pref;         // 2 pi^{5/2} K_ab K_cd / (p q sqrt(p+q)) (times sqrt(theta))
+        R theta;        // 1, or omega^2 / (omega^2 + rho) for erf(omega r12)/r12
 };
 
+// omega2 > 0: the long-range operator erf(omega r12)/r12 (omega2 = omega^2).
+// Its Rys representation is the Coulomb one with the t-integral cut at
+// t^2 = theta = omega^2 / (omega^2 + rho): with t = sqrt(theta) s, the
+// quadrature is that of T' = theta T, roots t^2 = theta s_i^2, weights
+// sqrt(theta) w_i (rys_coef applies theta to the root).
 template <typename R>
 B2_HD void prim_setup(PrimQ<R> &s, R p, R i2p, const R P[3], R q, R i2q, const R Q[3], const R A[3],
-                      const R C[3], R kk)
+                      const R C[3], R kk, R omega2 = (R)0)
 {
         s.ipq = (R)1 / (p + q);
         s.qf0 = q * s.ipq;
@@ -360,6 +366,13 @@ B2_HD void prim_setup(PrimQ<R> &s, R p, R i2p, const R P[3], R q, R i2q, const R
         }
         s.T = p * s.qf0 * (s.PQ[0] * s.PQ[0] + s.PQ[1] * s.PQ[1] + s.PQ[2] * s.PQ[2]);
         s.pref = (R)34.98683665524972497 * kk * ((R)4 * i2p * i2q) * b2sqrt(s.ipq);
+        s.theta = (R)1;
+        if (omega2 > (R)0) {
+                const R rho = p * s.qf0;
+                s.theta = omega2 / (omega2 + rho);
+                s.T *= s.theta;
+                s.pref *= b2sqrt(s.theta);
+        }
 }
 
 // Root-dependent recurrence coefficients of one primitive quartet.
@@ -371,6 +384,7 @@ struct RysCoef {
 template <typename R>
 B2_HD void rys_coef(RysCoef<R> &rc, R u, const PrimQ<R> &s)
 {
+        u *= s.theta;
         const R qf = s.qf0 * u, pf = s.pf0 * u;
         rc.b00 = (R)0.5 * u * s.ipq;
         rc.b10 = s.i2p * ((R)1 - qf);

@@ -30,7 +30,7 @@ EXPORTS = (
     'b200jk_stats', 'b200jk_hostcheck_cart_quartet', 'b200jk_class_stats', 'b200jk_set_profiling',
     'b200jk_measure_fp64_peak', 'b200jk_get_jk_noalloc', 'b200jk_set_mixed_threshold',
     'b200jk_hostcheck_cart_quartet_fp32', 'b200jk_grad_jk', 'b200jk_grad_stats', 'b200jk_get_grad_q_cond',
-    'b200jk_set_shard', 'b200jk_grad_class_stats', 'b200jk_autotune', 'b200jk_get_tuning', 'b200jk_set_tuning', 'b200jk_set_tile', 'b200jk_batch_get_jk_async', 'b200jk_batch_create', 'b200jk_batch_destroy', 'b200jk_batch_get_jk', 'b200jk_batch_stats', 'b200jk_debug_fail_alloc', 'b200jk_set_prescreen', 'b200jk_grad_contract', 'b200jk_plan_update_coords',
+    'b200jk_set_shard', 'b200jk_grad_class_stats', 'b200jk_autotune', 'b200jk_get_tuning', 'b200jk_set_tuning', 'b200jk_set_tile', 'b200jk_batch_get_jk_async', 'b200jk_batch_create', 'b200jk_batch_destroy', 'b200jk_batch_get_jk', 'b200jk_batch_stats', 'b200jk_debug_fail_alloc', 'b200jk_set_prescreen', 'b200jk_grad_contract', 'b200jk_plan_update_coords', 'b200jk_set_class_thresholds', 'b200jk_get_class_thresholds', 'b200jk_autotune_mixed', 'b200jk_int1e',
 )
 
 
@@ -89,6 +89,10 @@ def load(path=LIB_PATH):
         lib.b200jk_set_prescreen.argtypes = [vp, ip]
         lib.b200jk_grad_contract.argtypes = [vp, vp, vp, ip, dp, vp]
         lib.b200jk_plan_update_coords.argtypes = [vp, vp, ip]
+        lib.b200jk_int1e.argtypes = [vp, vp, vp, ip, vp]
+        lib.b200jk_set_class_thresholds.argtypes = [vp, vp, ip]
+        lib.b200jk_get_class_thresholds.argtypes = [vp, vp, ip, ctypes.POINTER(ip)]
+        lib.b200jk_autotune_mixed.argtypes = [vp, vp, ip, dp, vp, vp]
         lib.b200jk_debug_fail_alloc.argtypes = [ip]
         lib.b200jk_grad_jk.argtypes = [vp, vp, ip, ip, ip, vp, vp, ip, dp, vp]
         lib.b200jk_grad_stats.argtypes = [vp, ctypes.POINTER(ctypes.c_int64), ctypes.POINTER(ctypes.c_int64),
@@ -231,6 +235,57 @@ class Plan:
     def set_shard(self, index, count):
         """Evaluate only bra pairs ij = index (mod count): partial J/K for one of count GPUs."""
         check(load().b200jk_set_shard(self._h, int(index), int(count)))
+
+    def int1e(self, device=False):
+        """(S, hcore): overlap and kinetic + nuclear-attraction matrices of the
+        basis (host arrays, or CUDA tensors with device=True)."""
+        if device:
+            import torch
+            dev = torch.device('cuda', self.device)
+            S = torch.empty((self.nao, self.nao), dtype=torch.float64, device=dev)
+            H = torch.empty_like(S)
+            stream = torch.cuda.current_stream(dev).cuda_stream
+            check(load().b200jk_int1e(self._h, ctypes.c_void_p(S.data_ptr()), ctypes.c_void_p(H.data_ptr()), 1,
+                                      ctypes.c_void_p(stream)))
+            return S, H
+        S = numpy.empty((self.nao, self.nao))
+        H = numpy.empty((self.nao, self.nao))
+        check(load().b200jk_int1e(self._h, _ptr(S), _ptr(H), 0, None))
+        return S, H
+
+    def class_thresholds(self):
+        """The float32 threshold of every quartet class (55) in mixed builds."""
+        out = numpy.zeros(64)
+        n = ctypes.c_int(0)
+        check(load().b200jk_get_class_thresholds(self._h, _ptr(out), 64, ctypes.byref(n)))
+        return out[:n.value].copy()
+
+    def set_class_thresholds(self, tau=None):
+        """Per-class float32 thresholds (55 values), or None for the single one."""
+        if tau is None:
+            check(load().b200jk_set_class_thresholds(self._h, None, 0))
+            return
+        t = numpy.ascontiguousarray(tau, dtype=numpy.double)
+        check(load().b200jk_set_class_thresholds(self._h, _ptr(t), t.size))
+
+    def autotune_mixed(self, dm, budget=1e-7):
+        """Pick per-class float32 thresholds for dm within an E2 error budget
+        (Eh); returns {'tau', 'dE2', 'max_dJ', 'max_dK'} of the accepted build."""
+        res = numpy.zeros(4)
+        try:
+            import torch
+            is_dev = isinstance(dm, torch.Tensor) and dm.is_cuda
+        except ImportError:
+            is_dev = False
+        if is_dev:
+            d = dm.contiguous()
+            stream = torch.cuda.current_stream(d.device).cuda_stream
+            check(load().b200jk_autotune_mixed(self._h, ctypes.c_void_p(d.data_ptr()), 1, float(budget), _ptr(res),
+                                               ctypes.c_void_p(stream)))
+        else:
+            d = numpy.ascontiguousarray(dm, dtype=numpy.double)
+            check(load().b200jk_autotune_mixed(self._h, _ptr(d), 0, float(budget), _ptr(res), None))
+        return {'tau': res[0], 'dE2': res[1], 'max_dJ': res[2], 'max_dK': res[3]}
 
     def set_mixed_threshold(self, tau):
         """tau of precision=PREC_MIXED: quartets with q_ij q_kl max|D| < tau run in float32."""

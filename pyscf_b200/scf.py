@@ -2,7 +2,8 @@
 
 ``get_jk(mol, dm, hermi, vhfopt, with_j, with_k, omega)`` mirrors
 pyscf.scf.hf.get_jk (pyscf/scf/hf.py:948-1022), including the split of a
-complex density into real and imaginary parts.
+complex density into real and imaginary parts and the range-separated
+operators of omega > 0 (erf) and omega < 0 (erfc).
 
 ``patch_pyscf()`` makes an unmodified ``scf.RHF(mol).run()`` use the GPU
 engine for every J/K build:
@@ -23,8 +24,6 @@ _saved = {}
 
 
 def get_jk(mol, dm, hermi=1, vhfopt=None, with_j=True, with_k=True, omega=None):
-    if omega:
-        raise NotImplementedError('range-separated J/K (omega != 0) is not implemented in pyscf_b200')
     dm = numpy.asarray(dm, order='C')
     dm_shape = dm.shape
     dm_dtype = dm.dtype
@@ -32,7 +31,12 @@ def get_jk(mol, dm, hermi=1, vhfopt=None, with_j=True, with_k=True, omega=None):
     if dm_dtype == numpy.complex128:
         dm = numpy.vstack((dm.real, dm.imag)).reshape(-1, nao, nao)
         hermi = 0
-    vj, vk = _vhf.direct(dm, mol._atm, mol._bas, mol._env, vhfopt, hermi, mol.cart, with_j, with_k)
+    env = mol._env
+    if omega:
+        # mol.with_range_coulomb(omega) (pyscf/scf/hf.py:1006): the operator is
+        # selected by env[PTR_RANGE_OMEGA]
+        env = _vhf._with_omega(env, omega)
+    vj, vk = _vhf.direct(dm, mol._atm, mol._bas, env, vhfopt, hermi, mol.cart, with_j, with_k)
     if dm_dtype == numpy.complex128:
         if with_j:
             vj = vj.reshape((2,) + dm_shape)

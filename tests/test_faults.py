@@ -47,13 +47,18 @@ def test_g_shell_is_unsupported(h2o):
     assert 'l > 3' in msg
 
 
-def test_range_separated_coulomb_is_unsupported(h2o):
+def test_short_range_coulomb_is_not_a_plan(h2o):
+    """env[PTR_RANGE_OMEGA] < 0 (erfc) has no plan of its own: the Python
+    layer builds it as full minus long range; the C ABI says so."""
     from pyscf_b200 import lib
     env = h2o['env'].copy()
-    env[8] = 0.3             # env[PTR_RANGE_OMEGA] (pyscf/gto/mole.py:76)
+    env[8] = -0.3            # env[PTR_RANGE_OMEGA] (pyscf/gto/mole.py:76)
     rc, msg = _create(h2o['atm'], h2o['bas'], env)
     assert rc == lib.B200JK_EUNSUPPORTED
-    assert 'omega' in msg.lower() or 'range' in msg.lower()
+    assert 'short-range' in msg
+    env[8] = float('nan')
+    rc, msg = _create(h2o['atm'], h2o['bas'], env)
+    assert rc == lib.B200JK_EINVAL
 
 
 @pytest.mark.parametrize('slot, value, text', [
@@ -101,13 +106,16 @@ def test_alloc_hook_arguments():
     assert l.b200jk_debug_fail_alloc(0) == lib.B200JK_OK
 
 
-def test_python_layer_rejects_omega_and_other_intors(h2o):
-    """_vhf.direct keeps the reference's Python-side errors: an intor other
-    than int2e and a range-separated molecule are refused before the engine
-    is reached (pyscf/scf/_vhf.py:405-464 accepts only what its drivers have)."""
+def test_python_layer_rejects_other_intors_and_screens(h2o):
+    """VHFOpt accepts what the engine implements -- the int2e Coulomb family
+    (full, long and short range through env[PTR_RANGE_OMEGA]) with the
+    reference's s8, J-only and K-only screens -- and refuses the rest before
+    any device work."""
     from pyscf_b200 import _vhf
-    dm = numpy.eye(13)
-    env = h2o['env'].copy()
-    env[8] = 0.3
-    with pytest.raises((NotImplementedError, RuntimeError, ValueError)):
-        _vhf.direct(dm, h2o['atm'], h2o['bas'], env, vhfopt=None, hermi=1)
+
+    class Mol:
+        _atm, _bas, _env, cart = h2o['atm'], h2o['bas'], h2o['env'], False
+    with pytest.raises(NotImplementedError):
+        _vhf.VHFOpt(Mol(), intor='int2e_ip1')
+    with pytest.raises(NotImplementedError):
+        _vhf.VHFOpt(Mol(), prescreen='CVHFgrad_jk_prescreen')

@@ -93,3 +93,44 @@ def test_batch_cuda_graph(b2):
         for f, j, k in zip(fs, vj, vk):
             assert abs(j.cpu().numpy() - f['vj_' + key]).max() < TOL_JK
             assert abs(k.cpu().numpy() - f['vk_' + key]).max() < TOL_JK
+
+
+def test_batch512_sample_matches_reference(b2):
+    """The 512-molecule batch workload (bench's batch line), built in one
+    batched build: 16 sampled molecules against the reference drivers' J/K of
+    the same densities (tests/golden/make_batch_jk_golden.py): rows of their
+    first three shells element-wise, PySCF fingerprints and E2."""
+    import os
+    import torch
+    from conftest import GOLDEN
+    path = os.path.join(GOLDEN, 'batch_jk_sample.npz')
+    if not os.path.exists(path):
+        pytest.skip('batch_jk_sample.npz missing (tests/golden/make_batch_jk_golden.py)')
+    g = dict(numpy.load(path))
+    f = dict(numpy.load(os.path.join(GOLDEN, 'batch_h2o_vdz512.npz')))
+    rng = numpy.random.default_rng(405)
+    plans, dms = [], []
+    for m in range(len(f['nao'])):
+        a0, a1 = f['atm_off'][m], f['atm_off'][m + 1]
+        b0, b1 = f['bas_off'][m], f['bas_off'][m + 1]
+        e0, e1 = f['env_off'][m], f['env_off'][m + 1]
+        plans.append(b2.Plan(f['atm'][a0:a1], f['bas'][b0:b1], f['env'][e0:e1], direct_scf_tol=1e-13))
+        nao, nocc = int(f['nao'][m]), 5 * int(f['nwater'][m])
+        c = rng.standard_normal((nao, nocc)) / numpy.sqrt(nao)
+        dms.append(torch.tensor(c @ c.T, device='cuda:0'))
+    batch = b2.Batch(plans)
+    vj, vk = batch.get_jk_device(dms, hermi=1)
+    torch.cuda.synchronize()
+    for m in g['sample']:
+        j = vj[m].cpu().numpy()
+        k = vk[m].cpu().numpy()
+        d = dms[m].cpu().numpy()
+        rows = g['m%03d_rows' % m]
+        assert abs(j[rows] - g['m%03d_vj_rows' % m]).max() < TOL_JK, m
+        assert abs(k[rows] - g['m%03d_vk_rows' % m]).max() < TOL_JK, m
+        e2 = 0.5 * numpy.sum(d * j) - 0.25 * numpy.sum(d * k)
+        assert abs(e2 - float(g['m%03d_e2' % m])) < 1e-9 * max(1.0, abs(e2)), m
+        fpj = float(numpy.dot(numpy.cos(numpy.arange(j.size)), j.ravel()))
+        fpk = float(numpy.dot(numpy.cos(numpy.arange(k.size)), k.ravel()))
+        assert abs(fpj - float(g['m%03d_fp_j' % m])) < 1e-8 * max(1.0, abs(fpj)), m
+        assert abs(fpk - float(g['m%03d_fp_k' % m])) < 1e-8 * max(1.0, abs(fpk)), m

@@ -180,6 +180,7 @@ def test_plan_update_coords_matches_new_plan(b2):
     f = _grad_fixture('h2o_631g')
     p = _plan(b2, f)
     p.get_jk(f['dm0'], hermi=1)
+    p.int1e()
     coords = f['coords'].copy()
     coords[1, 2] += 0.05
     env2 = grad._env_with_coords(f['atm'], f['env'], coords)
@@ -190,3 +191,70 @@ def test_plan_update_coords_matches_new_plan(b2):
     assert abs(vj1 - vj2).max() < 1e-12 and abs(vk1 - vk2).max() < 1e-12
     assert abs(p.grad_contract(f['dm0']) - q.grad_contract(f['dm0'])).max() < 1e-12
     assert abs(p.q_cond - q.q_cond).max() == 0.0
+    # one-electron integrals follow the move too
+    S1, H1 = p.int1e()
+    S2, H2 = q.int1e()
+    assert abs(S1 - S2).max() == 0.0 and abs(H1 - H2).max() == 0.0
+
+
+def _e_nuc(atm, coords):
+    z = numpy.asarray(atm)[:, 0].astype(float)
+    e = 0.0
+    for a in range(len(z)):
+        for b in range(a):
+            e += z[a] * z[b] / numpy.linalg.norm(coords[a] - coords[b])
+    return e
+
+
+def test_rhf_gradient_finite_differences_h2o16(b2):
+    """(H2O)16/cc-pVDZ (the gradient bench workload): the analytic gradient
+    (reference one-electron part + GPU two-electron part, fused) against
+    central differences (h = 1e-4 Bohr) of RHF energies computed entirely on
+    the GPU -- one-electron integrals, unscreened J/K, SCF to 1e-12 -- at
+    the 12 seeded coordinates, to 1e-7 Eh/Bohr."""
+    from pyscf_b200 import grad, rhf
+    f = _grad_fixture('h2o16_vdz')
+    p0 = b2.Plan(f['atm'], f['bas'], f['env'], direct_scf_tol=1e-13)
+    de = f['de'] - f['de_2e'] + grad.grad_2e_fused(p0, f['dm0'])
+    h = 1e-4
+    plan = b2.Plan(f['atm'], f['bas'], f['env'], direct_scf_tol=0.0)
+    nelec = int(f['nelec'])
+
+    def energy(coords):
+        plan.update_coords(grad._env_with_coords(f['atm'], f['env'], coords))
+        S, H = plan.int1e()
+        conv, e, *_ = rhf.kernel(H, S, nelec, _e_nuc(f['atm'], coords), lambda d: plan.get_jk(d, hermi=1),
+                                 conv_tol=1e-12, dm0=f['dm0'])
+        assert conv
+        return e
+    c0 = f['coords']
+    for t in f['fd_coords']:
+        cp, cm = c0.copy(), c0.copy()
+        cp[t // 3, t % 3] += h
+        cm[t // 3, t % 3] -= h
+        fd = (energy(cp) - energy(cm)) / (2 * h)
+        assert abs(fd - de.ravel()[t]) < 1e-7, (t, fd, de.ravel()[t])
+
+
+def test_autograd_two_electron_energy_h2o16(b2):
+    """The autograd Function on the (H2O)16 workload: dE2/dR through the
+    fused backward equals the reference's de_2e, and central differences of
+    its own forward (plan moved between geometries) to 1e-7."""
+    import torch
+    from pyscf_b200 import grad
+    f = _grad_fixture('h2o16_vdz')
+    coords = torch.tensor(f['coords'], dtype=torch.float64, requires_grad=True)
+    dm = torch.tensor(f['dm0'], device='cuda:0')
+    e2 = grad.two_electron_energy(coords, dm, f['atm'], f['bas'], f['env'])
+    e2.backward()
+    g = coords.grad.numpy()
+    assert abs(g - f['de_2e']).max() < TOL_DE
+    h = 1e-4
+    c0 = f['coords']
+    for t in (5, 70, 131):
+        cp, cm = c0.copy(), c0.copy()
+        cp[t // 3, t % 3] += h
+        cm[t // 3, t % 3] -= h
+        ep = grad.two_electron_energy(torch.tensor(cp), dm, f['atm'], f['bas'], f['env']).item()
+        em = grad.two_electron_energy(torch.tensor(cm), dm, f['atm'], f['bas'], f['env']).item()
+        assert abs((ep - em) / (2 * h) - g[t // 3, t % 3]) < 1e-7

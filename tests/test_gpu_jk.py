@@ -186,7 +186,7 @@ def test_autotune_keeps_results(b2):
     p = plan_for(b2, f)
     tun = p.autotune(f['dm_conv'])
     tun32 = p.tuning(b2.PREC_MIXED)
-    assert len(tun) == len(tun32) == 55 and set(tun) | set(tun32) <= {0, 1}
+    assert len(tun) == len(tun32) == 55 and set(tun) <= {0, 1, 2} and set(tun32) <= {0, 1}
     for dm, rj, rk in [(f['dm_rand'], f['vj_rand'], f['vk_rand']), (f['dm_conv'], f['vj_conv'], f['vk_conv'])]:
         vj, vk = p.get_jk(dm, hermi=1)
         assert abs(vj - rj).max() < TOL_JK
@@ -227,3 +227,37 @@ def test_set_tuning_every_variant(b2):
     vj, vk = p.get_jk(f['dm_rand'], hermi=1, precision=b2.PREC_MIXED)
     assert abs(vj - f['vj_rand']).max() < 2e-5 * abs(f['vj_rand']).max()
     assert abs(vk - f['vk_rand']).max() < 2e-5 * abs(f['vk_rand']).max()
+
+
+@pytest.mark.parametrize('name', ['h2o8_vdz', 'h2o2_vtz'])
+def test_bra_run_variant(b2, name):
+    """Variant 2 of the register family (bra runs: K[a,*] and ket-side J
+    carried across four bra pairs) on every class that has it reproduces the
+    reference J/K in FP64, in the float64 pass of mixed builds, and falls back
+    to the plain kernels for non-symmetric densities; float32 passes refuse it."""
+    f = load_fixture(name)
+    p = plan_for(b2, f)
+    two = [0] * 55
+    for t in range(55):
+        one = [0] * 55
+        one[t] = 2
+        try:
+            p.set_tuning(one)
+            two[t] = 2
+        except RuntimeError:
+            pass
+    assert sum(two) > 0
+    with pytest.raises(RuntimeError):
+        p.set_tuning(two, b2.PREC_MIXED)
+    p.set_tuning(two)
+    vj, vk = p.get_jk(f['dm_rand'], hermi=1)
+    assert abs(vj - f['vj_rand']).max() < TOL_JK
+    assert abs(vk - f['vk_rand']).max() < TOL_JK
+    vj, vk = p.get_jk(f['dm_ns'], hermi=0)
+    assert abs(vj - f['vj_ns']).max() < TOL_JK
+    assert abs(vk - f['vk_ns']).max() < TOL_JK
+    if 'dm_conv' in f:
+        p.set_mixed_threshold(1e-6)
+        vj, vk = p.get_jk(f['dm_conv'], hermi=1, precision=b2.PREC_MIXED)
+        assert abs(vj - f['vj_conv']).max() < 1e-8
+        assert abs(vk - f['vk_conv']).max() < 1e-8

@@ -116,3 +116,35 @@ def test_c20h42_mixed_scf_report(b2):
     assert max(r['max_dJ'] for r in rows) < 1e-8
     assert max(r['max_dK'] for r in rows) < 1e-8
     assert rows[-1]['fp32_fraction'] > rows[0]['fp32_fraction']
+
+
+def test_class_thresholds_and_mixed_tuner():
+    """Per-class float32 thresholds: all zero is the FP64 build; the tuner's
+    choice keeps E2 within its budget of the FP64 build and of the
+    reference's J/K."""
+    import numpy
+    from pyscf_b200 import lib
+    from conftest import load_fixture
+    if lib.device_count() == 0:
+        pytest.fail('no CUDA device visible to libb200jk')
+    f = load_fixture('h2o8_vdz')
+    p = lib.Plan(f['atm'], f['bas'], f['env'], direct_scf_tol=1e-13)
+    d = f['dm_conv']
+    p.set_class_thresholds(numpy.zeros(55))
+    vj, vk = p.get_jk(d, hermi=1, precision=lib.PREC_MIXED)
+    assert p.stats()['fp32_quartets'] == 0
+    assert abs(vj - f['vj_conv']).max() < 1e-10 and abs(vk - f['vk_conv']).max() < 1e-10
+    with pytest.raises(RuntimeError):
+        p.set_class_thresholds(numpy.zeros(54))
+    res = p.autotune_mixed(d, budget=1e-7)
+    tau = p.class_thresholds()
+    assert res['tau'] in (0.0, 1e-2, 1e-3, 1e-4, 1e-5, 1e-6, 1e-7, 1e-8)
+    assert set(numpy.unique(tau)) <= {0.0, res['tau']}
+    assert abs(res['dE2']) <= 1e-7
+    vj, vk = p.get_jk(d, hermi=1, precision=lib.PREC_MIXED)
+    e2 = 0.5 * numpy.sum(d * vj) - 0.25 * numpy.sum(d * vk)
+    e2_ref = 0.5 * numpy.sum(d * f['vj_conv']) - 0.25 * numpy.sum(d * f['vk_conv'])
+    assert abs(e2 - e2_ref) <= 2e-7
+    # back to the single threshold
+    p.set_mixed_threshold(1e-6)
+    assert (p.class_thresholds() == 1e-6).all()

@@ -103,3 +103,33 @@ def test_grad_reference_fingerprint():
     h = float(f['fd_h'])
     fd = (f['fd_energies'][:, 0] - f['fd_energies'][:, 1]) / (2 * h)
     assert abs(f['de'].ravel()[f['fd_coords']] - fd).max() < 5e-6
+
+
+def test_h2o_vdz_long_range_fingerprints():
+    # pyscf/scf/test/test_rhf.py:930-952: numpy.random.seed(1) dm (nao, nao),
+    # mf.get_j(mol, dm, omega=1.5) and mf.get_k(mol, dm, hermi=0, omega=1.5):
+    # erf(omega r12)/r12 (env[PTR_RANGE_OMEGA] = 1.5) pins the oracle's
+    # attenuated integrals
+    f = load_fixture('h2o_vdz')
+    nao = int(f['nao'])
+    numpy.random.seed(1)
+    dm = numpy.random.random((nao, nao))
+    env = f['env'].copy()
+    env[8] = 1.5
+    vj, _, _ = oracle.get_jk(dm, f['atm'], f['bas'], env, hermi=1)
+    assert abs(lib_fp(vj) - -10.015956161068031) < 1e-11
+    _, vk, _ = oracle.get_jk(dm, f['atm'], f['bas'], env, hermi=0)
+    assert abs(lib_fp(vk) - -11.399103957754445) < 1e-11
+
+
+def test_short_range_is_full_minus_long_range():
+    # erfc(w r)/r = 1/r - erf(w r)/r, element by element of the oracle's J/K
+    f = load_fixture('h2o_631g')
+    dm = f['dm_rand']
+    full = oracle.get_jk(dm, f['atm'], f['bas'], f['env'], hermi=1, screen=False)
+    e_lr, e_sr = f['env'].copy(), f['env'].copy()
+    e_lr[8], e_sr[8] = 0.3, -0.3
+    lr = oracle.get_jk(dm, f['atm'], f['bas'], e_lr, hermi=1, screen=False)
+    sr = oracle.get_jk(dm, f['atm'], f['bas'], e_sr, hermi=1, screen=False)
+    for i in range(2):
+        assert abs(lr[i] + sr[i] - full[i]).max() < 1e-12
