@@ -29,7 +29,13 @@ Besides the FP64 headline the line carries, measured in the same run:
   scf     C20H42/cc-pVDZ RHF with incremental builds, FP64 and mixed: per
           build the mixed J/K against the FP64 J/K of the same density change
           and per iteration the energy against the FP64 SCF; final energies
-          against the reference's RHF energy (tests/golden/mol_c20h42_vdz.npz).
+          against the reference's RHF energy (tests/golden/mol_c20h42_vdz.npz);
+  batch_scf  whole SCF iterations of the 512 molecules as one CUDA-graph
+          replay, and the convergence of the first 64 against the reference
+          energies of tests/golden/batch_scf_sample.npz;
+  incore  the in-core path of (H2O)8/cc-pVDZ: GPU fill of the s8 integral
+          tensor and J/K contracted from it (HBM roofline of the contraction)
+          against the direct build of the same density.
 
 --impl reference times the reference's own CPU implementation of the path
 (PySCF's CVHFnr_direct_drv compiled from the reference sources, oracle/_ref,
@@ -364,11 +370,84 @@ def batch_scf_report(local, steps):
     e1_.record(stream)
     e1_.synchronize()
     ms = e0_.elapsed_time(e1_) / steps
-    e, de = scf.run(0)
+    done = steps + 2      # the start() and capture() iterations
+    del scf
+    # convergence of the first 64 molecules (they hold the 8 with reference
+    # energies) to the reference's conv_tol, from the same core guess
+    ref = dict(numpy.load(os.path.join(GOLDEN, 'batch_scf_sample.npz')))
+    sub = batch_scf.BatchRHF(plans[:64], nelec[:64], enuc[:64])
+    sub.start()
+    sub.capture()
+    it = 2
+    while True:
+        e, de = sub.run(5)
+        it += 5
+        if (de < 1e-10).all() or it >= 60:
+            break
+    conv = {'molecules': 64, 'iterations': it, 'max_dE_last_iteration': float(de.max()),
+            'max_idempotency_error': float(sub.idem_err.max()),
+            'max_abs_E_minus_reference': float(max(abs(e[m] - er) for m, er in zip(ref['sample'], ref['e_rhf']))),
+            'reference_molecules': [int(m) for m in ref['sample']]}
     return {'workload': '512 x (H2O)n cc-pVDZ, one SCF iteration of all molecules per CUDA-graph replay '
                         '(batched J/K, Fock, CDIIS, purified density)', 'molecules': len(plans),
-            'ms_per_iteration': ms, 'replays_timed': steps, 'setup_s': setup,
-            'max_dE_last_iteration': float(de.max()), 'max_idempotency_error': float(scf.idem_err.max())}
+            'ms_per_iteration': ms, 'replays_timed': steps, 'iterations_before_timing': done - steps,
+            'setup_s': setup, 'convergence_first_64': conv}
+
+
+def incore_report(local, steps):
+    """The in-core path on the reference's CPU-runnable workload, (H2O)8/
+    cc-pVDZ (the reference's RHF.get_jk goes in core there): GPU fill of the
+    s8 tensor, then J/K builds contracted from it (tensor 1.37 GB > L2, so no
+    flush is needed), against the direct build of the same density."""
+    import torch
+    from pyscf_b200 import lib, incore
+    f = dict(numpy.load(os.path.join(GOLDEN, 'mol_h2o8_vdz.npz')))
+    dev = torch.device('cuda', local)
+    stream = torch.cuda.current_stream(dev)
+    plan = lib.Plan(f['atm'], f['bas'], f['env'], direct_scf_tol=1e-13, device=local)
+    ev = [torch.cuda.Event(enable_timing=True) for _ in range(2)]
+
+    def timed(fn, n):
+        ev[0].record(stream)
+        for _ in range(n):
+            r = fn()
+        ev[1].record(stream)
+        ev[1].synchronize()
+        return ev[0].elapsed_time(ev[1]) / n, r
+
+    t0 = time.perf_counter()
+    eri = plan.int2e_s8(device=True)
+    torch.cuda.synchronize(dev)
+    first_fill = time.perf_counter() - t0
+    del eri
+    fill_ms, eri = timed(lambda: plan.int2e_s8(device=True), 1)
+    d = torch.as_tensor(f['dm_conv'], device=dev)
+    for _ in range(3):
+        incore.incore(eri, d, hermi=1)
+    jk_ms, (vj, vk) = timed(lambda: incore.incore(eri, d, hermi=1), max(steps, 3))
+    err = max(float(abs(vj.cpu().numpy() - f['vj_conv']).max()), float(abs(vk.cpu().numpy() - f['vk_conv']).max()))
+    for _ in range(3):
+        plan.get_jk_device(d, hermi=1)
+    direct_ms, _ = timed(lambda: plan.get_jk_device(d, hermi=1), max(steps, 3))
+    nbytes = eri.numel() * 8
+    gbs = nbytes / (jk_ms * 1e-3) / 1e9
+    peak = _hbm_peak()
+    return {'workload': 'h2o8_vdz (nao 192), RHF.get_jk in-core branch: s8 tensor filled on the GPU, J/K contracted '
+                        'from it', 'tensor_bytes': nbytes, 'fill_ms': fill_ms, 'first_fill_s': first_fill,
+            'jk_ms_per_build': jk_ms, 'direct_jk_ms_per_build': direct_ms,
+            'speedup_vs_direct': direct_ms / jk_ms, 'max_abs_err_vs_reference': err,
+            'roofline': {'bound': 'hbm', 'kernel': 'incore_pass_kernel<8,true>', 'achieved': gbs, 'peak': peak,
+                         'unit': 'GB/s', 'frac': gbs / peak if peak else None,
+                         'bytes': 'the s8 tensor read once per build (8 bytes an entry)',
+                         'peak_source': 'MEASURED_PEAKS.json hbm_gbs'}}
+
+
+def _hbm_peak():
+    try:
+        with open(os.path.join(ROOT, 'MEASURED_PEAKS.json')) as fh:
+            return float(json.load(fh)['hbm_gbs'])
+    except (OSError, KeyError, ValueError):
+        return 6650.0
 
 
 def scf_report(local, tau):
@@ -551,6 +630,13 @@ def run_gpu(args):
         except Exception as e:  # the batched-SCF line must not sink the J/K measurement
             batch_scf_line = {'error': str(e)[:200]}
 
+    incore_line = None
+    if world == 1:
+        try:
+            incore_line = incore_report(local, args.steps)
+        except Exception as e:  # the in-core line must not sink the J/K measurement
+            incore_line = {'error': str(e)[:200]}
+
     # end to end through the public API, host arrays in pinned memory
     dm_host = torch.from_numpy(f['dm']).pin_memory().numpy()
     out = torch.empty((2, nao, nao), dtype=torch.float64).pin_memory().numpy()
@@ -597,6 +683,7 @@ def run_gpu(args):
             'batch': batch_line,
             'scf': scf_line,
             'batch_scf': batch_scf_line,
+            'incore': incore_line,
             'e2e': {'value': q_per_build / t_e2e, 'unit': 'shell quartets/s',
                     's_per_build': t_e2e, 'h2d_bytes_per_step': int(nao * nao * 8),
                     'd2h_bytes_per_step': int(2 * nao * nao * 8),

@@ -128,6 +128,33 @@ int b200jk_plan_dims(const b200jk_plan *plan, int *nao, int *nbas);
  * |AB|^2) >= e^-60). */
 int b200jk_int1e(b200jk_plan *plan, double *ovlp, double *hcore, int dev_ptrs, void *stream);
 
+/* The s8-packed two-electron integral tensor of the plan's basis, the array
+ * mol.intor('int2e', aosym='s8') returns (GTO2e_cart_or_sph,
+ * pyscf/lib/vhf/fill_nr_s8.c:110-138): entry (ij|kl), i >= j, k >= l, pair
+ * index ij = i(i+1)/2 + j >= kl, at ij(ij+1)/2 + kl; len must be
+ * npair(npair+1)/2 with npair = nao(nao+1)/2.  Quartets of shells with
+ * q_ij q_kl <= 1e-14 are zero, as in the reference (CVHFnr_schwarz_cond with
+ * the optimizer's default cutoff, pyscf/lib/vhf/optimizer.c:40, :71-88).
+ * eri is device memory of the plan's GPU (dev_ptr = 1) or host memory; it is
+ * overwritten.  The long-range operator of the plan (env[PTR_RANGE_OMEGA] > 0)
+ * applies. */
+int b200jk_int2e_s8(b200jk_plan *plan, double *eri, long long len, int dev_ptr, void *stream);
+
+/* J/K from a stored integral tensor: the in-core path _vhf.incore
+ * (pyscf/scf/_vhf.py:318-401, CVHFnrs8_incore_drv / CVHFnrs4_incore_drv with
+ * pyscf/lib/vhf/nr_incore.c).  eri is the s8 tensor (eri_len =
+ * npair(npair+1)/2) or the s4 matrix (eri_len = npair^2, row ij, column kl);
+ * any other length is B200JK_EINVAL ("Array shape not consistent", as the
+ * reference's RuntimeError).  dms (n_dm, nao, nao); vj, vk outputs of the same
+ * shape, overwritten: J = einsum('ijkl,ji->kl'), K = einsum('ijkl,jk->il')
+ * over the full tensor, then the reference's hermi_triu (vj always, vk for
+ * hermi != 0).  hermi = 1 (2) takes the densities to be symmetric
+ * (antisymmetric), as the reference's s2il (s1il + hermi_triu) kernels do.
+ * All arrays are device memory of `device` (dev_ptrs = 1) or host memory (the
+ * tensor is then copied to the GPU on every call).  No plan is needed. */
+int b200jk_incore_jk(const double *eri, long long eri_len, int nao, const double *dms, int n_dm, int hermi,
+                     int with_j, int with_k, double *vj, double *vk, int dev_ptrs, int device, void *stream);
+
 /* Copy q_cond (nbas x nbas, C order) to host memory. */
 int b200jk_get_q_cond(const b200jk_plan *plan, double *q_cond);
 

@@ -100,6 +100,11 @@ class ShortRangePlan:
         lj, lk = self.lr.get_jk_device(dms, hermi, with_j, with_k, precision)
         return (fj - lj if with_j else None), (fk - lk if with_k else None)
 
+    def int2e_s8(self, device=True):
+        eri = self.full.int2e_s8(device)
+        eri -= self.lr.int2e_s8(device)
+        return eri
+
     def grad_jk(self, dms, with_j=True, with_k=True, direct_scf_tol=1e-14):
         fj, fk = self.full.grad_jk(dms, with_j, with_k, direct_scf_tol)
         lj, lk = self.lr.grad_jk(dms, with_j, with_k, direct_scf_tol)

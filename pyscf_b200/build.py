@@ -6,8 +6,9 @@ The library is a plain shared object with a C ABI (include/b200jk.h); the
 Python package loads it with ctypes.  It is built next to the sources so it
 travels with the repository snapshot.  The per-class kernels are split into
 one translation unit per quartet class (jk_classes.cu compiled 55 times), the
-gradient kernels into one per bra class (grad_classes.cu, 10 times), all
-compiled in parallel.
+gradient kernels and the s8 integral fill into one per bra class
+(grad_classes.cu and fill_classes.cu, 10 times each), all compiled in
+parallel.
 """
 import os
 import subprocess
@@ -21,7 +22,8 @@ CSRC = os.path.join(HERE, 'csrc')
 OBJ = os.path.join(HERE, '_build')
 LIB = os.path.join(HERE, 'libb200jk.so')
 HEADERS = ['rys_math.cuh', 'jk_kernels.cuh', 'jk_launch.h', 'rys_table.inc', 'rys_table_f.inc',
-           'grad_kernels.cuh', 'grad_launch.h', 'int1e_kernels.cuh']
+           'grad_kernels.cuh', 'grad_launch.h', 'int1e_kernels.cuh', 'fill_kernels.cuh', 'fill_launch.h',
+           'incore_launch.h']
 ARCH = ['-gencode', 'arch=compute_100a,code=sm_100a']
 PAIR_CLASSES = [(la, lb) for la in range(4) for lb in range(la + 1)]
 QUARTET_CLASSES = [(la, lb, lc, ld) for x, (la, lb) in enumerate(PAIR_CLASSES)
@@ -37,7 +39,8 @@ def nvcc_path():
 
 def _deps():
     files = [os.path.join(CSRC, f) for f in
-             ['b200jk.cu', 'jk_classes.cu', 'jk_qcond.cu', 'grad_classes.cu', 'hostcheck.cpp'] + HEADERS]
+             ['b200jk.cu', 'jk_classes.cu', 'jk_qcond.cu', 'grad_classes.cu', 'fill_classes.cu', 'incore.cu',
+              'hostcheck.cpp'] + HEADERS]
     files.append(os.path.join(ROOT, 'include', 'b200jk.h'))
     files.append(os.path.abspath(__file__))
     return files
@@ -54,22 +57,26 @@ def up_to_date(target=LIB):
 _RYS = ['rys_math.cuh', 'rys_table.inc', 'rys_table_f.inc']
 _JK = _RYS + ['jk_kernels.cuh', 'jk_launch.h']
 _GRAD = _JK + ['grad_kernels.cuh', 'grad_launch.h']
+_FILL = _JK + ['fill_kernels.cuh', 'fill_launch.h']
 UNIT_DEPS = {
-    'b200jk.cu': _GRAD + ['int1e_kernels.cuh', '../../include/b200jk.h'],
+    'b200jk.cu': _GRAD + _FILL + ['int1e_kernels.cuh', 'incore_launch.h', '../../include/b200jk.h'],
     'jk_qcond.cu': _JK,
     'jk_classes.cu': _JK,
     'grad_classes.cu': _GRAD,
+    'fill_classes.cu': _FILL,
+    'incore.cu': ['incore_launch.h'],
     'hostcheck.cpp': _RYS + ['../../include/b200jk.h'],
 }
 
 
 def _stale(obj, src, flags_file):
-    """Whether obj must be rebuilt: missing, older than its source, one of
-    its headers or this script, or built with other flags."""
+    """Whether obj must be rebuilt: missing, older than its source or one of
+    its headers, or built with other flags (the command line, recorded next
+    to the object, stands for everything this script decides about it)."""
     if not os.path.exists(obj) or not os.path.exists(flags_file):
         return True
     t = os.path.getmtime(obj)
-    deps = [os.path.join(CSRC, src)] + [os.path.join(CSRC, h) for h in UNIT_DEPS[src]] + [os.path.abspath(__file__)]
+    deps = [os.path.join(CSRC, src)] + [os.path.join(CSRC, h) for h in UNIT_DEPS[src]]
     return any(os.path.getmtime(d) > t for d in deps)
 
 
@@ -110,6 +117,12 @@ def _units():
         o = os.path.join(OBJ, 'grad_%d%d.o' % (la, lb))
         units.append((common + ['-DB2_BRA_LA=%d' % la, '-DB2_BRA_LB=%d' % lb,
                                 os.path.join(CSRC, 'grad_classes.cu'), '-o', o], o))
+    for la, lb in PAIR_CLASSES:
+        o = os.path.join(OBJ, 'fill_%d%d.o' % (la, lb))
+        units.append((common + ['-DB2_BRA_LA=%d' % la, '-DB2_BRA_LB=%d' % lb,
+                                os.path.join(CSRC, 'fill_classes.cu'), '-o', o], o))
+    o = os.path.join(OBJ, 'incore.o')
+    units.append((common + [os.path.join(CSRC, 'incore.cu'), '-o', o], o))
     o = os.path.join(OBJ, 'hostcheck.o')
     units.append((['g++', '-O2', '-std=c++17', '-fPIC', '-I', os.path.join(ROOT, 'include'), '-I', CSRC,
                    '-c', os.path.join(CSRC, 'hostcheck.cpp'), '-o', o], o))

@@ -29,6 +29,8 @@
 #include "jk_launch.h"
 #include "grad_launch.h"
 #include "int1e_kernels.cuh"
+#include "fill_launch.h"
+#include "incore_launch.h"
 #include "../../include/b200jk.h"
 
 using namespace b200jk;
@@ -308,6 +310,21 @@ struct b200jk_plan {
         DevArr<int> i1_seg_cart;
         DevArr<double> i1_S, i1_H, i1_zero, i1_out;
         int i1_npair = -1;
+        // s8 integral fill: the pair lists of its Schwarz cutoff and the
+        // count/scan workspace (built on first use)
+        bool fill_ready = false;
+        PairClassDev fill_pc[NPAIRCLASS];
+        DevArr<double> fill_one;
+        DevArr<int> fill_nkl, fill_kst;
+        DevArr<long long> fill_nchunk, fill_chunk_off;
+        DevArr<unsigned char> fill_cub;
+        void release_fill()
+        {
+                for (auto &c : fill_pc) c.release();
+                fill_one.release(); fill_nkl.release(); fill_kst.release();
+                fill_nchunk.release(); fill_chunk_off.release(); fill_cub.release();
+                fill_ready = false;
+        }
         std::vector<double> h_qcond;
         PairClassDev pc[NPAIRCLASS];
         DevArr<double4> PP;
@@ -347,6 +364,7 @@ struct b200jk_plan {
                 D.release(); Dc.release(); Ds.release(); Jacc.release(); Kacc.release(); outJ.release(); outK.release();
                 i1_pair.release(); i1_off.release(); i1_seg.release(); i1_atoms.release(); i1_seg_cart.release();
                 i1_S.release(); i1_H.release(); i1_zero.release(); i1_out.release();
+                release_fill();
                 dmax.release(); stats.release(); nkl.release(); kst.release(); nchunk.release(); chunk_off.release(); cub_tmp.release();
                 for (auto e : cls_ev) cudaEventDestroy(e);
                 if (ev0) cudaEventDestroy(ev0);
@@ -905,6 +923,7 @@ int b200jk_plan_update_coords(b200jk_plan *P, const double *env, int env_len)
         std::swap(P->h_atoms, T->h_atoms);
         P->nuc_model_ok = T->nuc_model_ok;
         P->i1_npair = -1;              // the one-electron pair list is planned again on next use
+        P->release_fill();             // so are the integral fill's pair lists
         P->shell_pairs = T->shell_pairs;
         P->prim_pairs = T->prim_pairs;
         P->st = T->st;
@@ -2458,6 +2477,237 @@ extern "C" int b200jk_get_jk_noalloc(b200jk_plan *P, const double *dms, int n_dm
                                 P->cart, hermi, vk + (size_t)d * nn);
                         CUDA_TRY(cudaGetLastError());
                 }
+        }
+        CUDA_TRY(cudaStreamSynchronize(s));
+        return B200JK_OK;
+}
+
+// ---------------------------------------------------------------------------
+// The s8 two-electron integral tensor (mol.intor('int2e', aosym='s8'),
+// GTO2e_cart_or_sph, pyscf/lib/vhf/fill_nr_s8.c:110-138) and J/K from a
+// stored tensor (_vhf.incore, pyscf/scf/_vhf.py:318-401).
+
+typedef int (*fill_launcher_t)(int, int, const FillArgs &, cudaStream_t, int, std::string &);
+static const fill_launcher_t g_fill_launch[NPAIRCLASS] = {
+        launch_fill_00, launch_fill_10, launch_fill_11, launch_fill_20, launch_fill_21,
+        launch_fill_22, launch_fill_30, launch_fill_31, launch_fill_32, launch_fill_33};
+
+// pair lists of the fill: every pair that can pass q_ij q_kl > 1e-14 with
+// some kl (the plan's own lists drop pairs at its direct_scf_tol)
+static int ensure_fill(b200jk_plan *P)
+{
+        if (P->fill_ready) return B200JK_OK;
+        const int nbas = P->nbas;
+        double qmax = 0;
+        for (double v : P->h_qcond) qmax = std::max(qmax, v);
+        size_t maxn = 1;
+        int rc;
+        for (int X = 0; X < NPAIRCLASS; X++) {
+                std::vector<PairLite> hv;
+                std::vector<double> q;
+                for (const PairLite &p : P->all_pairs[X]) {
+                        const double v = P->h_qcond[(size_t)P->segl[p.i].parent * nbas + P->segl[p.j].parent];
+                        if (v * qmax > B2_FILL_CUTOFF) { hv.push_back(p); q.push_back(v); }
+                }
+                // bucket-major, descending bound inside a bucket (the count
+                // kernel's prefix search)
+                std::vector<size_t> idx(hv.size());
+                std::iota(idx.begin(), idx.end(), 0);
+                std::stable_sort(idx.begin(), idx.end(), [&](size_t a, size_t b) {
+                        const int ba = prim_bucket(hv[a].nprim), bb = prim_bucket(hv[b].nprim);
+                        if (ba != bb) return ba < bb;
+                        return q[a] > q[b];
+                });
+                std::vector<PairLite> h2(hv.size());
+                std::vector<double> q2(hv.size());
+                for (size_t t = 0; t < idx.size(); t++) { h2[t] = hv[idx[t]]; q2[t] = q[idx[t]]; }
+                P->fill_pc[X].release();
+                if ((rc = upload_pairs(P, P->fill_pc[X], X, h2, q2))) return rc;
+                maxn = std::max(maxn, h2.size());
+        }
+        const size_t nseg = maxn * B2_NBUCKET;
+        if ((rc = dev_upload(P->fill_one, std::vector<double>(1, 1.0))) || (rc = dev_alloc(P->fill_nkl, nseg)) ||
+            (rc = dev_alloc(P->fill_kst, nseg)) || (rc = dev_alloc(P->fill_nchunk, nseg + 1)) ||
+            (rc = dev_alloc(P->fill_chunk_off, nseg + 1)))
+                return rc;
+        size_t tmp = 0;
+        CUDA_TRY(cub::DeviceScan::ExclusiveSum(nullptr, tmp, P->fill_nchunk.p, P->fill_chunk_off.p, (int)nseg + 1));
+        if ((rc = dev_alloc(P->fill_cub, std::max<size_t>(tmp, 1)))) return rc;
+        P->fill_ready = true;
+        return B200JK_OK;
+}
+
+int b200jk_int2e_s8(b200jk_plan *P, double *eri, long long len, int dev_ptr, void *stream)
+{
+        if (!P) return fail(B200JK_EINVAL, "plan is NULL");
+        if (!eri) return fail(B200JK_EINVAL, "eri is NULL");
+        const long long npair = (long long)P->nao * (P->nao + 1) / 2;
+        const long long need = npair * (npair + 1) / 2;
+        if (len != need)
+                return fail(B200JK_EINVAL, "eri holds " + std::to_string(len) + " entries; the s8 tensor of nao = " +
+                                                   std::to_string(P->nao) + " has " + std::to_string(need));
+        CUDA_TRY(cudaSetDevice(P->device));
+        int rc;
+        if (dev_ptr && (rc = check_dev_ptr(eri, P->device, "eri"))) return rc;
+        if ((rc = ensure_fill(P))) return rc;
+        cudaStream_t s = stream ? (cudaStream_t)stream : P->stream;
+        DevArr<double> tmp;
+        double *out = eri;
+        if (!dev_ptr) {
+                if ((rc = dev_alloc(tmp, (size_t)need))) return rc;
+                out = tmp.p;
+        }
+        auto run = [&]() -> int {
+                CUDA_TRY(cudaMemsetAsync(out, 0, sizeof(double) * need, s));
+                auto qcs = quartet_classes();
+                for (size_t t = 0; t < qcs.size(); t++) {
+                        const PairClassDev &bra = P->fill_pc[qcs[t].X], &ket = P->fill_pc[qcs[t].Y];
+                        if (bra.n == 0 || ket.n == 0) continue;
+                        const int la = bra.la, lb = bra.lb, lc = ket.la, ld = ket.lb;
+                        const int same = qcs[t].X == qcs[t].Y;
+                        const int nseg = bra.n * B2_NBUCKET;
+                        const int chunk = fill_chunk(la, lb, lc, ld);
+                        count_kernel<<<grid_for(nseg, 256), 256, 0, s>>>(
+                                bra.view(), ket.view(), same, B2_FILL_CUTOFF, P->fill_one.p, chunk, 0.0, 0, 0, 1,
+                                P->fill_nkl.p, P->fill_kst.p, P->fill_nchunk.p);
+                        CUDA_TRY(cudaGetLastError());
+                        CUDA_TRY(cudaMemsetAsync(P->fill_nchunk.p + nseg, 0, sizeof(long long), s));
+                        size_t tb = P->fill_cub.n;
+                        CUDA_TRY(cub::DeviceScan::ExclusiveSum(P->fill_cub.p, tb, P->fill_nchunk.p, P->fill_chunk_off.p,
+                                                               nseg + 1, s));
+                        FillArgs f = FillArgs();
+                        JKArgs &a = f.jk;
+                        a.tiled = 0;
+                        a.bra = bra.view();
+                        a.ket = ket.view();
+                        a.PP = P->PP.p; a.PK = P->PK.p;
+                        a.chunk_off = P->fill_chunk_off.p;
+                        a.nkl = P->fill_nkl.p;
+                        a.kst = P->fill_kst.p;
+                        a.table = table_ptr();
+                        a.table_f = table_f_ptr();
+                        a.goff = P->goff_all.p + P->goff_at[t];
+                        a.tol = B2_FILL_CUTOFF;
+                        a.nbas = P->nbas; a.naoc = P->naoc; a.same = same;
+                        a.omega2 = P->omega2;
+                        f.cart_seg = P->cart_seg.p;
+                        f.seg_info = P->seg_info.p;
+                        f.c2s = P->c2s.p;
+                        f.cart = P->cart;
+                        f.eri = out;
+                        std::string err;
+                        if (g_fill_launch[qcs[t].X](lc, ld, f, s, P->nsm, err)) return fail(B200JK_ECUDA, err);
+                }
+                if (!dev_ptr) CUDA_TRY(cudaMemcpyAsync(eri, out, sizeof(double) * need, cudaMemcpyDeviceToHost, s));
+                CUDA_TRY(cudaStreamSynchronize(s));
+                return B200JK_OK;
+        };
+        rc = run();
+        tmp.release();
+        return rc;
+}
+
+// workspace of the in-core contraction, one per device (calls are serialised)
+struct IncoreWS {
+        std::mutex mu;
+        DevArr<double> A1, A2, Jp, t, Dt, eri, dms, vj, vk;
+        DevArr<int4> items;
+        std::vector<int4> h_items;
+        int items_nao = -1, items_s8 = -1;
+};
+static IncoreWS g_incore_ws[64];
+
+int b200jk_incore_jk(const double *eri, long long eri_len, int nao, const double *dms, int n_dm, int hermi,
+                     int with_j, int with_k, double *vj, double *vk, int dev_ptrs, int device, void *stream)
+{
+        if (!eri) return fail(B200JK_EINVAL, "eri is NULL");
+        if (nao <= 0) return fail(B200JK_EINVAL, "nao must be positive");
+        if (!dms || n_dm <= 0) return fail(B200JK_EINVAL, "no density matrices");
+        if (hermi < 0 || hermi > 2) return fail(B200JK_EINVAL, "hermi must be 0, 1 or 2");
+        if (with_j && !vj) return fail(B200JK_EINVAL, "vj is NULL while with_j is set");
+        if (with_k && !vk) return fail(B200JK_EINVAL, "vk is NULL while with_k is set");
+        if (device < 0 || device >= 64) return fail(B200JK_EINVAL, "device index out of range");
+        const long long npair = (long long)nao * (nao + 1) / 2;
+        int s8;
+        if (eri_len == npair * (npair + 1) / 2) s8 = 1;
+        else if (eri_len == npair * npair) s8 = 0;
+        else
+                return fail(B200JK_EINVAL, "Array shape not consistent: eri has " + std::to_string(eri_len) +
+                                                   " entries, neither the s8 (" + std::to_string(npair * (npair + 1) / 2) +
+                                                   ") nor the s4 (" + std::to_string(npair * npair) +
+                                                   ") tensor of nao = " + std::to_string(nao));
+        if (incore_block(nao) == 0) return fail(B200JK_EUNSUPPORTED, "nao too large for the in-core contraction");
+        int ndev = 0;
+        if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) {
+                cudaGetLastError();
+                return fail(B200JK_ECUDA, "no CUDA device is available");
+        }
+        if (device >= ndev) return fail(B200JK_EINVAL, "device index out of range");
+        CUDA_TRY(cudaSetDevice(device));
+        int rc;
+        if (dev_ptrs && ((rc = check_dev_ptr(eri, device, "eri")) || (rc = check_dev_ptr(dms, device, "dms")) ||
+                         (with_j && (rc = check_dev_ptr(vj, device, "vj"))) ||
+                         (with_k && (rc = check_dev_ptr(vk, device, "vk")))))
+                return rc;
+        if (!with_j && !with_k) return B200JK_OK;
+        IncoreWS &W = g_incore_ws[device];
+        std::lock_guard<std::mutex> lk(W.mu);
+        const size_t nn = (size_t)nao * nao;
+        const int twopass = s8 && hermi == 0 && with_k;
+        if ((rc = dev_alloc(W.A1, nn)) || (rc = dev_alloc(W.Jp, (size_t)npair)) || (rc = dev_alloc(W.t, (size_t)npair)) ||
+            (twopass && ((rc = dev_alloc(W.A2, nn)) || (rc = dev_alloc(W.Dt, nn)))))
+                return rc;
+        const double *E = eri, *Dd = dms;
+        double *oj = vj, *ok = vk;
+        cudaStream_t s = stream ? (cudaStream_t)stream : 0;
+        if (!dev_ptrs) {
+                if ((rc = dev_alloc(W.eri, (size_t)eri_len)) || (rc = dev_alloc(W.dms, nn * n_dm)) ||
+                    (with_j && (rc = dev_alloc(W.vj, nn * n_dm))) || (with_k && (rc = dev_alloc(W.vk, nn * n_dm))))
+                        return rc;
+                CUDA_TRY(cudaMemcpyAsync(W.eri.p, eri, sizeof(double) * eri_len, cudaMemcpyHostToDevice, s));
+                CUDA_TRY(cudaMemcpyAsync(W.dms.p, dms, sizeof(double) * nn * n_dm, cudaMemcpyHostToDevice, s));
+                E = W.eri.p; Dd = W.dms.p; oj = W.vj.p; ok = W.vk.p;
+        }
+        const int B = incore_block(nao);
+        if (W.items_nao != nao || W.items_s8 != s8) {
+                incore_items(nao, s8, B, 2048, W.h_items);
+                if ((rc = dev_upload(W.items, W.h_items))) return rc;
+                W.items_nao = nao;
+                W.items_s8 = s8;
+        }
+        std::string err;
+        for (int d = 0; d < n_dm; d++) {
+                const double *D = Dd + (size_t)d * nn;
+                CUDA_TRY(cudaMemsetAsync(W.A1.p, 0, sizeof(double) * nn, s));
+                CUDA_TRY(cudaMemsetAsync(W.Jp.p, 0, sizeof(double) * npair, s));
+                if (launch_incore_tridm(D, nao, W.t.p, s, err)) return fail(B200JK_ECUDA, err);
+                IncoreArgs a;
+                a.eri = E; a.s8 = s8; a.nao = nao; a.npair = npair;
+                a.D = D; a.t = W.t.p; a.A = W.A1.p; a.Jp = with_j ? W.Jp.p : nullptr;
+                a.items = W.items.p; a.nitems = (int)W.h_items.size();
+                // one read of the tensor gives J and the K images (a J-only
+                // call drops the images: the pass is bound by the read)
+                if (launch_incore_pass(a, s, err)) return fail(B200JK_ECUDA, err);
+                if (twopass) {
+                        // the pair-swapped images of a general density: A(D^T)^T
+                        CUDA_TRY(cudaMemsetAsync(W.A2.p, 0, sizeof(double) * nn, s));
+                        if (launch_incore_transpose(D, nao, W.Dt.p, s, err)) return fail(B200JK_ECUDA, err);
+                        IncoreArgs b = a;
+                        b.D = W.Dt.p; b.A = W.A2.p; b.Jp = nullptr;
+                        if (launch_incore_pass(b, s, err)) return fail(B200JK_ECUDA, err);
+                }
+                if (with_j && launch_incore_unpack_j(W.Jp.p, nao, oj + (size_t)d * nn, s, err))
+                        return fail(B200JK_ECUDA, err);
+                if (with_k) {
+                        const int mode = !s8 ? 3 : (hermi == 0 ? 0 : (hermi == 1 ? 1 : 2));
+                        if (launch_incore_finish_k(W.A1.p, twopass ? W.A2.p : nullptr, nao, mode, hermi,
+                                                   ok + (size_t)d * nn, s, err))
+                                return fail(B200JK_ECUDA, err);
+                }
+        }
+        if (!dev_ptrs) {
+                if (with_j) CUDA_TRY(cudaMemcpyAsync(vj, W.vj.p, sizeof(double) * nn * n_dm, cudaMemcpyDeviceToHost, s));
+                if (with_k) CUDA_TRY(cudaMemcpyAsync(vk, W.vk.p, sizeof(double) * nn * n_dm, cudaMemcpyDeviceToHost, s));
         }
         CUDA_TRY(cudaStreamSynchronize(s));
         return B200JK_OK;

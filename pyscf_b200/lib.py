@@ -31,6 +31,7 @@ EXPORTS = (
     'b200jk_measure_fp64_peak', 'b200jk_get_jk_noalloc', 'b200jk_set_mixed_threshold',
     'b200jk_hostcheck_cart_quartet_fp32', 'b200jk_grad_jk', 'b200jk_grad_stats', 'b200jk_get_grad_q_cond',
     'b200jk_set_shard', 'b200jk_grad_class_stats', 'b200jk_autotune', 'b200jk_get_tuning', 'b200jk_set_tuning', 'b200jk_set_tile', 'b200jk_batch_get_jk_async', 'b200jk_batch_create', 'b200jk_batch_destroy', 'b200jk_batch_get_jk', 'b200jk_batch_stats', 'b200jk_debug_fail_alloc', 'b200jk_set_prescreen', 'b200jk_grad_contract', 'b200jk_plan_update_coords', 'b200jk_set_class_thresholds', 'b200jk_get_class_thresholds', 'b200jk_autotune_mixed', 'b200jk_int1e',
+    'b200jk_int2e_s8', 'b200jk_incore_jk',
 )
 
 
@@ -90,6 +91,8 @@ def load(path=LIB_PATH):
         lib.b200jk_grad_contract.argtypes = [vp, vp, vp, ip, dp, vp]
         lib.b200jk_plan_update_coords.argtypes = [vp, vp, ip]
         lib.b200jk_int1e.argtypes = [vp, vp, vp, ip, vp]
+        lib.b200jk_int2e_s8.argtypes = [vp, vp, ctypes.c_longlong, ip, vp]
+        lib.b200jk_incore_jk.argtypes = [vp, ctypes.c_longlong, ip, vp, ip, ip, ip, ip, vp, vp, ip, ip, vp]
         lib.b200jk_set_class_thresholds.argtypes = [vp, vp, ip]
         lib.b200jk_get_class_thresholds.argtypes = [vp, vp, ip, ctypes.POINTER(ip)]
         lib.b200jk_autotune_mixed.argtypes = [vp, vp, ip, dp, vp, vp]
@@ -252,6 +255,23 @@ class Plan:
         H = numpy.empty((self.nao, self.nao))
         check(load().b200jk_int1e(self._h, _ptr(S), _ptr(H), 0, None))
         return S, H
+
+    def int2e_s8(self, device=True):
+        """The s8-packed ERI tensor of the basis (mol.intor('int2e',
+        aosym='s8')): a CUDA tensor of nao_pair (nao_pair + 1) / 2 doubles,
+        or a host array with device=False."""
+        npair = self.nao * (self.nao + 1) // 2
+        n = npair * (npair + 1) // 2
+        if device:
+            import torch
+            dev = torch.device('cuda', self.device)
+            eri = torch.empty(n, dtype=torch.float64, device=dev)
+            stream = torch.cuda.current_stream(dev).cuda_stream
+            check(load().b200jk_int2e_s8(self._h, ctypes.c_void_p(eri.data_ptr()), n, 1, ctypes.c_void_p(stream)))
+            return eri
+        eri = numpy.empty(n)
+        check(load().b200jk_int2e_s8(self._h, _ptr(eri), n, 0, None))
+        return eri
 
     def class_thresholds(self):
         """The float32 threshold of every quartet class (55) in mixed builds."""

@@ -14,6 +14,11 @@ engine for every J/K build:
   * ``SCF._is_mem_enough`` returns False so RHF.get_jk takes the direct branch
     instead of building the in-core ERI tensor (pyscf/scf/hf.py:2400-2414,
     2150-2152), as ``mf.max_memory = 0`` does in the reference tests.
+``patch_pyscf(incore=True)`` instead keeps the reference's in-core choice
+for small molecules and runs it on the GPU: ``RHF.get_jk`` fills the s8
+tensor once on the GPU and contracts every build from it, and
+``pyscf.scf._vhf.incore`` is rebound (dot_eri_dm looks it up at call time,
+pyscf/scf/hf.py:887-935), see pyscf_b200/incore.py.
 ``unpatch_pyscf()`` restores the originals.
 """
 import numpy
@@ -63,8 +68,9 @@ def _no_incore(self):
     return False
 
 
-def patch_pyscf():
-    """Route PySCF's direct-SCF J/K through the GPU engine (idempotent)."""
+def patch_pyscf(incore=False):
+    """Route PySCF's J/K through the GPU engine (idempotent): direct builds
+    always; with incore=True the in-core branch of RHF.get_jk on the GPU."""
     import pyscf.scf._vhf as ref_vhf
     import pyscf.scf.hf as ref_hf
     if _saved:
@@ -75,6 +81,12 @@ def patch_pyscf():
     ref_vhf.direct = _vhf.direct
     ref_hf.SCF.init_direct_scf = _init_direct_scf
     ref_hf.SCF._is_mem_enough = _no_incore
+    if incore:
+        from . import incore as gpu_incore
+        _saved['incore'] = ref_vhf.incore
+        _saved['rhf_get_jk'] = ref_hf.RHF.get_jk
+        ref_vhf.incore = gpu_incore.incore
+        ref_hf.RHF.get_jk = gpu_incore.rhf_get_jk
 
 
 def unpatch_pyscf():
@@ -85,3 +97,6 @@ def unpatch_pyscf():
     ref_vhf.direct = _saved.pop('direct')
     ref_hf.SCF.init_direct_scf = _saved.pop('init_direct_scf')
     ref_hf.SCF._is_mem_enough = _saved.pop('_is_mem_enough')
+    if 'incore' in _saved:
+        ref_vhf.incore = _saved.pop('incore')
+        ref_hf.RHF.get_jk = _saved.pop('rhf_get_jk')

@@ -119,3 +119,25 @@ def test_python_layer_rejects_other_intors_and_screens(h2o):
         _vhf.VHFOpt(Mol(), intor='int2e_ip1')
     with pytest.raises(NotImplementedError):
         _vhf.VHFOpt(Mol(), prescreen='CVHFgrad_jk_prescreen')
+
+
+def test_incore_shape_checks_before_any_device_work():
+    """_vhf.incore raises RuntimeError when the tensor fits neither symmetry
+    (pyscf/scf/_vhf.py:397-399); the C ABI returns EINVAL with the same text
+    before it looks for a GPU."""
+    from pyscf_b200 import lib, incore
+    l = lib.load()
+    nao = 4
+    dm = numpy.eye(nao)
+    out = numpy.empty((nao, nao))
+    bad = numpy.zeros(7)
+    rc = l.b200jk_incore_jk(lib._ptr(bad), bad.size, nao, lib._ptr(dm), 1, 1, 1, 1, lib._ptr(out), lib._ptr(out),
+                            0, 0, None)
+    assert rc == lib.B200JK_EINVAL
+    assert 'Array shape not consistent' in l.b200jk_last_error().decode()
+    with pytest.raises(RuntimeError, match='Array shape not consistent'):
+        incore.incore(bad, dm, hermi=1)
+    rc = l.b200jk_incore_jk(lib._ptr(bad), bad.size, nao, lib._ptr(dm), 1, 3, 1, 1, lib._ptr(out), lib._ptr(out),
+                            0, 0, None)
+    assert rc == lib.B200JK_EINVAL
+    assert incore.incore(bad, dm, with_j=False, with_k=False) == (None, None)
