@@ -229,23 +229,31 @@ def _timed_builds(plan, d, flush, stream, steps, dist, build):
     return times, dict(quartets=nq, prim_quartets=npq, fp32_quartets=nq32, kernel_launches=launches), out
 
 
-def batch_report(local, flush, stream, steps, tau):
-    """Batched J/K of the 512-molecule workload vs one-by-one builds."""
+def batch_report(local, flush, stream, steps, tau, dist=None):
+    """Batched J/K of the 512-molecule workload vs one-by-one builds.  With
+    several ranks each GPU takes whole molecules (pyscf_b200.dist.
+    shard_molecules, no collective on the data path) and only the batched
+    FP64 build is timed; the caller combines the ranks' numbers."""
     import torch
     from pyscf_b200 import lib
+    from pyscf_b200 import dist as b2dist
     f = dict(numpy.load(os.path.join(GOLDEN, 'batch_h2o_vdz512.npz')))
     dev = torch.device('cuda', local)
+    nmol = len(f['nao'])
+    mine = set(b2dist.my_molecules(list(numpy.diff(f['bas_off'])))) if dist is not None else set(range(nmol))
     plans, dms = [], []
     rng = numpy.random.default_rng(405)
-    for m in range(len(f['nao'])):
+    for m in range(nmol):
+        nao, nocc = int(f['nao'][m]), 5 * int(f['nwater'][m])
+        c = rng.standard_normal((nao, nocc)) / numpy.sqrt(nao)
+        if m not in mine:
+            continue
         a0, a1 = f['atm_off'][m], f['atm_off'][m + 1]
         b0, b1 = f['bas_off'][m], f['bas_off'][m + 1]
         e0, e1 = f['env_off'][m], f['env_off'][m + 1]
         p = lib.Plan(f['atm'][a0:a1], f['bas'][b0:b1], f['env'][e0:e1], direct_scf_tol=1e-13, device=local)
         p.set_mixed_threshold(tau)
         plans.append(p)
-        nao, nocc = int(f['nao'][m]), 5 * int(f['nwater'][m])
-        c = rng.standard_normal((nao, nocc)) / numpy.sqrt(nao)
         dms.append(torch.tensor(c @ c.T, device=dev))
     batch = lib.Batch(plans)
 
@@ -266,6 +274,9 @@ def batch_report(local, flush, stream, steps, tau):
     ms_b64 = timed(lambda: batch.get_jk_device(dms, hermi=1), steps)
     q = batch.stats()['quartets']
     launches = batch.stats()['kernel_launches']
+    if dist is not None:
+        # this rank's numbers; the caller combines them over the ranks
+        return {'batched_fp64_ms': ms_b64, 'quartets_per_build': q}
     ms_b32 = timed(lambda: batch.get_jk_device(dms, hermi=1, precision=lib.PREC_MIXED), steps)
     f32 = batch.stats()['fp32_quartets'] / max(1, batch.stats()['quartets'])
 
@@ -615,6 +626,22 @@ def run_gpu(args):
             batch_line = batch_report(local, flush, stream, args.steps, args.tau)
         except Exception as e:  # the batch line must not sink the J/K measurement
             batch_line = {'error': str(e)[:200]}
+    else:
+        # whole molecules per GPU; every rank takes part in the two
+        # reductions whatever its local outcome
+        try:
+            part = batch_report(local, flush, stream, args.steps, args.tau, dist=dist)
+        except Exception as e:  # the batch line must not sink the J/K measurement
+            part = {'batched_fp64_ms': float('nan'), 'quartets_per_build': 0, 'error': str(e)[:200]}
+        ms_b = _max_over_ranks(part['batched_fp64_ms'], dist, dev)
+        q_b = _sum_over_ranks(part['quartets_per_build'], dist, dev)
+        batch_line = {'workload': '512 x (H2O)n, n ~ U{1..16} (seed 404), 3x3x2 lattice sites, cc-pVDZ',
+                      'sharding': 'whole molecules per GPU (longest processing time first), no data-path '
+                                  'collective', 'n_gpus': world, 'quartets_per_build': q_b,
+                      'batched_fp64_ms_max_over_ranks': ms_b,
+                      'batched_fp64_quartets_per_s': q_b / (ms_b * 1e-3) if ms_b == ms_b and ms_b > 0 else None}
+        if 'error' in part:
+            batch_line['error_rank%d' % rank] = part['error']
 
     scf_line = None
     if world == 1:

@@ -128,6 +128,19 @@ int b200jk_plan_dims(const b200jk_plan *plan, int *nao, int *nbas);
  * |AB|^2) >= e^-60). */
 int b200jk_int1e(b200jk_plan *plan, double *ovlp, double *hcore, int dev_ptrs, void *stream);
 
+/* One-electron part of the RHF nuclear gradient, contracted on the GPU:
+ * de[natm][3] (overwritten) = the hcore and overlap lines of grad_elec
+ * (pyscf/grad/rhf.py:57-66),
+ *   de[k] = einsum('xij,ij->x', hcore_deriv(k), dm)
+ *         - 2 einsum('xij,ij->x', s1[:, p0:p1], dme[p0:p1]),
+ * hcore_deriv the int1e_ipkin + int1e_ipnuc + int1e_iprinv derivatives of
+ * hcore_generator (:121-143) and s1 = -int1e_ipovlp (:145-146).  dm and dme
+ * (the energy-weighted density, make_rdm1e) are symmetric (nao, nao); the
+ * nuclear repulsion term (grad_nuc) and the two-electron term
+ * (b200jk_grad_contract) are separate.  Host or device memory as dev_ptrs.
+ * Point or fractional charges only (as b200jk_int1e). */
+int b200jk_grad_int1e(b200jk_plan *plan, const double *dm, const double *dme, double *de, int dev_ptrs, void *stream);
+
 /* The s8-packed two-electron integral tensor of the plan's basis, the array
  * mol.intor('int2e', aosym='s8') returns (GTO2e_cart_or_sph,
  * pyscf/lib/vhf/fill_nr_s8.c:110-138): entry (ij|kl), i >= j, k >= l, pair

@@ -307,8 +307,8 @@ struct b200jk_plan {
         DevArr<int4> i1_pair;
         DevArr<long long> i1_off;
         DevArr<double4> i1_seg, i1_atoms;
-        DevArr<int> i1_seg_cart;
-        DevArr<double> i1_S, i1_H, i1_zero, i1_out;
+        DevArr<int> i1_seg_cart, i1_seg_atom;
+        DevArr<double> i1_S, i1_H, i1_zero, i1_out, i1_de;
         int i1_npair = -1;
         // s8 integral fill: the pair lists of its Schwarz cutoff and the
         // count/scan workspace (built on first use)
@@ -363,6 +363,7 @@ struct b200jk_plan {
                 cart_seg.release(); cart_comp.release(); ao_loc_d.release();
                 D.release(); Dc.release(); Ds.release(); Jacc.release(); Kacc.release(); outJ.release(); outK.release();
                 i1_pair.release(); i1_off.release(); i1_seg.release(); i1_atoms.release(); i1_seg_cart.release();
+                i1_seg_atom.release(); i1_de.release();
                 i1_S.release(); i1_H.release(); i1_zero.release(); i1_out.release();
                 release_fill();
                 dmax.release(); stats.release(); nkl.release(); kst.release(); nchunk.release(); chunk_off.release(); cub_tmp.release();
@@ -933,6 +934,38 @@ int b200jk_plan_update_coords(b200jk_plan *P, const double *env, int env_len)
         return B200JK_OK;
 }
 
+// the one-electron pair list: every segment pair with a primitive pair (no
+// Schwarz screening), element offsets, segments and atoms on the device
+static int ensure_i1(b200jk_plan *P)
+{
+        if (P->i1_npair >= 0) return B200JK_OK;
+        const size_t nc = (size_t)P->naoc * P->naoc, nn = (size_t)P->nao * P->nao;
+        int rc;
+        std::vector<int4> hp;
+        std::vector<long long> off(1, 0);
+        for (int X = 0; X < NPAIRCLASS; X++)
+                for (const PairLite &q : P->all_pairs[X]) {
+                        hp.push_back(make_int4(q.i, q.j, q.prim0, q.nprim));
+                        off.push_back(off.back() + (long long)ncart(P->segl[q.i].l) * ncart(P->segl[q.j].l));
+                }
+        std::vector<double4> hs(P->segl.size());
+        std::vector<int> hc(P->segl.size()), ha(P->segl.size());
+        for (size_t t = 0; t < P->segl.size(); t++) {
+                hs[t] = make_double4(P->segl[t].R[0], P->segl[t].R[1], P->segl[t].R[2], (double)P->segl[t].l);
+                hc[t] = P->segl[t].cart_off;
+                ha[t] = P->shell_atom[P->segl[t].parent];
+        }
+        if ((rc = dev_upload(P->i1_pair, hp)) || (rc = dev_upload(P->i1_off, off)) || (rc = dev_upload(P->i1_seg, hs)) ||
+            (rc = dev_upload(P->i1_seg_cart, hc)) || (rc = dev_upload(P->i1_seg_atom, ha)) ||
+            (rc = dev_upload(P->i1_atoms, P->h_atoms)) ||
+            (rc = dev_alloc(P->i1_S, nc)) || (rc = dev_alloc(P->i1_H, nc)) || (rc = dev_alloc(P->i1_zero, nc)) ||
+            (rc = dev_alloc(P->i1_out, 2 * nn)))
+                return rc;
+        CUDA_TRY(cudaMemset(P->i1_zero.p, 0, sizeof(double) * nc));
+        P->i1_npair = (int)hp.size();
+        return B200JK_OK;
+}
+
 int b200jk_int1e(b200jk_plan *P, double *ovlp, double *hcore, int dev_ptrs, void *stream)
 {
         if (!P) return fail(B200JK_EINVAL, "plan is NULL");
@@ -946,29 +979,7 @@ int b200jk_int1e(b200jk_plan *P, double *ovlp, double *hcore, int dev_ptrs, void
                          (hcore && (rc = check_dev_ptr(hcore, P->device, "hcore")))))
                 return rc;
         const size_t nc = (size_t)P->naoc * P->naoc, nn = (size_t)P->nao * P->nao;
-        if (P->i1_npair < 0) {
-                // every segment pair with a primitive pair (no Schwarz screening here)
-                std::vector<int4> hp;
-                std::vector<long long> off(1, 0);
-                for (int X = 0; X < NPAIRCLASS; X++)
-                        for (const PairLite &q : P->all_pairs[X]) {
-                                hp.push_back(make_int4(q.i, q.j, q.prim0, q.nprim));
-                                off.push_back(off.back() + (long long)ncart(P->segl[q.i].l) * ncart(P->segl[q.j].l));
-                        }
-                std::vector<double4> hs(P->segl.size());
-                std::vector<int> hc(P->segl.size());
-                for (size_t t = 0; t < P->segl.size(); t++) {
-                        hs[t] = make_double4(P->segl[t].R[0], P->segl[t].R[1], P->segl[t].R[2], (double)P->segl[t].l);
-                        hc[t] = P->segl[t].cart_off;
-                }
-                if ((rc = dev_upload(P->i1_pair, hp)) || (rc = dev_upload(P->i1_off, off)) || (rc = dev_upload(P->i1_seg, hs)) ||
-                    (rc = dev_upload(P->i1_seg_cart, hc)) || (rc = dev_upload(P->i1_atoms, P->h_atoms)) ||
-                    (rc = dev_alloc(P->i1_S, nc)) || (rc = dev_alloc(P->i1_H, nc)) || (rc = dev_alloc(P->i1_zero, nc)) ||
-                    (rc = dev_alloc(P->i1_out, 2 * nn)))
-                        return rc;
-                CUDA_TRY(cudaMemset(P->i1_zero.p, 0, sizeof(double) * nc));
-                P->i1_npair = (int)hp.size();
-        }
+        if ((rc = ensure_i1(P))) return rc;
         cudaStream_t s = stream ? (cudaStream_t)stream : P->stream;
         CUDA_TRY(cudaMemsetAsync(P->i1_S.p, 0, sizeof(double) * nc, s));
         CUDA_TRY(cudaMemsetAsync(P->i1_H.p, 0, sizeof(double) * nc, s));
@@ -1002,6 +1013,63 @@ int b200jk_int1e(b200jk_plan *P, double *ovlp, double *hcore, int dev_ptrs, void
                 if (ovlp) CUDA_TRY(cudaMemcpyAsync(ovlp, os, sizeof(double) * nn, cudaMemcpyDeviceToHost, s));
                 if (hcore) CUDA_TRY(cudaMemcpyAsync(hcore, oh, sizeof(double) * nn, cudaMemcpyDeviceToHost, s));
         }
+        CUDA_TRY(cudaStreamSynchronize(s));
+        return B200JK_OK;
+}
+
+int b200jk_grad_int1e(b200jk_plan *P, const double *dm, const double *dme, double *de, int dev_ptrs, void *stream)
+{
+        if (!P) return fail(B200JK_EINVAL, "plan is NULL");
+        if (!dm || !dme || !de) return fail(B200JK_EINVAL, "NULL argument");
+        if (!P->nuc_model_ok)
+                return fail(B200JK_EUNSUPPORTED, "finite-nucleus models and ECP atoms are not implemented in the "
+                                                 "nuclear-attraction integrals");
+        CUDA_TRY(cudaSetDevice(P->device));
+        int rc;
+        if (dev_ptrs && ((rc = check_dev_ptr(dm, P->device, "dm")) || (rc = check_dev_ptr(dme, P->device, "dme")) ||
+                         (rc = check_dev_ptr(de, P->device, "de"))))
+                return rc;
+        if ((rc = ensure_i1(P))) return rc;
+        const size_t nn = (size_t)P->nao * P->nao;
+        const int natm = (int)P->h_atoms.size();
+        if ((rc = dev_alloc(P->i1_de, 3 * (size_t)natm))) return rc;
+        cudaStream_t s = stream ? (cudaStream_t)stream : P->stream;
+        // the Cartesian D and W live in the overlap/hcore scratch
+        const double *dD = dm, *dW = dme;
+        if (!dev_ptrs) {
+                CUDA_TRY(cudaMemcpyAsync(P->i1_out.p, dm, sizeof(double) * nn, cudaMemcpyHostToDevice, s));
+                CUDA_TRY(cudaMemcpyAsync(P->i1_out.p + nn, dme, sizeof(double) * nn, cudaMemcpyHostToDevice, s));
+                dD = P->i1_out.p;
+                dW = P->i1_out.p + nn;
+        }
+        const long long nc = (long long)P->naoc * P->naoc;
+        out_to_cart_kernel<<<grid_for(nc, 256), 256, 0, s>>>(dD, P->nao, P->naoc, P->cart_seg.p, P->cart_comp.p,
+                                                             P->seg_info.p, P->c2s.p, P->cart, P->i1_S.p, nullptr, nullptr);
+        CUDA_TRY(cudaGetLastError());
+        out_to_cart_kernel<<<grid_for(nc, 256), 256, 0, s>>>(dW, P->nao, P->naoc, P->cart_seg.p, P->cart_comp.p,
+                                                             P->seg_info.p, P->c2s.p, P->cart, P->i1_H.p, nullptr, nullptr);
+        CUDA_TRY(cudaGetLastError());
+        double *out = dev_ptrs ? de : P->i1_de.p;
+        CUDA_TRY(cudaMemsetAsync(out, 0, sizeof(double) * 3 * natm, s));
+        long long nelem = 0;
+        CUDA_TRY(cudaMemcpy(&nelem, P->i1_off.p + P->i1_npair, sizeof(long long), cudaMemcpyDeviceToHost));
+        if (nelem > 0) {
+                Int1eGradArgs ga;
+                Int1eArgs &a = ga.g;
+                a.pair = P->i1_pair.p; a.elem_off = P->i1_off.p; a.npair = P->i1_npair;
+                a.seg = P->i1_seg.p; a.seg_cart = P->i1_seg_cart.p;
+                a.PP = P->PP.p; a.PK = P->PK.p; a.PE = P->PE.p;
+                a.atoms = P->i1_atoms.p; a.natm = natm; a.naoc = P->naoc;
+                a.table = table_ptr();
+                a.S = nullptr; a.H = nullptr;
+                ga.seg_atom = P->i1_seg_atom.p;
+                ga.D = P->i1_S.p;
+                ga.W = P->i1_H.p;
+                ga.de = out;
+                int1e_grad_kernel<<<grid_for(nelem, 128), 128, 0, s>>>(ga);
+                CUDA_TRY(cudaGetLastError());
+        }
+        if (!dev_ptrs) CUDA_TRY(cudaMemcpyAsync(de, out, sizeof(double) * 3 * natm, cudaMemcpyDeviceToHost, s));
         CUDA_TRY(cudaStreamSynchronize(s));
         return B200JK_OK;
 }

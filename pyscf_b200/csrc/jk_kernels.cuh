@@ -949,7 +949,9 @@ __device__ __forceinline__ void group_eval_block(double *sm, const JKArgs &a, in
         R *G = reinterpret_cast<R *>(sm) + S::G;
         R *H = reinterpret_cast<R *>(sm) + S::H;
         const R *table = table_of<R>(a) + RysLayout<R>::offset(K::NR);
-        for (int t = gl; t < K::NG; t += GS) G[t] = (R)0;
+        // the first primitive quartet stores the block, later ones add to it
+        // (every pair has at least one primitive pair)
+        bool first = true;
         for (int ip = 0; ip < pb.y; ip++) {
                 const double4 P = a.PP[pb.x + ip];
                 const double2 KP = a.PK[pb.x + ip];
@@ -998,7 +1000,7 @@ __device__ __forceinline__ void group_eval_block(double *sm, const JKArgs &a, in
 #pragma unroll
                                                 for (int r = 0; r < K::NR; r++)
                                                         v += H[r * K::SA + ox] * H[(K::NR + r) * K::SA + oy] * H[(2 * K::NR + r) * K::SA + oz];
-                                                G[t] += v;
+                                                G[t] = first ? v : G[t] + v;
                                         }
                                 }
                         } else {
@@ -1009,9 +1011,10 @@ __device__ __forceinline__ void group_eval_block(double *sm, const JKArgs &a, in
 #pragma unroll
                                         for (int r = 0; r < K::NR; r++)
                                                 v += H[r * K::SA + ox] * H[(K::NR + r) * K::SA + oy] * H[(2 * K::NR + r) * K::SA + oz];
-                                        G[t] += v;
+                                        G[t] = first ? v : G[t] + v;
                                 }
                         }
+                        first = false;
                 }
         }
         __syncwarp(gmask);

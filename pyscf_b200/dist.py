@@ -50,3 +50,37 @@ def grad_jk(plan, dm, with_j=True, with_k=True, direct_scf_tol=1e-14, group=None
     shard_plan(plan, group)
     vj, vk = plan.grad_jk_device(dm, with_j=with_j, with_k=with_k, direct_scf_tol=direct_scf_tol)
     return reduce_jk(vj, vk, group)
+
+
+# ---------------------------------------------------------------------------
+# Batches of molecules: whole molecules per GPU, no collective on the data path.
+
+def molecule_cost(nbas):
+    """Work estimate of one molecule's J/K build: its s8 shell quartets before
+    screening, P(P+1)/2 with P = nbas(nbas+1)/2 shell pairs."""
+    p = nbas * (nbas + 1) // 2
+    return p * (p + 1) // 2
+
+
+def shard_molecules(costs, world):
+    """Partition of a batch over `world` GPUs: longest processing time first
+    (each molecule, largest cost first, to the least loaded rank; ties to the
+    lowest rank).  Returns one sorted index list per rank; deterministic, so
+    every rank computes the same partition without communicating."""
+    import heapq
+    order = sorted(range(len(costs)), key=lambda m: (-costs[m], m))
+    heap = [(0, r) for r in range(world)]
+    heapq.heapify(heap)
+    parts = [[] for _ in range(world)]
+    for m in order:
+        load, r = heapq.heappop(heap)
+        parts[r].append(m)
+        heapq.heappush(heap, (load + costs[m], r))
+    return [sorted(p) for p in parts]
+
+
+def my_molecules(nbas_list, group=None):
+    """This rank's molecules of a batch (indices into nbas_list)."""
+    import torch.distributed as dist
+    rank, world = dist.get_rank(group), dist.get_world_size(group)
+    return shard_molecules([molecule_cost(n) for n in nbas_list], world)[rank]

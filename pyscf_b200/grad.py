@@ -167,7 +167,66 @@ def _torch_function():
                 g_dm = grad_out.to(veff.device) * veff
             return g_coords, g_dm, None, None, None, None
 
-    return TwoElectronEnergy
+    class RHFEnergy(torch.autograd.Function):
+        """E(R) = tr(D h(R)) + 1/2 tr(D J[D]) - 1/4 tr(D K[D]) + E_nuc(R) for a
+        symmetric AO density D at nuclear coordinates R (Bohr, (natm, 3)),
+        with the gradient of the SCF energy: the backward pass is the
+        derivative of the Lagrangian E - tr(W (S(R) - S)) at fixed D and the
+        energy-weighted density W, i.e. grad_elec + grad_nuc
+        (pyscf/grad/rhf.py:33-76, 86-107) when D and W are the converged ones
+        (W = 2 C_occ e_occ C_occ^T, or 1/2 D F D).  Everything runs on the GPU:
+        int1e and J/K forward, b200jk_grad_int1e + b200jk_grad_contract
+        backward.  Usage:
+            E = RHFEnergy.apply(coords, dm, dme, atm, bas, env, cart)
+        """
+
+        @staticmethod
+        def forward(ctx, coords, dm, dme, atm, bas, env, cart=False):
+            c = coords.detach().cpu().numpy().astype(numpy.double)
+            env2 = _env_with_coords(atm, env, c)
+            plan = _ad_plan(atm, bas, env2, cart, dm.device.index if dm.is_cuda else 0)
+            d = dm.detach().cpu().numpy()
+            S, H = plan.int1e()
+            vj, vk = plan.get_jk(d, hermi=1)
+            e = float(numpy.sum(d * H) + 0.5 * numpy.sum(d * (vj - 0.5 * vk)) + _e_nuc(atm, c))
+            ctx.plan = plan
+            ctx.env = env2
+            ctx.coords = c
+            ctx.atm = atm
+            ctx.d = d
+            ctx.w = dme.detach().cpu().numpy()
+            return torch.tensor(e, dtype=coords.dtype, device=coords.device)
+
+        @staticmethod
+        def backward(ctx, grad_out):
+            g_coords = None
+            if ctx.needs_input_grad[0]:
+                if not numpy.array_equal(ctx.plan.env, ctx.env):
+                    ctx.plan.update_coords(ctx.env)
+                g = (ctx.plan.grad_int1e(ctx.d, ctx.w) + grad_2e_fused(ctx.plan, ctx.d) +
+                     _grad_nuc(ctx.atm, ctx.coords))
+                g_coords = grad_out * torch.from_numpy(g).to(grad_out.device, grad_out.dtype)
+            return g_coords, None, None, None, None, None, None
+
+    return TwoElectronEnergy, RHFEnergy
+
+
+def _e_nuc(atm, coords):
+    z = numpy.asarray(atm)[:, 0].astype(float)
+    e = 0.0
+    for a in range(len(z)):
+        for b in range(a):
+            e += z[a] * z[b] / numpy.linalg.norm(coords[a] - coords[b])
+    return e
+
+
+def _grad_nuc(atm, coords):
+    """grad_nuc (pyscf/grad/rhf.py:86-107) for point charges."""
+    z = numpy.asarray(atm)[:, 0].astype(float)
+    dr = coords[:, None, :] - coords[None]
+    r = numpy.linalg.norm(dr, axis=2)
+    numpy.fill_diagonal(r, numpy.inf)
+    return -numpy.einsum('i,j,ijx,ij->ix', z, z, dr, 1.0 / r ** 3)
 
 
 _fn = None
@@ -178,4 +237,13 @@ def two_electron_energy(coords, dm, atm, bas, env, cart=False):
     global _fn
     if _fn is None:
         _fn = _torch_function()
-    return _fn.apply(coords, dm, atm, bas, env, cart)
+    return _fn[0].apply(coords, dm, atm, bas, env, cart)
+
+
+def rhf_energy(coords, dm, dme, atm, bas, env, cart=False):
+    """The RHF energy at coords for the density dm as a differentiable torch
+    scalar whose gradient is the SCF energy gradient (see RHFEnergy)."""
+    global _fn
+    if _fn is None:
+        _fn = _torch_function()
+    return _fn[1].apply(coords, dm, dme, atm, bas, env, cart)

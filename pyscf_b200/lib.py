@@ -31,7 +31,7 @@ EXPORTS = (
     'b200jk_measure_fp64_peak', 'b200jk_get_jk_noalloc', 'b200jk_set_mixed_threshold',
     'b200jk_hostcheck_cart_quartet_fp32', 'b200jk_grad_jk', 'b200jk_grad_stats', 'b200jk_get_grad_q_cond',
     'b200jk_set_shard', 'b200jk_grad_class_stats', 'b200jk_autotune', 'b200jk_get_tuning', 'b200jk_set_tuning', 'b200jk_set_tile', 'b200jk_batch_get_jk_async', 'b200jk_batch_create', 'b200jk_batch_destroy', 'b200jk_batch_get_jk', 'b200jk_batch_stats', 'b200jk_debug_fail_alloc', 'b200jk_set_prescreen', 'b200jk_grad_contract', 'b200jk_plan_update_coords', 'b200jk_set_class_thresholds', 'b200jk_get_class_thresholds', 'b200jk_autotune_mixed', 'b200jk_int1e',
-    'b200jk_int2e_s8', 'b200jk_incore_jk',
+    'b200jk_int2e_s8', 'b200jk_incore_jk', 'b200jk_grad_int1e',
 )
 
 
@@ -92,6 +92,7 @@ def load(path=LIB_PATH):
         lib.b200jk_plan_update_coords.argtypes = [vp, vp, ip]
         lib.b200jk_int1e.argtypes = [vp, vp, vp, ip, vp]
         lib.b200jk_int2e_s8.argtypes = [vp, vp, ctypes.c_longlong, ip, vp]
+        lib.b200jk_grad_int1e.argtypes = [vp, vp, vp, vp, ip, vp]
         lib.b200jk_incore_jk.argtypes = [vp, ctypes.c_longlong, ip, vp, ip, ip, ip, ip, vp, vp, ip, ip, vp]
         lib.b200jk_set_class_thresholds.argtypes = [vp, vp, ip]
         lib.b200jk_get_class_thresholds.argtypes = [vp, vp, ip, ctypes.POINTER(ip)]
@@ -255,6 +256,18 @@ class Plan:
         H = numpy.empty((self.nao, self.nao))
         check(load().b200jk_int1e(self._h, _ptr(S), _ptr(H), 0, None))
         return S, H
+
+    def grad_int1e(self, dm, dme):
+        """One-electron part of the RHF nuclear gradient (natm, 3): the hcore
+        and overlap lines of grad_elec for the density dm and the
+        energy-weighted density dme (host arrays)."""
+        dm = numpy.ascontiguousarray(dm, dtype=numpy.double)
+        dme = numpy.ascontiguousarray(dme, dtype=numpy.double)
+        if dm.shape != (self.nao, self.nao) or dme.shape != (self.nao, self.nao):
+            raise RuntimeError('dm and dme must be (nao, nao) = (%d, %d)' % (self.nao, self.nao))
+        de = numpy.empty((self.atm.shape[0], 3))
+        check(load().b200jk_grad_int1e(self._h, _ptr(dm), _ptr(dme), _ptr(de), 0, None))
+        return de
 
     def int2e_s8(self, device=True):
         """The s8-packed ERI tensor of the basis (mol.intor('int2e',

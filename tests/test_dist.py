@@ -68,3 +68,57 @@ def test_shard_arguments_checked():
     from pyscf_b200 import lib
     l = lib.load()
     assert l.b200jk_set_shard(None, 0, 1) == lib.B200JK_EINVAL
+
+
+def _batch_worker(rank, world, port, q):
+    import torch
+    import torch.distributed as dist
+    from pyscf_b200 import dist as b2dist
+    os.environ['MASTER_ADDR'] = '127.0.0.1'
+    os.environ['MASTER_PORT'] = str(port)
+    dist.init_process_group('gloo', rank=rank, world_size=world)
+    try:
+        from conftest import GOLDEN
+        f = numpy.load(os.path.join(GOLDEN, 'batch_h2o_vdz512.npz'))
+        nbas = numpy.diff(f['bas_off'])
+        mine = b2dist.my_molecules(list(nbas))
+        # every rank's list, gathered only to check the partition here
+        n = torch.tensor([len(mine)])
+        sizes = [torch.zeros(1, dtype=torch.int64) for _ in range(world)]
+        dist.all_gather(sizes, n)
+        width = int(max(s.item() for s in sizes))
+        pad = torch.full((width,), -1, dtype=torch.int64)
+        pad[:len(mine)] = torch.tensor(mine, dtype=torch.int64)
+        lists = [torch.zeros(width, dtype=torch.int64) for _ in range(world)]
+        dist.all_gather(lists, pad)
+        q.put((rank, [[int(x) for x in l if x >= 0] for l in lists], [int(x) for x in nbas]))
+    finally:
+        dist.destroy_process_group()
+
+
+@pytest.mark.parametrize('world', [2, 4])
+def test_batch_shards_whole_molecules_gloo(world):
+    """The 512-molecule batch split over `world` ranks by whole molecules:
+    every rank derives the same partition with no communication, the parts
+    are disjoint and cover the batch, and the estimated work of the most
+    loaded rank is within one molecule's of the mean."""
+    import torch.multiprocessing as mp
+    from pyscf_b200 import dist as b2dist
+    ctx = mp.get_context('spawn')
+    q = ctx.Queue()
+    port = _free_port()
+    procs = [ctx.Process(target=_batch_worker, args=(r, world, port, q)) for r in range(world)]
+    for p in procs:
+        p.start()
+    for p in procs:
+        p.join(120)
+        assert p.exitcode == 0
+    res = sorted(q.get(timeout=10) for _ in range(world))
+    parts = res[0][1]
+    assert all(r[1] == parts for r in res)
+    flat = sorted(m for p in parts for m in p)
+    nbas = res[0][2]
+    assert flat == list(range(len(nbas)))
+    cost = [b2dist.molecule_cost(n) for n in nbas]
+    loads = [sum(cost[m] for m in p) for p in parts]
+    assert max(loads) - sum(loads) / world <= max(cost)
