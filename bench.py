@@ -778,6 +778,20 @@ def run_one_build(args):
                       'variants': ','.join('%d:%d' % (t, v) for t, v in enumerate(plan.tuning()) if v)}))
 
 
+def run_one_incore():
+    import torch
+    from pyscf_b200 import lib, incore
+    f = dict(numpy.load(os.path.join(GOLDEN, 'mol_h2o8_vdz.npz')))
+    plan = lib.Plan(f['atm'], f['bas'], f['env'], direct_scf_tol=1e-13)
+    eri = plan.int2e_s8(device=True)
+    d = torch.as_tensor(f['dm_conv'], device='cuda:0')
+    for _ in range(2):
+        vj, vk = incore.incore(eri, d, hermi=1)
+    torch.cuda.synchronize()
+    print(json.dumps({'workload': 'h2o8_vdz in-core', 'max_dJ': float(abs(vj.cpu().numpy() - f['vj_conv']).max()),
+                      'max_dK': float(abs(vk.cpu().numpy() - f['vk_conv']).max())}))
+
+
 class _Mol:
     def __init__(self, f):
         self._atm, self._bas, self._env = f['atm'], f['bas'], f['env']
@@ -795,6 +809,9 @@ def main():
     ap.add_argument('--tau', type=float, default=1e-6, help='float32 threshold of the mixed-precision line')
     ap.add_argument('--one-build', action='store_true',
                     help='plan + one FP64 J/K build of the workload, nothing else (the case profiled under ncu)')
+    ap.add_argument('--one-incore', action='store_true',
+                    help='fill the s8 tensor of (H2O)8/cc-pVDZ and run two in-core J/K builds, nothing else '
+                         '(the case profiled under ncu)')
     ap.add_argument('--autotune', action='store_true', help='--one-build: run the autotuner first')
     ap.add_argument('--variants', default=None,
                     help='--one-build: comma-separated class:variant pairs (a bare class index means variant 1), '
@@ -804,6 +821,8 @@ def main():
         run_reference(args)
     elif args.one_build:
         run_one_build(args)
+    elif args.one_incore:
+        run_one_incore()
     else:
         run_gpu(args)
 
