@@ -80,21 +80,25 @@ def _stale(obj, src, flags_file):
     return any(os.path.getmtime(d) > t for d in deps)
 
 
-# quartet classes whose register-family kernels are compiled for 4 blocks per
-# SM (at most 128 registers a thread): the classes where that build was the
-# faster one on the FP64 build of (H2O)64/cc-pVTZ against the compiler's own
-# allocation (class CUDA events, both builds with launch variants 0 and 2; a
-# few spills buy 16 resident warps instead of 12 or fewer).  B2_THREAD_MINB=<n> in the environment overrides it
-# for every class.
-THREAD_MINB4 = {(1, 0, 0, 0), (1, 1, 0, 0), (2, 0, 0, 0), (2, 1, 0, 0), (3, 1, 0, 0), (3, 2, 0, 0),
-                (3, 3, 0, 0)}
+# blocks per SM the register-family kernels of a quartet class are compiled
+# for (absent: 0, the compiler's own allocation): 4 caps a thread at 128
+# registers, 3 at 168.  Each entry is the faster build of the class on the
+# FP64 build of (H2O)64/cc-pVTZ (class CUDA events, builds compiled with 0,
+# 3 and 4 for every class, launch variants 0 and 2 each): a few spills buy
+# 12 or 16 resident warps instead of 8.  B2_THREAD_MINB=<n> in the
+# environment overrides it for every class.
+THREAD_MINB = {
+    (1, 0, 0, 0): 4, (1, 1, 0, 0): 4, (2, 0, 0, 0): 4, (2, 1, 0, 0): 4,
+    (2, 1, 1, 0): 3, (3, 0, 1, 0): 3, (2, 0, 1, 1): 3, (2, 2, 0, 0): 3, (3, 1, 0, 0): 3,
+    (3, 0, 3, 0): 3, (3, 3, 0, 0): 3, (3, 2, 0, 0): 3, (3, 0, 2, 0): 3,
+}
 
 
 def _thread_minb(cls):
     env = os.environ.get('B2_THREAD_MINB')
     if env:
         return int(env)
-    return 4 if cls in THREAD_MINB4 else 0
+    return THREAD_MINB.get(cls, 0)
 
 
 def _units():

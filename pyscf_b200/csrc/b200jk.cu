@@ -2680,7 +2680,8 @@ struct IncoreWS {
         std::mutex mu;
         DevArr<double> A1, A2, Jp, t, Dt, eri, dms, vj, vk;
         DevArr<int4> items;
-        std::vector<int4> h_items;
+        std::vector<int4> h_items;     // the fast kernel's four item lists, then the general ones
+        int nf[4] = {0, 0, 0, 0};
         int items_nao = -1, items_s8 = -1;
 };
 static IncoreWS g_incore_ws[64];
@@ -2738,7 +2739,14 @@ int b200jk_incore_jk(const double *eri, long long eri_len, int nao, const double
         }
         const int B = incore_block(nao);
         if (W.items_nao != nao || W.items_s8 != s8) {
-                incore_items(nao, s8, B, 2048, W.h_items);
+                std::vector<int4> fast[4], general;
+                incore_items(nao, s8, B, 2048, fast, general);
+                W.h_items.clear();
+                for (int v = 0; v < 4; v++) {
+                        W.nf[v] = (int)fast[v].size();
+                        W.h_items.insert(W.h_items.end(), fast[v].begin(), fast[v].end());
+                }
+                W.h_items.insert(W.h_items.end(), general.begin(), general.end());
                 if ((rc = dev_upload(W.items, W.h_items))) return rc;
                 W.items_nao = nao;
                 W.items_s8 = s8;
@@ -2752,7 +2760,13 @@ int b200jk_incore_jk(const double *eri, long long eri_len, int nao, const double
                 IncoreArgs a;
                 a.eri = E; a.s8 = s8; a.nao = nao; a.npair = npair;
                 a.D = D; a.t = W.t.p; a.A = W.A1.p; a.Jp = with_j ? W.Jp.p : nullptr;
-                a.items = W.items.p; a.nitems = (int)W.h_items.size();
+                int off = 0;
+                for (int v = 0; v < 4; v++) {
+                        a.fitems[v] = W.items.p + off;
+                        a.nf[v] = W.nf[v];
+                        off += W.nf[v];
+                }
+                a.items = W.items.p + off; a.nitems = (int)W.h_items.size() - off;
                 // one read of the tensor gives J and the K images (a J-only
                 // call drops the images: the pass is bound by the read)
                 if (launch_incore_pass(a, s, err)) return fail(B200JK_ECUDA, err);

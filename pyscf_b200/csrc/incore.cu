@@ -22,11 +22,17 @@
 // AO blocks (i in block I, j in block J, I >= J, B AOs a block) and a window
 // of packed columns kl.  Each thread takes one column kl of a 256-column
 // chunk and walks the block's rows, so every row's chunk is one coalesced
-// 2 KB read and each entry is read from HBM once.  The K images land in
-// shared-memory slabs A[I rows, :] and A[J rows, :] (one shared atomic per
-// row of a lane's register sums, after a warp reduction where all lanes
-// share k), flushed to HBM once per block; J row sums are reduce-scattered
-// across the warp.  The bound is HBM: 8 bytes per stored entry.
+// 2 KB read and each entry is read from HBM once.  Three kernels share the
+// windows: incore_fast_kernel takes the interior of the packed matrix (full
+// blocks I > J, columns before the block's rows: no per-entry test or
+// weight), its EDGE variant the rest of those blocks (q <= p tested per
+// entry), and incore_pass_kernel the diagonal blocks I == J and the partial
+// last block row with every test.  The fast kernels send the K images and
+// J row sums of a lane's register sums straight to the accumulators with
+// float64 reductions (after a warp reduction where all lanes share k); the
+// general one stages them in shared-memory slabs.  J row sums are
+// reduce-scattered across the warp.  The bound is HBM: 8 bytes per stored
+// entry.
 #include <vector>
 #include "incore_launch.h"
 
@@ -192,6 +198,141 @@ __global__ void __launch_bounds__(NT, 2) incore_pass_kernel(IncoreArgs a)
                 }
 }
 
+// The interior of the packed matrix: full AO blocks I > J (so i > j for
+// every row) and, for s8, columns before the block's first row (so q < p for
+// every entry).  No entry needs a validity test, rows follow each other by
+// their length, and the only symmetry weight is the column's own k == l,
+// applied once to the K sums of a lane.  The K images and the J row sums go
+// straight to the (L2-resident) accumulators with fire-and-forget float64
+// reductions, about one per four entries, so the block keeps only the two
+// density slabs in shared memory and needs no flush.
+// EDGE: the windows of such a block that reach its rows (s8): an entry is
+// stored only for q <= p and counts half on the packed diagonal q == p.
+// DIAG: a diagonal block I == J, whose rows are the pairs j <= i (the others
+// are skipped, uniformly over the block) and count half for j == i.
+template <int B, bool S8, bool EDGE, bool DIAG>
+__device__ __forceinline__ void incore_fast_body(const IncoreArgs &a, const int4 it)
+{
+        extern __shared__ __align__(16) double sm[];
+        const int nao = a.nao;
+        double *DI = sm, *DJ = DI + B * nao;
+        const int i0 = it.x * B, j0 = it.y * B;
+        const int tid = threadIdx.x, lane = tid & 31;
+        for (int e = tid; e < B * nao; e += NT) {
+                const int r = e / nao, x = e % nao;
+                DI[e] = a.D[(size_t)(i0 + r) * nao + x];
+                DJ[e] = a.D[(size_t)(j0 + r) * nao + x];
+        }
+        __syncthreads();
+        double *AI = a.A + (size_t)i0 * nao, *AJ = a.A + (size_t)j0 * nao;
+        const long long c0 = it.z, c1 = it.w;
+        for (long long qb = c0; qb < c1; qb += NT) {
+                const long long q = qb + tid;
+                const bool active = q < c1;
+                int k = 0, l = 0;
+                if (active) pair_of(q, k, l);
+                const double tq = active ? a.t[q] : 0.0;
+                const double wkl = k == l ? 0.5 : 1.0;
+                const int k0 = __shfl_sync(0xffffffffu, k, 0);
+                const bool kuni = __all_sync(0xffffffffu, !active || k == k0);
+                double acc2[B], acc4[B];
+#pragma unroll
+                for (int jj = 0; jj < B; jj++) {
+                        acc2[jj] = 0.0;
+                        acc4[jj] = 0.0;
+                }
+                double colj = 0.0;
+                for (int ii = 0; ii < B; ii++) {
+                        const int i = i0 + ii;
+                        const long long p0 = (long long)i * (i + 1) / 2 + j0;
+                        // edge windows: rows before the chunk hold none of its columns
+                        if (EDGE && p0 + B - 1 < qb) continue;
+                        const double *row = a.eri + (S8 ? p0 * (p0 + 1) / 2 : p0 * a.npair) + q;
+                        double v[B];
+#pragma unroll
+                        for (int jj = 0; jj < B; jj++) {
+                                // DIAG rows j > i do not exist
+                                const bool rowok = !DIAG || jj <= ii;
+                                if (EDGE) {
+                                        const long long p = p0 + jj;
+                                        v[jj] = rowok && active && q <= p ? __ldg(row) * (q == p ? 0.5 : 1.0) : 0.0;
+                                } else {
+                                        v[jj] = rowok && active ? __ldg(row) : 0.0;
+                                }
+                                row += S8 ? p0 + jj + 1 : a.npair;   // next row: p + 1 entries on (s8)
+                        }
+                        const double dik = DI[ii * nao + k], dil = DI[ii * nao + l];
+                        double acc1 = 0.0, acc3 = 0.0, rp[B];
+#pragma unroll
+                        for (int jj = 0; jj < B; jj++) {
+                                // the K images of a row j == i count half (DIAG)
+                                const double vk = DIAG && jj == ii ? 0.5 * v[jj] : v[jj];
+                                acc1 += vk * DJ[jj * nao + k];
+                                acc3 += vk * DJ[jj * nao + l];
+                                acc2[jj] += vk * dik;
+                                acc4[jj] += vk * dil;
+                                colj += v[jj] * __ldg(a.t + p0 + jj);
+                                rp[jj] = v[jj] * tq;
+                        }
+                        if (active && acc1 != 0.0) atomicAdd(AI + (size_t)ii * nao + l, wkl * acc1);
+                        if (kuni) {
+                                acc3 = warp_sum_d(wkl * acc3);
+                                if (lane == 0 && acc3 != 0.0) atomicAdd(AI + (size_t)ii * nao + k0, acc3);
+                        } else if (active && acc3 != 0.0) {
+                                atomicAdd(AI + (size_t)ii * nao + k, wkl * acc3);
+                        }
+                        if (S8 && a.Jp) {
+                                int rrow;
+                                const double s = reduce_scatter<B>(rp, lane, rrow);
+                                if ((lane & (32 / B - 1)) == 0 && s != 0.0) atomicAdd(a.Jp + p0 + rrow, s);
+                        }
+                }
+#pragma unroll
+                for (int jj = 0; jj < B; jj++) {
+                        acc2[jj] *= wkl;
+                        acc4[jj] *= wkl;
+                        if (active && acc2[jj] != 0.0) atomicAdd(AJ + (size_t)jj * nao + l, acc2[jj]);
+                }
+                if (kuni) {
+                        int rrow;
+                        const double s = reduce_scatter<B>(acc4, lane, rrow);
+                        if ((lane & (32 / B - 1)) == 0 && s != 0.0) atomicAdd(AJ + (size_t)rrow * nao + k0, s);
+                } else if (active) {
+#pragma unroll
+                        for (int jj = 0; jj < B; jj++)
+                                if (acc4[jj] != 0.0) atomicAdd(AJ + (size_t)jj * nao + k, acc4[jj]);
+                }
+                if (a.Jp && active && colj != 0.0) atomicAdd(a.Jp + q, colj);
+        }
+}
+
+// One launch for the four variants: blocks take the items of variant 0
+// (the bulk of the tensor) first, then those of 1, 2 and 3, which fill the
+// tail of the launch.
+template <int B, bool S8>
+__global__ void __launch_bounds__(NT, 2) incore_fast_kernel(IncoreArgs a)
+{
+        // (the item lists are selected by constant indices: a run-time index
+        // into the parameter array would copy it to local memory)
+        int b = blockIdx.x;
+        if (b < a.nf[0]) {
+                incore_fast_body<B, S8, false, false>(a, a.fitems[0][b]);
+                return;
+        }
+        b -= a.nf[0];
+        if (b < a.nf[1]) {
+                incore_fast_body<B, S8, true, false>(a, a.fitems[1][b]);
+                return;
+        }
+        b -= a.nf[1];
+        if (b < a.nf[2]) {
+                incore_fast_body<B, S8, false, true>(a, a.fitems[2][b]);
+                return;
+        }
+        b -= a.nf[2];
+        incore_fast_body<B, S8, true, true>(a, a.fitems[3][b]);
+}
+
 __global__ void tridm_kernel(const double *__restrict__ D, int nao, double *__restrict__ t)
 {
         const long long np = (long long)nao * (nao + 1) / 2;
@@ -258,13 +399,24 @@ int launch_pass(const IncoreArgs &a, cudaStream_t s, std::string &err)
         const size_t smem = sizeof(double) * (4 * (size_t)B * a.nao + B * B);
         cudaError_t e = cudaFuncSetAttribute(incore_pass_kernel<B, S8>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                              (int)smem);
+        const size_t smem_fast = sizeof(double) * 2 * (size_t)B * a.nao;
+        if (e == cudaSuccess)
+                e = cudaFuncSetAttribute(incore_fast_kernel<B, S8>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                         (int)smem_fast);
         if (e != cudaSuccess) {
                 err = std::string("in-core kernel configuration: ") + cudaGetErrorString(e);
                 return 1;
         }
-        if (a.nitems == 0) return 0;
-        incore_pass_kernel<B, S8><<<a.nitems, NT, smem, s>>>(a);
-        return check("in-core kernel launch", err);
+        const int nfast = a.nf[0] + a.nf[1] + a.nf[2] + a.nf[3];
+        if (nfast > 0) {
+                incore_fast_kernel<B, S8><<<nfast, NT, smem_fast, s>>>(a);
+                if (check("in-core kernel launch", err)) return 1;
+        }
+        if (a.nitems > 0) {
+                incore_pass_kernel<B, S8><<<a.nitems, NT, smem, s>>>(a);
+                if (check("in-core kernel launch", err)) return 1;
+        }
+        return 0;
 }
 
 } // namespace
@@ -280,19 +432,38 @@ int incore_block(int nao)
         return 0;
 }
 
-void incore_items(int nao, int s8, int B, long long window, std::vector<int4> &items)
+void incore_items(int nao, int s8, int B, long long window, std::vector<int4> (&fast)[4],
+                  std::vector<int4> &general)
 {
-        items.clear();
+        for (auto &v : fast) v.clear();
+        general.clear();
         const long long npair = (long long)nao * (nao + 1) / 2;
         const int nb = (nao + B - 1) / B;
+        auto split = [&](std::vector<int4> &v, int I, int J, long long c0, long long c1) {
+                for (long long c = c0; c < c1; c += window)
+                        v.push_back(make_int4(I, J, (int)c, (int)std::min(c1, c + window)));
+        };
         for (int I = 0; I < nb; I++)
                 for (int J = 0; J <= I; J++) {
                         const int imax = std::min(nao, (I + 1) * B) - 1;
                         const int jmax = std::min(std::min(nao, (J + 1) * B) - 1, imax);
                         const long long pmax = (long long)imax * (imax + 1) / 2 + jmax;
                         const long long ncol = s8 ? pmax + 1 : npair;
-                        for (long long c = 0; c < ncol; c += window)
-                                items.push_back(make_int4(I, J, (int)c, (int)std::min(ncol, c + window)));
+                        const bool full = (I + 1) * B <= nao;
+                        const int diag = I == J ? 2 : 0;
+                        if (!full) {
+                                split(general, I, J, 0, ncol);
+                        } else if (!s8) {
+                                split(fast[diag], I, J, 0, ncol);
+                        } else {
+                                // the block's first row (i0, j0): columns
+                                // before it are below the packed diagonal for
+                                // every row of the block
+                                const long long i0 = (long long)I * B;
+                                const long long pmin = i0 * (i0 + 1) / 2 + (long long)J * B;
+                                split(fast[diag], I, J, 0, pmin);
+                                split(fast[diag + 1], I, J, pmin, ncol);
+                        }
                 }
 }
 

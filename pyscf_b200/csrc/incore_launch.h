@@ -17,8 +17,13 @@ struct IncoreArgs {
         const double *t;        // npair: D_ij + D_ji (i > j), D_ii (i == j)
         double *A;              // nao x nao accumulator of the pair-order K images (zeroed by the caller)
         double *Jp;             // npair accumulator of packed J, or nullptr (zeroed by the caller)
-        const int4 *items;      // (I block, J block, first column, end column) per thread block
+        const int4 *items;      // general items: (I block, J block, first column, end column) per thread block
         int nitems;
+        // items of the fast kernel's variants, index EDGE + 2 DIAG: full blocks
+        // (I > J, or I == J for DIAG), windows before the block's rows or (s8,
+        // EDGE) the ones that reach them
+        const int4 *fitems[4];
+        int nf[4];
 };
 
 // AO rows per block of the contraction for a basis of nao functions (0 when
@@ -26,8 +31,13 @@ struct IncoreArgs {
 int incore_block(int nao);
 // the work items of a pass: AO-block pairs I >= J crossed with column windows
 // of at most `window` packed columns (s8: only the columns <= the block's
-// last row)
-void incore_items(int nao, int s8, int B, long long window, std::vector<int4> &items);
+// last row).  fast[v], v = EDGE + 2 DIAG, gets the windows of full blocks
+// (DIAG: I == J, else I > J): for s8 the columns before the block's first
+// row (EDGE = 0: no entry there needs a validity test) and the rest (EDGE =
+// 1: q <= p tested per entry, half weight on q == p); for s4 every window
+// (EDGE = 0).  `general` gets the blocks of the partial last block row.
+void incore_items(int nao, int s8, int B, long long window, std::vector<int4> (&fast)[4],
+                  std::vector<int4> &general);
 
 int launch_incore_pass(const IncoreArgs &a, cudaStream_t s, std::string &err);
 // t = packed D + D^T (diagonal once) of a nao x nao density
