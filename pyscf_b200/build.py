@@ -94,6 +94,24 @@ THREAD_MINB = {
 }
 
 
+# parts of the register family per quartet class where the build overrides
+# the register budget's choice (thread_parts<> in jk_kernels.cuh; a part
+# re-runs the primitive loop for its share of the bra components).
+# B2_THREAD_PARTS="la lb lc ld:n,..." in the environment replaces it.
+THREAD_PARTS = {}
+
+
+def _thread_parts(cls):
+    env = os.environ.get('B2_THREAD_PARTS')
+    table = THREAD_PARTS
+    if env:
+        table = {}
+        for item in env.split(','):
+            c, n = item.split(':')
+            table[tuple(int(x) for x in c.split())] = int(n)
+    return table.get(cls)
+
+
 def _thread_minb(cls):
     env = os.environ.get('B2_THREAD_MINB')
     if env:
@@ -115,8 +133,10 @@ def _units():
         o = os.path.join(OBJ, 'jk_%s.o' % tag)
         units.append((common + ['-DB2_BRA_LA=%d' % la, '-DB2_BRA_LB=%d' % lb, '-DB2_KET_LC=%d' % lc,
                                 '-DB2_KET_LD=%d' % ld, '-DB2_FN_NAME=launch_jk_%s' % tag,
-                                '-DB2_THREAD_MINB=%d' % _thread_minb((la, lb, lc, ld)),
-                                os.path.join(CSRC, 'jk_classes.cu'), '-o', o], o))
+                                '-DB2_THREAD_MINB=%d' % _thread_minb((la, lb, lc, ld))] +
+                     (['-DB2_THREAD_PARTS=%d' % _thread_parts((la, lb, lc, ld))]
+                      if _thread_parts((la, lb, lc, ld)) else []) +
+                     [os.path.join(CSRC, 'jk_classes.cu'), '-o', o], o))
     for la, lb in PAIR_CLASSES:
         o = os.path.join(OBJ, 'grad_%d%d.o' % (la, lb))
         units.append((common + ['-DB2_BRA_LA=%d' % la, '-DB2_BRA_LB=%d' % lb,

@@ -22,17 +22,18 @@
 // AO blocks (i in block I, j in block J, I >= J, B AOs a block) and a window
 // of packed columns kl.  Each thread takes one column kl of a 256-column
 // chunk and walks the block's rows, so every row's chunk is one coalesced
-// 2 KB read and each entry is read from HBM once.  Three kernels share the
-// windows: incore_fast_kernel takes the interior of the packed matrix (full
-// blocks I > J, columns before the block's rows: no per-entry test or
-// weight), its EDGE variant the rest of those blocks (q <= p tested per
-// entry), and incore_pass_kernel the diagonal blocks I == J and the partial
-// last block row with every test.  The fast kernels send the K images and
-// J row sums of a lane's register sums straight to the accumulators with
-// float64 reductions (after a warp reduction where all lanes share k); the
-// general one stages them in shared-memory slabs.  J row sums are
-// reduce-scattered across the warp.  The bound is HBM: 8 bytes per stored
-// entry.
+// 2 KB read and each entry is read from HBM once.  Two kernels share the
+// windows: incore_fast_kernel takes every full block, in one launch of four
+// variants -- the interior of the packed matrix (blocks I > J, columns
+// before the block's rows: no per-entry test or weight), the windows of such
+// blocks that reach their rows (EDGE: q <= p tested per entry), and the same
+// two for the diagonal blocks I == J (DIAG: rows j > i skipped, the K images
+// of j == i halved) -- and incore_pass_kernel the blocks of the partial last
+// block row with every test.  The fast kernel sends the K images and J row
+// sums of a lane's register sums straight to the accumulators with float64
+// reductions (after a warp reduction where all lanes share k); the general
+// one stages them in shared-memory slabs.  J row sums are reduce-scattered
+// across the warp.  The bound is HBM: 8 bytes per stored entry.
 #include <vector>
 #include "incore_launch.h"
 

@@ -319,8 +319,8 @@ __host__ __device__ constexpr int ket_run()
 // translation-unit flag, set per class by the build from measured times):
 // 0 leaves register allocation to the compiler (an explicit 1 does not: it
 // lets the allocator use far more registers); 4 caps a thread at 128
-// registers, trading a few spills for 16 resident warps instead of 12 or 8 on
-// the latency-bound classes whose blocks need more.  Float64 kernels only:
+// registers and 3 at 168, trading a few spills for 16 or 12 resident warps
+// instead of 8 on the latency-bound classes whose blocks need more.  Float64 kernels only:
 // the float32 ones need far fewer registers, and a cap above their natural
 // count would only let them grow.
 #ifndef B2_THREAD_MINB
@@ -823,11 +823,17 @@ __global__ void __launch_bounds__(128, B2_THREAD_MINB) jk_thread_run_kernel(JKAr
 
 // Parts of the register family for a class: 0 = class goes to the shared-
 // memory family.  Budget: live integrals of a part plus the three 2D slices
-// of one root.
+// of one root.  B2_THREAD_PARTS (a translation-unit flag of a class unit,
+// set by the build from measured times) replaces the budget's choice for
+// that unit's class, which must be a register-family class; it must divide
+// the bra's Cartesian components.
 template <int LA, int LB, int LC, int LD>
 __host__ __device__ constexpr int thread_parts()
 {
         using K = Class4<LA, LB, LC, LD>;
+#if defined(B2_THREAD_PARTS) && defined(B2_KET_LD)
+        if (LA == B2_BRA_LA && LB == B2_BRA_LB && LC == B2_KET_LC && LD == B2_KET_LD) return B2_THREAD_PARTS;
+#endif
         if (K::SA > 18 || K::NR > 4) return (K::NG + 3 * K::SA <= 80) ? 1 : 0;
         for (int np = 1; np <= K::NA && np <= 5; np++)
                 if (K::NA % np == 0 && K::NG / np + 3 * K::SA <= (np == 1 ? 80 : 72)) return np;
