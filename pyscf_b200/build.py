@@ -84,38 +84,50 @@ def _stale(obj, src, flags_file):
 # for (absent: 0, the compiler's own allocation): 4 caps a thread at 128
 # registers, 3 at 168.  Each entry is the faster build of the class on the
 # FP64 build of (H2O)64/cc-pVTZ (class CUDA events, builds compiled with 0,
-# 3 and 4 for every class, launch variants 0 and 2 each): a few spills buy
-# 12 or 16 resident warps instead of 8.  B2_THREAD_MINB=<n> in the
-# environment overrides it for every class.
+# 3 and 4 for every class, launch variants 0 and 2 each, with the part
+# counts below): a few spills buy 12 or 16 resident warps instead of 8.
+# B2_THREAD_MINB=<n> (every class) or "la lb lc ld:n,..." in the environment
+# overrides it.
 THREAD_MINB = {
     (1, 0, 0, 0): 4, (1, 1, 0, 0): 4, (2, 0, 0, 0): 4, (2, 1, 0, 0): 4,
-    (2, 1, 1, 0): 3, (3, 0, 1, 0): 3, (2, 0, 1, 1): 3, (2, 2, 0, 0): 3, (3, 1, 0, 0): 3,
-    (3, 0, 3, 0): 3, (3, 3, 0, 0): 3, (3, 2, 0, 0): 3, (3, 0, 2, 0): 3,
+    (3, 0, 1, 0): 3, (2, 2, 0, 0): 3, (3, 1, 0, 0): 3,
 }
 
 
 # parts of the register family per quartet class where the build overrides
 # the register budget's choice (thread_parts<> in jk_kernels.cuh; a part
-# re-runs the primitive loop for its share of the bra components).
+# re-runs the primitive loop for its share of the bra components): fewer
+# parts than the budget allows, measured faster on the FP64 build of
+# (H2O)64/cc-pVTZ ((31|10) 397 -> 204 ms with 2 parts instead of 5, (21|10)
+# 595 -> 466 ms with 1 instead of 2): re-running the roots and 2D integrals
+# costs more than the spills of the larger blocks.
 # B2_THREAD_PARTS="la lb lc ld:n,..." in the environment replaces it.
-THREAD_PARTS = {}
+THREAD_PARTS = {
+    (3, 1, 1, 0): 2, (3, 0, 1, 1): 2, (3, 0, 3, 0): 2, (3, 3, 0, 0): 2,
+    (2, 1, 1, 0): 1, (2, 0, 1, 1): 1, (3, 0, 2, 0): 1, (3, 2, 0, 0): 1,
+}
+
+
+def _class_table(text):
+    """'la lb lc ld:n,...' -> {(la, lb, lc, ld): n}"""
+    table = {}
+    for item in text.split(','):
+        c, n = item.split(':')
+        table[tuple(int(x) for x in c.split())] = int(n)
+    return table
 
 
 def _thread_parts(cls):
     env = os.environ.get('B2_THREAD_PARTS')
-    table = THREAD_PARTS
-    if env:
-        table = {}
-        for item in env.split(','):
-            c, n = item.split(':')
-            table[tuple(int(x) for x in c.split())] = int(n)
+    table = _class_table(env) if env else THREAD_PARTS
     return table.get(cls)
 
 
 def _thread_minb(cls):
     env = os.environ.get('B2_THREAD_MINB')
     if env:
-        return int(env)
+        # one value for every class, or a per-class table
+        return _class_table(env).get(cls, 0) if ':' in env else int(env)
     return THREAD_MINB.get(cls, 0)
 
 
