@@ -145,6 +145,7 @@ def _units():
         o = os.path.join(OBJ, 'jk_%s.o' % tag)
         units.append((common + ['-DB2_BRA_LA=%d' % la, '-DB2_BRA_LB=%d' % lb, '-DB2_KET_LC=%d' % lc,
                                 '-DB2_KET_LD=%d' % ld, '-DB2_FN_NAME=launch_jk_%s' % tag,
+                                '-DB2_NP_NAME=launch_jk_%s_np' % tag,
                                 '-DB2_THREAD_MINB=%d' % _thread_minb((la, lb, lc, ld))] +
                      (['-DB2_THREAD_PARTS=%d' % _thread_parts((la, lb, lc, ld))]
                       if _thread_parts((la, lb, lc, ld)) else []) +

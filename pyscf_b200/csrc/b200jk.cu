@@ -409,6 +409,72 @@ static double class_tau(const b200jk_plan *P, size_t t)
         return P->fp32_tau;
 }
 
+// the parts of the register family of every class, as its unit was built
+int b200jk::family_thread_parts(int la, int lb, int lc, int ld)
+{
+        typedef int (*np_fn)();
+        struct Entry { int la, lb, lc, ld; np_fn fn; };
+        static const Entry table[] = {
+                {0, 0, 0, 0, launch_jk_0000_np},
+                {1, 0, 0, 0, launch_jk_1000_np},
+                {1, 0, 1, 0, launch_jk_1010_np},
+                {1, 1, 0, 0, launch_jk_1100_np},
+                {1, 1, 1, 0, launch_jk_1110_np},
+                {1, 1, 1, 1, launch_jk_1111_np},
+                {2, 0, 0, 0, launch_jk_2000_np},
+                {2, 0, 1, 0, launch_jk_2010_np},
+                {2, 0, 1, 1, launch_jk_2011_np},
+                {2, 0, 2, 0, launch_jk_2020_np},
+                {2, 1, 0, 0, launch_jk_2100_np},
+                {2, 1, 1, 0, launch_jk_2110_np},
+                {2, 1, 1, 1, launch_jk_2111_np},
+                {2, 1, 2, 0, launch_jk_2120_np},
+                {2, 1, 2, 1, launch_jk_2121_np},
+                {2, 2, 0, 0, launch_jk_2200_np},
+                {2, 2, 1, 0, launch_jk_2210_np},
+                {2, 2, 1, 1, launch_jk_2211_np},
+                {2, 2, 2, 0, launch_jk_2220_np},
+                {2, 2, 2, 1, launch_jk_2221_np},
+                {2, 2, 2, 2, launch_jk_2222_np},
+                {3, 0, 0, 0, launch_jk_3000_np},
+                {3, 0, 1, 0, launch_jk_3010_np},
+                {3, 0, 1, 1, launch_jk_3011_np},
+                {3, 0, 2, 0, launch_jk_3020_np},
+                {3, 0, 2, 1, launch_jk_3021_np},
+                {3, 0, 2, 2, launch_jk_3022_np},
+                {3, 0, 3, 0, launch_jk_3030_np},
+                {3, 1, 0, 0, launch_jk_3100_np},
+                {3, 1, 1, 0, launch_jk_3110_np},
+                {3, 1, 1, 1, launch_jk_3111_np},
+                {3, 1, 2, 0, launch_jk_3120_np},
+                {3, 1, 2, 1, launch_jk_3121_np},
+                {3, 1, 2, 2, launch_jk_3122_np},
+                {3, 1, 3, 0, launch_jk_3130_np},
+                {3, 1, 3, 1, launch_jk_3131_np},
+                {3, 2, 0, 0, launch_jk_3200_np},
+                {3, 2, 1, 0, launch_jk_3210_np},
+                {3, 2, 1, 1, launch_jk_3211_np},
+                {3, 2, 2, 0, launch_jk_3220_np},
+                {3, 2, 2, 1, launch_jk_3221_np},
+                {3, 2, 2, 2, launch_jk_3222_np},
+                {3, 2, 3, 0, launch_jk_3230_np},
+                {3, 2, 3, 1, launch_jk_3231_np},
+                {3, 2, 3, 2, launch_jk_3232_np},
+                {3, 3, 0, 0, launch_jk_3300_np},
+                {3, 3, 1, 0, launch_jk_3310_np},
+                {3, 3, 1, 1, launch_jk_3311_np},
+                {3, 3, 2, 0, launch_jk_3320_np},
+                {3, 3, 2, 1, launch_jk_3321_np},
+                {3, 3, 2, 2, launch_jk_3322_np},
+                {3, 3, 3, 0, launch_jk_3330_np},
+                {3, 3, 3, 1, launch_jk_3331_np},
+                {3, 3, 3, 2, launch_jk_3332_np},
+                {3, 3, 3, 3, launch_jk_3333_np}};
+        for (const Entry &e : table)
+                if (e.la == la && e.lb == lb && e.lc == lc && e.ld == ld) return e.fn();
+        return 0;
+}
+
 static int dispatch_jk(b200jk_plan *P, int la, int lb, int lc, int ld, const JKArgs &a, int fp32, cudaStream_t s,
                        const JKArgs *margs = nullptr, const long long *mchunk = nullptr, int nmol = 0, int variant = 0)
 {

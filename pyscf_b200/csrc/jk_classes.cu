@@ -158,4 +158,9 @@ int B2_FN_NAME(const JKArgs &a, cudaStream_t s, int nsm, int fp32, int variant, 
 #undef B2_L
 }
 
+// B2_NP_NAME is launch_jk_<la><lb><lc><ld>_np: the parts of the register
+// family this unit's class was built with (0: shared-memory family), which
+// the host planner reads instead of recomputing the budget
+int B2_NP_NAME() { return thread_parts<B2_BRA_LA, B2_BRA_LB, B2_KET_LC, B2_KET_LD>(); }
+
 } // namespace b200jk

@@ -8,20 +8,11 @@
 
 namespace b200jk {
 
-// quartets per chunk of the kernel family used for class (la lb | lc ld)
-// host twin of thread_parts<> (jk_kernels.cuh): parts of the register
-// family, 0 for the shared-memory family
-inline int family_thread_parts(int la, int lb, int lc, int ld)
-{
-        const int na = ncart(la);
-        const int ng = na * ncart(lb) * ncart(lc) * ncart(ld);
-        const int sa = (la + 1) * (lb + 1) * (lc + 1) * (ld + 1);
-        const int nr = (la + lb + lc + ld) / 2 + 1;
-        if (sa > 18 || nr > 4) return (ng + 3 * sa <= 80) ? 1 : 0;
-        for (int np = 1; np <= na && np <= 5; np++)
-                if (na % np == 0 && ng / np + 3 * sa <= (np == 1 ? 80 : 72)) return np;
-        return 0;
-}
+// parts of the register family of class (la lb | lc ld) as its translation
+// unit was built (thread_parts<> in jk_kernels.cuh with the build's
+// per-class choice), 0 for the shared-memory family; defined in b200jk.cu
+// from the units' launch_jk_*_np
+int family_thread_parts(int la, int lb, int lc, int ld);
 inline int family_is_thread(int la, int lb, int lc, int ld) { return family_thread_parts(la, lb, lc, ld) > 0; }
 // lanes per quartet of the shared-memory family (group_size<> in jk_kernels.cuh)
 inline int family_group(int la, int lb, int lc, int ld)
@@ -199,6 +190,62 @@ int launch_jk_3332(const JKArgs &a, cudaStream_t s, int nsm, int fp32, int varia
                    const JKArgs *margs, const long long *mchunk, int nmol, std::string &err);
 int launch_jk_3333(const JKArgs &a, cudaStream_t s, int nsm, int fp32, int variant,
                    const JKArgs *margs, const long long *mchunk, int nmol, std::string &err);
+// the parts each class unit was built with (see family_thread_parts)
+int launch_jk_0000_np();
+int launch_jk_1000_np();
+int launch_jk_1010_np();
+int launch_jk_1100_np();
+int launch_jk_1110_np();
+int launch_jk_1111_np();
+int launch_jk_2000_np();
+int launch_jk_2010_np();
+int launch_jk_2011_np();
+int launch_jk_2020_np();
+int launch_jk_2100_np();
+int launch_jk_2110_np();
+int launch_jk_2111_np();
+int launch_jk_2120_np();
+int launch_jk_2121_np();
+int launch_jk_2200_np();
+int launch_jk_2210_np();
+int launch_jk_2211_np();
+int launch_jk_2220_np();
+int launch_jk_2221_np();
+int launch_jk_2222_np();
+int launch_jk_3000_np();
+int launch_jk_3010_np();
+int launch_jk_3011_np();
+int launch_jk_3020_np();
+int launch_jk_3021_np();
+int launch_jk_3022_np();
+int launch_jk_3030_np();
+int launch_jk_3100_np();
+int launch_jk_3110_np();
+int launch_jk_3111_np();
+int launch_jk_3120_np();
+int launch_jk_3121_np();
+int launch_jk_3122_np();
+int launch_jk_3130_np();
+int launch_jk_3131_np();
+int launch_jk_3200_np();
+int launch_jk_3210_np();
+int launch_jk_3211_np();
+int launch_jk_3220_np();
+int launch_jk_3221_np();
+int launch_jk_3222_np();
+int launch_jk_3230_np();
+int launch_jk_3231_np();
+int launch_jk_3232_np();
+int launch_jk_3300_np();
+int launch_jk_3310_np();
+int launch_jk_3311_np();
+int launch_jk_3320_np();
+int launch_jk_3321_np();
+int launch_jk_3322_np();
+int launch_jk_3330_np();
+int launch_jk_3331_np();
+int launch_jk_3332_np();
+int launch_jk_3333_np();
 
 int launch_qcond(int la, int lb, const QArgs &q, cudaStream_t s, std::string &err);
 
