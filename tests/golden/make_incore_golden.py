@@ -14,7 +14,9 @@ mol_h2o_631g.npz, mol_h2o2_vtz.npz and mol_h2o8_vdz.npz (same atm/bas/env):
   * scf.hf.dot_eri_dm(eri, dm, hermi) -> _vhf.incore (pyscf/scf/_vhf.py:
     318-401) for the fixture's dm_rand (hermi=1), dm_ns (hermi=0) and
     dm_anti = (dm_ns - dm_ns^T)/2 (hermi=2); for H2O/6-31G also from the s4
-    tensor ao2mo.restore(4, eri, nao).
+    tensor ao2mo.restore(4, eri, nao);
+  * make_variants(): H2O/cc-pVDZ in the Cartesian basis and under the erf
+    and erfc operators (incore_h2o_vdz_variants.npz).
 
     OMP_NUM_THREADS=8 python tests/golden/make_incore_golden.py
 """
@@ -91,6 +93,37 @@ def make(name):
           % (name, nao, eri.size, out['eri_nzero'], t_fill, t_jk, path), flush=True)
 
 
+def make_variants():
+    """H2O/cc-pVDZ (d shells): the whole s8 tensor of the spherical and of
+    the Cartesian basis (int2e_cart), and of the spherical basis under
+    env[PTR_RANGE_OMEGA] = 0.5 (erf, long range) and -0.5 (erfc, short
+    range), as mol.intor('int2e', aosym='s8') returns them; with the in-core
+    J/K (hermi=1) of a symmetric density of U(-1, 1) entries
+    (numpy.random.default_rng(11)).  Written to incore_h2o_vdz_variants.npz."""
+    f = dict(numpy.load(os.path.join(HERE, 'mol_h2o_vdz.npz')))
+    out = {}
+    for tag, cart, omega in (('full', False, 0.0), ('cart', True, 0.0), ('lr', False, 0.5), ('sr', False, -0.5)):
+        g = dict(f)
+        g['cart'] = numpy.int32(cart)
+        env = numpy.array(f['env'], dtype=numpy.double)
+        env[8] = omega   # PTR_RANGE_OMEGA (pyscf/gto/mole.py:76)
+        g['env'] = env
+        mol = mol_of(g)
+        nao = mol.nao_nr()
+        eri = mol.intor('int2e', aosym='s8')
+        rng = numpy.random.default_rng(11)
+        a = rng.uniform(-1, 1, (nao, nao))
+        dm = (a + a.T) * 0.5
+        vj, vk = scf.hf.dot_eri_dm(eri, dm, 1)
+        out.update({'%s_eri' % tag: eri, '%s_env' % tag: env, '%s_dm' % tag: dm, '%s_vj' % tag: vj,
+                    '%s_vk' % tag: vk, '%s_nao' % tag: numpy.int32(nao)})
+        print(tag, nao, eri.size, flush=True)
+    numpy.savez_compressed(os.path.join(HERE, 'incore_h2o_vdz_variants.npz'), **out)
+
+
 if __name__ == '__main__':
-    for n in (sys.argv[1:] or NAMES):
-        make(n)
+    for n in (sys.argv[1:] or NAMES + ('variants',)):
+        if n == 'variants':
+            make_variants()
+        else:
+            make(n)

@@ -138,3 +138,32 @@ def test_rhf_on_incore_builds():
                              lambda dm: incore.incore(eri, dm, hermi=1), conv_tol=1e-10)
     assert conv
     assert abs(e - float(f['e_rhf'])) < 1e-8, (e, float(f['e_rhf']))
+
+
+@pytest.mark.parametrize('tag', ['full', 'cart', 'lr', 'sr'])
+def test_int2e_s8_cartesian_and_range_separated(tag):
+    """The GPU fill in the Cartesian basis (int2e_cart) and under the erf and
+    erfc operators (env[PTR_RANGE_OMEGA] = 0.5, -0.5; erfc as full minus long
+    range) against the reference's whole tensors of H2O/cc-pVDZ, 1e-12 per
+    entry, and the in-core J/K of each against the reference's."""
+    import torch
+    from pyscf_b200 import lib, incore
+    path = os.path.join(GOLDEN, 'incore_h2o_vdz_variants.npz')
+    if not os.path.exists(path):
+        pytest.skip('incore_h2o_vdz_variants.npz missing (tests/golden/make_incore_golden.py)')
+    if lib.device_count() == 0:
+        pytest.fail('no CUDA device visible to libb200jk')
+    g = dict(numpy.load(path))
+    f = load_fixture('h2o_vdz')
+
+    class Mol:
+        _atm, _bas, _env, cart = f['atm'], f['bas'], g['%s_env' % tag], tag == 'cart'
+    eri = incore.int2e_s8(Mol(), device=True)
+    ref = g['%s_eri' % tag]
+    assert eri.numel() == ref.size
+    assert abs(eri.cpu().numpy() - ref).max() < 1e-12
+    vj, vk = incore.incore(eri, g['%s_dm' % tag], hermi=1)
+    _close(vj, g['%s_vj' % tag])
+    _close(vk, g['%s_vk' % tag])
+    del eri
+    torch.cuda.empty_cache()

@@ -115,3 +115,15 @@ def test_incore_fixture_matches_direct_fixture():
     scale = max(1.0, abs(f['vj_rand']).max())
     assert abs(g['vj_rand'] - f['vj_rand']).max() < 1e-9 * scale
     assert abs(g['vk_rand'] - f['vk_rand']).max() < 1e-9 * scale
+
+
+def test_range_separated_fixtures_add_up():
+    """erf + erfc = 1: the reference's long- and short-range s8 tensors of
+    H2O/cc-pVDZ add up to the full-range one (to the Schwarz cutoff, 1e-14,
+    under which each operator leaves its own entries at zero)."""
+    path = os.path.join(GOLDEN, 'incore_h2o_vdz_variants.npz')
+    if not os.path.exists(path):
+        pytest.skip('incore_h2o_vdz_variants.npz missing')
+    g = dict(numpy.load(path))
+    assert abs(g['lr_eri'] + g['sr_eri'] - g['full_eri']).max() < 1e-12
+    assert g['cart_eri'].size > g['full_eri'].size   # 25 Cartesian AOs against 24
