@@ -618,6 +618,21 @@ def run_gpu(args):
         grad_line = {'workload': 'h2o16_vdz', 'nao': int(fg['nao']), 'ms_per_build': tg / args.steps * 1e3,
                      'quartet_sides_per_build': gq / args.steps, 'quartet_sides_per_s': gq / tg,
                      'screen': 'CVHFgrad_jk_prescreen, tol 1e-14'}
+        if world == 1:
+            # the two-electron force as the RHF gradient computes it: the
+            # fused contraction with D x D, no vj/vk (b200jk_grad_contract)
+            gplan.grad_contract(dg)
+            ft = []
+            for _ in range(args.steps):
+                flush.fill_(1.0)
+                e0 = torch.cuda.Event(enable_timing=True)
+                e1 = torch.cuda.Event(enable_timing=True)
+                e0.record(stream)
+                gplan.grad_contract(dg)
+                e1.record(stream)
+                e1.synchronize()
+                ft.append(e0.elapsed_time(e1))
+            grad_line['fused_force_ms_per_build'] = float(numpy.mean(ft))
     except Exception as e:  # the gradient line must not sink the J/K measurement
         grad_line = {'error': str(e)[:200]}
 

@@ -1965,7 +1965,7 @@ static int grad_build(b200jk_plan *P, const double *dms, int n_dm, int with_j, i
                         const PairClassDev &ket = g.ket[Y];
                         if (ket.n == 0) continue;
                         const int nseg = bra.n * B2_NBUCKET;
-                        const int chunk = grad_chunk(bra.la, bra.lb, ket.la, ket.lb);
+                        const int chunk = grad_chunk(bra.la, bra.lb, ket.la, ket.lb, fused);
                         count_kernel<<<grid_for(nseg, 256), 256, 0, s>>>(bra.view(), ket.view(), 0, tol, g.fac.p, chunk,
                                                                         0.0, 0, P->shard, P->nshard, g.nkl.p, g.kst.p,
                                                                         g.nchunk.p);

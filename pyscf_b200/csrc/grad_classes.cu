@@ -33,7 +33,31 @@ int launch_grad_impl(const GradArgs &a, cudaStream_t s, int nsm, std::string &er
         constexpr int GS = grad_group_size<LA, LB, LC, LD>();
         static GradCfg cfg;
         static std::mutex mu;
-        if constexpr (grad_thread_family<LA, LB, LC, LD>()) {
+        if constexpr (FUSED && grad_force_regs<LA, LB, LC, LD>()) {
+                // the fused contraction's register family (one ket per lane)
+                {
+                        std::lock_guard<std::mutex> lk(mu);
+                        if (!cfg.ready) {
+                                int nb = 0;
+                                cfg.block = 128;
+                                cfg.status = cudaOccupancyMaxActiveBlocksPerMultiprocessor(
+                                        &nb, grad_force_kernel<LA, LB, LC, LD>, 128, 0);
+                                cfg.grid = (nb > 0 ? nb : 1) * nsm;
+                                cfg.ready = true;
+                        }
+                }
+                if (cfg.status != cudaSuccess) {
+                        err = std::string("gradient kernel configuration: ") + cudaGetErrorString(cfg.status);
+                        return 1;
+                }
+                grad_force_kernel<LA, LB, LC, LD><<<cfg.grid, cfg.block, 0, s>>>(a);
+                cudaError_t e = cudaGetLastError();
+                if (e != cudaSuccess) {
+                        err = std::string("gradient kernel launch: ") + cudaGetErrorString(e);
+                        return 1;
+                }
+                return 0;
+        } else if constexpr (grad_thread_family<LA, LB, LC, LD>()) {
                 {
                         std::lock_guard<std::mutex> lk(mu);
                         if (!cfg.ready) {

@@ -863,4 +863,163 @@ static __global__ void grad_cart_to_out_kernel(const double *V, int nv, int nao,
         out[t] = scale * v;
 }
 
+// ---------------------------------------------------------------------------
+// Register family of the fused force contraction (b200jk_grad_contract) for
+// mid-size classes.  A quartet's contribution to the forces is six numbers,
+// fs[q] = sum_t G[q, t] w[t], with w[t] = 2 D_ab Ds_cd - X_bc X_ad - X_bd X_ac
+// fixed by the density blocks.  So the lane computes w once per quartet and
+// assembles each root's derivative integrals straight into fs: NG weights
+// and the three 2D slices live in registers, not the six derivative blocks
+// of grad_thread_kernel, which brings classes up to NG + 3 SE <= 102 (those of
+// one p or d shell with two s or p shells) from the shared-memory family to
+// one ket per lane.
+template <int LA, int LB, int LC, int LD>
+__host__ __device__ constexpr bool grad_force_regs()
+{
+        using GC = GClass<LA, LB, LC, LD, 0>;
+        return !grad_thread_family<LA, LB, LC, LD>() && GC::NG + 3 * GC::SE <= 102;
+}
+
+template <int LA, int LB, int LC, int LD, int T>
+__device__ __forceinline__ void grad_force_one(double fs[6], const double *w, const double *Ex, const double *Ey,
+                                               const double *Ez, double ta, double tb)
+{
+        using K = Class4<LA, LB, LC, LD>;
+        using GC = GClass<LA, LB, LC, LD, 0>;
+        constexpr int id = T % K::ND, ic = (T / K::ND) % K::NC, ib = (T / K::NCD) % K::NB, ia = T / (K::NCD * K::NB);
+        constexpr int ax = cart_lx(LA, ia), ay = cart_ly(LA, ia), az = cart_lz(LA, ia);
+        constexpr int bx = cart_lx(LB, ib), by = cart_ly(LB, ib), bz = cart_lz(LB, ib);
+        constexpr int ox = GC::eidx(ax, bx, cart_lx(LC, ic), cart_lx(LD, id));
+        constexpr int oy = GC::eidx(ay, by, cart_ly(LC, ic), cart_ly(LD, id));
+        constexpr int oz = GC::eidx(az, bz, cart_lz(LC, ic), cart_lz(LD, id));
+        constexpr int SA = GC::STEP_A, SB = GC::STEP_B;
+        const double wt = w[T];
+        const double ex = Ex[ox] * wt, ey = Ey[oy], ez = Ez[oz];
+        double dax = ta * Ex[ox + SA], day = ta * Ey[oy + SA], daz = ta * Ez[oz + SA];
+        if constexpr (ax > 0) dax -= ax * Ex[ox - SA];
+        if constexpr (ay > 0) day -= ay * Ey[oy - SA];
+        if constexpr (az > 0) daz -= az * Ez[oz - SA];
+        double dbx = tb * Ex[ox + SB], dby = tb * Ey[oy + SB], dbz = tb * Ez[oz + SB];
+        if constexpr (bx > 0) dbx -= bx * Ex[ox - SB];
+        if constexpr (by > 0) dby -= by * Ey[oy - SB];
+        if constexpr (bz > 0) dbz -= bz * Ez[oz - SB];
+        const double eyz = ey * ez;
+        fs[0] += wt * dax * eyz;
+        fs[1] += ex * day * ez;
+        fs[2] += ex * ey * daz;
+        fs[3] += wt * dbx * eyz;
+        fs[4] += ex * dby * ez;
+        fs[5] += ex * ey * dbz;
+}
+
+template <int LA, int LB, int LC, int LD, int... Ts>
+__device__ __forceinline__ void grad_force_assemble(double fs[6], const double *w, const double *Ex,
+                                                    const double *Ey, const double *Ez, double ta, double tb,
+                                                    std::integer_sequence<int, Ts...>)
+{
+        (grad_force_one<LA, LB, LC, LD, Ts>(fs, w, Ex, Ey, Ez, ta, tb), ...);
+}
+
+
+template <int LA, int LB, int LC, int LD>
+__global__ void __launch_bounds__(128) grad_force_kernel(GradArgs a)
+{
+        using K = Class4<LA, LB, LC, LD>;
+        using GC = GClass<LA, LB, LC, LD, 0>;
+        constexpr int NG = K::NG, NR = GC::NR, SE = GC::SE;
+        const int lane = threadIdx.x & 31;
+        const int nseg = a.bra.n * B2_NBUCKET;
+        const long long total = a.chunk_off[nseg];
+        const long long nwarps = ((long long)gridDim.x * blockDim.x) >> 5;
+        const size_t n = (size_t)a.naoc;
+        const double *table = a.table + rys_padded_offset(NR);
+        unsigned long long nq = 0, npq = 0;
+        for (long long chunk = ((long long)blockIdx.x * blockDim.x + threadIdx.x) >> 5; chunk < total;
+             chunk += nwarps) {
+                const int sgi = find_bra(a.chunk_off, nseg, chunk);
+                const int ij = sgi / B2_NBUCKET;
+                const int pos = (int)(chunk - a.chunk_off[sgi]) * 32 + lane;
+                const int kl = a.ket.boff[sgi % B2_NBUCKET] + a.kst[sgi] + pos;
+                const int4 sb = a.bra.sh[ij];
+                const int2 pb = a.bra.pr[ij];
+                const double4 Ab = a.bra.A[ij];
+                const double4 ABb = a.bra.AB[ij];
+                const double AB[3] = {ABb.x, ABb.y, ABb.z};
+                int4 sk = make_int4(0, 0, 0, 0);
+                bool sideA = false, sideB = false;
+                if (pos < a.nkl[sgi]) {
+                        sk = a.ket.sh[kl];
+                        const int kk = max(sk.z, sk.w), ll = min(sk.z, sk.w);
+                        sideA = grad_side_passes(a, sb.z, sb.w, kk, ll);
+                        sideB = Ab.w == 0.0 && grad_side_passes(a, sb.w, sb.z, kk, ll);
+                }
+                const bool active = sideA || sideB;
+                double fs[6] = {0.0, 0.0, 0.0, 0.0, 0.0, 0.0};
+                if (active) {
+                        // the weights of the quartet's Cartesian components
+                        const int ia = sb.x, ib = sb.y, ic = sk.x, id = sk.y;
+                        const double *X = a.Dc;
+                        double w[NG];
+#pragma unroll
+                        for (int t = 0; t < NG; t++) {
+                                const int d = t % K::ND, c = (t / K::ND) % K::NC;
+                                const int b = (t / K::NCD) % K::NB, xa = t / (K::NCD * K::NB);
+                                w[t] = grad_force_weight(__ldg(X + (ia + xa) * n + ib + b), __ldg(a.Ds + (ic + c) * n + id + d),
+                                                         __ldg(X + (ib + b) * n + ic + c), __ldg(X + (ia + xa) * n + id + d),
+                                                         __ldg(X + (ib + b) * n + id + d), __ldg(X + (ia + xa) * n + ic + c));
+                        }
+                        const int2 pk = a.ket.pr[kl];
+                        const double4 Ak = a.ket.A[kl];
+                        const double4 CDk = a.ket.AB[kl];
+                        const double fac = Ak.w != 0.0 ? 0.5 : 1.0;
+                        const double A0[3] = {0.0, 0.0, 0.0};
+                        const double C[3] = {Ak.x - Ab.x, Ak.y - Ab.y, Ak.z - Ab.z};
+                        const double CD[3] = {CDk.x, CDk.y, CDk.z};
+                        nq += (unsigned long long)sideA + (unsigned long long)sideB;
+                        npq += (unsigned long long)pb.y * pk.y;
+                        for (int ip = 0; ip < pb.y; ip++) {
+                                const double4 P = a.PP[pb.x + ip];
+                                const double2 KP = a.PK[pb.x + ip];
+                                const double2 EP = a.PE[pb.x + ip];
+                                const double Kab = KP.x * fac;
+                                const double Pv[3] = {P.x - Ab.x, P.y - Ab.y, P.z - Ab.z};
+                                const double ta = 2.0 * EP.x, tb = 2.0 * EP.y;
+                                for (int kp = 0; kp < pk.y; kp++) {
+                                        const double4 Q = a.PP[pk.x + kp];
+                                        const double2 KQ = a.PK[pk.x + kp];
+                                        const double Qv[3] = {Q.x - Ab.x, Q.y - Ab.y, Q.z - Ab.z};
+                                        PrimQ<double> sq;
+                                        prim_setup<double>(sq, P.w, KP.y, Pv, Q.w, KQ.y, Qv, A0, C, Kab * KQ.x, a.omega2);
+                                        double u[NR], wr[NR];
+                                        rys_roots_slice<NR, double>(sq.T, table, u, wr);
+#pragma unroll
+                                        for (int r = 0; r < NR; r++) {
+                                                RysCoef<double> rc;
+                                                rys_coef<double>(rc, u[r], sq);
+                                                double Ex[SE], Ey[SE], Ez[SE];
+                                                grad_slice<LA, LB, LC, LD, 0>(Ex, 1.0, rc, 0, AB[0], CD[0]);
+                                                grad_slice<LA, LB, LC, LD, 0>(Ey, 1.0, rc, 1, AB[1], CD[1]);
+                                                grad_slice<LA, LB, LC, LD, 0>(Ez, sq.pref * wr[r], rc, 2, AB[2], CD[2]);
+                                                grad_force_assemble<LA, LB, LC, LD>(fs, w, Ex, Ey, Ez, ta, tb,
+                                                                                    std::make_integer_sequence<int, NG>{});
+                                        }
+                                }
+                        }
+                        if (!sideA) fs[0] = fs[1] = fs[2] = 0.0;
+                        if (!sideB) fs[3] = fs[4] = fs[5] = 0.0;
+                }
+                grad_force_flush(a, sb, fs, lane);
+        }
+        if (a.stats) {
+                for (int o = 16; o > 0; o >>= 1) {
+                        nq += __shfl_xor_sync(0xffffffffu, nq, o);
+                        npq += __shfl_xor_sync(0xffffffffu, npq, o);
+                }
+                if (lane == 0 && nq) {
+                        atomicAdd(a.stats + 0, nq);
+                        atomicAdd(a.stats + 1, npq);
+                }
+        }
+}
+
 } // namespace b200jk

@@ -9,12 +9,14 @@
 namespace b200jk {
 
 // quartets per chunk of a warp for class (la lb | lc ld): one per lane in the
-// register family (host twin of grad_thread_family), 8 per group otherwise
-inline int grad_chunk(int la, int lb, int lc, int ld)
+// register family (host twin of grad_thread_family, and for the fused force
+// contraction of grad_force_regs), 8 per group otherwise
+inline int grad_chunk(int la, int lb, int lc, int ld, bool fused = false)
 {
         const int ng = ncart(la) * ncart(lb) * ncart(lc) * ncart(ld);
         const int se = (la + 2) * (lb + 2) * (lc + 1) * (ld + 1);
         if (6 * ng + 3 * se <= 104) return 32;
+        if (fused && ng + 3 * se <= 102) return 32;
         const int gs = ng <= 100 ? 8 : (ng <= 400 ? 16 : 32);
         return 8 * (32 / gs);
 }
