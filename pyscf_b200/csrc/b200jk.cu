@@ -2045,7 +2045,7 @@ static int grad_build(b200jk_plan *P, const double *dms, int n_dm, int with_j, i
                         class_l(Y, c.lc, c.ld);
                         c.quartets = (int64_t)hs[2 * t];
                         c.prim_quartets = (int64_t)hs[2 * t + 1];
-                        c.family = 1;
+                        c.family = grad_register_family(c.la, c.lb, c.lc, c.ld, fused) ? 0 : 1;
                         c.ms = 0;
                         if (P->profiling && ran[t]) {
                                 float cm = 0;

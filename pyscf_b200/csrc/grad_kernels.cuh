@@ -272,6 +272,84 @@ __device__ __forceinline__ void grad_eval_pass(double *sm, const GradArgs &a, in
         __syncwarp(gmask);
 }
 
+// The fused force contraction's pass of the shared-memory family: instead
+// of building NCP derivative blocks in shared memory and contracting them
+// afterwards, each lane assembles all six derivative components of its
+// Cartesian components straight into fq[6] with the quartet's weights w
+// (shared memory, NG doubles): no block to clear or update, one pass.
+template <int LA, int LB, int LC, int LD, int GS>
+__device__ __forceinline__ void grad_eval_force(double *sm, const GradArgs &a, int2 pb, int2 pk, const double4 O,
+                                                const double AB[3], const double C[3], const double CD[3],
+                                                double fac, const double *w, int gl, unsigned gmask, double fq[6])
+{
+        using GC = GClass<LA, LB, LC, LD, 0>;
+        using S = GradSmem<LA, LB, LC, LD, 0>;
+        constexpr int NR = GC::NR, SE = GC::SE, NG = GC::NG;
+        constexpr int SA = GC::STEP_A, SB = GC::STEP_B;
+        double *E = sm + S::E;
+        const double *table = a.table + rys_padded_offset(NR);
+        const double A[3] = {0.0, 0.0, 0.0};
+        for (int ip = 0; ip < pb.y; ip++) {
+                const double4 P = a.PP[pb.x + ip];
+                const double2 KP = a.PK[pb.x + ip];
+                const double2 EP = a.PE[pb.x + ip];
+                const double Kab = KP.x * fac;
+                const double Pv[3] = {P.x - O.x, P.y - O.y, P.z - O.z};
+                const double ta = 2.0 * EP.x, tb = 2.0 * EP.y;
+                for (int kp = 0; kp < pk.y; kp++) {
+                        const double4 Q = a.PP[pk.x + kp];
+                        const double2 KQ = a.PK[pk.x + kp];
+                        const double Qv[3] = {Q.x - O.x, Q.y - O.y, Q.z - O.z};
+                        __syncwarp(gmask);
+                        for (int task = gl; task < 3 * NR; task += GS) {
+                                const int r = task / 3, dir = task - 3 * r;
+                                PrimQ<double> sq;
+                                prim_setup<double>(sq, P.w, KP.y, Pv, Q.w, KQ.y, Qv, A, C, Kab * KQ.x, a.omega2);
+                                double ur, wr;
+                                rys_root_one<NR, double>(sq.T, table, r, ur, wr);
+                                RysCoef<double> rc;
+                                rys_coef<double>(rc, ur, sq);
+                                const double g00 = dir == 2 ? sq.pref * wr : 1.0;
+                                const double abx = dir == 0 ? AB[0] : (dir == 1 ? AB[1] : AB[2]);
+                                const double cdx = dir == 0 ? CD[0] : (dir == 1 ? CD[1] : CD[2]);
+                                grad_slice<LA, LB, LC, LD, 0>(E + (dir * NR + r) * SE, g00, rc, dir, abx, cdx);
+                        }
+                        __syncwarp(gmask);
+                        for (int t = gl; t < NG; t += GS) {
+                                const int2 o = __ldg(a.goff + t);
+                                const int ox = o.x & 1023, oy = (o.x >> 10) & 1023, oz = o.x >> 20;
+                                const int axn = gexp(o.y, 0, 0), ayn = gexp(o.y, 0, 1), azn = gexp(o.y, 0, 2);
+                                const int bxn = gexp(o.y, 1, 0), byn = gexp(o.y, 1, 1), bzn = gexp(o.y, 1, 2);
+                                const double wt = w[t];
+                                double f[6] = {0.0, 0.0, 0.0, 0.0, 0.0, 0.0};
+#pragma unroll
+                                for (int r = 0; r < NR; r++) {
+                                        const double *Ex = E + r * SE, *Ey = E + (NR + r) * SE, *Ez = E + (2 * NR + r) * SE;
+                                        const double ex = Ex[ox], ey = Ey[oy], ez = Ez[oz];
+                                        double dax = ta * Ex[ox + SA], day = ta * Ey[oy + SA], daz = ta * Ez[oz + SA];
+                                        if (axn) dax -= axn * Ex[ox - SA];
+                                        if (ayn) day -= ayn * Ey[oy - SA];
+                                        if (azn) daz -= azn * Ez[oz - SA];
+                                        double dbx = tb * Ex[ox + SB], dby = tb * Ey[oy + SB], dbz = tb * Ez[oz + SB];
+                                        if (bxn) dbx -= bxn * Ex[ox - SB];
+                                        if (byn) dby -= byn * Ey[oy - SB];
+                                        if (bzn) dbz -= bzn * Ez[oz - SB];
+                                        const double eyz = ey * ez, exz = ex * ez, exy = ex * ey;
+                                        f[0] += dax * eyz;
+                                        f[1] += day * exz;
+                                        f[2] += daz * exy;
+                                        f[3] += dbx * eyz;
+                                        f[4] += dby * exz;
+                                        f[5] += dbz * exy;
+                                }
+#pragma unroll
+                                for (int q = 0; q < 6; q++) fq[q] += wt * f[q];
+                        }
+                }
+        }
+        __syncwarp(gmask);
+}
+
 template <int LA, int LB, int LC, int LD>
 __host__ __device__ constexpr int grad_group_size()
 {
@@ -335,6 +413,35 @@ __global__ void __launch_bounds__(128) grad_jk_kernel(GradArgs a, int chunk_q)
                                 npq += (unsigned long long)pb.y * pk.y;
                         }
                         const int ic = sk.x, id = sk.y;
+                        if constexpr (FUSED) {
+                                // weights of the quartet's elements into the G area, then one
+                                // pass assembling all six derivative sums from them
+                                const double *X = a.Dc;
+                                double *w = sm + S::G;
+                                double *dsab = sm + S::DSAB, *dscd = sm + S::DSCD;
+                                double *xbc = sm + S::XBC, *xbd = sm + S::XBD;
+                                double *xac = sm + S::XAC, *xad = sm + S::XAD;
+                                for (int t = gl; t < K::NAB; t += GS) dsab[t] = __ldg(X + (ia + t / K::NB) * n + ib + t % K::NB);
+                                for (int t = gl; t < K::NCD; t += GS) dscd[t] = __ldg(a.Ds + (ic + t / K::ND) * n + id + t % K::ND);
+                                for (int t = gl; t < K::NB * K::NC; t += GS) xbc[t] = __ldg(X + (ib + t / K::NC) * n + ic + t % K::NC);
+                                for (int t = gl; t < K::NB * K::ND; t += GS) xbd[t] = __ldg(X + (ib + t / K::ND) * n + id + t % K::ND);
+                                for (int t = gl; t < K::NA * K::NC; t += GS) xac[t] = __ldg(X + (ia + t / K::NC) * n + ic + t % K::NC);
+                                for (int t = gl; t < K::NA * K::ND; t += GS) xad[t] = __ldg(X + (ia + t / K::ND) * n + id + t % K::ND);
+                                __syncwarp(gmask);
+                                for (int t = gl; t < NG; t += GS) {
+                                        const int d = t % K::ND, c = (t / K::ND) % K::NC;
+                                        const int b = (t / K::NCD) % K::NB, xa = t / (K::NCD * K::NB);
+                                        w[t] = grad_force_weight(dsab[xa * K::NB + b], dscd[c * K::ND + d], xbc[b * K::NC + c],
+                                                                 xad[xa * K::ND + d], xbd[b * K::ND + d], xac[xa * K::NC + c]);
+                                }
+                                __syncwarp(gmask);
+                                double fq[6] = {0.0, 0.0, 0.0, 0.0, 0.0, 0.0};
+                                grad_eval_force<LA, LB, LC, LD, GS>(sm, a, pb, pk, Ab, AB, C, CD, fac, w, gl, gmask, fq);
+#pragma unroll
+                                for (int q = 0; q < 6; q++)
+                                        if (q < 3 ? sideA : sideB) fs[q] += fq[q];
+                                continue;
+                        }
                         for (int pass = 0; pass < GC::NPASS; pass++) {
                                 const int c0 = pass * GC::NCP;
                                 // skip a pass whose components all belong to a failing side
@@ -342,32 +449,6 @@ __global__ void __launch_bounds__(128) grad_jk_kernel(GradArgs a, int chunk_q)
                                 if (!needA && !needB) continue;
                                 grad_eval_pass<LA, LB, LC, LD, 0, GS>(sm, a, pb, pk, Ab, AB, C, CD, fac, c0, gl, gmask);
                                 const double *G = sm + S::G;
-                                if constexpr (FUSED) {
-                                        const double *X = a.Dc;
-                                        double *dsab = sm + S::DSAB, *dscd = sm + S::DSCD;
-                                        double *xbc = sm + S::XBC, *xbd = sm + S::XBD;
-                                        double *xac = sm + S::XAC, *xad = sm + S::XAD;
-                                        for (int t = gl; t < K::NAB; t += GS) dsab[t] = __ldg(X + (ia + t / K::NB) * n + ib + t % K::NB);
-                                        for (int t = gl; t < K::NCD; t += GS) dscd[t] = __ldg(a.Ds + (ic + t / K::ND) * n + id + t % K::ND);
-                                        for (int t = gl; t < K::NB * K::NC; t += GS) xbc[t] = __ldg(X + (ib + t / K::NC) * n + ic + t % K::NC);
-                                        for (int t = gl; t < K::NB * K::ND; t += GS) xbd[t] = __ldg(X + (ib + t / K::ND) * n + id + t % K::ND);
-                                        for (int t = gl; t < K::NA * K::NC; t += GS) xac[t] = __ldg(X + (ia + t / K::NC) * n + ic + t % K::NC);
-                                        for (int t = gl; t < K::NA * K::ND; t += GS) xad[t] = __ldg(X + (ia + t / K::ND) * n + id + t % K::ND);
-                                        __syncwarp(gmask);
-                                        for (int t = gl; t < NG; t += GS) {
-                                                const int d = t % K::ND, c = (t / K::ND) % K::NC;
-                                                const int b = (t / K::NCD) % K::NB, xa = t / (K::NCD * K::NB);
-                                                const double w = grad_force_weight(dsab[xa * K::NB + b], dscd[c * K::ND + d],
-                                                                                   xbc[b * K::NC + c], xad[xa * K::ND + d],
-                                                                                   xbd[b * K::ND + d], xac[xa * K::NC + c]);
-#pragma unroll
-                                                for (int q = 0; q < 6; q++)
-                                                        if (q >= c0 && q < c0 + GC::NCP && (q < 3 ? sideA : sideB))
-                                                                fs[q] += G[(q - c0) * NG + t] * w;
-                                        }
-                                        __syncwarp(gmask);
-                                        continue;
-                                }
                                 for (int s = 0; s < a.n_dm; s++) {
                                         const double *Ds = a.Ds + s * nn;
                                         const double *X = a.Dc + s * nn;

@@ -8,15 +8,22 @@
 
 namespace b200jk {
 
-// quartets per chunk of a warp for class (la lb | lc ld): one per lane in the
-// register family (host twin of grad_thread_family, and for the fused force
-// contraction of grad_force_regs), 8 per group otherwise
-inline int grad_chunk(int la, int lb, int lc, int ld, bool fused = false)
+// whether class (la lb | lc ld) runs in a register family (one ket per lane):
+// host twin of grad_thread_family and, for the fused force contraction, of
+// grad_force_regs
+inline bool grad_register_family(int la, int lb, int lc, int ld, bool fused = false)
 {
         const int ng = ncart(la) * ncart(lb) * ncart(lc) * ncart(ld);
         const int se = (la + 2) * (lb + 2) * (lc + 1) * (ld + 1);
-        if (6 * ng + 3 * se <= 104) return 32;
-        if (fused && ng + 3 * se <= 102) return 32;
+        return 6 * ng + 3 * se <= 104 || (fused && ng + 3 * se <= 102);
+}
+
+// quartets per chunk of a warp for class (la lb | lc ld): one per lane in a
+// register family, 8 per group otherwise
+inline int grad_chunk(int la, int lb, int lc, int ld, bool fused = false)
+{
+        if (grad_register_family(la, lb, lc, ld, fused)) return 32;
+        const int ng = ncart(la) * ncart(lb) * ncart(lc) * ncart(ld);
         const int gs = ng <= 100 ? 8 : (ng <= 400 ? 16 : 32);
         return 8 * (32 / gs);
 }
