@@ -808,6 +808,21 @@ def run_one_incore():
                       'max_dK': float(abs(vk.cpu().numpy() - f['vk_conv']).max())}))
 
 
+def run_one_grad():
+    """Plan of (H2O)16/cc-pVDZ, then one gradient J/K build and two fused force
+    contractions of its density (the case profiled under ncu)."""
+    from pyscf_b200 import lib
+    f = dict(numpy.load(os.path.join(GOLDEN, 'grad_h2o16_vdz.npz')))
+    plan = lib.Plan(f['atm'], f['bas'], f['env'], direct_scf_tol=1e-13)
+    plan.grad_jk(f['dm0'])
+    jk_ms = plan.grad_stats()['last_build_ms']
+    for _ in range(2):
+        de = plan.grad_contract(f['dm0'])
+    print(json.dumps({'workload': 'h2o16_vdz gradient', 'grad_jk_ms': jk_ms,
+                      'fused_force_ms': plan.grad_stats()['last_build_ms'],
+                      'sum_de': float(numpy.asarray(de).sum())}))
+
+
 class _Mol:
     def __init__(self, f):
         self._atm, self._bas, self._env = f['atm'], f['bas'], f['env']
@@ -828,6 +843,9 @@ def main():
     ap.add_argument('--one-incore', action='store_true',
                     help='fill the s8 tensor of (H2O)8/cc-pVDZ and run two in-core J/K builds, nothing else '
                          '(the case profiled under ncu)')
+    ap.add_argument('--one-grad', action='store_true',
+                    help='one gradient J/K build and two fused force contractions of (H2O)16/cc-pVDZ, nothing '
+                         'else (the case profiled under ncu)')
     ap.add_argument('--autotune', action='store_true', help='--one-build: run the autotuner first')
     ap.add_argument('--variants', default=None,
                     help='--one-build: comma-separated class:variant pairs (a bare class index means variant 1), '
@@ -839,6 +857,8 @@ def main():
         run_one_build(args)
     elif args.one_incore:
         run_one_incore()
+    elif args.one_grad:
+        run_one_grad()
     else:
         run_gpu(args)
 
