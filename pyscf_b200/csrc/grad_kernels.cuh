@@ -953,12 +953,15 @@ static __global__ void grad_cart_to_out_kernel(const double *V, int nv, int nao,
 // and the three 2D slices live in registers, not the six derivative blocks
 // of grad_thread_kernel, which brings classes up to NG + 3 SE <= 102 (those of
 // one p or d shell with two s or p shells) from the shared-memory family to
-// one ket per lane.
+// one ket per lane.  Of grad_thread_kernel's own classes it takes those of 9
+// or more components ((10|10): 254 -> 164 registers, 14.0 -> 12.7 ms on
+// (H2O)16/cc-pVDZ); for the smaller ones the six blocks cost no occupancy
+// and the two kernels were within 4% either way.
 template <int LA, int LB, int LC, int LD>
 __host__ __device__ constexpr bool grad_force_regs()
 {
         using GC = GClass<LA, LB, LC, LD, 0>;
-        return !grad_thread_family<LA, LB, LC, LD>() && GC::NG + 3 * GC::SE <= 102;
+        return GC::NG + 3 * GC::SE <= 102 && (!grad_thread_family<LA, LB, LC, LD>() || GC::NG >= 9);
 }
 
 template <int LA, int LB, int LC, int LD, int T>
