@@ -396,9 +396,31 @@ typedef int (*jk_launcher_t)(const JKArgs &, cudaStream_t, int, int, int, const 
                              std::string &);
 
 // the launch variant of class t in precision pass `pass` (1: float32 quartets)
+// Launch variant of a float64 pass in a plan the autotuner has not timed:
+// the autotuner's choices on the FP64 build of (H2O)64/cc-pVTZ, where each
+// won by 15-25% per class -- bra runs (2) for eight register-family
+// classes of s and p kets, half-width groups (1) for (21|20) and (22|10).  Callers that never tune (a drop-in
+// SCF, whose first builds would pay for the timing) get them as they are.
+static int default_fp64_variant(size_t t)
+{
+        // index = position in quartet_classes(): bra pair class X (00, 10, 11,
+        // 20, 21, 22, 30, ...) major, ket pair class Y <= X minor
+        static const int table[] = {
+                2,                   // (00|00)
+                2, 2,                // (10|00) (10|10)
+                2, 2, 0,             // (11|00) (11|10) (11|11)
+                2, 2, 0, 0,          // (20|00) (20|10) (20|11) (20|20)
+                0, 0, 0, 1, 0,       // (21|00) (21|10) (21|11) (21|20) (21|21)
+                0, 1, 0, 0, 0, 0,    // (22|00) (22|10) ...
+                2,                   // (30|00)
+        };
+        return t < sizeof(table) / sizeof(table[0]) ? table[t] : 0;
+}
+
 static int class_variant(const b200jk_plan *P, size_t t, int pass)
 {
         const std::vector<int> &v = pass == 1 ? P->kvar32 : P->kvar;
+        if (v.empty()) return pass == 1 ? 0 : default_fp64_variant(t);
         return t < v.size() ? v[t] : 0;
 }
 
@@ -2359,7 +2381,10 @@ static int batch_build(b200jk_batch *B, const double *const *dms, int hermi, int
                 for (int pass = 0; pass < (tau > 0 ? 2 : 1); pass++) {
                         const int nm = ncnt[2 * t + pass];
                         if (nm == 0) continue;
-                        const int variant = class_variant(B->plans[0], t, pass);
+                        // bra runs (variant 2) need the tiled pass of one plan: a batch
+                        // runs those classes as variant 0
+                        int variant = class_variant(B->plans[0], t, pass);
+                        if (variant == 2) variant = 0;
                         const int chunk = family_chunk(la, lb, lc, ld, variant);
                         const JKArgs *dargs = B->args.p + at[2 * t + pass];
                         const int *dseg = B->segoff.p + sat[2 * t + pass];
