@@ -399,8 +399,14 @@ typedef int (*jk_launcher_t)(const JKArgs &, cudaStream_t, int, int, int, const 
 // Launch variant of a float64 pass in a plan the autotuner has not timed:
 // the autotuner's choices on the FP64 build of (H2O)64/cc-pVTZ, where each
 // won by 15-25% per class -- bra runs (2) for eight register-family
-// classes of s and p kets, half-width groups (1) for (21|20) and (22|10).  Callers that never tune (a drop-in
-// SCF, whose first builds would pay for the timing) get them as they are.
+// classes of s and p kets, half-width groups (1) for (21|20) and (22|10).
+// Callers that never tune (a drop-in SCF, whose first builds would pay for
+// the timing) get them on plans of DEFAULT_VARIANT_MIN_NAO or more AOs.
+// Smaller plans keep variant 0: bra runs give a warp four bra pairs, too
+// few warps for a small molecule (warm FP64 builds, defaults vs variant 0:
+// nao 192 22.7 vs 11.8 ms, 464 73.0 vs 61.0, 928 263.8 vs 254.8, 1856
+// 1975 vs 2022 ms).
+static const int DEFAULT_VARIANT_MIN_NAO = 1500;
 static int default_fp64_variant(size_t t)
 {
         // index = position in quartet_classes(): bra pair class X (00, 10, 11,
@@ -420,7 +426,7 @@ static int default_fp64_variant(size_t t)
 static int class_variant(const b200jk_plan *P, size_t t, int pass)
 {
         const std::vector<int> &v = pass == 1 ? P->kvar32 : P->kvar;
-        if (v.empty()) return pass == 1 ? 0 : default_fp64_variant(t);
+        if (v.empty()) return pass == 1 || P->nao < DEFAULT_VARIANT_MIN_NAO ? 0 : default_fp64_variant(t);
         return t < v.size() ? v[t] : 0;
 }
 
