@@ -229,6 +229,26 @@ def test_set_tuning_every_variant(b2):
     assert abs(vk - f['vk_rand']).max() < 2e-5 * abs(f['vk_rand']).max()
 
 
+def test_untuned_default_variants(b2):
+    """A plan that was never tuned runs variant 0 below 1500 AOs and the
+    measured defaults from there on (bra runs for eight s/p-ket classes,
+    half-width groups for (21|20) and (22|10)); float32 passes stay at 0 and
+    an explicit tuning replaces the defaults.  Parity of builds with the
+    defaults is covered by the 32-water sample (nao 1856) against the
+    reference drivers' J/K."""
+    small = plan_for(b2, load_fixture('h2o8_vdz'))
+    assert small.tuning() == [0] * 55
+    big = plan_for(b2, load_fixture('h2o64_vtz_sub32'))
+    expect = [0] * 55
+    for t in (0, 1, 2, 3, 4, 6, 7, 21):
+        expect[t] = 2
+    expect[13] = expect[16] = 1
+    assert big.tuning() == expect
+    assert big.tuning(b2.PREC_MIXED) == [0] * 55
+    big.set_tuning([0] * 55)
+    assert big.tuning() == [0] * 55
+
+
 @pytest.mark.parametrize('name', ['h2o8_vdz', 'h2o2_vtz'])
 def test_bra_run_variant(b2, name):
     """Variant 2 of the register family (bra runs: K[a,*] and ket-side J
