@@ -95,8 +95,11 @@ int b200jk_device_count(int *count);
  * Schwarz conditioner q_cond on GPU `device`.  direct_scf_tol <= 0 disables
  * screening (the reference's vhfopt=None).  The molecule arrays are checked
  * on the host before any device work: atom indices and env pointers out of
- * range give B200JK_EINVAL, l > 3 and env[PTR_RANGE_OMEGA] != 0 give
- * B200JK_EUNSUPPORTED, without touching a GPU. */
+ * range give B200JK_EINVAL, l > 3 and env[PTR_RANGE_OMEGA] < 0 (the
+ * short-range erfc operator: the long-range plan's build subtracted from the
+ * full one gives it) give B200JK_EUNSUPPORTED, without touching a GPU.
+ * env[PTR_RANGE_OMEGA] > 0 plans the long-range operator erf(omega r12)/r12
+ * (mol.with_range_coulomb(omega), pyscf/scf/_vhf.py:611-627). */
 int b200jk_plan_create(const int32_t *atm, int natm, const int32_t *bas, int nbas,
                        const double *env, int env_len, int cart, double direct_scf_tol,
                        int device, b200jk_plan **out);
@@ -218,7 +221,8 @@ int b200jk_set_profiling(b200jk_plan *plan, int on);
  * on FP64 J/K builds of the density dm (nao x nao, symmetric; host array, or
  * device array with dev_ptrs = 1), then the float32 pass's variants on mixed
  * builds at the plan's threshold, and keep the faster for later builds of
- * this plan (and of batches whose first plan it is).  Five builds.  No
+ * this plan (and of batches whose first plan it is; a batch runs bra runs
+ * as variant 0).  Five builds.  No
  * reference counterpart (PySCF has no kernel variants to tune). */
 int b200jk_autotune(b200jk_plan *plan, const double *dm, int dev_ptrs, void *stream);
 
@@ -229,7 +233,10 @@ int b200jk_set_tile(b200jk_plan *plan, int tile_b);
 
 /* The chosen variant per quartet class (55 classes, bra class >= ket class)
  * for float64 quartets (precision B200JK_PREC_FP64) or for the float32 pass
- * of mixed builds (B200JK_PREC_MIXED). */
+ * of mixed builds (B200JK_PREC_MIXED).  Before any tuning: 0 everywhere on
+ * plans of fewer than 1500 AOs; from 1500 AOs on, the float64 pass uses the
+ * autotuner's measured choices on a large cc-pVTZ workload (bra runs for
+ * eight classes of s and p kets, half-width groups for (21|20) and (22|10)). */
 int b200jk_get_tuning(const b200jk_plan *plan, int precision, int *variants, int max, int *n);
 
 /* Set the variants directly (n = 55; 0 everywhere, 1 or 2 only where the
