@@ -108,6 +108,15 @@ THREAD_PARTS = {
 }
 
 
+# blocks per SM of the shared-memory family's float64 kernels where the
+# build overrides warp_min_blocks<> (jk_kernels.cuh: 4 where the groups'
+# shared memory admits 4 blocks, else 0); B2_WARP_MINB="la lb lc ld:n,..."
+# in the environment replaces it.  Empty: without the cap of 4 (128
+# registers) the tuned half-width (21|20) and (22|10) kernels took 852 and
+# 359 ms instead of 720 and 327 ms on the FP64 build of (H2O)64/cc-pVTZ.
+WARP_MINB = {}
+
+
 def _class_table(text):
     """'la lb lc ld:n,...' -> {(la, lb, lc, ld): n}"""
     table = {}
@@ -120,6 +129,12 @@ def _class_table(text):
 def _thread_parts(cls):
     env = os.environ.get('B2_THREAD_PARTS')
     table = _class_table(env) if env else THREAD_PARTS
+    return table.get(cls)
+
+
+def _warp_minb(cls):
+    env = os.environ.get('B2_WARP_MINB')
+    table = _class_table(env) if env else WARP_MINB
     return table.get(cls)
 
 
@@ -149,6 +164,8 @@ def _units():
                                 '-DB2_THREAD_MINB=%d' % _thread_minb((la, lb, lc, ld))] +
                      (['-DB2_THREAD_PARTS=%d' % _thread_parts((la, lb, lc, ld))]
                       if _thread_parts((la, lb, lc, ld)) else []) +
+                     (['-DB2_WARP_MINB=%d' % _warp_minb((la, lb, lc, ld))]
+                      if _warp_minb((la, lb, lc, ld)) is not None else []) +
                      [os.path.join(CSRC, 'jk_classes.cu'), '-o', o], o))
     for la, lb in PAIR_CLASSES:
         o = os.path.join(OBJ, 'grad_%d%d.o' % (la, lb))

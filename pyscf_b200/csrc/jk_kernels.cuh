@@ -1051,6 +1051,10 @@ __host__ __device__ constexpr int warp_min_blocks()
         // float32 kernels: the compiler's choice (0, not 1, which lets the
         // allocator take far more registers)
         if (sizeof(R) == 4) return 0;
+#if defined(B2_WARP_MINB) && defined(B2_KET_LD)
+        // build-time override of a class unit (build.py WARP_MINB)
+        if (LA == B2_BRA_LA && LB == B2_BRA_LB && LC == B2_KET_LC && LD == B2_KET_LD) return B2_WARP_MINB;
+#endif
         return by_smem >= 4 ? 4 : 0;
 }
 
