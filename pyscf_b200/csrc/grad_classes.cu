@@ -29,7 +29,7 @@ constexpr size_t SMEM_MAX = 227 * 1024;
 template <int LA, int LB, int LC, int LD, bool FUSED>
 int launch_grad_impl(const GradArgs &a, cudaStream_t s, int nsm, std::string &err)
 {
-        using S = GradSmem<LA, LB, LC, LD, 0>;
+        using S = GradSmem<LA, LB, LC, LD, 0, FUSED>;
         constexpr int GS = grad_group_size<LA, LB, LC, LD>();
         static GradCfg cfg;
         static std::mutex mu;

@@ -48,13 +48,14 @@ struct GClass {
         B2_HD static constexpr int eidx(int a, int b, int c, int d) { return ((a * EB + b) * EC + c) * ED + d; }
 };
 
-// shared-memory layout of one group (doubles)
-template <int LA, int LB, int LC, int LD, int MODE>
+// shared-memory layout of one group (doubles); WONLY: the fused force
+// contraction, whose G area holds the NG weights instead of NCP blocks
+template <int LA, int LB, int LC, int LD, int MODE, bool WONLY = false>
 struct GradSmem {
         using GC = GClass<LA, LB, LC, LD, MODE>;
         using K = Class4<LA, LB, LC, LD>;
-        static constexpr int G = 0;                                  // [NCP][NG]
-        static constexpr int E = G + GC::NCP * GC::NG;               // [3][NR][SE]
+        static constexpr int G = 0;                                  // [NCP][NG] (WONLY: [NG])
+        static constexpr int E = G + (WONLY ? 1 : GC::NCP) * GC::NG; // [3][NR][SE]
         static constexpr int DSAB = E + 3 * GC::NR * GC::SE;
         static constexpr int DSCD = DSAB + K::NAB;
         static constexpr int XBC = DSCD + K::NCD;
@@ -283,7 +284,7 @@ __device__ __forceinline__ void grad_eval_force(double *sm, const GradArgs &a, i
                                                 double fac, const double *w, int gl, unsigned gmask, double fq[6])
 {
         using GC = GClass<LA, LB, LC, LD, 0>;
-        using S = GradSmem<LA, LB, LC, LD, 0>;
+        using S = GradSmem<LA, LB, LC, LD, 0, true>;
         constexpr int NR = GC::NR, SE = GC::SE, NG = GC::NG;
         constexpr int SA = GC::STEP_A, SB = GC::STEP_B;
         double *E = sm + S::E;
@@ -366,7 +367,7 @@ __global__ void __launch_bounds__(128) grad_jk_kernel(GradArgs a, int chunk_q)
 {
         using K = Class4<LA, LB, LC, LD>;
         using GC = GClass<LA, LB, LC, LD, 0>;
-        using S = GradSmem<LA, LB, LC, LD, 0>;
+        using S = GradSmem<LA, LB, LC, LD, 0, FUSED>;
         constexpr int GS = grad_group_size<LA, LB, LC, LD>();
         constexpr int NGRP = 32 / GS;
         constexpr int NG = K::NG;
@@ -442,7 +443,8 @@ __global__ void __launch_bounds__(128) grad_jk_kernel(GradArgs a, int chunk_q)
                                         if (q < 3 ? sideA : sideB) fs[q] += fq[q];
                                 continue;
                         }
-                        for (int pass = 0; pass < GC::NPASS; pass++) {
+                        // (the fused contraction never gets here: its group holds no blocks)
+                        for (int pass = 0; pass < (FUSED ? 0 : GC::NPASS); pass++) {
                                 const int c0 = pass * GC::NCP;
                                 // skip a pass whose components all belong to a failing side
                                 const bool needA = sideA && c0 < 3, needB = sideB && c0 + GC::NCP > 3;
